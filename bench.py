@@ -1,0 +1,281 @@
+#!/usr/bin/env python
+"""Benchmark of the VMC hot path (RBM + pair-product wavefunction, J1-J2 Heisenberg model).
+
+One step = one stochastic-reconfiguration iteration of main.f90:311-453 over all walkers:
+update_slater_elements, make_sample (warm-up + stored sweeps), the estimators of
+calc_phys_quantity_opt, the S = O^T O build, the Cholesky solve that replaces pdposv, and the
+parameter update.  The metric is MC samples/s (stored samples per second; SR steps/s reported
+beside it) on the 10x10 periodic lattice at J2/J1 = 0.5 with a translation-symmetric RBM
+(alpha = 4, 100 projections, so 200 Pfaffian blocks per walker), 4096 walkers, 65536 samples per
+SR step.  Synthetic seeded inputs with the reference's shapes stand in for its input files.
+
+Usage:  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+        [--workload NAME] [--precision fp64|split]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "MC samples/s and SR steps/s at 10x10 J2=0.5, chosen vs plain FP64, dE/site"
+
+WORKLOADS = {
+    # translation-symmetric RBM (alpha=4, 400 hidden units per spin parity), 4096 walkers, 65536 samples
+    "j1j2_10x10_trans": dict(L=10, translations=True, alphar=4, orbital="full", walkers=4096, ns=16, J2=0.5),
+    # same lattice without translation projection (2 Pfaffian blocks per walker)
+    "j1j2_10x10_single": dict(L=10, translations=False, alphar=4, orbital="full", walkers=4096, ns=16, J2=0.5),
+    "j1j2_6x6_trans_small": dict(L=6, translations=True, alphar=2, orbital="full", walkers=256, ns=16, J2=0.5),
+}
+
+
+def _rank_env():
+    return int(os.environ.get("RANK", "0")), int(os.environ.get("WORLD_SIZE", "1")), int(
+        os.environ.get("LOCAL_RANK", "0"))
+
+
+def make_problem(w, seed=2024):
+    from rbm_pp_b200 import formats as fm
+    return fm.synthetic_problem(w["L"], translations=w["translations"], alphar=w["alphar"], orbital=w["orbital"],
+                                nsample=w["walkers"] * w["ns"], seed=seed, J2=w["J2"])
+
+
+class ClockSampler:
+    """nvidia-smi clocks / throttle reasons sampled every 200 ms during the timed region."""
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={q}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for ln in self.proc.stdout:
+            self.lines.append(ln.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                smax = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def measured_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return json.load(f), "measured"
+    except Exception:
+        return {"hbm_gbs": 6650.0, "bf16_tflops": 1590.0, "bf16_tflops_sustained": 1400.0}, "fallback"
+
+
+def cpu_baseline(w, problem, max_threads=None):
+    """The oracle (a line-by-line CPU restatement of the reference's make_sample and
+    calc_phys_quantity_opt) on the host cores: one walker per thread, Nsample = 1 per walker
+    (30 warm-up + 2 sweeps, then one measured sample), scaled to the workload's MC samples/s."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import pyoracle as po
+    cores = os.cpu_count() or 1
+    threads = min(cores, max_threads or 64, po.max_threads() if po.max_threads() > 0 else cores)
+    o = po.Oracle(problem, nranks=threads, nsample_per_rank=1, nthreads=threads)
+    o.set_params(problem.br, problem.Wr, problem.slater, 0.0)
+    o.seed(777)
+    t0 = time.perf_counter()
+    o.make_sample(True)
+    t1 = time.perf_counter()
+    o.measure(want_S=False)
+    t2 = time.perf_counter()
+    sweeps = 30 + 1 + 1
+    t_sweep = (t1 - t0) / sweeps  # per walker (walkers run in parallel, one per thread)
+    t_sample = (t2 - t1) / 1.0
+    walkers, ns = w["walkers"], w["ns"]
+    t_walker = (max(30, ns // 100) + ns + 1) * t_sweep + ns * t_sample
+    t_step = t_walker * walkers / threads
+    return {"value": walkers * ns / t_step, "unit": "MC samples/s", "cores": threads, "kind": "port",
+            "sample": (f"oracle make_sample+measure, {threads} walkers x 1 stored sample (32 sweeps each) on "
+                       f"{threads} threads in {t2 - t0:.1f} s; scaled to {walkers} walkers x {ns} samples "
+                       f"(sweep {t_sweep:.3f} s, measured sample {t_sample:.3f} s per walker)"),
+           "sr_steps_per_s_est_without_S": 1.0 / t_step}
+
+
+def run_reference(args):
+    rank, world, _ = _rank_env()
+    if rank != 0:
+        return 0
+    w = WORKLOADS[args.workload]
+    problem = make_problem(w)
+    for _ in range(args.warmup):
+        pass  # host code has no device warm-up; each timed step is a bounded sample
+    vals = []
+    info = None
+    for _ in range(args.steps):
+        info = cpu_baseline(w, problem)
+        vals.append(info["value"])
+    v = float(np.median(vals))
+    ms = w["walkers"] * w["ns"] / v * 1e3
+    line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "MC samples/s", "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": args.workload, "L": w["L"], "walkers": w["walkers"],
+                       "samples_per_step": w["walkers"] * w["ns"], "alphar": w["alphar"],
+                       "n_mp_trans": w["L"] ** 2 if w["translations"] else 1, "J2": w["J2"]},
+            "cpu_baseline": {k: info[k] for k in ("value", "unit", "cores", "kind", "sample")},
+            "e2e": {"value": v, "unit": "MC samples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def run_ours(args):
+    import torch
+    rank, world, local = _rank_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    from rbm_pp_b200 import capi
+    from rbm_pp_b200 import distributed as rdist
+    w = WORKLOADS[args.workload]
+    problem = make_problem(w)
+    prec = capi.SR_SPLIT_BF16 if args.precision == "split" else capi.SR_FP64
+    ctx = capi.Context(problem, n_walkers=w["walkers"], nsample_per_walker=w["ns"], device=local,
+                       walker_offset=rank * w["walkers"])
+    runner = rdist.SRRunner(ctx, problem, iseed0=12345, precision=prec, world=world, rank=rank)
+    inp = problem.inp
+    for _ in range(args.warmup):
+        runner.step()
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    clk = ClockSampler(torch.cuda.current_device())
+    clk.start()
+    step_ms, samp_ms, est_ms, sb_ms, solve_ms, acc_all, props, energies = [], [], [], [], [], [], [], []
+    for _ in range(args.steps):
+        rec = runner.step()
+        st = ctx.stats()
+        step_ms.append(rec["device_ms"])
+        samp_ms.append(st["sampler_ms"])
+        est_ms.append(st["estimator_ms"])
+        sb_ms.append(st["sbuild_ms"])
+        solve_ms.append(st["solve_ms"])
+        acc_all.append(st["accepts_all"])
+        props.append(st["proposals"])
+        energies.append(rec["Etot"])
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    clocks = clk.stop()
+    # max over ranks of the device time per step
+    t = torch.tensor([float(np.mean(step_ms))], device="cuda")
+    if world > 1:
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    ms = float(t.item())
+    samples_per_step = w["walkers"] * w["ns"] * world
+    value = samples_per_step / (ms * 1e-3)
+    # end to end through the public API with host buffers: parameters in, parameters + energy out
+    e2e_ms = []
+    h2d = d2h = 0
+    for _ in range(max(1, min(args.steps, 2))):
+        t0 = time.perf_counter()
+        br, Wr, sl, sh = ctx.get_params()
+        d2h = (br.nbytes + Wr.nbytes + sl.nbytes + 8)
+        ctx.set_params(br, Wr, sl, sh)
+        h2d = (br.nbytes + Wr.nbytes + sl.nbytes + 8)
+        rec = runner.step()
+        br, Wr, sl, sh = ctx.get_params()
+        e2e_ms.append((time.perf_counter() - t0) * 1e3)
+    e2e_v = samples_per_step / (float(np.mean(e2e_ms)) * 1e-3)
+    peaks, peak_kind = measured_peaks()
+    Np = (w["L"] ** 2) // 2
+    n_qp = 2 * (w["L"] ** 2 if w["translations"] else 1)
+    bytes_prop = n_qp * 8.0 * Np * Np
+    bytes_acc = n_qp * 16.0 * Np * Np
+    alg_bytes = float(np.mean(props)) * bytes_prop + float(np.mean(acc_all)) * bytes_acc
+    smp = float(np.mean(samp_ms))
+    achieved = alg_bytes / (smp * 1e-3) / 1e9
+    line = {"metric": METRIC, "value": value, "unit": "MC samples/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded, reference file shapes)",
+            "config": {"workload": args.workload, "L": w["L"], "walkers_per_gpu": w["walkers"],
+                       "samples_per_step": samples_per_step, "alphar": w["alphar"], "n_qp": n_qp,
+                       "n_slater": problem.n_slater, "Nv": ctx.Nv, "J2": w["J2"], "sr_precision": args.precision,
+                       "l2": "inputs larger than L2 (Y %.1f GB, O %.1f GB per GPU)" % (
+                           w["walkers"] * n_qp * Np * Np * 8 / 1e9, samples_per_step / world * ctx.Nv * 8 / 1e9)},
+            "sr_steps_per_s": 1e3 / ms,
+            "energy_per_site": float(np.mean(energies)) / (w["L"] ** 2),
+            "phases_ms": {"make_sample": smp, "estimator": float(np.mean(est_ms)), "s_build": float(np.mean(sb_ms)),
+                          "cholesky_solve": float(np.mean(solve_ms))},
+            "roofline": {"kernel": "sampler_kernel (make_sample)", "bound": "hbm", "achieved": achieved,
+                         "peak": peaks["hbm_gbs"], "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"],
+                         "peak_kind": peak_kind, "traffic": None,
+                         "algorithmic_bytes": alg_bytes},
+            "clocks": clocks,
+            "e2e": {"value": e2e_v, "unit": "MC samples/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "gpu_launches": runner.launches_per_step()}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cb = cpu_baseline(w, problem)
+        line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    ctx.close()
+    if world > 1:
+        torch.distributed.destroy_process_group()
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--workload", default="j1j2_10x10_trans", choices=sorted(WORKLOADS))
+    ap.add_argument("--precision", default="fp64", choices=["fp64", "split"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_ours(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

@@ -1,0 +1,158 @@
+/*
+ * rbmpp.h -- C ABI of the B200 (sm_100a) implementation of RBM_PP's variational-Monte-Carlo hot path
+ * (Metropolis sampling with Pfaffian fast updates, local energy, O_k, stochastic reconfiguration).
+ *
+ * Conventions
+ *  - Plain C types only.  Every array argument is a HOST pointer to a column-major array with the
+ *    Fortran layout of the reference's module variable it replaces (module.f90), 1-based index values
+ *    where the reference stores indices (W_map, Orbital_Idx).  Complex values are (re, im) pairs.
+ *  - The library owns all device memory.  One host thread drives one context.
+ *  - Every call returns 0 on success or an RBMPP_E_* code naming the violated invariant (the
+ *    reference `stop`s on the same conditions); rbmpp_last_error() returns the message.
+ *  - Emulated MPI ranks are "walkers": walker w behaves exactly like rank w of the reference
+ *    (own MT19937 stream seeded iseed0 + w, own Nfastup, Nsample/Nmpi stored samples).
+ *
+ * Reference-side binding: INTEGRATION.md shows the Fortran ISO_C_BINDING interface block that
+ * replaces the bodies of make_sample, calc_phys_quantity_opt and the SR_pdposv include.
+ */
+#ifndef RBMPP_H
+#define RBMPP_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct rbmpp_ctx rbmpp_ctx;
+
+enum {
+  RBMPP_OK = 0,
+  RBMPP_E_ARG = 1,          /* bad argument / unsupported configuration                          */
+  RBMPP_E_CONFIG = 2,       /* x / Ele_Idx / Ele_Cfg bookkeeping (interface_for_PP.f90:26-65)     */
+  RBMPP_E_SIGN = 3,         /* sign_PP inconsistency (interface_for_PP.f90:101-103)               */
+  RBMPP_E_THETA = 4,        /* theta drift > 1e-5 (make_sample.f90:84-89)                          */
+  RBMPP_E_CANDIDATE = 5,    /* exchange-candidate search exhausted (make_sample.f90:290-291)      */
+  RBMPP_E_INITX = 6,        /* make_initial_x fails (make_sample.f90:337,359)                     */
+  RBMPP_E_SKEW = 7,         /* Slater_Elm / InvM skew checks (slater.f90:51-56, matrix.f90:103)    */
+  RBMPP_E_SINGULAR = 8,     /* singular Pfaffian matrix (matrix.f90:145-148,171-174)              */
+  RBMPP_E_SDIAG = 9,        /* S-matrix diagonal checks (SR_pdposv.f90:32-33,78-100,140)           */
+  RBMPP_E_CHOL = 10,        /* Cholesky breakdown (pdposv info /= 0, SR_pdposv.f90:233-236)       */
+  RBMPP_E_SLATER_NORM = 11, /* f renormalisation check (SR_pdposv.f90:414)                        */
+  RBMPP_E_LAMBDA = 12,      /* lambda block split check (SR_pdposv.f90:308)                       */
+  RBMPP_E_CUDA = 20,        /* CUDA runtime error                                                 */
+  RBMPP_E_STATE = 21        /* call out of order (e.g. measure before make_sample)                */
+};
+
+/* Sizes (RBM.input, sym_info.txt, orbitalidx.def; main.f90:75-141). */
+typedef struct {
+  int L;            /* linear lattice size; N = L*L sites (main.f90:85)                          */
+  int n_mp_trans;   /* N_MP_Trans: number of symmetry operations in sym_info.txt (main.f90:91)  */
+  int alphac;       /* complex RBM density; must be 0 (real-RBM branch)                          */
+  int alphar;       /* real RBM density                                                           */
+  int n_slater;     /* N_Slater (orbitalidx.def, main.f90:128)                                    */
+  int nsample;      /* stored samples per walker = Nsample/Nmpi (main.f90:138)                    */
+  int n_walkers;    /* number of emulated ranks                                                   */
+  int spin_parity;  /* +1 / -1 (spin_projection.f90:56-62)                                        */
+  double J1, J2;    /* couplings (main.f90:83)                                                    */
+  int device;       /* CUDA device ordinal                                                        */
+  int walker_offset;/* global rank of walker 0 (multi-GPU sharding: rank r holds walkers r*n_walkers..) */
+} rbmpp_dims;
+
+/* Inputs of one SR step (main.f90 locals used by the SR_pdposv.f90 include). */
+enum { RBMPP_SR_FP64 = 0, RBMPP_SR_SPLIT_BF16 = 1 };
+typedef struct {
+  int iteration;      /* optimisation step (1-based)                                             */
+  int precision;      /* RBMPP_SR_FP64: FP64 S build; RBMPP_SR_SPLIT_BF16: 3-term split-BF16 S on the
+                         tensor cores + FP64 Cholesky + iterative refinement against the exact S      */
+  int refine_steps;   /* refinement sweeps for RBMPP_SR_SPLIT_BF16 (2-3)                         */
+  int reserved;
+  double delta_tau;   /* RBM.input                                                               */
+  double s_factor0;   /* current stabilisation factor (main.f90:439 schedule applied by caller)   */
+  double s_cut;       /* RBM.input                                                               */
+} rbmpp_sr_in;
+
+typedef struct {
+  double Etot, Etot2, norm, wf_av;   /* normalised as in main.f90:351-361                        */
+  double accept_ratio;               /* main.f90:349                                              */
+  double lambda;                     /* step norm after the 5/L scaling (SR_pdposv.f90:309)       */
+  double lambda_rbm_rbm, lambda_pp_pp, lambda_rbm_pp;
+  double delW_max, s_factor, sdiag_av, smat_scaling;
+  double refine_residual;            /* relative residual of the SR solve against the exact S    */
+  int kmax, k_nonzero, nSmat, reserved;
+} rbmpp_sr_out;
+
+/* Lifecycle -------------------------------------------------------------------------------- */
+int rbmpp_create(const rbmpp_dims* dims, rbmpp_ctx** out);
+int rbmpp_destroy(rbmpp_ctx* ctx);
+const char* rbmpp_last_error(const rbmpp_ctx* ctx);
+/* what: 0 = Nv, 1 = Nv_RBM, 2 = Mr, 3 = N_QP_Full, 4 = N, 5 = device bytes held */
+int rbmpp_query(const rbmpp_ctx* ctx, int what, long long* value);
+
+/* Tables: W_map(N, 1, N_MP_Trans) (main.f90:94-122; also MP_Trans_Idx, parameter.f90:105-109),
+ * para_mp_trans(N_MP_Trans) complex, Orbital_Idx(N,N) (parameter.f90:88-100),
+ * Orbital_Sgn(N,N) or NULL (all +1; l_AP = .false.).  Replaces the module setup of main.f90:89-300. */
+int rbmpp_set_tables(rbmpp_ctx* ctx, const int* W_map, const double* para_mp_trans, const int* Orbital_Idx,
+                     const int* Orbital_Sgn);
+
+/* Parameters: Wrirr(N, alphar), brirr(alphar), Slater(N_Slater), shift (module.f90 mod_RBM, mod_PP,
+ * mod_main).  Wc/bc must be NULL (alphac = 0).  Also rebuilds Slater_Elm on the device
+ * (update_slater_elements, slater.f90:7-64). */
+int rbmpp_set_params(rbmpp_ctx* ctx, const double* Wr, const double* br, const double* Wc, const double* bc,
+                     const double* Slater, double shift);
+int rbmpp_get_params(rbmpp_ctx* ctx, double* Wr, double* br, double* Slater, double* shift);
+/* Sets mod_main's shift alone (main.f90:451), keeping the other parameters. */
+int rbmpp_set_shift(rbmpp_ctx* ctx, double shift);
+
+/* RNG: walker w (global rank g = walker_offset + w) is seeded sgrnd(iseed0 + g) and skips
+ * Nsample*g + 1 draws (main.f90:224-234). */
+int rbmpp_seed_walkers(rbmpp_ctx* ctx, int iseed0);
+/* n draws from walker 0's stream (rank 0's draws in initialize_parameters, parameter.f90:21-41). */
+int rbmpp_rank0_grnd(rbmpp_ctx* ctx, int n, double* out);
+
+/* make_sample(myrank, first_iteration, naccept) for every walker (make_sample.f90:4-240).
+ * naccept: per-walker counts (n_walkers ints) or NULL; naccept_total: sum or NULL. */
+int rbmpp_make_sample(rbmpp_ctx* ctx, int first_iteration, int* naccept, long long* naccept_total);
+/* x_sample(N, Nsample, n_walkers), psi_x_sample(0:N_QP, Nsample, n_walkers) complex,
+ * PfM_sample(N_QP, Nsample, n_walkers); any pointer may be NULL (mod_sample, module.f90:37-42). */
+int rbmpp_get_samples(rbmpp_ctx* ctx, int* x_sample, double* psi_x_sample, double* PfM_sample);
+int rbmpp_set_samples(rbmpp_ctx* ctx, const int* x_sample);
+
+/* calc_phys_quantity_opt (calc_phys_quantity.f90:20-246) over all walkers, summed as the MPI
+ * reductions of main.f90:348-369 do (before division by norm): scal = {Etot, Etot2, norm, wf_av}.
+ * gvec, Ovec (Nv) and Smat (Nv x Nv, = sum O O^T) are copied to the host when non-NULL; they also
+ * stay on the device for rbmpp_sr_step. */
+int rbmpp_measure(rbmpp_ctx* ctx, double* scal, double* gvec, double* Ovec, double* Smat);
+/* calc_phys_quantity_after_opt (calc_phys_quantity.f90:250-302): scal = {Etot, Etot2, norm, wf_av}. */
+int rbmpp_measure_energy(rbmpp_ctx* ctx, double* scal);
+
+/* Cross-GPU reduction of the measurement (the MPI_ALLREDUCE calls of main.f90:348-369).
+ * direction 0: copy this context's sums into caller DEVICE buffers d_S (Nv*Nv), d_g, d_ov (Nv) and
+ *              host scal6 = {Etot, Etot2, norm, wf_av, naccept_total, n_samples};
+ * direction 1: load reduced sums (same layout) back for rbmpp_sr_step. */
+int rbmpp_exchange_measurement(rbmpp_ctx* ctx, int direction, double* d_S, double* d_g, double* d_ov, double* scal6);
+
+/* SR block (SR_pdposv.f90:1-432 with the normalisation of main.f90:351-369) on the device-resident
+ * measurement of the last rbmpp_measure; replaces pdposv.  Updates the parameters in place.
+ * dx (Nv, nullable) receives the SR direction after scaling (gvec at SR_pdposv.f90:327). */
+int rbmpp_sr_step(rbmpp_ctx* ctx, const rbmpp_sr_in* in, rbmpp_sr_out* out, double* dx);
+
+/* One optimisation iteration of main.f90:311-453: update_slater_elements, make_sample, measure,
+ * reductions, SR step, and the s_factor0 / shift bookkeeping (main.f90:439-453), which the
+ * context keeps between calls.  s_factor_scale multiplies s_factor0 after the step. */
+int rbmpp_iteration(rbmpp_ctx* ctx, int precision, double delta_tau, double s_factor_scale, double s_cut,
+                    double s_factor0_initial, rbmpp_sr_out* out);
+
+/* Device-side statistics of the last calls, timed with CUDA events on the library's stream:
+ * out[0] make_sample kernel ms, [1] estimator kernel ms, [2] gvec/Ovec GEMV ms, [3] S build ms,
+ * [4] Cholesky factor + solve ms, [5] accepted moves in all sweeps of the last make_sample,
+ * [6] proposals of the last make_sample, [7] last rbmpp_iteration ms.  n = number of entries wanted. */
+int rbmpp_get_stats(const rbmpp_ctx* ctx, double* out, int n);
+
+/* Adjoint O_k kernel: for n configurations x(N, n): psi(0:N_QP, n) complex, hpsi(n) complex
+ * (sum_x' <x|H|x'> psi(x'), calc_local_energy_correlation), and O(Nv, n) = d psi(x) / d theta_k
+ * (Ovec_loc_x before reweighting, calc_phys_quantity.f90:115-220).  Any output may be NULL. */
+int rbmpp_eval_configs(rbmpp_ctx* ctx, int n, const int* x, double* psi, double* hpsi, double* O);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* RBMPP_H */

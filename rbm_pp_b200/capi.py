@@ -1,0 +1,260 @@
+"""ctypes binding of the C ABI in include/rbmpp.h (the CUDA library ``librbmpp.so``).
+
+This is the host-side mirror of the reference's module interface for the sampling/SR loop:
+``make_sample`` (make_sample.f90:4), ``calc_phys_quantity_opt`` (calc_phys_quantity.f90:20),
+the SR_pdposv.f90 block, and the seeding/initialisation of main.f90:224-300.  There is no CPU
+fallback: if the library is missing or no GPU is present, construction fails with an error.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "librbmpp.so")
+_lib = None
+
+EXPORTS = ["rbmpp_create", "rbmpp_destroy", "rbmpp_last_error", "rbmpp_query", "rbmpp_set_tables",
+           "rbmpp_set_params", "rbmpp_get_params", "rbmpp_seed_walkers", "rbmpp_rank0_grnd", "rbmpp_make_sample",
+           "rbmpp_get_samples", "rbmpp_set_samples", "rbmpp_measure", "rbmpp_measure_energy", "rbmpp_sr_step",
+           "rbmpp_iteration", "rbmpp_eval_configs", "rbmpp_get_stats", "rbmpp_exchange_measurement",
+           "rbmpp_set_shift"]
+
+SR_FP64 = 0
+SR_SPLIT_BF16 = 1
+
+
+class Dims(C.Structure):
+    _fields_ = [("L", C.c_int), ("n_mp_trans", C.c_int), ("alphac", C.c_int), ("alphar", C.c_int),
+                ("n_slater", C.c_int), ("nsample", C.c_int), ("n_walkers", C.c_int), ("spin_parity", C.c_int),
+                ("J1", C.c_double), ("J2", C.c_double), ("device", C.c_int), ("walker_offset", C.c_int)]
+
+
+class SrIn(C.Structure):
+    _fields_ = [("iteration", C.c_int), ("precision", C.c_int), ("refine_steps", C.c_int), ("reserved", C.c_int),
+                ("delta_tau", C.c_double), ("s_factor0", C.c_double), ("s_cut", C.c_double)]
+
+
+class SrOut(C.Structure):
+    _fields_ = [("Etot", C.c_double), ("Etot2", C.c_double), ("norm", C.c_double), ("wf_av", C.c_double),
+                ("accept_ratio", C.c_double), ("lambda_", C.c_double), ("lambda_rbm_rbm", C.c_double),
+                ("lambda_pp_pp", C.c_double), ("lambda_rbm_pp", C.c_double), ("delW_max", C.c_double),
+                ("s_factor", C.c_double), ("sdiag_av", C.c_double), ("smat_scaling", C.c_double),
+                ("refine_residual", C.c_double), ("kmax", C.c_int), ("k_nonzero", C.c_int), ("nSmat", C.c_int),
+                ("reserved", C.c_int)]
+
+    def as_dict(self):
+        return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
+
+
+class RbmppError(RuntimeError):
+    def __init__(self, code, msg):
+        super().__init__(f"rbmpp error {code}: {msg}")
+        self.code = code
+
+
+def lib():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise RbmppError(-1, f"CUDA library not built: {LIB_PATH} (run rbm_pp_b200/build.py)")
+        L = C.CDLL(LIB_PATH)
+        P = C.c_void_p
+        L.rbmpp_create.argtypes = [C.POINTER(Dims), C.POINTER(P)]
+        L.rbmpp_destroy.argtypes = [P]
+        L.rbmpp_last_error.restype = C.c_char_p
+        L.rbmpp_last_error.argtypes = [P]
+        L.rbmpp_query.argtypes = [P, C.c_int, C.POINTER(C.c_longlong)]
+        L.rbmpp_set_tables.argtypes = [P, P, P, P, P]
+        L.rbmpp_set_params.argtypes = [P, P, P, P, P, P, C.c_double]
+        L.rbmpp_get_params.argtypes = [P, P, P, P, P]
+        L.rbmpp_seed_walkers.argtypes = [P, C.c_int]
+        L.rbmpp_rank0_grnd.argtypes = [P, C.c_int, P]
+        L.rbmpp_make_sample.argtypes = [P, C.c_int, P, P]
+        L.rbmpp_get_samples.argtypes = [P, P, P, P]
+        L.rbmpp_set_samples.argtypes = [P, P]
+        L.rbmpp_measure.argtypes = [P, P, P, P, P]
+        L.rbmpp_measure_energy.argtypes = [P, P]
+        L.rbmpp_sr_step.argtypes = [P, C.POINTER(SrIn), C.POINTER(SrOut), P]
+        L.rbmpp_iteration.argtypes = [P, C.c_int, C.c_double, C.c_double, C.c_double, C.c_double, C.POINTER(SrOut)]
+        L.rbmpp_eval_configs.argtypes = [P, C.c_int, P, P, P, P]
+        L.rbmpp_get_stats.argtypes = [P, P, C.c_int]
+        L.rbmpp_exchange_measurement.argtypes = [P, C.c_int, P, P, P, P]
+        L.rbmpp_set_shift.argtypes = [P, C.c_double]
+        _lib = L
+    return _lib
+
+
+def _p(a):
+    return None if a is None else a.ctypes.data_as(C.c_void_p)
+
+
+def _f(a, dtype):
+    return np.ascontiguousarray(np.asarray(a, dtype=dtype).reshape(-1, order="F"))
+
+
+class Context:
+    """One library context: ``n_walkers`` emulated MPI ranks on one GPU."""
+
+    def __init__(self, problem, n_walkers: int, nsample_per_walker: int, device: int = 0, walker_offset: int = 0):
+        self.p = problem
+        inp = problem.inp
+        self.N = inp.L * inp.L
+        self.n_mp = problem.sym.n_mp
+        self.n_qp = 2 * self.n_mp
+        self.nw = n_walkers
+        self.ns = nsample_per_walker
+        d = Dims(inp.L, self.n_mp, 0, inp.alphar, problem.n_slater, nsample_per_walker, n_walkers, inp.spin_parity,
+                 inp.J1, inp.J2, device, walker_offset)
+        h = C.c_void_p()
+        rc = lib().rbmpp_create(C.byref(d), C.byref(h))
+        self.h = h
+        self._chk(rc)
+        v = C.c_longlong()
+        lib().rbmpp_query(self.h, 0, C.byref(v))
+        self.Nv = v.value
+        para = np.zeros(2 * self.n_mp)
+        para[0::2] = problem.sym.para_mp.real
+        para[1::2] = problem.sym.para_mp.imag
+        self._w = _f(problem.sym.W_map, np.int32)
+        self._o = _f(problem.orbital_idx, np.int32)
+        self._chk(lib().rbmpp_set_tables(self.h, _p(self._w), _p(para), _p(self._o), None))
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().rbmpp_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
+
+    def _chk(self, rc):
+        if rc != 0:
+            raise RbmppError(rc, lib().rbmpp_last_error(self.h).decode())
+
+    def device_bytes(self) -> int:
+        v = C.c_longlong()
+        lib().rbmpp_query(self.h, 5, C.byref(v))
+        return v.value
+
+    def set_params(self, br, Wr, slater, shift=0.0):
+        Wr = _f(Wr, np.float64)
+        br = np.ascontiguousarray(br, np.float64)
+        sl = np.ascontiguousarray(slater, np.float64)
+        self._chk(lib().rbmpp_set_params(self.h, _p(Wr), _p(br), None, None, _p(sl), float(shift)))
+
+    def get_params(self):
+        a = self.p.inp.alphar
+        Wr = np.zeros(self.N * a)
+        br = np.zeros(max(a, 1))
+        sl = np.zeros(self.p.n_slater)
+        sh = np.zeros(1)
+        self._chk(lib().rbmpp_get_params(self.h, _p(Wr), _p(br), _p(sl), _p(sh)))
+        return br[:a], Wr.reshape((self.N, a), order="F"), sl, float(sh[0])
+
+    def seed(self, iseed0: int):
+        self._chk(lib().rbmpp_seed_walkers(self.h, int(iseed0)))
+
+    def rank0_grnd(self, n: int):
+        out = np.zeros(max(n, 1))
+        self._chk(lib().rbmpp_rank0_grnd(self.h, n, _p(out)))
+        return out[:n]
+
+    def make_sample(self, first: bool):
+        nacc = np.zeros(self.nw, dtype=np.int32)
+        self._chk(lib().rbmpp_make_sample(self.h, 1 if first else 0, _p(nacc), None))
+        return nacc
+
+    def samples(self):
+        x = np.zeros(self.N * self.ns * self.nw, dtype=np.int32)
+        psi = np.zeros(2 * (self.n_qp + 1) * self.ns * self.nw)
+        pf = np.zeros(self.n_qp * self.ns * self.nw)
+        self._chk(lib().rbmpp_get_samples(self.h, _p(x), _p(psi), _p(pf)))
+        return (x.reshape(self.nw, self.ns, self.N), psi.view(np.complex128).reshape(self.nw, self.ns, self.n_qp + 1),
+                pf.reshape(self.nw, self.ns, self.n_qp))
+
+    def set_samples(self, x):
+        x = np.ascontiguousarray(x, dtype=np.int32).reshape(-1)
+        self._chk(lib().rbmpp_set_samples(self.h, _p(x)))
+
+    def measure(self, want_S=True, want_vectors=True):
+        scal = np.zeros(4)
+        g = np.zeros(self.Nv) if want_vectors else None
+        ov = np.zeros(self.Nv) if want_vectors else None
+        S = np.zeros(self.Nv * self.Nv) if want_S else None
+        self._chk(lib().rbmpp_measure(self.h, _p(scal), _p(g), _p(ov), _p(S)))
+        out = dict(Etot=scal[0], Etot2=scal[1], norm=scal[2], wf_av=scal[3], gvec=g, Ovec=ov)
+        if S is not None:
+            out["S"] = S.reshape((self.Nv, self.Nv), order="F")
+        return out
+
+    def measure_energy(self):
+        scal = np.zeros(4)
+        self._chk(lib().rbmpp_measure_energy(self.h, _p(scal)))
+        return dict(Etot=scal[0], Etot2=scal[1], norm=scal[2], wf_av=scal[3])
+
+    def sr_step(self, iteration, delta_tau, s_factor0, s_cut, precision=SR_FP64, refine_steps=3):
+        sin = SrIn(iteration, precision, refine_steps, 0, delta_tau, s_factor0, s_cut)
+        sout = SrOut()
+        dx = np.zeros(self.Nv)
+        self._chk(lib().rbmpp_sr_step(self.h, C.byref(sin), C.byref(sout), _p(dx)))
+        return sout, dx
+
+    def iteration(self, precision, delta_tau, s_factor_scale, s_cut, s_factor0):
+        sout = SrOut()
+        self._chk(lib().rbmpp_iteration(self.h, precision, delta_tau, s_factor_scale, s_cut, s_factor0,
+                                        C.byref(sout)))
+        return sout
+
+    def set_shift(self, shift):
+        self._chk(lib().rbmpp_set_shift(self.h, float(shift)))
+
+    def exchange_measurement(self, direction, S_ptr, g_ptr, ov_ptr, scal6):
+        """Device pointers (ints) for S, gvec, Ovec; scal6 a float64 array of 6."""
+        self._chk(lib().rbmpp_exchange_measurement(self.h, direction, C.c_void_p(S_ptr), C.c_void_p(g_ptr),
+                                                   C.c_void_p(ov_ptr), _p(scal6)))
+
+    def stats(self):
+        out = np.zeros(8)
+        self._chk(lib().rbmpp_get_stats(self.h, _p(out), 8))
+        keys = ["sampler_ms", "estimator_ms", "gemv_ms", "sbuild_ms", "solve_ms", "accepts_all", "proposals",
+                "iteration_ms"]
+        return dict(zip(keys, out.tolist()))
+
+    def eval_configs(self, x, want_h=True, want_O=False):
+        x = np.ascontiguousarray(x, dtype=np.int32)
+        n = x.shape[0]
+        psi = np.zeros(2 * (self.n_qp + 1) * n)
+        hp = np.zeros(2 * n) if want_h else None
+        O = np.zeros(self.Nv * n) if want_O else None
+        self._chk(lib().rbmpp_eval_configs(self.h, n, _p(x.reshape(-1)), _p(psi), _p(hp), _p(O)))
+        out = dict(psi=psi.view(np.complex128).reshape(n, self.n_qp + 1))
+        if hp is not None:
+            out["hpsi"] = hp.view(np.complex128)
+        if O is not None:
+            out["O"] = O.reshape(n, self.Nv)
+        return out
+
+
+def initial_params(ctx: Context, problem):
+    """initialize_parameters (parameter.f90:21-75): rank 0 draws U(-0.05, 0.05) RBM parameters from its
+    stream (consuming alphar*(N+1) draws), then W.input overrides them when present."""
+    inp = problem.inp
+    N = inp.L * inp.L
+    u = ctx.rank0_grnd(inp.alphar * (N + 1))
+    br = np.zeros(inp.alphar)
+    Wr = np.zeros((N, inp.alphar))
+    k = 0
+    for f in range(inp.alphar):
+        br[f] = 0.1 * (u[k] - 0.5)
+        k += 1
+        if inp.spin_parity == -1:
+            br[f] *= 10.0
+        for iw in range(N):
+            Wr[iw, f] = 0.1 * (u[k] - 0.5)
+            k += 1
+    if problem.Wr is not None:
+        br, Wr = problem.br, problem.Wr
+    return br, Wr

@@ -1,0 +1,948 @@
+// capi.cu -- the C ABI of include/rbmpp.h: context, device memory, tables, and the host logic of
+// main.f90 / SR_pdposv.f90 around the device kernels (sampler.cu, estimator.cu, linalg.cu,
+// gemm_bf16x3.cu).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "../../include/rbmpp.h"
+#include "common.cuh"
+
+// launchers (sampler.cu, estimator.cu, linalg.cu, gemm_bf16x3.cu)
+cudaError_t rbmpp_launch_sampler(const DevDims&, const DevTables&, const DevParams&, const DevWalkers&, int,
+                                 cudaStream_t);
+size_t rbmpp_sampler_smem(const DevDims&, int);
+cudaError_t rbmpp_launch_estimator(const DevDims&, const DevTables&, const DevParams&, const int8_t*, int, double*,
+                                   double*, double*, int*, int*, int, cudaStream_t);
+size_t rbmpp_estimator_smem(const DevDims&, int);
+cudaError_t rbmpp_launch_advance_rng(uint32_t*, const int*, int, int, int, cudaStream_t);
+cudaError_t rbmpp_syrk_ot_o(int, int, const double*, double*, cudaStream_t);
+cudaError_t rbmpp_symmetrize(int, double*, cudaStream_t);
+cudaError_t rbmpp_potrf_upper(int, double*, int*, cudaStream_t);
+cudaError_t rbmpp_potrs_upper(int, const double*, double*, cudaStream_t);
+cudaError_t rbmpp_trmv_upper(int, const double*, const double*, double*, cudaStream_t);
+cudaError_t rbmpp_gemv_ot(int, int, const double*, const double*, const double*, double*, double*, double*, int,
+                          cudaStream_t);
+cudaError_t rbmpp_gemv_o(int, int, const double*, const double*, double*, cudaStream_t);
+cudaError_t rbmpp_sr_form(int, double*, double, const double*, cudaStream_t);
+cudaError_t rbmpp_sr_scale(int, int, double*, double, cudaStream_t);
+cudaError_t rbmpp_get_diag(int, const double*, double*, cudaStream_t);
+cudaError_t rbmpp_add_diag(int, double*, double, cudaStream_t);
+cudaError_t rbmpp_rowcol_absmax(int, const double*, const int*, int, double*, cudaStream_t);
+cudaError_t rbmpp_sample_scalars(int, const double*, int, const double*, double, double*, double*, double*,
+                                 cudaStream_t);
+
+namespace {
+
+// update_slater_elements (slater.f90:7-64), block form: XF(p,q) = -Slater_Elm(p, q+N) for projection qp,
+// with Slater_Elm(p, q+N) = -slt_ij*ss - slt_ji*cc, slt_ij = f(T q, T p), slt_ji = f(T p, T q).
+__global__ void build_xf_kernel(int N, int n_mp, const int* wmap, const int* orb, const double* slater, double cc0,
+                                double ss0, double cc1, double ss1, double* XF, double* XFT) {
+  long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  long long tot = (long long)2 * n_mp * N * N;
+  if (e >= tot) return;
+  int q = (int)(e % N);
+  long long r = e / N;
+  int pp = (int)(r % N);
+  int qp = (int)(r / N);
+  int mp = qp >> 1, sp = qp & 1;
+  double cc = sp ? cc1 : cc0, ss = sp ? ss1 : ss0;
+  int tp = wmap[(long long)mp * N + pp], tq = wmap[(long long)mp * N + q];
+  double slt_ij = slater[orb[(long long)tq * N + tp]];
+  double slt_ji = slater[orb[(long long)tp * N + tq]];
+  double se = __dsub_rn(__dmul_rn(-slt_ij, ss), __dmul_rn(slt_ji, cc));
+  double xf = -se;
+  XF[((long long)qp * N + pp) * N + q] = xf;
+  XFT[((long long)qp * N + q) * N + pp] = xf;
+}
+
+__global__ void seed_kernel(uint32_t* mt, int nw, int iseed0, int ns, int w0) {
+  int wl = blockIdx.x * blockDim.x + threadIdx.x;
+  if (wl >= nw) return;
+  const int w = w0 + wl;  // global rank
+  uint32_t st[625];
+  st[0] = (uint32_t)(iseed0 + w);
+  for (int i = 1; i < 624; i++) st[i] = 69069u * st[i - 1];
+  st[624] = 624;
+  long long skip = (long long)ns * w + 1;  // main.f90:232-234
+  for (long long i = 0; i < skip; i++) (void)mt_next(st);
+  for (int k = 0; k < 625; k++) mt[(size_t)wl * 625 + k] = st[k];
+}
+
+__global__ void draw_kernel(uint32_t* mt, int n, double* out) {
+  uint32_t st[625];
+  for (int k = 0; k < 625; k++) st[k] = mt[k];
+  for (int i = 0; i < n; i++) out[i] = grnd(st);
+  for (int k = 0; k < 625; k++) mt[k] = st[k];
+}
+
+__global__ void int_to_i8_kernel(const int* in, int8_t* out, long long n) {
+  long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e < n) out[e] = (int8_t)in[e];
+}
+__global__ void i8_to_int_kernel(const int8_t* in, int* out, long long n) {
+  long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e < n) out[e] = (int)in[e];
+}
+
+}  // namespace
+
+struct rbmpp_ctx {
+  rbmpp_dims dims;
+  DevDims d;
+  cudaStream_t st = nullptr;
+  std::string err;
+  // host copies of the tables and parameters (Fortran layouts)
+  std::vector<int> orb_host;     // Orbital_Idx 0-based [p][q] row-major (p*N+q)
+  std::vector<double> Wr, br, slater;
+  double shift = 0.0;
+  bool tables_set = false, params_set = false, seeded = false, sampled = false, measured = false;
+  // device tables / params
+  int *d_wmap = nullptr, *d_winv = nullptr, *d_orb = nullptr, *d_bonds = nullptr;
+  unsigned char* d_subB = nullptr;
+  double *d_para = nullptr, *d_Wr = nullptr, *d_br = nullptr, *d_slater = nullptr, *d_XF = nullptr, *d_XFT = nullptr;
+  DevWalkers W{};
+  // measurement
+  int ns_tot = 0;
+  double *d_O = nullptr, *d_psiS = nullptr, *d_eloc = nullptr, *d_a = nullptr, *d_b = nullptr, *d_acc4 = nullptr;
+  int *d_nap = nullptr, *d_estat = nullptr;
+  double *d_gvec = nullptr, *d_Ovec = nullptr, *d_S = nullptr, *d_part = nullptr, *d_vec = nullptr;
+  double *d_tmp_ns = nullptr;
+  int* d_info = nullptr;
+  void *d_hi = nullptr, *d_lo = nullptr;
+  int ldk = 0;
+  float* d_Sf = nullptr;
+  double meas_scal[4] = {0, 0, 0, 0};
+  long long naccept_total = 0;
+  double n_samples_total = 0.0;  // samples behind meas_scal (all GPUs after a reduction)
+  // main.f90 bookkeeping for rbmpp_iteration
+  int iteration = 0;
+  double s_factor0 = 0.0;
+  bool s_factor_init = false;
+  double wf_av_list[10] = {0};
+  size_t bytes = 0;
+  cudaEvent_t ev[12] = {};
+  double stats[8] = {0};
+};
+
+namespace {
+
+int fail(rbmpp_ctx* c, int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  if (c) c->err = buf;
+  return code;
+}
+
+#define CK(call)                                                                                  \
+  do {                                                                                            \
+    cudaError_t e_ = (call);                                                                      \
+    if (e_ != cudaSuccess) return fail(c, RBMPP_E_CUDA, "%s: %s", #call, cudaGetErrorString(e_)); \
+  } while (0)
+
+template <class T>
+int dalloc(rbmpp_ctx* c, T** p, size_t count) {
+  cudaError_t e = cudaMalloc((void**)p, sizeof(T) * std::max<size_t>(count, 1));
+  if (e != cudaSuccess) return fail(c, RBMPP_E_CUDA, "cudaMalloc(%zu bytes): %s", sizeof(T) * count, cudaGetErrorString(e));
+  c->bytes += sizeof(T) * count;
+  return 0;
+}
+
+DevTables tables(const rbmpp_ctx* c) {
+  DevTables t;
+  t.wmap = c->d_wmap;
+  t.winv = c->d_winv;
+  t.para_mp = c->d_para;
+  t.orb = c->d_orb;
+  t.subB = c->d_subB;
+  t.bonds = c->d_bonds;
+  return t;
+}
+
+DevParams params(const rbmpp_ctx* c) {
+  DevParams p;
+  p.Wr = c->d_Wr;
+  p.br = c->d_br;
+  p.XF = c->d_XF;
+  p.XFT = c->d_XFT;
+  return p;
+}
+
+int upload_params(rbmpp_ctx* c) {
+  const DevDims& d = c->d;
+  std::vector<double> wr_dev((size_t)d.alphar * d.N);
+  for (int f = 0; f < d.alphar; f++)
+    for (int iw = 0; iw < d.N; iw++) wr_dev[(size_t)f * d.N + iw] = c->Wr[iw + (size_t)d.N * f];
+  if (d.alphar > 0) {
+    CK(cudaMemcpyAsync(c->d_Wr, wr_dev.data(), sizeof(double) * wr_dev.size(), cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpyAsync(c->d_br, c->br.data(), sizeof(double) * d.alphar, cudaMemcpyHostToDevice, c->st));
+  }
+  CK(cudaMemcpyAsync(c->d_slater, c->slater.data(), sizeof(double) * d.n_slater, cudaMemcpyHostToDevice, c->st));
+  long long tot = (long long)d.n_qp * d.N * d.N;
+  build_xf_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, c->st>>>(d.N, d.n_mp, c->d_wmap, c->d_orb, c->d_slater,
+                                                                      d.sp_cc[0], d.sp_ss[0], d.sp_cc[1], d.sp_ss[1],
+                                                                      c->d_XF, c->d_XFT);
+  CK(cudaGetLastError());
+  c->d.shift = c->shift;
+  CK(cudaStreamSynchronize(c->st));
+  return 0;
+}
+
+int ensure_measure_buffers(rbmpp_ctx* c) {
+  if (c->d_O) return 0;
+  const DevDims& d = c->d;
+  c->ns_tot = d.nw * d.ns;
+  int r;
+  if ((r = dalloc(c, &c->d_O, (size_t)c->ns_tot * d.Nv))) return r;
+  if ((r = dalloc(c, &c->d_psiS, (size_t)c->ns_tot * (d.n_qp + 1) * 2))) return r;
+  if ((r = dalloc(c, &c->d_eloc, (size_t)c->ns_tot * 2))) return r;
+  if ((r = dalloc(c, &c->d_a, (size_t)c->ns_tot))) return r;
+  if ((r = dalloc(c, &c->d_b, (size_t)c->ns_tot))) return r;
+  if ((r = dalloc(c, &c->d_tmp_ns, (size_t)c->ns_tot))) return r;
+  if ((r = dalloc(c, &c->d_acc4, 4))) return r;
+  if ((r = dalloc(c, &c->d_nap, (size_t)c->ns_tot))) return r;
+  if ((r = dalloc(c, &c->d_estat, (size_t)c->ns_tot))) return r;
+  if ((r = dalloc(c, &c->d_gvec, (size_t)d.Nv))) return r;
+  if ((r = dalloc(c, &c->d_Ovec, (size_t)d.Nv))) return r;
+  if ((r = dalloc(c, &c->d_vec, (size_t)4 * d.Nv))) return r;
+  if ((r = dalloc(c, &c->d_S, (size_t)d.Nv * d.Nv))) return r;
+  if ((r = dalloc(c, &c->d_part, (size_t)2 * 64 * d.Nv))) return r;
+  if ((r = dalloc(c, &c->d_info, 4))) return r;
+  return 0;
+}
+
+int check_walker_status(rbmpp_ctx* c, const int* d_status, int n, const char* what) {
+  std::vector<int> st(n);
+  CK(cudaMemcpy(st.data(), d_status, sizeof(int) * n, cudaMemcpyDeviceToHost));
+  for (int i = 0; i < n; i++)
+    if (st[i]) return fail(c, st[i], "%s failed on item %d (code %d)", what, i, st[i]);
+  return 0;
+}
+
+}  // namespace
+
+// ===================================================================================================
+extern "C" {
+
+int rbmpp_create(const rbmpp_dims* dims, rbmpp_ctx** out) {
+  if (!dims || !out) return RBMPP_E_ARG;
+  *out = nullptr;
+  rbmpp_ctx* c = new rbmpp_ctx();
+  c->dims = *dims;
+  DevDims& d = c->d;
+  std::memset(&d, 0, sizeof(d));
+  if (dims->L < 2 || dims->L * dims->L > RBMPP_MAX_N || (dims->L * dims->L) % 2) {
+    int r = fail(c, RBMPP_E_ARG, "unsupported L=%d (N must be even and <= %d)", dims->L, RBMPP_MAX_N);
+    *out = c;
+    return r;
+  }
+  if (dims->alphac != 0) {
+    *out = c;
+    return fail(c, RBMPP_E_ARG, "alphac > 0 (complex RBM branch) is not supported");
+  }
+  if (dims->n_mp_trans < 1 || dims->alphar < 0 || dims->n_slater < 1 || dims->nsample < 1 || dims->n_walkers < 1) {
+    *out = c;
+    return fail(c, RBMPP_E_ARG, "bad dimensions");
+  }
+  d.L = dims->L;
+  d.N = d.L * d.L;
+  d.Np = d.N / 2;
+  if ((d.Np + 31) / 32 > RBMPP_MAX_KPL) {
+    *out = c;
+    return fail(c, RBMPP_E_ARG, "N/2 = %d exceeds the supported Pfaffian block size", d.Np);
+  }
+  d.n_mp = dims->n_mp_trans;
+  d.n_qp = 2 * d.n_mp;
+  d.alphar = dims->alphar;
+  d.Mr = dims->alphar * d.n_mp * 2;
+  d.n_slater = dims->n_slater;
+  d.Nv = dims->alphar * (d.N + 1) + d.n_slater;
+  d.Nv_rbm = d.Nv - d.n_slater;
+  d.nw = dims->n_walkers;
+  d.ns = dims->nsample;
+  d.nupdate = d.N;                        // main.f90:139
+  d.nwarm = std::max(30, d.ns / 100);     // make_sample.f90:66
+  d.pf_sign = ((d.Np * (d.Np - 1) / 2) % 2) ? -1 : 1;
+  d.J1 = dims->J1;
+  d.J2 = dims->J2;
+  // spin projection weights, spin_projection.f90:25-63 (beta = 0, pi)
+  const double pi = std::acos(-1.0);
+  double beta[2] = {0.0, pi};
+  for (int s = 0; s < 2; s++) {
+    double co = std::cos(0.5 * beta[s]), si = std::sin(0.5 * beta[s]);
+    d.sp_cc[s] = co * co;
+    d.sp_cs[s] = co * si;
+    d.sp_ss[s] = si * si;
+  }
+  d.para_sp[0] = 1.0;
+  d.para_sp[1] = dims->spin_parity == 1 ? 1.0 : -1.0;
+  *out = c;
+  cudaError_t e = cudaSetDevice(dims->device);
+  if (e != cudaSuccess) return fail(c, RBMPP_E_CUDA, "cudaSetDevice: %s", cudaGetErrorString(e));
+  CK(cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking));
+  for (auto& e : c->ev) CK(cudaEventCreate(&e));
+  size_t smem = std::max(rbmpp_sampler_smem(d, 256), rbmpp_estimator_smem(d, 256));
+  int maxsm = 0;
+  CK(cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, dims->device));
+  if ((long long)smem > maxsm) return fail(c, RBMPP_E_ARG, "shared-memory workspace %zu B exceeds %d B", smem, maxsm);
+  int r;
+  const int N = d.N;
+  if ((r = dalloc(c, &c->d_wmap, (size_t)d.n_mp * N))) return r;
+  if ((r = dalloc(c, &c->d_winv, (size_t)d.n_mp * N))) return r;
+  if ((r = dalloc(c, &c->d_orb, (size_t)N * N))) return r;
+  if ((r = dalloc(c, &c->d_bonds, (size_t)8 * N))) return r;
+  if ((r = dalloc(c, &c->d_subB, (size_t)N))) return r;
+  if ((r = dalloc(c, &c->d_para, (size_t)2 * d.n_mp))) return r;
+  if ((r = dalloc(c, &c->d_Wr, (size_t)std::max(1, d.alphar) * N))) return r;
+  if ((r = dalloc(c, &c->d_br, (size_t)std::max(1, d.alphar)))) return r;
+  if ((r = dalloc(c, &c->d_slater, (size_t)d.n_slater))) return r;
+  if ((r = dalloc(c, &c->d_XF, (size_t)d.n_qp * N * N))) return r;
+  if ((r = dalloc(c, &c->d_XFT, (size_t)d.n_qp * N * N))) return r;
+  DevWalkers& W = c->W;
+  const size_t nw = d.nw, ns = d.ns;
+  if ((r = dalloc(c, &W.x, nw * N))) return r;
+  if ((r = dalloc(c, &W.idx, nw * N))) return r;
+  if ((r = dalloc(c, &W.cfg, nw * N))) return r;
+  if ((r = dalloc(c, &W.th, nw * std::max(1, d.Mr)))) return r;
+  if ((r = dalloc(c, &W.sgn, nw * d.n_mp))) return r;
+  if ((r = dalloc(c, &W.pf, nw * d.n_qp))) return r;
+  if ((r = dalloc(c, &W.psi, nw * d.n_qp * 2))) return r;
+  if ((r = dalloc(c, &W.Y, nw * d.n_qp * (size_t)d.Np * d.Np))) return r;
+  if ((r = dalloc(c, &W.mt, nw * 625))) return r;
+  if ((r = dalloc(c, &W.nfastup, nw))) return r;
+  if ((r = dalloc(c, &W.naccept, nw))) return r;
+  if ((r = dalloc(c, &W.nacc_all, nw))) return r;
+  if ((r = dalloc(c, &W.status, nw))) return r;
+  if ((r = dalloc(c, &W.xs, nw * ns * N))) return r;
+  if ((r = dalloc(c, &W.pfs, nw * ns * d.n_qp))) return r;
+  if ((r = dalloc(c, &W.psis, nw * ns * (d.n_qp + 1) * 2))) return r;
+  std::vector<int> nf(nw, std::min(100, N * 2));  // main.f90:309
+  CK(cudaMemcpy(W.nfastup, nf.data(), sizeof(int) * nw, cudaMemcpyHostToDevice));
+  // sublattice and bonds: define_sublattice (interface_for_PP.f90:110-136), bond_map (:382-427)
+  std::vector<unsigned char> subB(N);
+  {
+    int i = 0;
+    for (int i2 = 0; i2 < d.L; i2++)
+      for (int i1 = 0; i1 < d.L; i1++) subB[i++] = ((i1 + i2) % 2 == 1);
+  }
+  std::vector<int> bonds(8 * N);
+  for (int i0 = 1; i0 <= 4; i0++)
+    for (int i1 = 0; i1 < N; i1++) {
+      int ix = i1 / d.L, iy = i1 % d.L;
+      if (i0 == 1) ix = (ix + 1) % d.L;
+      else if (i0 == 2) iy = (iy + 1) % d.L;
+      else if (i0 == 3) {
+        ix = (ix + 1) % d.L;
+        iy = (iy + 1) % d.L;
+      } else {
+        ix = (ix + 1) % d.L;
+        iy = (iy - 1 + d.L) % d.L;
+      }
+      int b = (i0 - 1) * N + i1;
+      bonds[2 * b] = i1;
+      bonds[2 * b + 1] = ix * d.L + iy;
+    }
+  CK(cudaMemcpy(c->d_subB, subB.data(), N, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(c->d_bonds, bonds.data(), sizeof(int) * 8 * N, cudaMemcpyHostToDevice));
+  c->Wr.assign((size_t)N * d.alphar, 0.0);
+  c->br.assign(d.alphar, 0.0);
+  c->slater.assign(d.n_slater, 0.0);
+  return 0;
+}
+
+int rbmpp_destroy(rbmpp_ctx* c) {
+  if (!c) return 0;
+  void* ptrs[] = {c->d_wmap, c->d_winv, c->d_orb, c->d_bonds, c->d_subB, c->d_para, c->d_Wr, c->d_br, c->d_slater,
+                  c->d_XF, c->d_XFT, c->W.x, c->W.idx, c->W.cfg, c->W.th, c->W.sgn, c->W.pf, c->W.psi, c->W.Y,
+                  c->W.mt, c->W.nfastup, c->W.naccept, c->W.nacc_all, c->W.status, c->W.xs, c->W.pfs, c->W.psis, c->d_O, c->d_psiS,
+                  c->d_eloc, c->d_a, c->d_b, c->d_tmp_ns, c->d_acc4, c->d_nap, c->d_estat, c->d_gvec, c->d_Ovec,
+                  c->d_vec, c->d_S, c->d_part, c->d_info, c->d_hi, c->d_lo, c->d_Sf};
+  for (void* p : ptrs)
+    if (p) cudaFree(p);
+  for (auto& e : c->ev)
+    if (e) cudaEventDestroy(e);
+  if (c->st) cudaStreamDestroy(c->st);
+  delete c;
+  return 0;
+}
+
+const char* rbmpp_last_error(const rbmpp_ctx* c) { return c ? c->err.c_str() : "null context"; }
+
+int rbmpp_query(const rbmpp_ctx* c, int what, long long* v) {
+  if (!c || !v) return RBMPP_E_ARG;
+  switch (what) {
+    case 0: *v = c->d.Nv; break;
+    case 1: *v = c->d.Nv_rbm; break;
+    case 2: *v = c->d.Mr; break;
+    case 3: *v = c->d.n_qp; break;
+    case 4: *v = c->d.N; break;
+    case 5: *v = (long long)c->bytes; break;
+    default: return RBMPP_E_ARG;
+  }
+  return 0;
+}
+
+int rbmpp_set_tables(rbmpp_ctx* c, const int* W_map, const double* para, const int* orb_idx, const int* orb_sgn) {
+  if (!c || !W_map || !para || !orb_idx) return fail(c, RBMPP_E_ARG, "null table");
+  const DevDims& d = c->d;
+  const int N = d.N;
+  std::vector<int> wmap((size_t)d.n_mp * N), winv((size_t)d.n_mp * N);
+  for (int mp = 0; mp < d.n_mp; mp++) {
+    std::vector<char> seen(N, 0);
+    for (int i = 0; i < N; i++) {
+      int v = W_map[i + (size_t)N * mp];
+      if (v < 1 || v > N) return fail(c, RBMPP_E_ARG, "W_map wrong 1 (sym_info.txt)");
+      if (seen[v - 1]) return fail(c, RBMPP_E_ARG, "W_map wrong 2 (sym_info.txt)");
+      seen[v - 1] = 1;
+      wmap[(size_t)mp * N + i] = v - 1;
+      winv[(size_t)mp * N + (v - 1)] = i;
+    }
+  }
+  for (int mp = 0; mp < d.n_mp; mp++)
+    if (para[2 * mp + 1] != 0.0)
+      return fail(c, RBMPP_E_ARG, "complex para_mp_trans is not supported (real projection weights only)");
+  c->orb_host.assign((size_t)N * N, 0);
+  std::vector<int> cnt(d.n_slater, 0);
+  for (int p = 0; p < N; p++)
+    for (int q = 0; q < N; q++) {
+      int v = orb_idx[p + (size_t)N * q];  // Orbital_Idx(p, q), column-major
+      if (v < 1 || v > d.n_slater) return fail(c, RBMPP_E_ARG, "error4, orbitalidx");
+      if (orb_sgn && orb_sgn[p + (size_t)N * q] != 1)
+        return fail(c, RBMPP_E_ARG, "Orbital_Sgn /= 1 (anti-periodic boundary) is not supported");
+      c->orb_host[(size_t)p * N + q] = v - 1;
+      cnt[v - 1]++;
+    }
+  int inj = 1;
+  for (int k = 0; k < d.n_slater; k++)
+    if (cnt[k] > 1) inj = 0;
+  c->d.orb_injective = inj;
+  CK(cudaMemcpy(c->d_wmap, wmap.data(), sizeof(int) * wmap.size(), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(c->d_winv, winv.data(), sizeof(int) * winv.size(), cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(c->d_para, para, sizeof(double) * 2 * d.n_mp, cudaMemcpyHostToDevice));
+  CK(cudaMemcpy(c->d_orb, c->orb_host.data(), sizeof(int) * c->orb_host.size(), cudaMemcpyHostToDevice));
+  c->tables_set = true;
+  return 0;
+}
+
+int rbmpp_set_params(rbmpp_ctx* c, const double* Wr, const double* br, const double* Wc, const double* bc,
+                     const double* slater, double shift) {
+  if (!c) return RBMPP_E_ARG;
+  if (Wc || bc) return fail(c, RBMPP_E_ARG, "complex RBM parameters given but alphac = 0");
+  if (!c->tables_set) return fail(c, RBMPP_E_STATE, "rbmpp_set_tables must come first");
+  if (Wr) std::memcpy(c->Wr.data(), Wr, sizeof(double) * c->Wr.size());
+  if (br) std::memcpy(c->br.data(), br, sizeof(double) * c->br.size());
+  if (slater) std::memcpy(c->slater.data(), slater, sizeof(double) * c->slater.size());
+  c->shift = shift;
+  c->params_set = true;
+  return upload_params(c);
+}
+
+int rbmpp_get_params(rbmpp_ctx* c, double* Wr, double* br, double* slater, double* shift) {
+  if (!c) return RBMPP_E_ARG;
+  if (Wr) std::memcpy(Wr, c->Wr.data(), sizeof(double) * c->Wr.size());
+  if (br) std::memcpy(br, c->br.data(), sizeof(double) * c->br.size());
+  if (slater) std::memcpy(slater, c->slater.data(), sizeof(double) * c->slater.size());
+  if (shift) *shift = c->shift;
+  return 0;
+}
+
+int rbmpp_seed_walkers(rbmpp_ctx* c, int iseed0) {
+  if (!c) return RBMPP_E_ARG;
+  seed_kernel<<<(c->d.nw + 63) / 64, 64, 0, c->st>>>(c->W.mt, c->d.nw, iseed0, c->d.ns, c->dims.walker_offset);
+  CK(cudaGetLastError());
+  CK(cudaStreamSynchronize(c->st));
+  c->seeded = true;
+  return 0;
+}
+
+int rbmpp_rank0_grnd(rbmpp_ctx* c, int n, double* out) {
+  if (!c || n < 0) return RBMPP_E_ARG;
+  if (n == 0) return 0;
+  double* d_out = nullptr;
+  CK(cudaMalloc(&d_out, sizeof(double) * n));
+  draw_kernel<<<1, 1, 0, c->st>>>(c->W.mt, n, d_out);
+  cudaError_t e = cudaGetLastError();
+  if (e == cudaSuccess) e = cudaMemcpyAsync(out, d_out, sizeof(double) * n, cudaMemcpyDeviceToHost, c->st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->st);
+  cudaFree(d_out);
+  if (e != cudaSuccess) return fail(c, RBMPP_E_CUDA, "rank0_grnd: %s", cudaGetErrorString(e));
+  return 0;
+}
+
+int rbmpp_make_sample(rbmpp_ctx* c, int first, int* naccept, long long* naccept_total) {
+  if (!c) return RBMPP_E_ARG;
+  if (!c->params_set || !c->seeded) return fail(c, RBMPP_E_STATE, "set_params and seed_walkers must come first");
+  if (!first && !c->sampled) return fail(c, RBMPP_E_STATE, "make_sample(first=0) before any sample exists");
+  c->d.shift = c->shift;
+  CK(cudaEventRecord(c->ev[0], c->st));
+  CK(rbmpp_launch_sampler(c->d, tables(c), params(c), c->W, first ? 1 : 0, c->st));
+  CK(cudaEventRecord(c->ev[1], c->st));
+  CK(cudaStreamSynchronize(c->st));
+  int r = check_walker_status(c, c->W.status, c->d.nw, "make_sample");
+  if (r) return r;
+  float ms = 0.f;
+  CK(cudaEventElapsedTime(&ms, c->ev[0], c->ev[1]));
+  c->stats[0] = ms;
+  std::vector<int> na(c->d.nw), naa(c->d.nw);
+  CK(cudaMemcpy(na.data(), c->W.naccept, sizeof(int) * c->d.nw, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(naa.data(), c->W.nacc_all, sizeof(int) * c->d.nw, cudaMemcpyDeviceToHost));
+  long long tot = 0, tot_all = 0;
+  for (int v : na) tot += v;
+  for (int v : naa) tot_all += v;
+  c->stats[5] = (double)tot_all;
+  c->stats[6] = (double)c->d.nw * (double)(c->d.nwarm + c->d.ns + 1) * (double)c->d.nupdate;
+  if (naccept) std::memcpy(naccept, na.data(), sizeof(int) * c->d.nw);
+  if (naccept_total) *naccept_total = tot;
+  c->naccept_total = tot;
+  c->sampled = true;
+  c->measured = false;
+  return 0;
+}
+
+int rbmpp_get_samples(rbmpp_ctx* c, int* x, double* psi, double* pf) {
+  if (!c) return RBMPP_E_ARG;
+  const DevDims& d = c->d;
+  const long long nx = (long long)d.nw * d.ns * d.N;
+  if (x) {
+    int* dx = nullptr;
+    CK(cudaMalloc(&dx, sizeof(int) * nx));
+    i8_to_int_kernel<<<(unsigned)((nx + 255) / 256), 256, 0, c->st>>>(c->W.xs, dx, nx);
+    cudaError_t e = cudaMemcpyAsync(x, dx, sizeof(int) * nx, cudaMemcpyDeviceToHost, c->st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->st);
+    cudaFree(dx);
+    if (e != cudaSuccess) return fail(c, RBMPP_E_CUDA, "get_samples: %s", cudaGetErrorString(e));
+  }
+  if (psi) CK(cudaMemcpy(psi, c->W.psis, sizeof(double) * d.nw * d.ns * (d.n_qp + 1) * 2, cudaMemcpyDeviceToHost));
+  if (pf) CK(cudaMemcpy(pf, c->W.pfs, sizeof(double) * d.nw * d.ns * d.n_qp, cudaMemcpyDeviceToHost));
+  return 0;
+}
+
+int rbmpp_set_samples(rbmpp_ctx* c, const int* x) {
+  if (!c || !x) return RBMPP_E_ARG;
+  const DevDims& d = c->d;
+  const long long nx = (long long)d.nw * d.ns * d.N;
+  int* dx = nullptr;
+  CK(cudaMalloc(&dx, sizeof(int) * nx));
+  cudaError_t e = cudaMemcpyAsync(dx, x, sizeof(int) * nx, cudaMemcpyHostToDevice, c->st);
+  if (e == cudaSuccess) {
+    int_to_i8_kernel<<<(unsigned)((nx + 255) / 256), 256, 0, c->st>>>(dx, c->W.xs, nx);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(c->st);
+  cudaFree(dx);
+  if (e != cudaSuccess) return fail(c, RBMPP_E_CUDA, "set_samples: %s", cudaGetErrorString(e));
+  c->sampled = true;
+  return 0;
+}
+
+static int measure_common(rbmpp_ctx* c, bool with_o) {
+  const DevDims& d = c->d;
+  int r = ensure_measure_buffers(c);
+  if (r) return r;
+  c->d.shift = c->shift;
+  CK(cudaEventRecord(c->ev[2], c->st));
+  CK(rbmpp_launch_estimator(c->d, tables(c), params(c), c->W.xs, c->ns_tot, c->d_psiS, c->d_eloc,
+                            with_o ? c->d_O : nullptr, c->d_nap, c->d_estat, 1, c->st));
+  CK(cudaEventRecord(c->ev[3], c->st));
+  CK(cudaStreamSynchronize(c->st));
+  {
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, c->ev[2], c->ev[3]));
+    c->stats[1] = ms;
+  }
+  r = check_walker_status(c, c->d_estat, c->ns_tot, "calc_phys_quantity");
+  if (r) return r;
+  CK(rbmpp_sample_scalars(c->ns_tot, c->d_psiS, (d.n_qp + 1) * 2, c->d_eloc, c->shift, c->d_a, c->d_b, c->d_acc4,
+                          c->st));
+  CK(cudaMemcpyAsync(c->meas_scal, c->d_acc4, sizeof(double) * 4, cudaMemcpyDeviceToHost, c->st));
+  c->n_samples_total = (double)d.nw * (double)d.ns;
+  // the amplitude draws of the measurement advance each walker's stream
+  CK(rbmpp_launch_advance_rng(c->W.mt, c->d_nap, d.ns, d.nw, 0, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  return 0;
+}
+
+int rbmpp_measure(rbmpp_ctx* c, double* scal, double* gvec, double* Ovec, double* Smat) {
+  if (!c) return RBMPP_E_ARG;
+  if (!c->sampled) return fail(c, RBMPP_E_STATE, "measure before make_sample");
+  const DevDims& d = c->d;
+  int r = measure_common(c, true);
+  if (r) return r;
+  CK(cudaEventRecord(c->ev[4], c->st));
+  CK(rbmpp_gemv_ot(c->ns_tot, d.Nv, c->d_O, c->d_a, c->d_b, c->d_gvec, c->d_Ovec, c->d_part, 64, c->st));
+  CK(cudaEventRecord(c->ev[5], c->st));
+  CK(rbmpp_syrk_ot_o(d.Nv, c->ns_tot, c->d_O, c->d_S, c->st));
+  CK(cudaEventRecord(c->ev[6], c->st));
+  CK(cudaStreamSynchronize(c->st));
+  {
+    float a1 = 0.f, a2 = 0.f;
+    CK(cudaEventElapsedTime(&a1, c->ev[4], c->ev[5]));
+    CK(cudaEventElapsedTime(&a2, c->ev[5], c->ev[6]));
+    c->stats[2] = a1;
+    c->stats[3] = a2;
+  }
+  if (scal) std::memcpy(scal, c->meas_scal, sizeof(double) * 4);
+  if (gvec) CK(cudaMemcpy(gvec, c->d_gvec, sizeof(double) * d.Nv, cudaMemcpyDeviceToHost));
+  if (Ovec) CK(cudaMemcpy(Ovec, c->d_Ovec, sizeof(double) * d.Nv, cudaMemcpyDeviceToHost));
+  if (Smat) CK(cudaMemcpy(Smat, c->d_S, sizeof(double) * d.Nv * d.Nv, cudaMemcpyDeviceToHost));
+  c->measured = true;
+  return 0;
+}
+
+int rbmpp_measure_energy(rbmpp_ctx* c, double* scal) {
+  if (!c) return RBMPP_E_ARG;
+  if (!c->sampled) return fail(c, RBMPP_E_STATE, "measure before make_sample");
+  int r = measure_common(c, false);
+  if (r) return r;
+  if (scal) std::memcpy(scal, c->meas_scal, sizeof(double) * 4);
+  return 0;
+}
+
+int rbmpp_eval_configs(rbmpp_ctx* c, int n, const int* x, double* psi, double* hpsi, double* O) {
+  if (!c || n < 0 || !x) return RBMPP_E_ARG;
+  if (!c->params_set) return fail(c, RBMPP_E_STATE, "set_params must come first");
+  if (n == 0) return 0;
+  const DevDims& d = c->d;
+  int* dx = nullptr;
+  int8_t* dx8 = nullptr;
+  double *dpsi = nullptr, *dh = nullptr, *dO = nullptr;
+  int* dst = nullptr;
+  const long long nx = (long long)n * d.N;
+  int rc = 0;
+  cudaError_t e = cudaMalloc(&dx, sizeof(int) * nx);
+  if (!e) e = cudaMalloc(&dx8, nx);
+  if (!e) e = cudaMalloc(&dpsi, sizeof(double) * (size_t)n * (d.n_qp + 1) * 2);
+  if (!e) e = cudaMalloc(&dh, sizeof(double) * 2 * (size_t)n);
+  if (!e && O) e = cudaMalloc(&dO, sizeof(double) * (size_t)n * d.Nv);
+  if (!e) e = cudaMalloc(&dst, sizeof(int) * n);
+  if (!e) e = cudaMemcpyAsync(dx, x, sizeof(int) * nx, cudaMemcpyHostToDevice, c->st);
+  if (!e) {
+    int_to_i8_kernel<<<(unsigned)((nx + 255) / 256), 256, 0, c->st>>>(dx, dx8, nx);
+    e = cudaGetLastError();
+  }
+  if (!e) e = rbmpp_launch_estimator(c->d, tables(c), params(c), dx8, n, dpsi, dh, dO, nullptr, dst, 0, c->st);
+  if (!e) e = cudaStreamSynchronize(c->st);
+  if (!e) rc = check_walker_status(c, dst, n, "eval_configs");
+  if (!e && !rc && psi) e = cudaMemcpy(psi, dpsi, sizeof(double) * (size_t)n * (d.n_qp + 1) * 2, cudaMemcpyDeviceToHost);
+  if (!e && !rc && hpsi) e = cudaMemcpy(hpsi, dh, sizeof(double) * 2 * (size_t)n, cudaMemcpyDeviceToHost);
+  if (!e && !rc && O) e = cudaMemcpy(O, dO, sizeof(double) * (size_t)n * d.Nv, cudaMemcpyDeviceToHost);
+  cudaFree(dx);
+  cudaFree(dx8);
+  cudaFree(dpsi);
+  cudaFree(dh);
+  if (dO) cudaFree(dO);
+  cudaFree(dst);
+  if (e) return fail(c, RBMPP_E_CUDA, "eval_configs: %s", cudaGetErrorString(e));
+  return rc;
+}
+
+// ---------------------------------------------------------------------------------------------------
+// SR step: SR_pdposv.f90:1-432 (Nsave = 1) with main.f90:351-369 normalisation.
+// ---------------------------------------------------------------------------------------------------
+int rbmpp_sr_step(rbmpp_ctx* c, const rbmpp_sr_in* in, rbmpp_sr_out* out, double* dx_out) {
+  if (!c || !in || !out) return RBMPP_E_ARG;
+  if (!c->measured) return fail(c, RBMPP_E_STATE, "sr_step before measure");
+  if (in->precision != RBMPP_SR_FP64) return fail(c, RBMPP_E_ARG, "unknown SR precision %d", in->precision);
+  const DevDims& d = c->d;
+  const int Nv = d.Nv, Nrbm = d.Nv_rbm, N = d.N;
+  std::memset(out, 0, sizeof(*out));
+  const double norm = c->meas_scal[2];
+  const double ntot = c->n_samples_total;
+  out->norm = norm;
+  out->Etot = c->meas_scal[0] / norm;
+  out->Etot2 = c->meas_scal[1] / norm;
+  out->wf_av = c->meas_scal[3] / ntot;
+  out->accept_ratio = (double)c->naccept_total / ntot / (double)d.nupdate;
+  const double Etot = out->Etot;
+  std::vector<double> g(Nv), ov(Nv);
+  CK(cudaMemcpy(g.data(), c->d_gvec, sizeof(double) * Nv, cudaMemcpyDeviceToHost));
+  CK(cudaMemcpy(ov.data(), c->d_Ovec, sizeof(double) * Nv, cudaMemcpyDeviceToHost));
+  for (int k = 0; k < Nv; k++) {
+    g[k] = g[k] / norm;
+    ov[k] = ov[k] / norm;
+  }
+  for (int k = 0; k < Nv; k++) g[k] = g[k] - 2.0 * Etot * ov[k];  // :4-6
+  double* d_ov = c->d_vec;
+  double* d_x = c->d_vec + Nv;
+  double* d_y = c->d_vec + 2 * Nv;
+  double* d_diag = c->d_vec + 3 * Nv;
+  CK(cudaMemcpyAsync(d_ov, ov.data(), sizeof(double) * Nv, cudaMemcpyHostToDevice, c->st));
+  CK(rbmpp_sr_form(Nv, c->d_S, norm, d_ov, c->st));  // :11-15
+  std::vector<double> dg(Nv);
+  CK(rbmpp_get_diag(Nv, c->d_S, d_diag, c->st));
+  CK(cudaMemcpyAsync(dg.data(), d_diag, sizeof(double) * Nv, cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  double sr = 0, sp = 0;
+  int i1 = 0, i2 = 0;
+  for (int k = 0; k < Nv; k++)  // :18-31
+    if (dg[k] > 0.0) {
+      if (k < Nrbm) {
+        i1++;
+        sr += dg[k];
+      } else {
+        i2++;
+        sp += dg[k];
+      }
+    }
+  if (i1 != Nrbm) return fail(c, RBMPP_E_SDIAG, "i1/=Nv_RBM");
+  if (i2 != d.n_slater - d.n_slater / N) return fail(c, RBMPP_E_SDIAG, "i2 /= N_Slater - N_Slater/N");
+  sr = (Nrbm > 0) ? sr / (double)i1 : 1.0;
+  sp = sp / (double)i2;
+  const double scal = std::sqrt(sr / sp);  // :40
+  for (int k = Nrbm; k < Nv; k++) g[k] = g[k] * scal;
+  CK(rbmpp_sr_scale(Nv, Nrbm, c->d_S, scal, c->st));  // :54-74
+  CK(rbmpp_get_diag(Nv, c->d_S, d_diag, c->st));
+  CK(cudaMemcpyAsync(dg.data(), d_diag, sizeof(double) * Nv, cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  // :78-100 f_ii checks
+  std::vector<char> is_fii(Nv, 0);
+  for (int i = 0; i < N; i++) is_fii[c->orb_host[(size_t)i * N + i] + Nv - d.n_slater] = 1;
+  std::vector<int> zero_list;
+  for (int k = 0; k < Nv; k++) {
+    if (dg[k] < 0.0) return fail(c, RBMPP_E_SDIAG, "diagonal element of S matrix is not positive");
+    if (dg[k] == 0.0) {
+      if (!is_fii[k]) return fail(c, RBMPP_E_SDIAG, "diagonal element of S matrix is zero for other than f_ii parameters");
+      if (std::fabs(ov[k]) > 1e-300 || std::fabs(g[k]) > 1e-300)
+        return fail(c, RBMPP_E_SDIAG, "Ovec/gvec related with f_ii parameters is wrong");
+      zero_list.push_back(k);
+    } else if (is_fii[k]) {
+      return fail(c, RBMPP_E_SDIAG, "diagonal element of S matrix is positive for f_ii parameters");
+    }
+  }
+  if (!zero_list.empty()) {
+    int* d_list = nullptr;
+    double* d_m = nullptr;
+    CK(cudaMalloc(&d_list, sizeof(int) * zero_list.size()));
+    CK(cudaMalloc(&d_m, sizeof(double) * zero_list.size()));
+    std::vector<double> mx(zero_list.size());
+    cudaError_t e = cudaMemcpyAsync(d_list, zero_list.data(), sizeof(int) * zero_list.size(), cudaMemcpyHostToDevice, c->st);
+    if (!e) e = rbmpp_rowcol_absmax(Nv, c->d_S, d_list, (int)zero_list.size(), d_m, c->st);
+    if (!e) e = cudaMemcpyAsync(mx.data(), d_m, sizeof(double) * mx.size(), cudaMemcpyDeviceToHost, c->st);
+    if (!e) e = cudaStreamSynchronize(c->st);
+    cudaFree(d_list);
+    cudaFree(d_m);
+    if (e) return fail(c, RBMPP_E_CUDA, "f_ii check: %s", cudaGetErrorString(e));
+    for (double m : mx)
+      if (m > 1e-300) return fail(c, RBMPP_E_SDIAG, "Smat related with f_ii parameters is wrong");
+  }
+  double sdiag = 0, srb = 0, spp = 0;  // :104-140
+  i1 = i2 = 0;
+  int kmaxS = -100, kminS = -100;
+  double Smax = 0.0, Smin = std::exp(50.0);
+  for (int k = 0; k < Nv; k++)
+    if (dg[k] > 0.0) {
+      if (dg[k] > Smax) {
+        Smax = dg[k];
+        kmaxS = k + 1;
+      }
+      if (dg[k] < Smin) {
+        Smin = dg[k];
+        kminS = k + 1;
+      }
+      sdiag += dg[k];
+      if (k < Nrbm) {
+        i1++;
+        srb += dg[k];
+      } else {
+        i2++;
+        spp += dg[k];
+      }
+    }
+  (void)kmaxS;
+  (void)kminS;
+  sdiag = sdiag / (double)(i1 + i2);
+  srb = (Nrbm > 0) ? srb / (double)i1 : 1.0;
+  spp = spp / (double)i2;
+  if (std::fabs(srb / spp - 1.0) > 1e-5) return fail(c, RBMPP_E_SDIAG, "Sdiag_av_RBM/=Sdiag_av_PP");
+  const double rcut = sdiag * in->s_cut;
+  int nS = 0;
+  for (int k = 0; k < Nv; k++)
+    if (dg[k] > rcut) nS++;
+  const double s_factor = std::max(1e-4, in->s_factor0);  // :167-170
+  CK(rbmpp_add_diag(Nv, c->d_S, sdiag * s_factor, c->st));
+  // RNG: every rank draws at :172 (left-to-right .and.)
+  CK(rbmpp_launch_advance_rng(c->W.mt, nullptr, 0, d.nw, 1, c->st));
+  // pdposv('U') :232 -> Cholesky of the upper triangle + solve
+  CK(cudaEventRecord(c->ev[7], c->st));
+  CK(rbmpp_potrf_upper(Nv, c->d_S, c->d_info, c->st));
+  int info = 0;
+  CK(cudaMemcpyAsync(&info, c->d_info, sizeof(int), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaMemcpyAsync(d_x, g.data(), sizeof(double) * Nv, cudaMemcpyHostToDevice, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  if (info != 0) return fail(c, RBMPP_E_CHOL, "info (pdposv): %d", info);
+  CK(rbmpp_potrs_upper(Nv, c->d_S, d_x, c->st));
+  CK(cudaEventRecord(c->ev[8], c->st));
+  // lambda = sqrt(x^T S x) = ||U x|| and its block split (:251-277)
+  std::vector<double> x(Nv), ux(Nv), xr(Nv, 0.0), xp(Nv, 0.0);
+  CK(cudaMemcpyAsync(x.data(), d_x, sizeof(double) * Nv, cudaMemcpyDeviceToHost, c->st));
+  CK(rbmpp_trmv_upper(Nv, c->d_S, d_x, d_y, c->st));
+  CK(cudaMemcpyAsync(ux.data(), d_y, sizeof(double) * Nv, cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  {
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, c->ev[7], c->ev[8]));
+    c->stats[4] = ms;
+  }
+  double lam2 = 0.0;
+  for (int k = 0; k < Nv; k++) lam2 += ux[k] * ux[k];
+  for (int k = 0; k < Nv; k++) (k < Nrbm ? xr[k] : xp[k]) = x[k];
+  double lrr = 0, lpp = 0;
+  {
+    CK(cudaMemcpyAsync(d_y, xr.data(), sizeof(double) * Nv, cudaMemcpyHostToDevice, c->st));
+    CK(rbmpp_trmv_upper(Nv, c->d_S, d_y, d_diag, c->st));
+    CK(cudaMemcpyAsync(ux.data(), d_diag, sizeof(double) * Nv, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    for (int k = 0; k < Nv; k++) lrr += ux[k] * ux[k];
+    CK(cudaMemcpyAsync(d_y, xp.data(), sizeof(double) * Nv, cudaMemcpyHostToDevice, c->st));
+    CK(rbmpp_trmv_upper(Nv, c->d_S, d_y, d_diag, c->st));
+    CK(cudaMemcpyAsync(ux.data(), d_diag, sizeof(double) * Nv, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    for (int k = 0; k < Nv; k++) lpp += ux[k] * ux[k];
+  }
+  double lrp = lam2 - lrr - lpp;
+  double lam = std::sqrt(lam2);
+  // rank 0 draws at :281 and :313 (global walker 0 lives in the context with walker_offset 0)
+  if (c->dims.walker_offset == 0) CK(rbmpp_launch_advance_rng(c->W.mt, nullptr, 0, 1, 2, c->st));
+  lam = lam * 5.0 / (double)d.L;  // :309
+  out->lambda = lam;
+  out->lambda_rbm_rbm = lrr;
+  out->lambda_pp_pp = lpp;
+  out->lambda_rbm_pp = lrp;
+  if (lam > 1.0)
+    for (int k = 0; k < Nv; k++) x[k] = x[k] / lam;
+  for (int k = Nrbm; k < Nv; k++) x[k] = x[k] * scal;  // :325-327
+  double delW = 0.0;
+  int kmax = -100, knz = 0;
+  for (int k = 0; k < Nv; k++) {
+    if (std::fabs(in->delta_tau * x[k]) > delW) {
+      delW = std::fabs(in->delta_tau * x[k]);
+      kmax = k + 1;
+    }
+    if (std::fabs(x[k]) > 1e-12) knz++;
+  }
+  std::vector<double> gam(Nv);
+  int k1 = 0;
+  for (int f = 0; f < d.alphar; f++) gam[k1++] = c->br[f];
+  for (int f = 0; f < d.alphar; f++)
+    for (int iw = 0; iw < N; iw++) gam[k1++] = c->Wr[iw + (size_t)N * f];
+  for (int o = 0; o < d.n_slater; o++) gam[k1++] = c->slater[o];
+  const double max_change = 0.04;  // main.f90:50
+  for (int k = 0; k < Nv; k++) {   // :347-354
+    if (delW > max_change) gam[k] = gam[k] - in->delta_tau * x[k] * (max_change / delW);
+    else gam[k] = gam[k] - in->delta_tau * x[k];
+  }
+  const int off = d.alphar * (N + 1);  // :356-366
+  double r1 = 0.0;
+  for (int k = off; k < Nv; k++) r1 = r1 + std::fabs(gam[k]);
+  r1 = r1 / (double)d.n_slater;
+  for (int k = off; k < Nv; k++) gam[k] = gam[k] * 0.25 / r1;
+  k1 = 0;  // :385-413
+  for (int f = 0; f < d.alphar; f++) c->br[f] = gam[k1++];
+  for (int f = 0; f < d.alphar; f++)
+    for (int iw = 0; iw < N; iw++) c->Wr[iw + (size_t)N * f] = gam[k1++];
+  r1 = 0.0;
+  for (int o = 0; o < d.n_slater; o++) {
+    c->slater[o] = gam[k1++];
+    r1 += std::fabs(c->slater[o]);
+  }
+  r1 /= (double)d.n_slater;
+  if (std::fabs(r1 - 0.25) > 1e-6) return fail(c, RBMPP_E_SLATER_NORM, "r1/=slater_abs_av");
+  out->delW_max = delW;
+  out->kmax = kmax;
+  out->k_nonzero = knz;
+  out->s_factor = s_factor;
+  out->sdiag_av = sdiag;
+  out->smat_scaling = scal;
+  out->nSmat = nS;
+  if (dx_out) std::memcpy(dx_out, x.data(), sizeof(double) * Nv);
+  c->measured = false;  // S was factorised in place
+  return upload_params(c);
+}
+
+int rbmpp_exchange_measurement(rbmpp_ctx* c, int direction, double* d_S, double* d_g, double* d_ov, double* scal6) {
+  if (!c || !scal6) return RBMPP_E_ARG;
+  if (!c->measured) return fail(c, RBMPP_E_STATE, "exchange_measurement before measure");
+  const int Nv = c->d.Nv;
+  const size_t nS = (size_t)Nv * Nv * sizeof(double), nV = (size_t)Nv * sizeof(double);
+  if (direction == 0) {
+    if (d_S) CK(cudaMemcpyAsync(d_S, c->d_S, nS, cudaMemcpyDeviceToDevice, c->st));
+    if (d_g) CK(cudaMemcpyAsync(d_g, c->d_gvec, nV, cudaMemcpyDeviceToDevice, c->st));
+    if (d_ov) CK(cudaMemcpyAsync(d_ov, c->d_Ovec, nV, cudaMemcpyDeviceToDevice, c->st));
+    for (int k = 0; k < 4; k++) scal6[k] = c->meas_scal[k];
+    scal6[4] = (double)c->naccept_total;
+    scal6[5] = c->n_samples_total;
+  } else {
+    if (d_S) CK(cudaMemcpyAsync(c->d_S, d_S, nS, cudaMemcpyDeviceToDevice, c->st));
+    if (d_g) CK(cudaMemcpyAsync(c->d_gvec, d_g, nV, cudaMemcpyDeviceToDevice, c->st));
+    if (d_ov) CK(cudaMemcpyAsync(c->d_Ovec, d_ov, nV, cudaMemcpyDeviceToDevice, c->st));
+    for (int k = 0; k < 4; k++) c->meas_scal[k] = scal6[k];
+    c->naccept_total = (long long)scal6[4];
+    c->n_samples_total = scal6[5];
+  }
+  CK(cudaStreamSynchronize(c->st));
+  return 0;
+}
+
+int rbmpp_set_shift(rbmpp_ctx* c, double shift) {
+  if (!c) return RBMPP_E_ARG;
+  c->shift = shift;
+  c->d.shift = shift;
+  return 0;
+}
+
+int rbmpp_iteration(rbmpp_ctx* c, int precision, double delta_tau, double s_factor_scale, double s_cut,
+                    double s_factor0_initial, rbmpp_sr_out* out) {
+  if (!c || !out) return RBMPP_E_ARG;
+  if (!c->s_factor_init) {
+    c->s_factor0 = s_factor0_initial;
+    c->s_factor_init = true;
+  }
+  c->iteration++;
+  CK(cudaEventRecord(c->ev[9], c->st));
+  int r = rbmpp_make_sample(c, c->iteration == 1 ? 1 : 0, nullptr, nullptr);
+  if (r) return r;
+  r = rbmpp_measure(c, nullptr, nullptr, nullptr, nullptr);
+  if (r) return r;
+  rbmpp_sr_in in;
+  std::memset(&in, 0, sizeof(in));
+  in.iteration = c->iteration;
+  in.precision = precision;
+  in.refine_steps = 3;
+  in.delta_tau = delta_tau;
+  in.s_factor0 = c->s_factor0;
+  in.s_cut = s_cut;
+  r = rbmpp_sr_step(c, &in, out, nullptr);
+  if (r) return r;
+  // main.f90:439-453
+  c->s_factor0 = c->s_factor0 * s_factor_scale;
+  for (int k = 1; k < 10; k++) c->wf_av_list[k - 1] = c->wf_av_list[k];
+  c->wf_av_list[9] = out->wf_av;
+  double wf = 0.0;
+  for (int k = 0; k < 10; k++) wf = wf + c->wf_av_list[k];
+  wf = wf / 10.0;
+  c->shift = wf * 0.001 / (double)c->d.N / (double)c->d.N;
+  c->d.shift = c->shift;
+  CK(cudaEventRecord(c->ev[10], c->st));
+  CK(cudaEventSynchronize(c->ev[10]));
+  float ms = 0.f;
+  CK(cudaEventElapsedTime(&ms, c->ev[9], c->ev[10]));
+  c->stats[7] = ms;
+  return 0;
+}
+
+int rbmpp_get_stats(const rbmpp_ctx* c, double* out, int n) {
+  if (!c || !out || n < 0) return RBMPP_E_ARG;
+  for (int k = 0; k < n && k < 8; k++) out[k] = c->stats[k];
+  return 0;
+}
+
+}  // extern "C"

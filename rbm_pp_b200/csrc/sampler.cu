@@ -1,0 +1,586 @@
+// sampler.cu -- persistent Metropolis sampler: one CTA per walker runs the whole make_sample call
+// (make_sample.f90:4-240): warm-up + Nsample sweeps of Nupdate exchange proposals, Nfastup-scheduled
+// scratch recomputation with the drift check, rare global spin flips, sample storage.
+//
+// RNG draws happen on thread 0 in exactly the reference's order, so spin configurations and
+// accept/reject sequences are bit-identical to a rank of the reference (ties of the acceptance
+// test within rounding excepted).
+//
+// Per proposal and projection qp one warp gathers the new row u and column v of X from XF/XFT,
+// streams Y = X^{-1} (coalesced, lane <-> column) and evaluates the determinant ratio
+//     R = (u^T Y)_ua (Y v)_db - Y(db,ua) (u^T Y v - c)      (= Pf'/Pf, pfupdate_two.f90:27-88)
+// An accepted move applies the rank-2 Sherman-Morrison update of Y (pfupdate_two.f90:113-224).
+#include "walker_ops.cuh"
+
+namespace {
+
+// ---- per-warp determinant ratio for projection qp; result valid on all lanes ----
+template <int KPL>
+__device__ inline double warp_ratio(const DevDims& d, const DevParams& p, const double* Yq, int qp, const int* idx,
+                                    int ua, int db, int s_up, int s_dn, double* u, double* v) {
+  const int lane = threadIdx.x & 31, Np = d.Np, N = d.N;
+  const double* XFq = p.XF + (size_t)qp * N * N;
+  const double* XFTq = p.XFT + (size_t)qp * N * N;
+  const double c = XFq[(size_t)s_dn * N + s_up];
+  for (int j = lane; j < Np; j += 32) {
+    u[j] = (j == db) ? c : XFq[(size_t)s_dn * N + idx[Np + j]];
+    v[j] = (j == ua) ? c : XFTq[(size_t)s_up * N + idx[j]];
+  }
+  __syncwarp();
+  double acc[KPL];
+#pragma unroll
+  for (int m = 0; m < KPL; m++) acc[m] = 0.0;
+  int j = 0;
+  for (; j + 4 <= Np; j += 4) {
+    double y[4][KPL];
+#pragma unroll
+    for (int r = 0; r < 4; r++)
+#pragma unroll
+      for (int m = 0; m < KPL; m++) {
+        int k = lane + 32 * m;
+        y[r][m] = (k < Np) ? __ldg(Yq + (size_t)(j + r) * Np + k) : 0.0;
+      }
+#pragma unroll
+    for (int r = 0; r < 4; r++) {
+      double uj = u[j + r];
+#pragma unroll
+      for (int m = 0; m < KPL; m++) acc[m] = fma(uj, y[r][m], acc[m]);
+    }
+  }
+  for (; j < Np; j++) {
+    double uj = u[j];
+#pragma unroll
+    for (int m = 0; m < KPL; m++) {
+      int k = lane + 32 * m;
+      if (k < Np) acc[m] = fma(uj, __ldg(Yq + (size_t)j * Np + k), acc[m]);
+    }
+  }
+  double wv = 0.0, sb = 0.0, ra = 0.0, ydbua = 0.0;
+#pragma unroll
+  for (int m = 0; m < KPL; m++) {
+    int k = lane + 32 * m;
+    if (k < Np) {
+      double rho = __ldg(Yq + (size_t)db * Np + k);
+      wv = fma(acc[m], v[k], wv);
+      sb = fma(rho, v[k], sb);
+      if (k == ua) {
+        ra = acc[m];
+        ydbua = rho;
+      }
+    }
+  }
+  wv = warp_sum(wv);
+  sb = warp_sum(sb);
+  ra = warp_sum(ra);
+  ydbua = warp_sum(ydbua);
+  __syncwarp();
+  return ra * sb - ydbua * (wv - c);
+}
+
+// ---- per-warp rank-2 update of Y after an accepted exchange (u, v from warp_ratio) ----
+template <int KPL>
+__device__ inline void warp_update(const DevDims& d, double* Yq, int ua, int db, double c, const double* u,
+                                   const double* v, double* A, double* S) {
+  const int lane = threadIdx.x & 31, Np = d.Np;
+  double acc[KPL];
+#pragma unroll
+  for (int m = 0; m < KPL; m++) acc[m] = 0.0;
+  for (int j = 0; j < Np; j++) {
+    double uj = u[j], part = 0.0;
+#pragma unroll
+    for (int m = 0; m < KPL; m++) {
+      int k = lane + 32 * m;
+      if (k < Np) {
+        double y = Yq[(size_t)j * Np + k];
+        acc[m] = fma(uj, y, acc[m]);
+        part = fma(y, v[k], part);
+        if (k == ua) A[j] = y;
+      }
+    }
+    part = warp_sum(part);
+    if (lane == 0) S[j] = part;
+  }
+  double rho[KPL];
+  double wv = 0.0, ra = 0.0, ydbua = 0.0;
+#pragma unroll
+  for (int m = 0; m < KPL; m++) {
+    int k = lane + 32 * m;
+    rho[m] = 0.0;
+    if (k < Np) {
+      rho[m] = Yq[(size_t)db * Np + k];
+      wv = fma(acc[m], v[k], wv);
+      if (k == ua) {
+        ra = acc[m];
+        ydbua = rho[m];
+      }
+    }
+  }
+  wv = warp_sum(wv);
+  ra = warp_sum(ra);
+  ydbua = warp_sum(ydbua);
+  __syncwarp();
+  const double sb = S[db];
+  const double R1 = ra;
+  const double R = ra * sb - ydbua * (wv - c);
+  const double inv_r1 = 1.0 / R1, r1_over_r = R1 / R, wc = (wv - c) * inv_r1;
+  double bk[KPL], tk[KPL];
+#pragma unroll
+  for (int m = 0; m < KPL; m++) {
+    int k = lane + 32 * m;
+    double B = acc[m] - (k == ua ? 1.0 : 0.0);
+    bk[m] = B * inv_r1;
+    tk[m] = (rho[m] - ydbua * B * inv_r1) * r1_over_r;
+  }
+  for (int j = 0; j < Np; j++) {
+    double Aj = A[j];
+    double s1 = S[j] - Aj * wc - (j == db ? 1.0 : 0.0);
+#pragma unroll
+    for (int m = 0; m < KPL; m++) {
+      int k = lane + 32 * m;
+      if (k < Np) {
+        double* py = Yq + (size_t)j * Np + k;
+        *py = *py - Aj * bk[m] - s1 * tk[m];
+      }
+    }
+  }
+  __syncwarp();
+}
+
+struct SCtx {
+  DevDims d;
+  DevTables t;
+  DevParams p;
+  DevWalkers W;
+  int w;
+  WS s;
+  double* Yw;  // this walker's Y
+};
+
+__device__ inline int& status(const SCtx& c) { return c.s.iflag[F_STATUS]; }
+
+// Scratch inverse of every projection for labelling idx: writes Y (when write_y) and pf_out.
+// When diff is requested, also computes the reference's drift measures against the stored Y / pf.
+__device__ void cta_scratch_all(const SCtx& c, const int* idx, double* pf_out, bool write_y, bool diff) {
+  const DevDims& d = c.d;
+  const WS& s = c.s;
+  const int Np = d.Np, ld = Np + 1, tid = threadIdx.x;
+  double diff_inv = -1.0;
+  for (int qp = 0; qp < d.n_qp; qp++) {
+    cta_build_x(d, c.p, qp, idx, s.tile);
+    __syncthreads();
+    cta_gauss_jordan(d, s);
+    if (s.iflag[F_SINGULAR]) {
+      if (tid == 0) status(c) = ST_SINGULAR;
+      __syncthreads();
+      return;
+    }
+    double* Yq = c.Yw + (size_t)qp * Np * Np;
+    if (diff) {  // make_sample.f90:106-113
+      double mx = 0.0, md = 0.0;
+      for (int e = tid; e < Np * Np; e += blockDim.x) {
+        int a = e / Np, b = e - a * Np;
+        double nv = s.tile[a * ld + b];
+        mx = fmax(mx, fabs(nv));
+        md = fmax(md, fabs(Yq[e] - nv));
+      }
+      mx = warp_max(mx);
+      md = warp_max(md);
+      if ((tid & 31) == 0) {
+        s.red[tid >> 5] = mx;
+        s.red[32 + (tid >> 5)] = md;
+      }
+      __syncthreads();
+      if (tid == 0) {
+        double a = 0.0, b = 0.0;
+        for (int k = 0; k < (int)(blockDim.x >> 5); k++) {
+          a = fmax(a, s.red[k]);
+          b = fmax(b, s.red[32 + k]);
+        }
+        diff_inv = fmax(diff_inv, b / a);
+      }
+    }
+    if (write_y)
+      for (int e = tid; e < Np * Np; e += blockDim.x) {
+        int a = e / Np, b = e - a * Np;
+        Yq[e] = s.tile[a * ld + b];
+      }
+    if (tid == 0) pf_out[qp] = (double)d.pf_sign * s.dsc[D_DET];
+    __syncthreads();
+  }
+  if (tid == 0) s.dsc[D_DIFFINV] = diff_inv;
+  __syncthreads();
+}
+
+// calc_theta, x_to_Ele_Idx, calculate_MAll, sign_PP, calc_amplitude (make_sample.f90:54-60 / :345-350)
+__device__ void full_state(const SCtx& c) {
+  const WS& s = c.s;
+  cta_calc_theta(c.d, c.t, c.p, s.x, s.th);
+  if (threadIdx.x == 0) {
+    int e = x_to_ele(c.d, s.x, s.idx, s.cfg);
+    if (e) status(c) = e;
+  }
+  __syncthreads();
+  if (status(c)) return;
+  cta_scratch_all(c, s.idx, s.pf, true, false);
+  if (status(c)) return;
+  cta_sign_pp(c.d, c.t, s, s.idx, s.sgn);
+  __syncthreads();
+  if (threadIdx.x == 0)
+    for (int mp = 1; mp < c.d.n_mp; mp++)
+      if (s.pb[mp] != s.pb[0]) status(c) = ST_SIGN;
+  __syncthreads();
+  if (status(c)) return;
+  cta_amplitude(c.d, c.t, s, s.th, s.pf, s.sgn, s.psi, D_PSI0R);
+}
+
+// make_initial_x make_sample.f90:298-362
+__device__ void make_initial_x(const SCtx& c) {
+  const WS& s = c.s;
+  for (int it1 = 0; it1 < 1000000; it1++) {
+    if (threadIdx.x == 0) {
+      for (int i = 0; i < c.d.N; i++) s.x[i] = -1;
+      int i3 = 0, ok = 0;
+      for (int it2 = 0; it2 < 1000000; it2++) {
+        int i = nran(s.mt, c.d.N) - 1;
+        if (s.x[i] == -1) {
+          i3++;
+          s.x[i] = 1;
+        }
+        if (i3 == c.d.N / 2) {
+          ok = 1;
+          break;
+        }
+      }
+      if (!ok) status(c) = ST_INITX;
+    }
+    __syncthreads();
+    if (status(c)) return;
+    full_state(c);
+    if (status(c)) return;
+    if (hypot(s.dsc[D_PSI0R], s.dsc[D_PSI0I]) > 1e-300) return;
+  }
+  if (threadIdx.x == 0) status(c) = ST_INITX;
+  __syncthreads();
+}
+
+// Nfastup checkpoint make_sample.f90:74-128
+__device__ void checkpoint(const SCtx& c, int& nfastup) {
+  const DevDims& d = c.d;
+  const WS& s = c.s;
+  for (int j = threadIdx.x; j < d.Mr; j += blockDim.x) s.thp[j] = s.th[j];
+  for (int mp = threadIdx.x; mp < d.n_mp; mp += blockDim.x) s.sgnp[mp] = s.sgn[mp];
+  __syncthreads();
+  cta_calc_theta(d, c.t, c.p, s.x, s.th);
+  if (threadIdx.x == 0) {
+    int e = check_ele(d, s.x, s.idx, s.cfg);
+    if (e) status(c) = e;
+  }
+  __syncthreads();
+  if (status(c)) return;
+  cta_sign_pp(d, c.t, s, s.idx, s.sgn);
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int mp = 1; mp < d.n_mp; mp++)
+      if (s.pb[mp] != s.pb[0]) status(c) = ST_SIGN;
+    for (int mp = 0; mp < d.n_mp; mp++)
+      if (s.sgnp[mp] != s.sgn[mp]) status(c) = ST_SIGN;
+  }
+  for (int j = threadIdx.x; j < d.Mr; j += blockDim.x)
+    if (fabs(s.th[j] - s.thp[j]) > 1.0e-5) status(c) = ST_THETA;
+  __syncthreads();
+  if (status(c)) return;
+  // old Pf kept in pfp for the drift measure
+  for (int qp = threadIdx.x; qp < d.n_qp; qp += blockDim.x) s.pfp[qp] = s.pf[qp];
+  __syncthreads();
+  cta_scratch_all(c, s.idx, s.pf, true, true);
+  if (status(c)) return;
+  cta_amplitude(d, c.t, s, s.th, s.pf, s.sgn, s.psi, D_PSI0R);
+  if (threadIdx.x == 0) {
+    double r2 = 0.0;
+    for (int qp = 0; qp < d.n_qp; qp++) r2 = r2 + fabs(s.pf[qp]);
+    r2 = r2 / (double)d.n_qp;
+    double dpf = -1.0;
+    for (int qp = 0; qp < d.n_qp; qp++) dpf = fmax(dpf, fabs(s.pfp[qp] - s.pf[qp]) / r2);
+    double dinv = s.dsc[D_DIFFINV];
+    (void)grnd(s.mt);  // make_sample.f90:116
+    if (dinv > 1.0e-5 || dpf > 1.0e-5) {
+      nfastup = max(1, (int)floor((double)nfastup / 1.2 + 0.5));
+      if (dinv > 10.0 && dpf > 10.0) (void)grnd(s.mt);  // make_sample.f90:122
+    } else {
+      nfastup = min(100, (int)floor((double)nfastup * 1.1 + 0.5));
+    }
+    s.iflag[F_AUX] = nfastup;
+  }
+  __syncthreads();
+  nfastup = s.iflag[F_AUX];
+}
+
+// Global spin flip make_sample.f90:135-158 (RNG check already drawn by the caller).
+__device__ void global_flip(const SCtx& c) {
+  const DevDims& d = c.d;
+  const WS& s = c.s;
+  for (int i = threadIdx.x; i < d.N; i += blockDim.x) s.x2[i] = -s.x[i];
+  __syncthreads();
+  cta_calc_theta(d, c.t, c.p, s.x2, s.thp);
+  if (threadIdx.x == 0) {
+    int e = x_to_ele(d, s.x2, s.idx2, s.cfg2);
+    if (e) status(c) = e;
+  }
+  __syncthreads();
+  if (status(c)) return;
+  cta_scratch_all(c, s.idx2, s.pfp, false, false);  // Pf of the flipped configuration
+  if (status(c)) return;
+  cta_sign_pp(d, c.t, s, s.idx2, s.sgnp);
+  __syncthreads();
+  if (threadIdx.x == 0)
+    for (int mp = 1; mp < d.n_mp; mp++)
+      if (s.pb[mp] != s.pb[0]) status(c) = ST_SIGN;
+  __syncthreads();
+  if (status(c)) return;
+  cta_amplitude(d, c.t, s, s.thp, s.pfp, s.sgnp, s.psip, D_PSIPR);
+  if (threadIdx.x == 0) {
+    double r1 = (hypot(s.dsc[D_PSIPR], s.dsc[D_PSIPI]) + d.shift) / (hypot(s.dsc[D_PSI0R], s.dsc[D_PSI0I]) + d.shift);
+    int acc = grnd(s.mt) < r1 * r1;
+    if (acc) (void)grnd(s.mt);  // make_sample.f90:146
+    s.iflag[F_ACCEPT] = acc;
+  }
+  __syncthreads();
+  if (!s.iflag[F_ACCEPT]) return;
+  for (int i = threadIdx.x; i < d.N; i += blockDim.x) {
+    s.x[i] = s.x2[i];
+    s.idx[i] = s.idx2[i];
+    s.cfg[i] = s.cfg2[i];
+  }
+  for (int j = threadIdx.x; j < d.Mr; j += blockDim.x) s.th[j] = s.thp[j];
+  for (int mp = threadIdx.x; mp < d.n_mp; mp += blockDim.x) s.sgn[mp] = s.sgnp[mp];
+  for (int qp = threadIdx.x; qp < d.n_qp; qp += blockDim.x) {
+    s.psi[2 * qp] = s.psip[2 * qp];
+    s.psi[2 * qp + 1] = s.psip[2 * qp + 1];
+  }
+  if (threadIdx.x == 0) {
+    s.dsc[D_PSI0R] = s.dsc[D_PSIPR];
+    s.dsc[D_PSI0I] = s.dsc[D_PSIPI];
+  }
+  __syncthreads();
+  cta_scratch_all(c, s.idx, s.pf, true, false);  // Tmp_Inv_M of the accepted flipped state
+}
+
+template <int KPL>
+__global__ void __launch_bounds__(256) sampler_kernel(DevDims d, DevTables t, DevParams p, DevWalkers W, int first) {
+  extern __shared__ __align__(16) char smem[];
+  SCtx c;
+  c.d = d;
+  c.t = t;
+  c.p = p;
+  c.W = W;
+  c.w = blockIdx.x;
+  ws_layout(d, blockDim.x >> 5, smem, &c.s);
+  const WS& s = c.s;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, nwarps = blockDim.x >> 5;
+  const int w = c.w, N = d.N, Np = d.Np;
+  c.Yw = W.Y + (size_t)w * d.n_qp * Np * Np;
+
+  for (int k = tid; k < 625; k += blockDim.x) s.mt[k] = W.mt[(size_t)w * 625 + k];
+  if (tid == 0) status(c) = 0;
+  __syncthreads();
+  int nfastup = W.nfastup[w];
+
+  if (first) {
+    make_initial_x(c);
+  } else {
+    for (int i = tid; i < N; i += blockDim.x) s.x[i] = W.xs[((size_t)w * d.ns + (d.ns - 1)) * N + i];
+    __syncthreads();
+    full_state(c);
+    if (!status(c)) {
+      if (tid == 0) s.iflag[F_AUX] = grnd(s.mt) < 0.05;
+      __syncthreads();
+      if (s.iflag[F_AUX]) make_initial_x(c);
+    }
+  }
+
+  int naccept = 0, nacc_tmp = 0, nacc_all = 0;
+  for (int i0 = -d.nwarm; i0 <= d.ns && !status(c); i0++) {
+    if (nacc_tmp > nfastup) {
+      checkpoint(c, nfastup);
+      if (status(c)) break;
+      nacc_tmp = 0;
+    }
+    for (int iu = 0; iu < d.nupdate; iu++) {
+      if (tid == 0) s.iflag[F_FLIP] = grnd(s.mt) < 3.0e-4;
+      __syncthreads();
+      if (s.iflag[F_FLIP]) {
+        global_flip(c);
+        if (status(c)) break;
+      }
+      // make_spin_flip_candidate make_sample.f90:244-294
+      if (tid == 0) {
+        const int L = d.L;
+        int dist_max = nran(s.mt, L - 1) + 1, ok = 0;
+        for (int it = 0; it < 1000000; it++) {
+          int i1 = nran(s.mt, N);
+          int ix = (i1 - 1) / L, iy = (i1 - 1) - ix * L;
+          ix = ix + nran(s.mt, dist_max) - 1;
+          iy = iy + nran(s.mt, dist_max) - 1;
+          if (ix >= L) ix -= L;
+          if (iy >= L) iy -= L;
+          int i2 = ix * L + iy + 1;
+          if (s.x[i1 - 1] != s.x[i2 - 1]) {
+            s.iflag[F_I1] = i1 - 1;
+            s.iflag[F_I2] = i2 - 1;
+            ok = 1;
+            break;
+          }
+        }
+        if (!ok || dist_max <= 1) status(c) = ST_CANDIDATE;
+      }
+      __syncthreads();
+      if (status(c)) break;
+      const int i1 = s.iflag[F_I1], i2 = s.iflag[F_I2];
+      const int x1 = s.x[i1];
+      const int i3 = s.cfg[i1], i4 = s.cfg[i2];
+      int ua, db, s_up, s_dn;
+      if (x1 == 1) {
+        ua = i3;
+        db = i4 - Np;
+        s_up = i1;
+        s_dn = i2;
+      } else {
+        ua = i4;
+        db = i3 - Np;
+        s_up = i2;
+        s_dn = i1;
+      }
+      cta_update_theta(d, t, p, s.x, i1, i2, s.th, s.thp);
+      const int flipsign = (t.subB[i1] ? -1 : 1) * (t.subB[i2] ? -1 : 1);
+      for (int mp = tid; mp < d.n_mp; mp += blockDim.x) s.sgnp[mp] = -s.sgn[mp] * flipsign;
+      __syncthreads();
+      cta_rbm_factors(d, s.thp, s.rbm);
+      __syncthreads();
+      double* u = s.wu + (size_t)warp * Np;
+      double* v = s.wv + (size_t)warp * Np;
+      double pre = 0.0, pim = 0.0;
+      for (int qp = warp; qp < d.n_qp; qp += nwarps) {
+        double R = warp_ratio<KPL>(d, p, c.Yw + (size_t)qp * Np * Np, qp, s.idx, ua, db, s_up, s_dn, u, v);
+        if (lane == 0) {
+          double pfn = R * s.pf[qp];
+          s.pfp[qp] = pfn;
+          cplx cw = psi_wo_pf(d, t, s.rbm[qp], s.sgnp[qp >> 1], qp);
+          s.psip[2 * qp] = cw.re * pfn;
+          s.psip[2 * qp + 1] = cw.im * pfn;
+          pre += cw.re * pfn;
+          pim += cw.im * pfn;
+        }
+      }
+      if (lane == 0) {
+        s.red[warp] = pre;
+        s.red[32 + warp] = pim;
+      }
+      __syncthreads();
+      if (tid == 0) {
+        double re = 0.0, im = 0.0;
+        for (int k = 0; k < nwarps; k++) {
+          re += s.red[k];
+          im += s.red[32 + k];
+        }
+        s.dsc[D_PSIPR] = re;
+        s.dsc[D_PSIPI] = im;
+        (void)grnd(s.mt);  // sub.f90:72
+        double r1 = (hypot(re, im) + d.shift) / (hypot(s.dsc[D_PSI0R], s.dsc[D_PSI0I]) + d.shift);
+        s.iflag[F_ACCEPT] = grnd(s.mt) < r1 * r1;  // make_sample.f90:203-204
+      }
+      __syncthreads();
+      if (s.iflag[F_ACCEPT]) {  // make_sample.f90:205-219
+        for (int qp = warp; qp < d.n_qp; qp += nwarps) {
+          // rebuild u, v for this projection (same gathers as the ratio)
+          const double* XFq = p.XF + (size_t)qp * N * N;
+          const double* XFTq = p.XFT + (size_t)qp * N * N;
+          const double cc = XFq[(size_t)s_dn * N + s_up];
+          for (int j = lane; j < Np; j += 32) {
+            u[j] = (j == db) ? cc : XFq[(size_t)s_dn * N + s.idx[Np + j]];
+            v[j] = (j == ua) ? cc : XFTq[(size_t)s_up * N + s.idx[j]];
+          }
+          __syncwarp();
+          warp_update<KPL>(d, c.Yw + (size_t)qp * Np * Np, ua, db, cc, u, v, s.wA + (size_t)warp * Np,
+                           s.wS + (size_t)warp * Np);
+        }
+        for (int j = tid; j < d.Mr; j += blockDim.x) s.th[j] = s.thp[j];
+        for (int mp = tid; mp < d.n_mp; mp += blockDim.x) s.sgn[mp] = s.sgnp[mp];
+        for (int qp = tid; qp < d.n_qp; qp += blockDim.x) {
+          s.pf[qp] = s.pfp[qp];
+          s.psi[2 * qp] = s.psip[2 * qp];
+          s.psi[2 * qp + 1] = s.psip[2 * qp + 1];
+        }
+        __syncthreads();
+        if (tid == 0) {
+          s.x[i1] = -s.x[i1];
+          s.x[i2] = -s.x[i2];
+          s.cfg[i1] = i4;
+          s.cfg[i2] = i3;
+          s.idx[i3] = i2;
+          s.idx[i4] = i1;
+          s.dsc[D_PSI0R] = s.dsc[D_PSIPR];
+          s.dsc[D_PSI0I] = s.dsc[D_PSIPI];
+        }
+        __syncthreads();
+        if (i0 > 0) naccept++;
+        nacc_tmp++;
+        nacc_all++;
+      }
+    }
+    if (status(c)) break;
+    if (i0 > 0) {  // make_sample.f90:228-232
+      size_t sidx = (size_t)w * d.ns + (i0 - 1);
+      for (int i = tid; i < N; i += blockDim.x) W.xs[sidx * N + i] = (int8_t)s.x[i];
+      for (int qp = tid; qp < d.n_qp; qp += blockDim.x) W.pfs[sidx * d.n_qp + qp] = s.pf[qp];
+      double* ps = W.psis + sidx * (size_t)(d.n_qp + 1) * 2;
+      for (int k = tid; k < d.n_qp; k += blockDim.x) {
+        ps[2 * (k + 1)] = s.psi[2 * k];
+        ps[2 * (k + 1) + 1] = s.psi[2 * k + 1];
+      }
+      if (tid == 0) {
+        ps[0] = s.dsc[D_PSI0R];
+        ps[1] = s.dsc[D_PSI0I];
+      }
+    }
+    __syncthreads();
+  }
+  // persist walker state
+  for (int k = tid; k < 625; k += blockDim.x) W.mt[(size_t)w * 625 + k] = s.mt[k];
+  for (int i = tid; i < N; i += blockDim.x) {
+    W.x[(size_t)w * N + i] = (int8_t)s.x[i];
+    W.idx[(size_t)w * N + i] = (int16_t)s.idx[i];
+    W.cfg[(size_t)w * N + i] = (int16_t)s.cfg[i];
+  }
+  if (tid == 0) {
+    W.nfastup[w] = nfastup;
+    W.naccept[w] = naccept;
+    W.nacc_all[w] = nacc_all;
+    W.status[w] = status(c);
+  }
+}
+
+}  // namespace
+
+// Host launcher ------------------------------------------------------------------------------------
+size_t rbmpp_sampler_smem(const DevDims& d, int threads) { return ws_layout(d, threads / 32, nullptr, nullptr); }
+
+cudaError_t rbmpp_launch_sampler(const DevDims& d, const DevTables& t, const DevParams& p, const DevWalkers& W,
+                                 int first, cudaStream_t st) {
+  const int threads = 256;
+  size_t smem = rbmpp_sampler_smem(d, threads);
+  int kpl = (d.Np + 31) / 32;
+#define LAUNCH(K)                                                                                        \
+  do {                                                                                                   \
+    cudaError_t e = cudaFuncSetAttribute(sampler_kernel<K>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
+                                         (int)smem);                                                     \
+    if (e != cudaSuccess) return e;                                                                      \
+    sampler_kernel<K><<<d.nw, threads, smem, st>>>(d, t, p, W, first);                                   \
+    return cudaGetLastError();                                                                           \
+  } while (0)
+  if (kpl <= 1) LAUNCH(1);
+  if (kpl <= 2) LAUNCH(2);
+  if (kpl <= 4) LAUNCH(4);
+  if (kpl <= 8) LAUNCH(8);
+#undef LAUNCH
+  return cudaErrorInvalidValue;
+}

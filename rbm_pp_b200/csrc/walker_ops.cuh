@@ -1,0 +1,330 @@
+// walker_ops.cuh -- CTA-collective building blocks for one walker / one configuration.
+// Each routine cites the reference subroutine it restates.
+#pragma once
+#include "common.cuh"
+
+// Shared-memory workspace of one CTA (one walker or one configuration).
+struct WS {
+  uint32_t* mt;  // [625]
+  int* x;        // [N]   spins
+  int* idx;      // [N]   Ele_Idx (0-based sites)
+  int* cfg;      // [N]   Ele_Cfg
+  int* x2;       // [N]   global-flip candidate
+  int* idx2;
+  int* cfg2;
+  double* th;    // [Mr]
+  double* thp;   // [Mr]
+  int* sgn;      // [n_mp]
+  int* sgnp;     // [n_mp]
+  int* pb;       // [n_mp] sublattice parity per projection (sign_PP consistency)
+  double* pf;    // [n_qp]
+  double* pfp;   // [n_qp]
+  double* psi;   // [n_qp][2]
+  double* psip;  // [n_qp][2]
+  double* rbm;   // [n_qp] cosh products
+  double* tile;  // [Np][Np+1]
+  double* colbuf;  // [Np]
+  double* rowbuf;  // [Np]
+  int* perm;       // [Np]
+  double* wu;  // [nwarps][Np]
+  double* wv;  // [nwarps][Np]
+  double* wA;  // [nwarps][Np]
+  double* wS;  // [nwarps][Np]
+  double* red;     // [64]
+  int* iflag;      // [32]
+  double* dsc;     // [32]
+};
+
+// shared int slots
+#define F_STATUS 0
+#define F_I1 1
+#define F_I2 2
+#define F_ACCEPT 3
+#define F_FLIP 4
+#define F_PIV 5
+#define F_SINGULAR 6
+#define F_AUX 7
+// shared double slots
+#define D_DET 0
+#define D_PVAL 1
+#define D_PSI0R 2
+#define D_PSI0I 3
+#define D_PSIPR 4
+#define D_PSIPI 5
+#define D_DIFFINV 6
+#define D_DIFFPF 7
+
+__host__ __device__ inline size_t align16(size_t v) { return (v + 15) & ~(size_t)15; }
+
+// Carve the workspace; returns total bytes.  Same code on host (sizing) and device (pointers).
+__host__ __device__ inline size_t ws_layout(const DevDims& d, int nwarps, char* base, WS* w) {
+  size_t off = 0;
+  auto take = [&](size_t bytes) -> char* {
+    char* p = base ? base + off : nullptr;
+    off = align16(off + bytes);
+    return p;
+  };
+  const int N = d.N, Np = d.Np;
+  WS t;
+  t.mt = (uint32_t*)take(625 * 4);
+  t.x = (int*)take(N * 4);
+  t.idx = (int*)take(N * 4);
+  t.cfg = (int*)take(N * 4);
+  t.x2 = (int*)take(N * 4);
+  t.idx2 = (int*)take(N * 4);
+  t.cfg2 = (int*)take(N * 4);
+  t.th = (double*)take(d.Mr * 8);
+  t.thp = (double*)take(d.Mr * 8);
+  t.sgn = (int*)take(d.n_mp * 4);
+  t.sgnp = (int*)take(d.n_mp * 4);
+  t.pb = (int*)take(d.n_mp * 4);
+  t.pf = (double*)take(d.n_qp * 8);
+  t.pfp = (double*)take(d.n_qp * 8);
+  t.psi = (double*)take(d.n_qp * 16);
+  t.psip = (double*)take(d.n_qp * 16);
+  t.rbm = (double*)take(d.n_qp * 8);
+  t.tile = (double*)take((size_t)Np * (Np + 1) * 8);
+  t.colbuf = (double*)take(Np * 8);
+  t.rowbuf = (double*)take(Np * 8);
+  t.perm = (int*)take(Np * 4);
+  t.wu = (double*)take((size_t)nwarps * Np * 8);
+  t.wv = (double*)take((size_t)nwarps * Np * 8);
+  t.wA = (double*)take((size_t)nwarps * Np * 8);
+  t.wS = (double*)take((size_t)nwarps * Np * 8);
+  t.red = (double*)take(64 * 8);
+  t.iflag = (int*)take(32 * 4);
+  t.dsc = (double*)take(32 * 8);
+  if (w) *w = t;
+  return off;
+}
+
+// calc_theta RBM.f90:31-91 (real branch): th[j], j = mp*2*alphar + (s==+1 ? 0 : alphar) + f
+__device__ inline void cta_calc_theta(const DevDims& d, const DevTables& t, const DevParams& p, const int* x,
+                                      double* th) {
+  const int A2 = 2 * d.alphar;
+  for (int j = threadIdx.x; j < d.Mr; j += blockDim.x) {
+    int mp = j / A2, rem = j - mp * A2;
+    double s = rem < d.alphar ? 1.0 : -1.0;
+    int f = rem < d.alphar ? rem : rem - d.alphar;
+    const int* wm = t.wmap + (size_t)mp * d.N;
+    const double* Wf = p.Wr + (size_t)f * d.N;
+    double acc = p.br[f];
+    for (int i = 0; i < d.N; i++) acc = acc + Wf[wm[i]] * (double)x[i] * s;
+    th[j] = acc;
+  }
+}
+
+// update_theta RBM.f90:95-148 (x is the spin configuration BEFORE the exchange)
+__device__ inline void cta_update_theta(const DevDims& d, const DevTables& t, const DevParams& p, const int* x, int i1,
+                                        int i2, const double* th, double* thp) {
+  const int A2 = 2 * d.alphar;
+  const double x1 = (double)x[i1], x2 = (double)x[i2];
+  for (int j = threadIdx.x; j < d.Mr; j += blockDim.x) {
+    int mp = j / A2, rem = j - mp * A2;
+    double s = rem < d.alphar ? 1.0 : -1.0;
+    int f = rem < d.alphar ? rem : rem - d.alphar;
+    const double* Wf = p.Wr + (size_t)f * d.N;
+    int iw1 = t.wmap[(size_t)mp * d.N + i1], iw2 = t.wmap[(size_t)mp * d.N + i2];
+    double v = th[j];
+    v = v - 2.0 * Wf[iw1] * x1 * s;
+    v = v - 2.0 * Wf[iw2] * x2 * s;
+    thp[j] = v;
+  }
+}
+
+// x_to_Ele_Idx_Ele_Cfg interface_for_PP.f90:5-33 (thread 0); returns 0 or ST_CONFIG
+__device__ inline int x_to_ele(const DevDims& d, const int* x, int* idx, int* cfg) {
+  int i1 = 0, i2 = d.Np;
+  for (int i = 0; i < d.N; i++) {
+    if (x[i] == 1) {
+      if (i1 >= d.Np) return ST_CONFIG;
+      idx[i1] = i;
+      cfg[i] = i1++;
+    } else if (x[i] == -1) {
+      if (i2 >= d.N) return ST_CONFIG;
+      idx[i2] = i;
+      cfg[i] = i2++;
+    } else
+      return ST_CONFIG;
+  }
+  return (i1 == d.Np && i2 == d.N) ? 0 : ST_CONFIG;
+}
+
+// check_Ele_Idx_Ele_Cfg interface_for_PP.f90:37-65 (thread 0)
+__device__ inline int check_ele(const DevDims& d, const int* x, const int* idx, const int* cfg) {
+  unsigned seen[(RBMPP_MAX_N + 31) / 32];
+  for (int k = 0; k < (d.N + 31) / 32; k++) seen[k] = 0u;
+  for (int i = 0; i < d.N; i++) {
+    int s = idx[i];
+    if (s < 0 || s >= d.N) return ST_CONFIG;
+    if (cfg[s] != i) return ST_CONFIG;
+    if (x[s] != (i < d.Np ? 1 : -1)) return ST_CONFIG;
+    seen[s >> 5] |= 1u << (s & 31);
+  }
+  for (int s = 0; s < d.N; s++)
+    if (!(seen[s >> 5] & (1u << (s & 31)))) return ST_CONFIG;
+  return 0;
+}
+
+// sign_PP interface_for_PP.f90:71-106: warp per projection; the per-warp buffer wu holds the
+// translated positions.  Writes sgn[mp] and pb[mp] (parity of down electrons on sublattice B).
+__device__ inline void cta_sign_pp(const DevDims& d, const DevTables& t, const WS& s, const int* idx, int* sgn) {
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
+  int* tb = (int*)(s.wu + (size_t)warp * d.Np);  // Np doubles = N ints
+  for (int mp = warp; mp < d.n_mp; mp += nwarps) {
+    const int* wm = t.wmap + (size_t)mp * d.N;
+    for (int i = lane; i < d.N; i += 32) tb[i] = wm[idx[i]];
+    __syncwarp();
+    unsigned par = 0, parB = 0;
+    for (int i1 = 1 + lane; i1 < d.N; i1 += 32) {
+      int t1 = tb[i1];
+      if (i1 >= d.Np && t.subB[t1]) parB ^= 1u;
+      for (int i2 = 0; i2 < i1; i2++)
+        if (tb[i2] > t1) par ^= 1u;
+    }
+    par = __reduce_xor_sync(0xffffffffu, par);
+    parB = __reduce_xor_sync(0xffffffffu, parB);
+    if (lane == 0) {
+      sgn[mp] = ((par ^ parB) & 1u) ? -1 : 1;
+      s.pb[mp] = (int)parB;
+    }
+    __syncwarp();
+  }
+}
+
+// X(i, j) = XF(u_i, d_j) for the current labelling into the padded tile (rows: up electrons).
+__device__ inline void cta_build_x(const DevDims& d, const DevParams& p, int qp, const int* idx, double* tile) {
+  const int Np = d.Np, ld = Np + 1;
+  const double* XFq = p.XF + (size_t)qp * d.N * d.N;
+  for (int e = threadIdx.x; e < Np * Np; e += blockDim.x) {
+    int i = e / Np, j = e - i * Np;
+    tile[i * ld + j] = XFq[(size_t)idx[i] * d.N + idx[Np + j]];
+  }
+}
+
+// In-place Gauss-Jordan inverse with partial pivoting of the Np x Np tile (the role of
+// dgetrf/dgetri, matrix.f90:155-177) and its determinant (-> Pf through the block identity; the role
+// of dskpfa, matrix.f90:133-151).  After the call the tile holds Y = X^{-1}; dsc[D_DET] = det(X).
+// Sets iflag[F_SINGULAR] when a zero pivot is met.  All threads of the CTA must call it.
+__device__ inline void cta_gauss_jordan(const DevDims& d, const WS& s) {
+  const int n = d.Np, ld = n + 1;
+  double* T = s.tile;
+  const int tid = threadIdx.x, nt = blockDim.x, warp = tid >> 5, lane = tid & 31;
+  if (tid == 0) {
+    s.dsc[D_DET] = 1.0;
+    s.iflag[F_SINGULAR] = 0;
+  }
+  for (int k = 0; k < n; k++) {
+    if (warp == 0) {
+      double best = -1.0;
+      int bi = k;
+      for (int i = k + lane; i < n; i += 32) {
+        double v = fabs(T[i * ld + k]);
+        if (v > best) {
+          best = v;
+          bi = i;
+        }
+      }
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) {
+        double ob = __shfl_xor_sync(0xffffffffu, best, o);
+        int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+        if (ob > best || (ob == best && oi < bi)) {
+          best = ob;
+          bi = oi;
+        }
+      }
+      if (lane == 0) {
+        s.iflag[F_PIV] = bi;
+        s.dsc[D_PVAL] = best;
+      }
+    }
+    __syncthreads();
+    const int piv = s.iflag[F_PIV];
+    if (!(s.dsc[D_PVAL] > 0.0)) {
+      if (tid == 0) {
+        s.iflag[F_SINGULAR] = 1;
+        s.dsc[D_DET] = 0.0;
+      }
+      __syncthreads();
+      return;
+    }
+    if (piv != k)
+      for (int j = tid; j < n; j += nt) {
+        double a = T[k * ld + j];
+        T[k * ld + j] = T[piv * ld + j];
+        T[piv * ld + j] = a;
+      }
+    if (tid == 0) s.perm[k] = piv;
+    __syncthreads();
+    const double pivot = T[k * ld + k];
+    for (int j = tid; j < n; j += nt) {
+      s.rowbuf[j] = T[k * ld + j] / pivot;
+      s.colbuf[j] = T[j * ld + k];
+    }
+    if (tid == 0) s.dsc[D_DET] = (piv != k ? -s.dsc[D_DET] : s.dsc[D_DET]) * pivot;
+    __syncthreads();
+    for (int e = tid; e < n * n; e += nt) {
+      int i = e / n, j = e - i * n;
+      double v;
+      if (i == k) v = (j == k) ? 1.0 / pivot : s.rowbuf[j];
+      else if (j == k) v = -s.colbuf[i] / pivot;
+      else v = T[i * ld + j] - s.colbuf[i] * s.rowbuf[j];
+      T[i * ld + j] = v;
+    }
+    __syncthreads();
+  }
+  // undo the row interchanges on the columns of the inverse
+  for (int k = n - 1; k >= 0; k--) {
+    int pk = s.perm[k];
+    if (pk != k)
+      for (int i = tid; i < n; i += nt) {
+        double a = T[i * ld + k];
+        T[i * ld + k] = T[i * ld + pk];
+        T[i * ld + pk] = a;
+      }
+    __syncthreads();
+  }
+}
+
+// RBM cosh products per projection for theta vector th (sub.f90:42-46)
+__device__ inline void cta_rbm_factors(const DevDims& d, const double* th, double* rbm) {
+  for (int qp = threadIdx.x; qp < d.n_qp; qp += blockDim.x) {
+    double r = 1.0;
+    for (int f = 0; f < d.alphar; f++) r = r * cosh(th[qp * d.alphar + f]);
+    rbm[qp] = r;
+  }
+}
+
+// psi_wo_pf(qp) = rbm * sgn(mp) * para_mp(mp) * para_spin_proj(sp)  (sub.f90:47)
+__device__ inline cplx psi_wo_pf(const DevDims& d, const DevTables& t, double rbm, int sgn_mp, int qp) {
+  int mp = qp >> 1, sp = qp & 1;
+  cplx c = {rbm * (double)sgn_mp, 0.0};
+  cplx pm = {t.para_mp[2 * mp], t.para_mp[2 * mp + 1]};
+  c = cmul(c, pm);
+  return cscale(c, d.para_sp[sp]);
+}
+
+// calc_amplitude_RBM_PP sub.f90:4-89 for the current (th, pf, sgn): psi[qp], D_PSI0; one draw.
+__device__ inline void cta_amplitude(const DevDims& d, const DevTables& t, const WS& s, const double* th,
+                                     const double* pf, const int* sgn, double* psi, int psi0_slot) {
+  cta_rbm_factors(d, th, s.rbm);
+  __syncthreads();
+  for (int qp = threadIdx.x; qp < d.n_qp; qp += blockDim.x) {
+    cplx c = psi_wo_pf(d, t, s.rbm[qp], sgn[qp >> 1], qp);
+    psi[2 * qp] = c.re * pf[qp];
+    psi[2 * qp + 1] = c.im * pf[qp];
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double re = 0.0, im = 0.0;
+    for (int qp = 0; qp < d.n_qp; qp++) {
+      re += psi[2 * qp];
+      im += psi[2 * qp + 1];
+    }
+    s.dsc[psi0_slot] = re;
+    s.dsc[psi0_slot + 1] = im;
+    (void)grnd(s.mt);  // sub.f90:72
+  }
+  __syncthreads();
+}

@@ -1,0 +1,118 @@
+"""Parity of the CUDA path (through the C ABI) with the CPU oracle on identical inputs and RNG streams.
+
+Integer results (spin configurations, accept counts) must be bit-identical; amplitudes, Pfaffians,
+local energies and O_k within 1e-10 relative (FP64); SR steps within 1e-8 relative.
+"""
+import numpy as np
+import pytest
+
+import pyoracle as po
+from rbm_pp_b200 import capi
+from rbm_pp_b200 import formats as fm
+
+pytestmark = pytest.mark.gpu
+
+RTOL = 1e-10
+
+
+def _rel(a, b):
+    a = np.asarray(a)
+    b = np.asarray(b)
+    scale = max(np.abs(b).max(), 1e-300)
+    return float(np.abs(a - b).max() / scale)
+
+
+def _pair(L, translations, alphar, nw, ns, seed=5, orbital="full", J2=0.5):
+    p = fm.synthetic_problem(L, translations=translations, alphar=alphar, nsample=nw * ns, seed=seed,
+                             orbital=orbital, J2=J2)
+    o = po.Oracle(p, nranks=nw, nsample_per_rank=ns, nthreads=4)
+    g = capi.Context(p, n_walkers=nw, nsample_per_walker=ns)
+    o.set_params(p.br, p.Wr, p.slater, 0.0)
+    g.set_params(p.br, p.Wr, p.slater, 0.0)
+    return p, o, g
+
+
+def _random_configs(N, n, seed):
+    rng = np.random.default_rng(seed)
+    x = -np.ones((n, N), dtype=np.int32)
+    for r in x:
+        r[rng.choice(N, N // 2, replace=False)] = 1
+    return x
+
+
+@pytest.mark.parametrize("L,trans,alphar", [(4, False, 1), (4, True, 2), (6, False, 2), (6, True, 1)])
+def test_eval_configs_match_oracle(L, trans, alphar):
+    p, o, g = _pair(L, trans, alphar, nw=1, ns=4)
+    x = _random_configs(L * L, 24, seed=L + 10 * alphar)
+    ro = o.eval_configs(x, want_h=True, want_O=True)
+    rg = g.eval_configs(x, want_h=True, want_O=True)
+    assert _rel(rg["psi"], ro["psi"]) < RTOL
+    for k in range(x.shape[0]):
+        assert abs(rg["hpsi"][k] - ro["hpsi"][k]) <= RTOL * max(abs(ro["hpsi"][k]), abs(ro["psi"][k, 0]))
+        assert np.abs(rg["O"][k] - ro["O"][k].real).max() <= RTOL * max(np.abs(ro["O"][k]).max(), 1e-300)
+    g.close()
+
+
+def test_rng_seed_and_rank0_draws():
+    p, o, g = _pair(4, False, 1, nw=3, ns=8)
+    o.seed(4242)
+    g.seed(4242)
+    assert np.array_equal(o.rank_grnd(0, 500), g.rank0_grnd(500))
+    g.close()
+
+
+@pytest.mark.parametrize("L,trans,alphar,nw,ns", [(4, False, 1, 8, 16), (4, True, 1, 4, 8), (6, True, 2, 3, 4),
+                                                  (6, False, 2, 6, 8)])
+def test_make_sample_bit_exact(L, trans, alphar, nw, ns):
+    p, o, g = _pair(L, trans, alphar, nw=nw, ns=ns, seed=3 + L)
+    o.seed(777)
+    g.seed(777)
+    na_o = o.make_sample(True)
+    na_g = g.make_sample(True)
+    xo, psio, pfo = o.samples()
+    xg, psig, pfg = g.samples()
+    assert np.array_equal(na_o, na_g)
+    assert np.array_equal(xo, xg)
+    assert _rel(pfg, pfo) < 1e-9
+    assert _rel(psig, psio) < 1e-9
+    g.close()
+
+
+@pytest.mark.parametrize("L,trans,alphar", [(4, False, 1), (4, True, 1), (6, True, 1)])
+def test_measure_matches_oracle(L, trans, alphar):
+    nw, ns = 4, 8
+    p, o, g = _pair(L, trans, alphar, nw=nw, ns=ns, seed=11)
+    o.seed(99)
+    g.seed(99)
+    o.make_sample(True)
+    g.make_sample(True)
+    mo = o.measure(want_S=True)
+    mg = g.measure(want_S=True)
+    for k in ("Etot", "Etot2", "norm", "wf_av"):
+        assert abs(mg[k] - mo[k]) <= RTOL * abs(mo[k]), k
+    assert _rel(mg["gvec"], mo["gvec"]) < 1e-9
+    assert _rel(mg["Ovec"], mo["Ovec"]) < 1e-9
+    assert _rel(mg["S"], mo["S"]) < 1e-9
+    g.close()
+
+
+def test_sr_iterations_stay_in_lockstep():
+    """Three full optimisation iterations: samples stay bit-identical, energies and parameters agree."""
+    L, nw, ns = 4, 8, 16
+    p, o, g = _pair(L, False, 1, nw=nw, ns=ns, seed=12345)
+    loop = po.VMCLoop(o, p, iseed0=12345)
+    g.seed(12345)
+    br, Wr = capi.initial_params(g, p)
+    g.set_params(br, Wr, p.slater, 0.0)
+    for it in range(1, 4):
+        rec = loop.iteration_step()
+        sg = g.iteration(capi.SR_FP64, p.inp.delta_tau, p.inp.s_factor_scale, p.inp.s_cut, p.inp.s_factor0)
+        xo = o.samples()[0]
+        xg = g.samples()[0]
+        assert np.array_equal(xo, xg), it
+        assert abs(sg.Etot - rec["Etot"]) <= 1e-9 * abs(rec["Etot"])
+        bro, Wro, slo, sho = o.get_params()
+        brg, Wrg, slg, shg = g.get_params()
+        assert _rel(slg, slo) < 1e-8 and _rel(Wrg, Wro) < 1e-8
+        assert abs(shg - sho) <= 1e-9 * abs(sho) + 1e-300
+    g.close()
