@@ -147,6 +147,10 @@ int rbmpp_iteration(rbmpp_ctx* ctx, int precision, double delta_tau, double s_fa
  * [6] proposals of the last make_sample, [7] last rbmpp_iteration ms.  n = number of entries wanted. */
 int rbmpp_get_stats(const rbmpp_ctx* ctx, double* out, int n);
 
+/* Per-walker sampler state: Nfastup (adaptive recompute interval, make_sample.f90:120-127) and the
+ * accepted moves of the last make_sample over all sweeps.  Either pointer may be NULL. */
+int rbmpp_get_walker_state(const rbmpp_ctx* ctx, int* nfastup, int* naccept_all);
+
 /* Adjoint O_k kernel: for n configurations x(N, n): psi(0:N_QP, n) complex, hpsi(n) complex
  * (sum_x' <x|H|x'> psi(x'), calc_local_energy_correlation), and O(Nv, n) = d psi(x) / d theta_k
  * (Ovec_loc_x before reweighting, calc_phys_quantity.f90:115-220).  Any output may be NULL. */

@@ -20,7 +20,7 @@ EXPORTS = ["rbmpp_create", "rbmpp_destroy", "rbmpp_last_error", "rbmpp_query", "
            "rbmpp_set_params", "rbmpp_get_params", "rbmpp_seed_walkers", "rbmpp_rank0_grnd", "rbmpp_make_sample",
            "rbmpp_get_samples", "rbmpp_set_samples", "rbmpp_measure", "rbmpp_measure_energy", "rbmpp_sr_step",
            "rbmpp_iteration", "rbmpp_eval_configs", "rbmpp_get_stats", "rbmpp_exchange_measurement",
-           "rbmpp_set_shift"]
+           "rbmpp_set_shift", "rbmpp_get_walker_state"]
 
 SR_FP64 = 0
 SR_SPLIT_BF16 = 1
@@ -83,6 +83,7 @@ def lib():
         L.rbmpp_get_stats.argtypes = [P, P, C.c_int]
         L.rbmpp_exchange_measurement.argtypes = [P, C.c_int, P, P, P, P]
         L.rbmpp_set_shift.argtypes = [P, C.c_double]
+        L.rbmpp_get_walker_state.argtypes = [P, P, P]
         _lib = L
     return _lib
 
@@ -207,6 +208,11 @@ class Context:
         self._chk(lib().rbmpp_iteration(self.h, precision, delta_tau, s_factor_scale, s_cut, s_factor0,
                                         C.byref(sout)))
         return sout
+
+    def nfastup(self):
+        out = np.zeros(self.nw, dtype=np.int32)
+        self._chk(lib().rbmpp_get_walker_state(self.h, _p(out), None))
+        return out
 
     def set_shift(self, shift):
         self._chk(lib().rbmpp_set_shift(self.h, float(shift)))

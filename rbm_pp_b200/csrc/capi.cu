@@ -939,6 +939,14 @@ int rbmpp_iteration(rbmpp_ctx* c, int precision, double delta_tau, double s_fact
   return 0;
 }
 
+int rbmpp_get_walker_state(const rbmpp_ctx* cc, int* nfastup, int* nacc_all) {
+  rbmpp_ctx* c = const_cast<rbmpp_ctx*>(cc);
+  if (!c) return RBMPP_E_ARG;
+  if (nfastup) CK(cudaMemcpy(nfastup, c->W.nfastup, sizeof(int) * c->d.nw, cudaMemcpyDeviceToHost));
+  if (nacc_all) CK(cudaMemcpy(nacc_all, c->W.nacc_all, sizeof(int) * c->d.nw, cudaMemcpyDeviceToHost));
+  return 0;
+}
+
 int rbmpp_get_stats(const rbmpp_ctx* c, double* out, int n) {
   if (!c || !out || n < 0) return RBMPP_E_ARG;
   for (int k = 0; k < n && k < 8; k++) out[k] = c->stats[k];

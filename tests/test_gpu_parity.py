@@ -73,19 +73,26 @@ def test_make_sample_bit_exact(L, trans, alphar, nw, ns):
     xg, psig, pfg = g.samples()
     assert np.array_equal(na_o, na_g)
     assert np.array_equal(xo, xg)
-    assert _rel(pfg, pfo) < 1e-9
-    assert _rel(psig, psio) < 1e-9
+    assert np.array_equal(o.nfastup(), g.nfastup())
+    # stored Pf / psi are products of fast-update ratios on both sides; their drift is bounded by the
+    # reference's own 1e-5 recompute criterion (make_sample.f90:120), so compare at 1e-6
+    assert _rel(pfg, pfo) < 1e-6
+    assert _rel(psig, psio) < 1e-6
+    # and the stored amplitudes agree with a scratch evaluation of the same configurations
+    scratch = g.eval_configs(xg.reshape(-1, L * L), want_h=False)["psi"][:, 0]
+    assert _rel(np.abs(psig.reshape(-1, psig.shape[-1])[:, 0]), np.abs(scratch)) < 1e-6
     g.close()
 
 
-@pytest.mark.parametrize("L,trans,alphar", [(4, False, 1), (4, True, 1), (6, True, 1)])
+@pytest.mark.parametrize("L,trans,alphar", [(4, False, 1), (4, True, 1), (6, True, 1), (6, False, 2)])
 def test_measure_matches_oracle(L, trans, alphar):
+    """calc_phys_quantity_opt on identical stored samples (the oracle's chain loaded into the GPU)."""
     nw, ns = 4, 8
     p, o, g = _pair(L, trans, alphar, nw=nw, ns=ns, seed=11)
     o.seed(99)
     g.seed(99)
     o.make_sample(True)
-    g.make_sample(True)
+    g.set_samples(o.samples()[0])
     mo = o.measure(want_S=True)
     mg = g.measure(want_S=True)
     for k in ("Etot", "Etot2", "norm", "wf_av"):
