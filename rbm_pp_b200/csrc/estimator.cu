@@ -23,7 +23,7 @@ struct EstShared {
   double* diag;   // [1]     sum J x x
 };
 
-__host__ __device__ inline size_t est_layout(const DevDims& d, int nwarps, char* base, WS* w, EstShared* e) {
+__host__ __device__ __forceinline__ size_t est_layout(const DevDims& d, int nwarps, char* base, WS* w, EstShared* e) {
   size_t off = ws_layout(d, nwarps, base, w);
   auto take = [&](size_t bytes) -> char* {
     char* p = base ? base + off : nullptr;
@@ -42,7 +42,7 @@ __host__ __device__ inline size_t est_layout(const DevDims& d, int nwarps, char*
 
 // Ratio for one bond from the shared-memory inverse tile (ld = Np + 1).
 template <int KPL>
-__device__ inline double warp_ratio_tile(const DevDims& d, const DevParams& p, const double* T, int qp, const int* idx,
+__device__ __forceinline__ double warp_ratio_tile(const DevDims& d, const DevParams& p, const double* T, int qp, const int* idx,
                                          int ua, int db, int s_up, int s_dn, double* u, double* v) {
   const int lane = threadIdx.x & 31, Np = d.Np, N = d.N, ld = Np + 1;
   const double* XFq = p.XF + (size_t)qp * N * N;
@@ -87,13 +87,15 @@ __device__ inline double warp_ratio_tile(const DevDims& d, const DevParams& p, c
 }
 
 template <int KPL>
-__global__ void __launch_bounds__(256) estimator_kernel(DevDims d, DevTables t, DevParams p, const int8_t* xs, int n,
-                                                        double* out_psi, double* out_hpsi, double* O, int* out_nap,
-                                                        int* out_status, int reweight) {
+__global__ void __launch_bounds__(256)
+    estimator_kernel(const __grid_constant__ DevDims d, const __grid_constant__ DevTables t,
+                     const __grid_constant__ DevParams p, const int8_t* xs, int n, double* out_psi, double* out_hpsi,
+                     double* O, int* out_nap, int* out_status, int reweight) {
   extern __shared__ __align__(16) char smem[];
-  WS s;
-  EstShared e;
-  est_layout(d, blockDim.x >> 5, smem, &s, &e);
+  __shared__ WS s;
+  __shared__ EstShared e;
+  if (threadIdx.x == 0) est_layout(d, blockDim.x >> 5, smem, &s, &e);
+  __syncthreads();
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, nwarps = blockDim.x >> 5;
   const int N = d.N, Np = d.Np, ld = Np + 1;
   const int cfgi = blockIdx.x;

@@ -16,7 +16,7 @@ namespace {
 
 // ---- per-warp determinant ratio for projection qp; result valid on all lanes ----
 template <int KPL>
-__device__ inline double warp_ratio(const DevDims& d, const DevParams& p, const double* Yq, int qp, const int* idx,
+__device__ __forceinline__ double warp_ratio(const DevDims& d, const DevParams& p, const double* Yq, int qp, const int* idx,
                                     int ua, int db, int s_up, int s_dn, double* u, double* v) {
   const int lane = threadIdx.x & 31, Np = d.Np, N = d.N;
   const double* XFq = p.XF + (size_t)qp * N * N;
@@ -79,7 +79,7 @@ __device__ inline double warp_ratio(const DevDims& d, const DevParams& p, const 
 
 // ---- per-warp rank-2 update of Y after an accepted exchange (u, v from warp_ratio) ----
 template <int KPL>
-__device__ inline void warp_update(const DevDims& d, double* Yq, int ua, int db, double c, const double* u,
+__device__ __forceinline__ void warp_update(const DevDims& d, double* Yq, int ua, int db, double c, const double* u,
                                    const double* v, double* A, double* S) {
   const int lane = threadIdx.x & 31, Np = d.Np;
   double acc[KPL];
@@ -147,20 +147,20 @@ __device__ inline void warp_update(const DevDims& d, double* Yq, int ua, int db,
 }
 
 struct SCtx {
-  DevDims d;
-  DevTables t;
-  DevParams p;
-  DevWalkers W;
+  const DevDims& d;
+  const DevTables& t;
+  const DevParams& p;
+  const DevWalkers& W;
   int w;
-  WS s;
-  double* Yw;  // this walker's Y
+  const WS& s;  // pointer table kept in shared memory
+  double* Yw;   // this walker's Y
 };
 
-__device__ inline int& status(const SCtx& c) { return c.s.iflag[F_STATUS]; }
+__device__ __forceinline__ int& status(const SCtx& c) { return c.s.iflag[F_STATUS]; }
 
 // Scratch inverse of every projection for labelling idx: writes Y (when write_y) and pf_out.
 // When diff is requested, also computes the reference's drift measures against the stored Y / pf.
-__device__ void cta_scratch_all(const SCtx& c, const int* idx, double* pf_out, bool write_y, bool diff) {
+__device__ __forceinline__ void cta_scratch_all(const SCtx& c, const int* idx, double* pf_out, bool write_y, bool diff) {
   const DevDims& d = c.d;
   const WS& s = c.s;
   const int Np = d.Np, ld = Np + 1, tid = threadIdx.x;
@@ -212,7 +212,7 @@ __device__ void cta_scratch_all(const SCtx& c, const int* idx, double* pf_out, b
 }
 
 // calc_theta, x_to_Ele_Idx, calculate_MAll, sign_PP, calc_amplitude (make_sample.f90:54-60 / :345-350)
-__device__ void full_state(const SCtx& c) {
+__device__ __forceinline__ void full_state(const SCtx& c) {
   const WS& s = c.s;
   cta_calc_theta(c.d, c.t, c.p, s.x, s.th);
   if (threadIdx.x == 0) {
@@ -234,7 +234,7 @@ __device__ void full_state(const SCtx& c) {
 }
 
 // make_initial_x make_sample.f90:298-362
-__device__ void make_initial_x(const SCtx& c) {
+__device__ __forceinline__ void make_initial_x(const SCtx& c) {
   const WS& s = c.s;
   for (int it1 = 0; it1 < 1000000; it1++) {
     if (threadIdx.x == 0) {
@@ -264,7 +264,7 @@ __device__ void make_initial_x(const SCtx& c) {
 }
 
 // Nfastup checkpoint make_sample.f90:74-128
-__device__ void checkpoint(const SCtx& c, int& nfastup) {
+__device__ __forceinline__ void checkpoint(const SCtx& c, int& nfastup) {
   const DevDims& d = c.d;
   const WS& s = c.s;
   for (int j = threadIdx.x; j < d.Mr; j += blockDim.x) s.thp[j] = s.th[j];
@@ -316,7 +316,7 @@ __device__ void checkpoint(const SCtx& c, int& nfastup) {
 }
 
 // Global spin flip make_sample.f90:135-158 (RNG check already drawn by the caller).
-__device__ void global_flip(const SCtx& c) {
+__device__ __forceinline__ void global_flip(const SCtx& c) {
   const DevDims& d = c.d;
   const WS& s = c.s;
   for (int i = threadIdx.x; i < d.N; i += blockDim.x) s.x2[i] = -s.x[i];
@@ -366,19 +366,17 @@ __device__ void global_flip(const SCtx& c) {
 }
 
 template <int KPL>
-__global__ void __launch_bounds__(256) sampler_kernel(DevDims d, DevTables t, DevParams p, DevWalkers W, int first) {
+__global__ void __launch_bounds__(256, 1)
+    sampler_kernel(const __grid_constant__ DevDims d, const __grid_constant__ DevTables t,
+                   const __grid_constant__ DevParams p, const __grid_constant__ DevWalkers W, int first) {
   extern __shared__ __align__(16) char smem[];
-  SCtx c;
-  c.d = d;
-  c.t = t;
-  c.p = p;
-  c.W = W;
-  c.w = blockIdx.x;
-  ws_layout(d, blockDim.x >> 5, smem, &c.s);
-  const WS& s = c.s;
+  __shared__ WS ws;
+  if (threadIdx.x == 0) ws_layout(d, blockDim.x >> 5, smem, &ws);
+  __syncthreads();
+  const SCtx c{d, t, p, W, (int)blockIdx.x, ws, W.Y + (size_t)blockIdx.x * d.n_qp * d.Np * d.Np};
+  const WS& s = ws;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, nwarps = blockDim.x >> 5;
   const int w = c.w, N = d.N, Np = d.Np;
-  c.Yw = W.Y + (size_t)w * d.n_qp * Np * Np;
 
   for (int k = tid; k < 625; k += blockDim.x) s.mt[k] = W.mt[(size_t)w * 625 + k];
   if (tid == 0) status(c) = 0;

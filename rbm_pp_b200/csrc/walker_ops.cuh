@@ -54,10 +54,10 @@ struct WS {
 #define D_DIFFINV 6
 #define D_DIFFPF 7
 
-__host__ __device__ inline size_t align16(size_t v) { return (v + 15) & ~(size_t)15; }
+__host__ __device__ __forceinline__ size_t align16(size_t v) { return (v + 15) & ~(size_t)15; }
 
 // Carve the workspace; returns total bytes.  Same code on host (sizing) and device (pointers).
-__host__ __device__ inline size_t ws_layout(const DevDims& d, int nwarps, char* base, WS* w) {
+__host__ __device__ __forceinline__ size_t ws_layout(const DevDims& d, int nwarps, char* base, WS* w) {
   size_t off = 0;
   auto take = [&](size_t bytes) -> char* {
     char* p = base ? base + off : nullptr;
@@ -99,7 +99,7 @@ __host__ __device__ inline size_t ws_layout(const DevDims& d, int nwarps, char* 
 }
 
 // calc_theta RBM.f90:31-91 (real branch): th[j], j = mp*2*alphar + (s==+1 ? 0 : alphar) + f
-__device__ inline void cta_calc_theta(const DevDims& d, const DevTables& t, const DevParams& p, const int* x,
+__device__ __forceinline__ void cta_calc_theta(const DevDims& d, const DevTables& t, const DevParams& p, const int* x,
                                       double* th) {
   const int A2 = 2 * d.alphar;
   for (int j = threadIdx.x; j < d.Mr; j += blockDim.x) {
@@ -115,7 +115,7 @@ __device__ inline void cta_calc_theta(const DevDims& d, const DevTables& t, cons
 }
 
 // update_theta RBM.f90:95-148 (x is the spin configuration BEFORE the exchange)
-__device__ inline void cta_update_theta(const DevDims& d, const DevTables& t, const DevParams& p, const int* x, int i1,
+__device__ __forceinline__ void cta_update_theta(const DevDims& d, const DevTables& t, const DevParams& p, const int* x, int i1,
                                         int i2, const double* th, double* thp) {
   const int A2 = 2 * d.alphar;
   const double x1 = (double)x[i1], x2 = (double)x[i2];
@@ -133,7 +133,7 @@ __device__ inline void cta_update_theta(const DevDims& d, const DevTables& t, co
 }
 
 // x_to_Ele_Idx_Ele_Cfg interface_for_PP.f90:5-33 (thread 0); returns 0 or ST_CONFIG
-__device__ inline int x_to_ele(const DevDims& d, const int* x, int* idx, int* cfg) {
+__device__ __forceinline__ int x_to_ele(const DevDims& d, const int* x, int* idx, int* cfg) {
   int i1 = 0, i2 = d.Np;
   for (int i = 0; i < d.N; i++) {
     if (x[i] == 1) {
@@ -151,7 +151,7 @@ __device__ inline int x_to_ele(const DevDims& d, const int* x, int* idx, int* cf
 }
 
 // check_Ele_Idx_Ele_Cfg interface_for_PP.f90:37-65 (thread 0)
-__device__ inline int check_ele(const DevDims& d, const int* x, const int* idx, const int* cfg) {
+__device__ __forceinline__ int check_ele(const DevDims& d, const int* x, const int* idx, const int* cfg) {
   unsigned seen[(RBMPP_MAX_N + 31) / 32];
   for (int k = 0; k < (d.N + 31) / 32; k++) seen[k] = 0u;
   for (int i = 0; i < d.N; i++) {
@@ -168,7 +168,7 @@ __device__ inline int check_ele(const DevDims& d, const int* x, const int* idx, 
 
 // sign_PP interface_for_PP.f90:71-106: warp per projection; the per-warp buffer wu holds the
 // translated positions.  Writes sgn[mp] and pb[mp] (parity of down electrons on sublattice B).
-__device__ inline void cta_sign_pp(const DevDims& d, const DevTables& t, const WS& s, const int* idx, int* sgn) {
+__device__ __forceinline__ void cta_sign_pp(const DevDims& d, const DevTables& t, const WS& s, const int* idx, int* sgn) {
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
   int* tb = (int*)(s.wu + (size_t)warp * d.Np);  // Np doubles = N ints
   for (int mp = warp; mp < d.n_mp; mp += nwarps) {
@@ -193,7 +193,7 @@ __device__ inline void cta_sign_pp(const DevDims& d, const DevTables& t, const W
 }
 
 // X(i, j) = XF(u_i, d_j) for the current labelling into the padded tile (rows: up electrons).
-__device__ inline void cta_build_x(const DevDims& d, const DevParams& p, int qp, const int* idx, double* tile) {
+__device__ __forceinline__ void cta_build_x(const DevDims& d, const DevParams& p, int qp, const int* idx, double* tile) {
   const int Np = d.Np, ld = Np + 1;
   const double* XFq = p.XF + (size_t)qp * d.N * d.N;
   for (int e = threadIdx.x; e < Np * Np; e += blockDim.x) {
@@ -206,7 +206,7 @@ __device__ inline void cta_build_x(const DevDims& d, const DevParams& p, int qp,
 // dgetrf/dgetri, matrix.f90:155-177) and its determinant (-> Pf through the block identity; the role
 // of dskpfa, matrix.f90:133-151).  After the call the tile holds Y = X^{-1}; dsc[D_DET] = det(X).
 // Sets iflag[F_SINGULAR] when a zero pivot is met.  All threads of the CTA must call it.
-__device__ inline void cta_gauss_jordan(const DevDims& d, const WS& s) {
+__device__ __forceinline__ void cta_gauss_jordan(const DevDims& d, const WS& s) {
   const int n = d.Np, ld = n + 1;
   double* T = s.tile;
   const int tid = threadIdx.x, nt = blockDim.x, warp = tid >> 5, lane = tid & 31;
@@ -288,7 +288,7 @@ __device__ inline void cta_gauss_jordan(const DevDims& d, const WS& s) {
 }
 
 // RBM cosh products per projection for theta vector th (sub.f90:42-46)
-__device__ inline void cta_rbm_factors(const DevDims& d, const double* th, double* rbm) {
+__device__ __forceinline__ void cta_rbm_factors(const DevDims& d, const double* th, double* rbm) {
   for (int qp = threadIdx.x; qp < d.n_qp; qp += blockDim.x) {
     double r = 1.0;
     for (int f = 0; f < d.alphar; f++) r = r * cosh(th[qp * d.alphar + f]);
@@ -297,7 +297,7 @@ __device__ inline void cta_rbm_factors(const DevDims& d, const double* th, doubl
 }
 
 // psi_wo_pf(qp) = rbm * sgn(mp) * para_mp(mp) * para_spin_proj(sp)  (sub.f90:47)
-__device__ inline cplx psi_wo_pf(const DevDims& d, const DevTables& t, double rbm, int sgn_mp, int qp) {
+__device__ __forceinline__ cplx psi_wo_pf(const DevDims& d, const DevTables& t, double rbm, int sgn_mp, int qp) {
   int mp = qp >> 1, sp = qp & 1;
   cplx c = {rbm * (double)sgn_mp, 0.0};
   cplx pm = {t.para_mp[2 * mp], t.para_mp[2 * mp + 1]};
@@ -306,7 +306,7 @@ __device__ inline cplx psi_wo_pf(const DevDims& d, const DevTables& t, double rb
 }
 
 // calc_amplitude_RBM_PP sub.f90:4-89 for the current (th, pf, sgn): psi[qp], D_PSI0; one draw.
-__device__ inline void cta_amplitude(const DevDims& d, const DevTables& t, const WS& s, const double* th,
+__device__ __forceinline__ void cta_amplitude(const DevDims& d, const DevTables& t, const WS& s, const double* th,
                                      const double* pf, const int* sgn, double* psi, int psi0_slot) {
   cta_rbm_factors(d, th, s.rbm);
   __syncthreads();
