@@ -39,7 +39,8 @@ enum {
   RBMPP_E_SLATER_NORM = 11, /* f renormalisation check (SR_pdposv.f90:414)                        */
   RBMPP_E_LAMBDA = 12,      /* lambda block split check (SR_pdposv.f90:308)                       */
   RBMPP_E_CUDA = 20,        /* CUDA runtime error                                                 */
-  RBMPP_E_STATE = 21        /* call out of order (e.g. measure before make_sample)                */
+  RBMPP_E_STATE = 21,       /* call out of order (e.g. measure before make_sample)                */
+  RBMPP_E_TIMEOUT = 22      /* a bounded device-side wait ran out (copy pipeline did not progress) */
 };
 
 /* Sizes (RBM.input, sym_info.txt, orbitalidx.def; main.f90:75-141). */

@@ -7,6 +7,7 @@
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <string>
 #include <vector>
@@ -18,6 +19,9 @@
 cudaError_t rbmpp_launch_sampler(const DevDims&, const DevTables&, const DevParams&, const DevWalkers&, int,
                                  cudaStream_t);
 size_t rbmpp_sampler_smem(const DevDims&, int);
+int rbmpp_stream_stages(const DevDims&, int);
+cudaError_t rbmpp_launch_sampler_stream(const DevDims&, const DevTables&, const DevParams&, const DevWalkers&, int, int,
+                                        cudaStream_t);
 cudaError_t rbmpp_launch_estimator(const DevDims&, const DevTables&, const DevParams&, const int8_t*, int, double*,
                                    double*, double*, int*, int*, int, cudaStream_t);
 size_t rbmpp_estimator_smem(const DevDims&, int);
@@ -129,6 +133,7 @@ struct rbmpp_ctx {
   size_t bytes = 0;
   cudaEvent_t ev[12] = {};
   double stats[8] = {0};
+  int stream_stages = 0;  // > 0: TMA-streamed sampler with this many stages
 };
 
 namespace {
@@ -294,6 +299,8 @@ int rbmpp_create(const rbmpp_dims* dims, rbmpp_ctx** out) {
   int maxsm = 0;
   CK(cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, dims->device));
   if ((long long)smem > maxsm) return fail(c, RBMPP_E_ARG, "shared-memory workspace %zu B exceeds %d B", smem, maxsm);
+  c->stream_stages = rbmpp_stream_stages(d, maxsm);
+  if (getenv("RBMPP_SAMPLER") && std::string(getenv("RBMPP_SAMPLER")) == "direct") c->stream_stages = 0;
   int r;
   const int N = d.N;
   if ((r = dalloc(c, &c->d_wmap, (size_t)d.n_mp * N))) return r;
@@ -484,7 +491,10 @@ int rbmpp_make_sample(rbmpp_ctx* c, int first, int* naccept, long long* naccept_
   if (!first && !c->sampled) return fail(c, RBMPP_E_STATE, "make_sample(first=0) before any sample exists");
   c->d.shift = c->shift;
   CK(cudaEventRecord(c->ev[0], c->st));
-  CK(rbmpp_launch_sampler(c->d, tables(c), params(c), c->W, first ? 1 : 0, c->st));
+  if (c->stream_stages > 0)
+    CK(rbmpp_launch_sampler_stream(c->d, tables(c), params(c), c->W, first ? 1 : 0, c->stream_stages, c->st));
+  else
+    CK(rbmpp_launch_sampler(c->d, tables(c), params(c), c->W, first ? 1 : 0, c->st));
   CK(cudaEventRecord(c->ev[1], c->st));
   CK(cudaStreamSynchronize(c->st));
   int r = check_walker_status(c, c->W.status, c->d.nw, "make_sample");

@@ -1,0 +1,529 @@
+// sampler_stream.cu -- Metropolis sampler that streams each walker's projections through shared memory
+// with TMA bulk copies (make_sample.f90:4-240, same RNG order as sampler.cu).
+//
+// One CTA per walker: warp 0 is the control warp (its lane 0 draws the random numbers and issues every
+// bulk copy), warps 1..4 consume tiles.  A tile is one projection's Y = X^{-1} (Np x Np FP64, row
+// major).  Every proposal is one pass over the n_qp tiles through an ST-stage ring:
+//   producer:  cp.async.bulk global->shared (mbarrier complete_tx), and after the consumer releases a
+//              modified tile, cp.async.bulk shared->global before the stage is refilled;
+//   consumer:  applies the deferred rank-2 update of the previously accepted exchange (if any) to the
+//              tile in place, then evaluates the determinant ratio of the current proposal on it.
+// So a proposal costs one read of Y and an accepted move one write: the algorithmic minimum
+// (pfupdate_two.f90 reads InvM once per ratio and rewrites it per accepted move).
+// The first tiles of a pass are requested before the candidate is drawn, which hides the serial RNG.
+#include "sampler_common.cuh"
+
+namespace {
+
+constexpr int kWarps = 5;
+constexpr int kConsumers = kWarps - 1;
+#define ST_TIMEOUT 22
+
+struct Stream {
+  double* stage;  // [ST][Np*Np]; also the Gauss-Jordan tile outside passes
+  uint64_t* full;
+  uint64_t* empty;
+  int* dirty;
+  double* wR;  // [kWarps][Np] row sums of the deferred update
+  int ST;
+  uint32_t tile_bytes;
+};
+
+__host__ __device__ __forceinline__ size_t stream_layout(const DevDims& d, int ST, char* base, WS* w, Stream* st) {
+  size_t off = ws_layout(d, kWarps, base, w, false);
+  auto take = [&](size_t bytes, size_t align) -> char* {
+    off = (off + align - 1) / align * align;
+    char* p = base ? base + off : nullptr;
+    off += bytes;
+    return p;
+  };
+  Stream t;
+  t.ST = ST;
+  t.tile_bytes = 8u * (uint32_t)d.Np * (uint32_t)d.Np;
+  size_t stage_bytes = (size_t)ST * t.tile_bytes, gj = (size_t)d.Np * (d.Np + 1) * 8;
+  t.stage = (double*)take(stage_bytes > gj ? stage_bytes : gj, 128);
+  t.full = (uint64_t*)take(8 * (size_t)ST, 8);
+  t.empty = (uint64_t*)take(8 * (size_t)ST, 8);
+  t.dirty = (int*)take(4 * (size_t)ST, 4);
+  t.wR = (double*)take((size_t)kWarps * d.Np * 8, 16);
+  if (w) w->tile = t.stage;
+  if (st) *st = t;
+  return off;
+}
+
+struct Move {
+  int ua, db, s_up, s_dn;  // up electron, down electron (local index), their sites before the move
+};
+
+// u, v of an exchange for projection qp into per-warp buffers (the gathers of pfupdate_two.f90:48-52)
+__device__ __forceinline__ double gather_uv(const DevDims& d, const DevParams& p, int qp, const int* idx, const Move& m,
+                                            double* u, double* v) {
+  const int lane = threadIdx.x & 31, Np = d.Np, N = d.N;
+  const double* XFq = p.XF + (size_t)qp * N * N;
+  const double* XFTq = p.XFT + (size_t)qp * N * N;
+  const double c = XFq[(size_t)m.s_dn * N + m.s_up];
+  for (int j = lane; j < Np; j += 32) {
+    u[j] = (j == m.db) ? c : XFq[(size_t)m.s_dn * N + idx[Np + j]];
+    v[j] = (j == m.ua) ? c : XFTq[(size_t)m.s_up * N + idx[j]];
+  }
+  return c;
+}
+
+// Deferred rank-2 update of the tile for an accepted exchange (the algebra of pfupdate_two.f90:113-224
+// in block form): Y' = Y - A B^T / R1 - s1 t1^T / R2.
+template <int KPL>
+__device__ __forceinline__ void warp_apply_update(const DevDims& d, double* Y, const Move& m, double c, const double* u,
+                                                  const double* v, double* S) {
+  const int lane = threadIdx.x & 31, Np = d.Np;
+  double acc[KPL], rho[KPL];
+#pragma unroll
+  for (int q = 0; q < KPL; q++) acc[q] = 0.0;
+  for (int j = 0; j < Np; j++) {
+    double uj = u[j], part = 0.0;
+#pragma unroll
+    for (int q = 0; q < KPL; q++) {
+      int k = lane + 32 * q;
+      if (k < Np) {
+        double y = Y[j * Np + k];
+        acc[q] = fma(uj, y, acc[q]);
+        part = fma(y, v[k], part);
+      }
+    }
+    part = warp_sum(part);
+    if (lane == 0) S[j] = part;
+  }
+  double wv = 0.0, ra = 0.0, ydbua = 0.0;
+#pragma unroll
+  for (int q = 0; q < KPL; q++) {
+    int k = lane + 32 * q;
+    rho[q] = 0.0;
+    if (k < Np) {
+      rho[q] = Y[m.db * Np + k];
+      wv = fma(acc[q], v[k], wv);
+      if (k == m.ua) {
+        ra = acc[q];
+        ydbua = rho[q];
+      }
+    }
+  }
+  wv = warp_sum(wv);
+  ra = warp_sum(ra);
+  ydbua = warp_sum(ydbua);
+  __syncwarp();
+  const double R1 = ra, R = ra * S[m.db] - ydbua * (wv - c);
+  const double inv_r1 = 1.0 / R1, r1_over_r = R1 / R, wc = (wv - c) * inv_r1;
+  double bk[KPL], tk[KPL];
+#pragma unroll
+  for (int q = 0; q < KPL; q++) {
+    int k = lane + 32 * q;
+    double B = acc[q] - (k == m.ua ? 1.0 : 0.0);
+    bk[q] = B * inv_r1;
+    tk[q] = (rho[q] - ydbua * B * inv_r1) * r1_over_r;
+  }
+  for (int j = 0; j < Np; j++) {
+    const double Aj = Y[j * Np + m.ua];
+    const double s1 = S[j] - Aj * wc - (j == m.db ? 1.0 : 0.0);
+    __syncwarp();
+#pragma unroll
+    for (int q = 0; q < KPL; q++) {
+      int k = lane + 32 * q;
+      if (k < Np) Y[j * Np + k] = Y[j * Np + k] - Aj * bk[q] - s1 * tk[q];
+    }
+  }
+  __syncwarp();
+}
+
+// Ratio R = (u^T Y)_ua (Y v)_db - Y(db,ua) (u^T Y v - c) on the shared-memory tile
+template <int KPL>
+__device__ __forceinline__ double warp_tile_ratio(const DevDims& d, const double* Y, const Move& m, double c,
+                                                  const double* u, const double* v) {
+  const int lane = threadIdx.x & 31, Np = d.Np;
+  double acc[KPL];
+#pragma unroll
+  for (int q = 0; q < KPL; q++) acc[q] = 0.0;
+  for (int j = 0; j < Np; j++) {
+    double uj = u[j];
+#pragma unroll
+    for (int q = 0; q < KPL; q++) {
+      int k = lane + 32 * q;
+      if (k < Np) acc[q] = fma(uj, Y[j * Np + k], acc[q]);
+    }
+  }
+  double wv = 0.0, sb = 0.0, ra = 0.0, ydbua = 0.0;
+#pragma unroll
+  for (int q = 0; q < KPL; q++) {
+    int k = lane + 32 * q;
+    if (k < Np) {
+      double rho = Y[m.db * Np + k];
+      wv = fma(acc[q], v[k], wv);
+      sb = fma(rho, v[k], sb);
+      if (k == m.ua) {
+        ra = acc[q];
+        ydbua = rho;
+      }
+    }
+  }
+  wv = warp_sum(wv);
+  sb = warp_sum(sb);
+  ra = warp_sum(ra);
+  ydbua = warp_sum(ydbua);
+  return ra * sb - ydbua * (wv - c);
+}
+
+struct Pipe {
+  uint32_t T0;        // tiles issued before this pass (same value in every thread)
+  int last_issued[16];  // per stage: last tile index loaded (producer thread only), -1 if none
+};
+
+// producer (thread 0): previous stores performed, then the first min(ST, n_qp) loads of a pass
+__device__ __forceinline__ void pass_issue_first(const SCtx& c, const Stream& sm, Pipe& pp) {
+  bulk_wait_all();
+  fence_proxy_async_global();
+  const int n = c.d.n_qp, n0 = n < sm.ST ? n : sm.ST;
+  const size_t NN = (size_t)c.d.Np * c.d.Np;
+  for (int t = 0; t < n0; t++) {
+    uint32_t T = pp.T0 + t;
+    int s = (int)(T % sm.ST);
+    mbar_arrive_expect_tx(&sm.full[s], sm.tile_bytes);
+    bulk_load(sm.stage + (size_t)s * NN, c.Yw + (size_t)t * NN, sm.tile_bytes, &sm.full[s]);
+    pp.last_issued[s] = (int)T;
+  }
+}
+
+// producer (thread 0): refill the ring for the rest of the pass and store released modified tiles
+__device__ __forceinline__ bool pass_produce(const SCtx& c, const Stream& sm, Pipe& pp, volatile int* abort_flag) {
+  const int n = c.d.n_qp, ST = sm.ST;
+  const size_t NN = (size_t)c.d.Np * c.d.Np;
+  for (int t = ST; t < n; t++) {
+    uint32_t T = pp.T0 + t, Tp = T - ST;
+    int s = (int)(T % ST);
+    if (!mbar_wait(&sm.empty[s], (Tp / ST) & 1u)) return false;
+    if (sm.dirty[s]) {
+      bulk_store(c.Yw + (size_t)(t - ST) * NN, sm.stage + (size_t)s * NN, sm.tile_bytes);
+      bulk_commit();
+      bulk_wait_read_all();
+      sm.dirty[s] = 0;
+    }
+    if (*abort_flag) return false;
+    mbar_arrive_expect_tx(&sm.full[s], sm.tile_bytes);
+    bulk_load(sm.stage + (size_t)s * NN, c.Yw + (size_t)t * NN, sm.tile_bytes, &sm.full[s]);
+    pp.last_issued[s] = (int)T;
+  }
+  for (int t = (n > ST ? n - ST : 0); t < n; t++) {
+    uint32_t T = pp.T0 + t;
+    int s = (int)(T % ST);
+    if (!mbar_wait(&sm.empty[s], (T / ST) & 1u)) return false;
+    if (sm.dirty[s]) {
+      bulk_store(c.Yw + (size_t)t * NN, sm.stage + (size_t)s * NN, sm.tile_bytes);
+      bulk_commit();
+      sm.dirty[s] = 0;
+    }
+  }
+  bulk_wait_read_all();
+  return true;
+}
+
+// consumers (warps 1..): deferred update (pend) and/or proposal ratio (prop) per tile
+template <int KPL>
+__device__ __forceinline__ bool pass_consume(const SCtx& c, const Stream& sm, const Pipe& pp, bool pend,
+                                             const Move& mk, bool prop, const Move& mn, double& pre, double& pim,
+                                             volatile int* abort_flag) {
+  const DevDims& d = c.d;
+  const WS& s = c.s;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, Np = d.Np, n = d.n_qp;
+  const size_t NN = (size_t)Np * Np;
+  double* U0 = s.wA + (size_t)warp * Np;
+  double* V0 = s.wS + (size_t)warp * Np;
+  double* S0 = sm.wR + (size_t)warp * Np;
+  double* u = s.wu + (size_t)warp * Np;
+  double* v = s.wv + (size_t)warp * Np;
+  for (int t = warp - 1; t < n; t += kConsumers) {
+    const uint32_t T = pp.T0 + t;
+    const int st = (int)(T % sm.ST);
+    double ck = 0.0, cn = 0.0;
+    if (pend) ck = gather_uv(d, c.p, t, s.idx, mk, U0, V0);
+    if (prop) cn = gather_uv(d, c.p, t, s.idx, mn, u, v);
+    __syncwarp();
+    if (*abort_flag) return false;
+    if (!mbar_wait(&sm.full[st], (T / sm.ST) & 1u)) return false;
+    double* Y = sm.stage + (size_t)st * NN;
+    if (pend) {
+      warp_apply_update<KPL>(d, Y, mk, ck, U0, V0, S0);
+      fence_proxy_async_smem();
+    }
+    if (prop) {
+      double R = warp_tile_ratio<KPL>(d, Y, mn, cn, u, v);
+      if (lane == 0) {
+        const double pfn = R * s.pf[t];
+        s.pfp[t] = pfn;
+        cplx cw = psi_wo_pf(d, c.t, s.rbm[t], s.sgnp[t >> 1], t);
+        s.psip[2 * t] = cw.re * pfn;
+        s.psip[2 * t + 1] = cw.im * pfn;
+        pre += cw.re * pfn;
+        pim += cw.im * pfn;
+      }
+    }
+    __syncwarp();
+    if (lane == 0) {
+      if (pend) sm.dirty[st] = 1;
+      mbar_arrive(&sm.empty[st]);
+    }
+  }
+  return true;
+}
+
+// Runs one pass (all threads).  The producer's first loads must already be issued.
+template <int KPL>
+__device__ __forceinline__ void run_pass(const SCtx& c, const Stream& sm, Pipe& pp, bool pend, const Move& mk,
+                                         bool prop, const Move& mn, volatile int* abort_flag) {
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  double pre = 0.0, pim = 0.0;
+  bool ok = true;
+  if (warp == 0) {
+    if (lane == 0) ok = pass_produce(c, sm, pp, abort_flag);
+  } else {
+    ok = pass_consume<KPL>(c, sm, pp, pend, mk, prop, mn, pre, pim, abort_flag);
+  }
+  if (!ok) {
+    *abort_flag = 1;
+    status(c) = ST_TIMEOUT;
+  }
+  if (lane == 0 && warp > 0) {
+    c.s.red[warp] = pre;
+    c.s.red[32 + warp] = pim;
+  }
+  __syncthreads();
+  pp.T0 += (uint32_t)c.d.n_qp;
+}
+
+// all stores of this CTA performed and visible to generic accesses of Y
+__device__ __forceinline__ void drain(const SCtx& c) {
+  if (threadIdx.x == 0) {
+    bulk_wait_all();
+    fence_proxy_async_global();
+  }
+  __syncthreads();
+}
+
+template <int KPL>
+__global__ void __launch_bounds__(kWarps * 32, 1)
+    sampler_stream_kernel(const __grid_constant__ DevDims d, const __grid_constant__ DevTables t,
+                          const __grid_constant__ DevParams p, const __grid_constant__ DevWalkers W, int first,
+                          int ST) {
+  extern __shared__ __align__(128) char smem[];
+  __shared__ WS ws;
+  __shared__ Stream sm;
+  __shared__ int pend_s[5];
+  __shared__ int abort_flag;
+  const int tid = threadIdx.x;
+  if (tid == 0) {
+    stream_layout(d, ST, smem, &ws, &sm);
+    for (int k = 0; k < ST; k++) {
+      mbar_init(&sm.full[k], 1);
+      mbar_init(&sm.empty[k], 1);
+      sm.dirty[k] = 0;
+    }
+    fence_mbar_init();
+    pend_s[0] = 0;
+    abort_flag = 0;
+  }
+  __syncthreads();
+  const SCtx c{d, t, p, W, (int)blockIdx.x, ws, W.Y + (size_t)blockIdx.x * d.n_qp * d.Np * d.Np};
+  const WS& s = ws;
+  const int w = c.w, N = d.N, Np = d.Np;
+  Pipe pp;
+  pp.T0 = 0;
+  for (int k = 0; k < 16; k++) pp.last_issued[k] = -1;
+
+  for (int k = tid; k < 625; k += blockDim.x) s.mt[k] = W.mt[(size_t)w * 625 + k];
+  if (tid == 0) status(c) = 0;
+  __syncthreads();
+  int nfastup = W.nfastup[w];
+
+  if (first) {
+    make_initial_x(c);
+  } else {
+    for (int i = tid; i < N; i += blockDim.x) s.x[i] = W.xs[((size_t)w * d.ns + (d.ns - 1)) * N + i];
+    __syncthreads();
+    full_state(c);
+    if (!status(c)) {
+      if (tid == 0) s.iflag[F_AUX] = grnd(s.mt) < 0.05;
+      __syncthreads();
+      if (s.iflag[F_AUX]) make_initial_x(c);
+    }
+  }
+  const Move none{0, 0, 0, 0};
+  int naccept = 0, nacc_tmp = 0, nacc_all = 0;
+  for (int i0 = -d.nwarm; i0 <= d.ns && !status(c); i0++) {
+    if (nacc_tmp > nfastup) {
+      if (pend_s[0]) {  // apply the deferred update before the drift check
+        Move mk{pend_s[1], pend_s[2], pend_s[3], pend_s[4]};
+        if (tid == 0) pass_issue_first(c, sm, pp);
+        __syncthreads();
+        run_pass<KPL>(c, sm, pp, true, mk, false, none, &abort_flag);
+        if (tid == 0) pend_s[0] = 0;
+      }
+      drain(c);
+      if (status(c)) break;
+      checkpoint(c, nfastup);
+      if (status(c)) break;
+      nacc_tmp = 0;
+    }
+    for (int iu = 0; iu < d.nupdate; iu++) {
+      if (tid == 0) s.iflag[F_FLIP] = grnd(s.mt) < 3.0e-4;
+      __syncthreads();
+      if (s.iflag[F_FLIP]) {
+        drain(c);
+        global_flip(c);
+        if (status(c)) break;
+        if (tid == 0 && s.iflag[F_ACCEPT]) pend_s[0] = 0;  // Y recomputed for the flipped state
+        __syncthreads();
+      }
+      if (tid == 0) {
+        pass_issue_first(c, sm, pp);
+        candidate_search(c);
+      }
+      __syncthreads();
+      if (status(c)) break;
+      const int i1 = s.iflag[F_I1], i2 = s.iflag[F_I2];
+      const int i3 = s.cfg[i1], i4 = s.cfg[i2];
+      Move mn;
+      if (s.x[i1] == 1) {
+        mn = Move{i3, i4 - Np, i1, i2};
+      } else {
+        mn = Move{i4, i3 - Np, i2, i1};
+      }
+      const bool pend = pend_s[0] != 0;
+      const Move mk{pend_s[1], pend_s[2], pend_s[3], pend_s[4]};
+      cta_update_theta(d, t, p, s.x, i1, i2, s.th, s.thp);
+      const int flipsign = (t.subB[i1] ? -1 : 1) * (t.subB[i2] ? -1 : 1);
+      for (int mp = tid; mp < d.n_mp; mp += blockDim.x) s.sgnp[mp] = -s.sgn[mp] * flipsign;
+      __syncthreads();
+      cta_rbm_factors(d, s.thp, s.rbm);
+      __syncthreads();
+      run_pass<KPL>(c, sm, pp, pend, mk, true, mn, &abort_flag);
+      if (status(c)) break;
+      if (tid == 0) {
+        double re = 0.0, im = 0.0;
+        for (int k = 1; k < kWarps; k++) {
+          re += s.red[k];
+          im += s.red[32 + k];
+        }
+        s.dsc[D_PSIPR] = re;
+        s.dsc[D_PSIPI] = im;
+        (void)grnd(s.mt);  // sub.f90:72
+        double r1 = (hypot(re, im) + d.shift) / (hypot(s.dsc[D_PSI0R], s.dsc[D_PSI0I]) + d.shift);
+        s.iflag[F_ACCEPT] = grnd(s.mt) < r1 * r1;  // make_sample.f90:203-204
+      }
+      __syncthreads();
+      if (s.iflag[F_ACCEPT]) {  // make_sample.f90:205-219; the Y update is deferred to the next pass
+        for (int j = tid; j < d.Mr; j += blockDim.x) s.th[j] = s.thp[j];
+        for (int mp = tid; mp < d.n_mp; mp += blockDim.x) s.sgn[mp] = s.sgnp[mp];
+        for (int qp = tid; qp < d.n_qp; qp += blockDim.x) {
+          s.pf[qp] = s.pfp[qp];
+          s.psi[2 * qp] = s.psip[2 * qp];
+          s.psi[2 * qp + 1] = s.psip[2 * qp + 1];
+        }
+        __syncthreads();
+        if (tid == 0) {
+          s.x[i1] = -s.x[i1];
+          s.x[i2] = -s.x[i2];
+          s.cfg[i1] = i4;
+          s.cfg[i2] = i3;
+          s.idx[i3] = i2;
+          s.idx[i4] = i1;
+          s.dsc[D_PSI0R] = s.dsc[D_PSIPR];
+          s.dsc[D_PSI0I] = s.dsc[D_PSIPI];
+          pend_s[0] = 1;
+          pend_s[1] = mn.ua;
+          pend_s[2] = mn.db;
+          pend_s[3] = mn.s_up;
+          pend_s[4] = mn.s_dn;
+        }
+        if (i0 > 0) naccept++;
+        nacc_tmp++;
+        nacc_all++;
+      } else if (tid == 0) {
+        pend_s[0] = 0;  // a deferred update, if any, was applied and stored by this pass
+      }
+      __syncthreads();
+    }
+    if (status(c)) break;
+    if (i0 > 0) {  // make_sample.f90:228-232
+      size_t sidx = (size_t)w * d.ns + (i0 - 1);
+      for (int i = tid; i < N; i += blockDim.x) W.xs[sidx * N + i] = (int8_t)s.x[i];
+      for (int qp = tid; qp < d.n_qp; qp += blockDim.x) W.pfs[sidx * d.n_qp + qp] = s.pf[qp];
+      double* ps = W.psis + sidx * (size_t)(d.n_qp + 1) * 2;
+      for (int k = tid; k < d.n_qp; k += blockDim.x) {
+        ps[2 * (k + 1)] = s.psi[2 * k];
+        ps[2 * (k + 1) + 1] = s.psi[2 * k + 1];
+      }
+      if (tid == 0) {
+        ps[0] = s.dsc[D_PSI0R];
+        ps[1] = s.dsc[D_PSI0I];
+      }
+    }
+    __syncthreads();
+  }
+  if (!status(c) && pend_s[0]) {  // leave Y consistent with the final state
+    Move mk{pend_s[1], pend_s[2], pend_s[3], pend_s[4]};
+    if (tid == 0) pass_issue_first(c, sm, pp);
+    __syncthreads();
+    run_pass<KPL>(c, sm, pp, true, mk, false, none, &abort_flag);
+  }
+  // every bulk copy of this CTA has landed before the CTA exits (bounded waits)
+  if (tid == 0) {
+    for (int k = 0; k < sm.ST && k < 16; k++)
+      if (pp.last_issued[k] >= 0) (void)mbar_wait(&sm.full[k], ((uint32_t)pp.last_issued[k] / sm.ST) & 1u);
+    bulk_wait_all();
+  }
+  __syncthreads();
+  for (int k = tid; k < 625; k += blockDim.x) W.mt[(size_t)w * 625 + k] = s.mt[k];
+  for (int i = tid; i < N; i += blockDim.x) {
+    W.x[(size_t)w * N + i] = (int8_t)s.x[i];
+    W.idx[(size_t)w * N + i] = (int16_t)s.idx[i];
+    W.cfg[(size_t)w * N + i] = (int16_t)s.cfg[i];
+  }
+  if (tid == 0) {
+    W.nfastup[w] = nfastup;
+    W.naccept[w] = naccept;
+    W.nacc_all[w] = nacc_all;
+    W.status[w] = status(c);
+  }
+}
+
+}  // namespace
+
+// Stage count and shared memory of the streaming sampler; 0 when it does not apply.
+int rbmpp_stream_stages(const DevDims& d, int max_smem) {
+  if (d.Np > 64) return 0;
+  const size_t tile = (size_t)8 * d.Np * d.Np;
+  int st = d.n_qp < 8 ? d.n_qp : 8;
+  while (st >= 1) {
+    size_t need = stream_layout(d, st, nullptr, nullptr, nullptr);
+    if ((long long)need <= max_smem) return st;
+    st--;
+  }
+  (void)tile;
+  return 0;
+}
+
+size_t rbmpp_stream_smem(const DevDims& d, int st) { return stream_layout(d, st, nullptr, nullptr, nullptr); }
+
+cudaError_t rbmpp_launch_sampler_stream(const DevDims& d, const DevTables& t, const DevParams& p, const DevWalkers& W,
+                                        int first, int st, cudaStream_t stream) {
+  size_t smem = rbmpp_stream_smem(d, st);
+  int kpl = (d.Np + 31) / 32;
+#define LAUNCH(K)                                                                                               \
+  do {                                                                                                          \
+    cudaError_t e = cudaFuncSetAttribute(sampler_stream_kernel<K>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
+                                         (int)smem);                                                            \
+    if (e != cudaSuccess) return e;                                                                             \
+    sampler_stream_kernel<K><<<d.nw, kWarps * 32, smem, stream>>>(d, t, p, W, first, st);                       \
+    return cudaGetLastError();                                                                                  \
+  } while (0)
+  if (kpl <= 1) LAUNCH(1);
+  if (kpl <= 2) LAUNCH(2);
+#undef LAUNCH
+  return cudaErrorInvalidValue;
+}

@@ -57,7 +57,8 @@ struct WS {
 __host__ __device__ __forceinline__ size_t align16(size_t v) { return (v + 15) & ~(size_t)15; }
 
 // Carve the workspace; returns total bytes.  Same code on host (sizing) and device (pointers).
-__host__ __device__ __forceinline__ size_t ws_layout(const DevDims& d, int nwarps, char* base, WS* w) {
+__host__ __device__ __forceinline__ size_t ws_layout(const DevDims& d, int nwarps, char* base, WS* w,
+                                                     bool own_tile = true) {
   size_t off = 0;
   auto take = [&](size_t bytes) -> char* {
     char* p = base ? base + off : nullptr;
@@ -83,7 +84,7 @@ __host__ __device__ __forceinline__ size_t ws_layout(const DevDims& d, int nwarp
   t.psi = (double*)take(d.n_qp * 16);
   t.psip = (double*)take(d.n_qp * 16);
   t.rbm = (double*)take(d.n_qp * 8);
-  t.tile = (double*)take((size_t)Np * (Np + 1) * 8);
+  t.tile = own_tile ? (double*)take((size_t)Np * (Np + 1) * 8) : nullptr;
   t.colbuf = (double*)take(Np * 8);
   t.rowbuf = (double*)take(Np * 8);
   t.perm = (int*)take(Np * 4);

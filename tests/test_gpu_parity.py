@@ -123,3 +123,24 @@ def test_sr_iterations_stay_in_lockstep():
         assert _rel(slg, slo) < 1e-8 and _rel(Wrg, Wro) < 1e-8
         assert abs(shg - sho) <= 1e-9 * abs(sho) + 1e-300
     g.close()
+
+
+@pytest.mark.parametrize("L,trans,alphar,nw,ns", [(4, True, 1, 4, 8), (6, True, 2, 3, 4)])
+def test_stream_and_direct_samplers_agree(L, trans, alphar, nw, ns, monkeypatch):
+    """The TMA-streamed sampler (deferred updates) and the direct sampler (immediate updates) give the
+    same chains and the same stored amplitudes to rounding."""
+    p = fm.synthetic_problem(L, translations=trans, alphar=alphar, nsample=nw * ns, seed=21)
+    out = []
+    for mode in ("stream", "direct"):
+        monkeypatch.setenv("RBMPP_SAMPLER", mode)
+        g = capi.Context(p, n_walkers=nw, nsample_per_walker=ns)
+        g.set_params(p.br, p.Wr, p.slater, 0.0)
+        g.seed(31)
+        na = g.make_sample(True)
+        na2 = g.make_sample(False)
+        out.append((na, na2, *g.samples()))
+        g.close()
+    (a1, a2, xa, pa, fa), (b1, b2, xb, pb, fb) = out
+    assert np.array_equal(a1, b1) and np.array_equal(a2, b2)
+    assert np.array_equal(xa, xb)
+    assert _rel(fa, fb) < 1e-8
