@@ -2,7 +2,7 @@
 // with TMA bulk copies (make_sample.f90:4-240, same RNG order as sampler.cu).
 //
 // One CTA per walker: warp 0 is the control warp (its lane 0 draws the random numbers and issues every
-// bulk copy), warps 1..4 consume tiles.  A tile is one projection's Y = X^{-1} (Np x Np FP64, row
+// bulk copy; the warp evaluates theta' and the cosh products of the proposal), warps 1..8 consume tiles.  A tile is one projection's Y = X^{-1} (Np x Np FP64, row
 // major).  Every proposal is one pass over the n_qp tiles through an ST-stage ring:
 //   producer:  cp.async.bulk global->shared (mbarrier complete_tx), and after the consumer releases a
 //              modified tile, cp.async.bulk shared->global before the stage is refilled;
@@ -10,12 +10,13 @@
 //              tile in place, then evaluates the determinant ratio of the current proposal on it.
 // So a proposal costs one read of Y and an accepted move one write: the algorithmic minimum
 // (pfupdate_two.f90 reads InvM once per ratio and rewrites it per accepted move).
-// The first tiles of a pass are requested before the candidate is drawn, which hides the serial RNG.
+// The first tiles of a pass are requested before the candidate is drawn, and the consumers apply the
+// deferred update while the control warp draws the candidate, which hides the serial part of a proposal.
 #include "sampler_common.cuh"
 
 namespace {
 
-constexpr int kWarps = 5;
+constexpr int kWarps = 9;  // warp 0: control (RNG, candidate, theta', producer); warps 1..8: consumers
 constexpr int kConsumers = kWarps - 1;
 #define ST_TIMEOUT 22
 
@@ -24,7 +25,10 @@ struct Stream {
   uint64_t* full;
   uint64_t* empty;
   int* dirty;
-  double* wR;  // [kWarps][Np] row sums of the deferred update
+  double* wU0;  // [kWarps][Np] gathered row / column of the deferred exchange
+  double* wV0;
+  double* wS;   // [kWarps][Np] Y v of the deferred exchange
+  double* wA;   // [kWarps][Np] column ua of Y
   int ST;
   uint32_t tile_bytes;
 };
@@ -45,7 +49,10 @@ __host__ __device__ __forceinline__ size_t stream_layout(const DevDims& d, int S
   t.full = (uint64_t*)take(8 * (size_t)ST, 8);
   t.empty = (uint64_t*)take(8 * (size_t)ST, 8);
   t.dirty = (int*)take(4 * (size_t)ST, 4);
-  t.wR = (double*)take((size_t)kWarps * d.Np * 8, 16);
+  t.wU0 = (double*)take((size_t)kWarps * d.Np * 8, 16);
+  t.wV0 = (double*)take((size_t)kWarps * d.Np * 8, 16);
+  t.wS = (double*)take((size_t)kWarps * d.Np * 8, 16);
+  t.wA = (double*)take((size_t)kWarps * d.Np * 8, 16);
   if (w) w->tile = t.stage;
   if (st) *st = t;
   return off;
@@ -55,47 +62,76 @@ struct Move {
   int ua, db, s_up, s_dn;  // up electron, down electron (local index), their sites before the move
 };
 
-// u, v of an exchange for projection qp into per-warp buffers (the gathers of pfupdate_two.f90:48-52)
-__device__ __forceinline__ double gather_uv(const DevDims& d, const DevParams& p, int qp, const int* idx, const Move& m,
-                                            double* u, double* v) {
+// Lane-held gathers of one exchange for one projection: u = new row ua of X, v = new column db of X,
+// c = their shared corner (the gathers of pfupdate_two.f90:48-52 in block form).
+template <int KPL>
+struct UV {
+  double u[KPL], v[KPL], c;
+};
+
+template <int KPL>
+__device__ __forceinline__ void gather_regs(const DevDims& d, const DevParams& p, int qp, const int* idx,
+                                            const Move& m, UV<KPL>& g) {
   const int lane = threadIdx.x & 31, Np = d.Np, N = d.N;
   const double* XFq = p.XF + (size_t)qp * N * N;
   const double* XFTq = p.XFT + (size_t)qp * N * N;
-  const double c = XFq[(size_t)m.s_dn * N + m.s_up];
-  for (int j = lane; j < Np; j += 32) {
-    u[j] = (j == m.db) ? c : XFq[(size_t)m.s_dn * N + idx[Np + j]];
-    v[j] = (j == m.ua) ? c : XFTq[(size_t)m.s_up * N + idx[j]];
+  g.c = __ldg(XFq + (size_t)m.s_dn * N + m.s_up);
+#pragma unroll
+  for (int q = 0; q < KPL; q++) {
+    const int j = lane + 32 * q;
+    g.u[q] = 0.0;
+    g.v[q] = 0.0;
+    if (j < Np) {
+      g.u[q] = (j == m.db) ? 0.0 : __ldg(XFq + (size_t)m.s_dn * N + idx[Np + j]);
+      g.v[q] = (j == m.ua) ? 0.0 : __ldg(XFTq + (size_t)m.s_up * N + idx[j]);
+    }
   }
-  return c;
+}
+
+template <int KPL>
+__device__ __forceinline__ double store_regs(const DevDims& d, const Move& m, const UV<KPL>& g, double* u, double* v) {
+  const int lane = threadIdx.x & 31;
+#pragma unroll
+  for (int q = 0; q < KPL; q++) {
+    const int j = lane + 32 * q;
+    if (j < d.Np) {
+      u[j] = (j == m.db) ? g.c : g.u[q];
+      v[j] = (j == m.ua) ? g.c : g.v[q];
+    }
+  }
+  return g.c;
 }
 
 // Deferred rank-2 update of the tile for an accepted exchange (the algebra of pfupdate_two.f90:113-224
-// in block form): Y' = Y - A B^T / R1 - s1 t1^T / R2.
+// in block form): Y' = Y - A B^T / R1 - s1 t1^T / R2, with A = Y e_ua, B = u^T Y - e_ua^T,
+// s1 = Y v - A (u^T Y v - c)/R1 - e_db, t1 = e_db^T Y - Y(db,ua) B^T / R1, R2 = R / R1.
 template <int KPL>
 __device__ __forceinline__ void warp_apply_update(const DevDims& d, double* Y, const Move& m, double c, const double* u,
-                                                  const double* v, double* S) {
+                                                  const double* v, double* S, double* A) {
   const int lane = threadIdx.x & 31, Np = d.Np;
   double acc[KPL], rho[KPL];
 #pragma unroll
   for (int q = 0; q < KPL; q++) acc[q] = 0.0;
+#pragma unroll 5
   for (int j = 0; j < Np; j++) {
-    double uj = u[j], part = 0.0;
+    const double uj = u[j];
 #pragma unroll
     for (int q = 0; q < KPL; q++) {
-      int k = lane + 32 * q;
-      if (k < Np) {
-        double y = Y[j * Np + k];
-        acc[q] = fma(uj, y, acc[q]);
-        part = fma(y, v[k], part);
-      }
+      const int k = lane + 32 * q;
+      if (k < Np) acc[q] = fma(uj, Y[j * Np + k], acc[q]);
     }
-    part = warp_sum(part);
-    if (lane == 0) S[j] = part;
+  }
+  for (int j = lane; j < Np; j += 32) {  // row sums, lane <-> row
+    double a = 0.0;
+#pragma unroll 5
+    for (int k = 0; k < Np; k++) a = fma(Y[j * Np + k], v[k], a);
+    S[j] = a;
+    A[j] = Y[j * Np + m.ua];
   }
   double wv = 0.0, ra = 0.0, ydbua = 0.0;
 #pragma unroll
   for (int q = 0; q < KPL; q++) {
-    int k = lane + 32 * q;
+    const int k = lane + 32 * q;
     rho[q] = 0.0;
     if (k < Np) {
       rho[q] = Y[m.db * Np + k];
@@ -115,18 +151,18 @@ __device__ __forceinline__ void warp_apply_update(const DevDims& d, double* Y, c
   double bk[KPL], tk[KPL];
 #pragma unroll
   for (int q = 0; q < KPL; q++) {
-    int k = lane + 32 * q;
-    double B = acc[q] - (k == m.ua ? 1.0 : 0.0);
+    const int k = lane + 32 * q;
+    const double B = acc[q] - (k == m.ua ? 1.0 : 0.0);
     bk[q] = B * inv_r1;
     tk[q] = (rho[q] - ydbua * B * inv_r1) * r1_over_r;
   }
+#pragma unroll 4
   for (int j = 0; j < Np; j++) {
-    const double Aj = Y[j * Np + m.ua];
+    const double Aj = A[j];
     const double s1 = S[j] - Aj * wc - (j == m.db ? 1.0 : 0.0);
-    __syncwarp();
 #pragma unroll
     for (int q = 0; q < KPL; q++) {
-      int k = lane + 32 * q;
+      const int k = lane + 32 * q;
       if (k < Np) Y[j * Np + k] = Y[j * Np + k] - Aj * bk[q] - s1 * tk[q];
     }
   }
@@ -141,20 +177,21 @@ __device__ __forceinline__ double warp_tile_ratio(const DevDims& d, const double
   double acc[KPL];
 #pragma unroll
   for (int q = 0; q < KPL; q++) acc[q] = 0.0;
+#pragma unroll 5
   for (int j = 0; j < Np; j++) {
-    double uj = u[j];
+    const double uj = u[j];
 #pragma unroll
     for (int q = 0; q < KPL; q++) {
-      int k = lane + 32 * q;
+      const int k = lane + 32 * q;
       if (k < Np) acc[q] = fma(uj, Y[j * Np + k], acc[q]);
     }
   }
   double wv = 0.0, sb = 0.0, ra = 0.0, ydbua = 0.0;
 #pragma unroll
   for (int q = 0; q < KPL; q++) {
-    int k = lane + 32 * q;
+    const int k = lane + 32 * q;
     if (k < Np) {
-      double rho = Y[m.db * Np + k];
+      const double rho = Y[m.db * Np + k];
       wv = fma(acc[q], v[k], wv);
       sb = fma(rho, v[k], sb);
       if (k == m.ua) {
@@ -171,15 +208,19 @@ __device__ __forceinline__ double warp_tile_ratio(const DevDims& d, const double
 }
 
 struct Pipe {
-  uint32_t T0;        // tiles issued before this pass (same value in every thread)
-  int last_issued[16];  // per stage: last tile index loaded (producer thread only), -1 if none
+  uint32_t T0;          // tiles issued before this pass (same value in every thread)
+  int last_issued[16];  // per stage: last tile index loaded (thread 0 only), -1 if none
 };
 
-// producer (thread 0): previous stores performed, then the first min(ST, n_qp) loads of a pass
+__device__ __forceinline__ void bulk_wait_older_than_8() { asm volatile("cp.async.bulk.wait_group 8;" ::: "memory"); }
+
+// producer (thread 0): first min(ST, n_qp) loads of a pass.  Stores of the previous pass for these
+// projections completed long ago unless the pass is short.
 __device__ __forceinline__ void pass_issue_first(const SCtx& c, const Stream& sm, Pipe& pp) {
-  bulk_wait_all();
-  fence_proxy_async_global();
   const int n = c.d.n_qp, n0 = n < sm.ST ? n : sm.ST;
+  if (n < 2 * sm.ST) bulk_wait_all();
+  else bulk_wait_older_than_8();
+  fence_proxy_async_global();
   const size_t NN = (size_t)c.d.Np * c.d.Np;
   for (int t = 0; t < n0; t++) {
     uint32_t T = pp.T0 + t;
@@ -194,6 +235,7 @@ __device__ __forceinline__ void pass_issue_first(const SCtx& c, const Stream& sm
 __device__ __forceinline__ bool pass_produce(const SCtx& c, const Stream& sm, Pipe& pp, volatile int* abort_flag) {
   const int n = c.d.n_qp, ST = sm.ST;
   const size_t NN = (size_t)c.d.Np * c.d.Np;
+  bool waited_tail = false;
   for (int t = ST; t < n; t++) {
     uint32_t T = pp.T0 + t, Tp = T - ST;
     int s = (int)(T % ST);
@@ -205,6 +247,11 @@ __device__ __forceinline__ bool pass_produce(const SCtx& c, const Stream& sm, Pi
       sm.dirty[s] = 0;
     }
     if (*abort_flag) return false;
+    if (!waited_tail && t >= n - ST) {  // these projections were stored at the end of the previous pass
+      bulk_wait_all();
+      fence_proxy_async_global();
+      waited_tail = true;
+    }
     mbar_arrive_expect_tx(&sm.full[s], sm.tile_bytes);
     bulk_load(sm.stage + (size_t)s * NN, c.Yw + (size_t)t * NN, sm.tile_bytes, &sm.full[s]);
     pp.last_issued[s] = (int)T;
@@ -223,36 +270,117 @@ __device__ __forceinline__ bool pass_produce(const SCtx& c, const Stream& sm, Pi
   return true;
 }
 
-// consumers (warps 1..): deferred update (pend) and/or proposal ratio (prop) per tile
+// Control warp, proposal pass: candidate (thread 0), then theta', sgn', cosh products on the warp,
+// then publish the move to the consumers (who meanwhile apply the deferred update).
+__device__ __forceinline__ void control_propose(const SCtx& c, volatile int* cand_flag, int pass_id, int* mv) {
+  const DevDims& d = c.d;
+  const WS& s = c.s;
+  const int lane = threadIdx.x & 31;
+  if (lane == 0) candidate_search(c);
+  __syncwarp();
+  if (!status(c)) {
+    const int i1 = s.iflag[F_I1], i2 = s.iflag[F_I2];
+    const int i3 = s.cfg[i1], i4 = s.cfg[i2];
+    if (lane == 0) {
+      if (s.x[i1] == 1) {
+        mv[0] = i3;
+        mv[1] = i4 - d.Np;
+        mv[2] = i1;
+        mv[3] = i2;
+      } else {
+        mv[0] = i4;
+        mv[1] = i3 - d.Np;
+        mv[2] = i2;
+        mv[3] = i1;
+      }
+    }
+    // update_theta RBM.f90:95-148 and the new signs (make_sample.f90:195-197) on the warp
+    const int A2 = 2 * d.alphar;
+    const double x1 = (double)s.x[i1], x2 = (double)s.x[i2];
+    for (int j = lane; j < d.Mr; j += 32) {
+      int mp = j / A2, rem = j - mp * A2;
+      double sg = rem < d.alphar ? 1.0 : -1.0;
+      int f = rem < d.alphar ? rem : rem - d.alphar;
+      const double* Wf = c.p.Wr + (size_t)f * d.N;
+      int iw1 = c.t.wmap[(size_t)mp * d.N + i1], iw2 = c.t.wmap[(size_t)mp * d.N + i2];
+      double v = s.th[j];
+      v = v - 2.0 * Wf[iw1] * x1 * sg;
+      v = v - 2.0 * Wf[iw2] * x2 * sg;
+      s.thp[j] = v;
+    }
+    const int flipsign = (c.t.subB[i1] ? -1 : 1) * (c.t.subB[i2] ? -1 : 1);
+    for (int mp = lane; mp < d.n_mp; mp += 32) s.sgnp[mp] = -s.sgn[mp] * flipsign;
+    __syncwarp();
+    for (int qp = lane; qp < d.n_qp; qp += 32) {
+      double r = 1.0;
+      for (int f = 0; f < d.alphar; f++) r = r * cosh(s.thp[qp * d.alphar + f]);
+      s.rbm[qp] = r;
+    }
+  }
+  __syncwarp();
+  __threadfence_block();
+  if (lane == 0) *cand_flag = pass_id;
+}
+
+// consumers: deferred update (pend) and/or proposal ratio (prop) per tile
 template <int KPL>
 __device__ __forceinline__ bool pass_consume(const SCtx& c, const Stream& sm, const Pipe& pp, bool pend,
-                                             const Move& mk, bool prop, const Move& mn, double& pre, double& pim,
-                                             volatile int* abort_flag) {
+                                             const Move& mk, bool prop, volatile int* cand_flag, int pass_id,
+                                             const int* mv, double& pre, double& pim, volatile int* abort_flag) {
   const DevDims& d = c.d;
   const WS& s = c.s;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, Np = d.Np, n = d.n_qp;
   const size_t NN = (size_t)Np * Np;
-  double* U0 = s.wA + (size_t)warp * Np;
-  double* V0 = s.wS + (size_t)warp * Np;
-  double* S0 = sm.wR + (size_t)warp * Np;
+  double* U0 = sm.wU0 + (size_t)warp * Np;
+  double* V0 = sm.wV0 + (size_t)warp * Np;
+  double* S0 = sm.wS + (size_t)warp * Np;
+  double* A0 = sm.wA + (size_t)warp * Np;
   double* u = s.wu + (size_t)warp * Np;
   double* v = s.wv + (size_t)warp * Np;
-  for (int t = warp - 1; t < n; t += kConsumers) {
+  UV<KPL> gk, gn;
+  Move mn{0, 0, 0, 0};
+  bool have_move = false;
+  int t = warp - 1;
+  if (pend && t < n) gather_regs<KPL>(d, c.p, t, s.idx, mk, gk);
+  for (; t < n; t += kConsumers) {
     const uint32_t T = pp.T0 + t;
     const int st = (int)(T % sm.ST);
-    double ck = 0.0, cn = 0.0;
-    if (pend) ck = gather_uv(d, c.p, t, s.idx, mk, U0, V0);
-    if (prop) cn = gather_uv(d, c.p, t, s.idx, mn, u, v);
+    const int tn = t + kConsumers;
+    double ck = 0.0;
+    if (pend) {
+      ck = store_regs<KPL>(d, mk, gk, U0, V0);
+      if (tn < n) gather_regs<KPL>(d, c.p, tn, s.idx, mk, gk);
+    }
     __syncwarp();
     if (*abort_flag) return false;
     if (!mbar_wait(&sm.full[st], (T / sm.ST) & 1u)) return false;
     double* Y = sm.stage + (size_t)st * NN;
     if (pend) {
-      warp_apply_update<KPL>(d, Y, mk, ck, U0, V0, S0);
+      warp_apply_update<KPL>(d, Y, mk, ck, U0, V0, S0, A0);
       fence_proxy_async_smem();
     }
     if (prop) {
-      double R = warp_tile_ratio<KPL>(d, Y, mn, cn, u, v);
+      if (!have_move) {
+        bool ok = false;
+        for (int it = 0; it < (1 << 24); it++) {
+          if (*cand_flag == pass_id) {
+            ok = true;
+            break;
+          }
+          if (*abort_flag) break;
+          __nanosleep(64);
+        }
+        __syncwarp();
+        __threadfence_block();
+        if (!ok || status(c)) return false;
+        mn = Move{mv[0], mv[1], mv[2], mv[3]};
+        have_move = true;
+        gather_regs<KPL>(d, c.p, t, s.idx, mn, gn);
+      }
+      const double cn = store_regs<KPL>(d, mn, gn, u, v);
+      __syncwarp();
+      if (tn < n) gather_regs<KPL>(d, c.p, tn, s.idx, mn, gn);
+      const double R = warp_tile_ratio<KPL>(d, Y, mn, cn, u, v);
       if (lane == 0) {
         const double pfn = R * s.pf[t];
         s.pfp[t] = pfn;
@@ -272,21 +400,26 @@ __device__ __forceinline__ bool pass_consume(const SCtx& c, const Stream& sm, co
   return true;
 }
 
-// Runs one pass (all threads).  The producer's first loads must already be issued.
+// One pass over all projections (all threads).  prop: evaluate a new proposal (control warp draws
+// it); pend: apply the deferred update of the previously accepted exchange mk.
 template <int KPL>
 __device__ __forceinline__ void run_pass(const SCtx& c, const Stream& sm, Pipe& pp, bool pend, const Move& mk,
-                                         bool prop, const Move& mn, volatile int* abort_flag) {
+                                         bool prop, volatile int* cand_flag, int pass_id, int* mv,
+                                         volatile int* abort_flag) {
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   double pre = 0.0, pim = 0.0;
   bool ok = true;
   if (warp == 0) {
-    if (lane == 0) ok = pass_produce(c, sm, pp, abort_flag);
+    if (lane == 0) pass_issue_first(c, sm, pp);
+    __syncwarp();
+    if (prop) control_propose(c, cand_flag, pass_id, mv);
+    if (lane == 0 && !status(c)) ok = pass_produce(c, sm, pp, abort_flag);
   } else {
-    ok = pass_consume<KPL>(c, sm, pp, pend, mk, prop, mn, pre, pim, abort_flag);
+    ok = pass_consume<KPL>(c, sm, pp, pend, mk, prop, cand_flag, pass_id, mv, pre, pim, abort_flag);
   }
   if (!ok) {
     *abort_flag = 1;
-    status(c) = ST_TIMEOUT;
+    if (!status(c)) status(c) = ST_TIMEOUT;
   }
   if (lane == 0 && warp > 0) {
     c.s.red[warp] = pre;
@@ -314,7 +447,8 @@ __global__ void __launch_bounds__(kWarps * 32, 1)
   __shared__ WS ws;
   __shared__ Stream sm;
   __shared__ int pend_s[5];
-  __shared__ int abort_flag;
+  __shared__ int mv[4];
+  __shared__ int abort_flag, cand_flag;
   const int tid = threadIdx.x;
   if (tid == 0) {
     stream_layout(d, ST, smem, &ws, &sm);
@@ -326,14 +460,16 @@ __global__ void __launch_bounds__(kWarps * 32, 1)
     fence_mbar_init();
     pend_s[0] = 0;
     abort_flag = 0;
+    cand_flag = -1;
   }
   __syncthreads();
   const SCtx c{d, t, p, W, (int)blockIdx.x, ws, W.Y + (size_t)blockIdx.x * d.n_qp * d.Np * d.Np};
   const WS& s = ws;
-  const int w = c.w, N = d.N, Np = d.Np;
+  const int w = c.w, N = d.N;
   Pipe pp;
   pp.T0 = 0;
   for (int k = 0; k < 16; k++) pp.last_issued[k] = -1;
+  int pass_id = 0;
 
   for (int k = tid; k < 625; k += blockDim.x) s.mt[k] = W.mt[(size_t)w * 625 + k];
   if (tid == 0) status(c) = 0;
@@ -357,10 +493,8 @@ __global__ void __launch_bounds__(kWarps * 32, 1)
   for (int i0 = -d.nwarm; i0 <= d.ns && !status(c); i0++) {
     if (nacc_tmp > nfastup) {
       if (pend_s[0]) {  // apply the deferred update before the drift check
-        Move mk{pend_s[1], pend_s[2], pend_s[3], pend_s[4]};
-        if (tid == 0) pass_issue_first(c, sm, pp);
-        __syncthreads();
-        run_pass<KPL>(c, sm, pp, true, mk, false, none, &abort_flag);
+        const Move mk{pend_s[1], pend_s[2], pend_s[3], pend_s[4]};
+        run_pass<KPL>(c, sm, pp, true, mk, false, &cand_flag, ++pass_id, mv, &abort_flag);
         if (tid == 0) pend_s[0] = 0;
       }
       drain(c);
@@ -379,30 +513,12 @@ __global__ void __launch_bounds__(kWarps * 32, 1)
         if (tid == 0 && s.iflag[F_ACCEPT]) pend_s[0] = 0;  // Y recomputed for the flipped state
         __syncthreads();
       }
-      if (tid == 0) {
-        pass_issue_first(c, sm, pp);
-        candidate_search(c);
-      }
-      __syncthreads();
+      const bool pend = pend_s[0] != 0;
+      const Move mk{pend_s[1], pend_s[2], pend_s[3], pend_s[4]};
+      run_pass<KPL>(c, sm, pp, pend, mk, true, &cand_flag, ++pass_id, mv, &abort_flag);
       if (status(c)) break;
       const int i1 = s.iflag[F_I1], i2 = s.iflag[F_I2];
       const int i3 = s.cfg[i1], i4 = s.cfg[i2];
-      Move mn;
-      if (s.x[i1] == 1) {
-        mn = Move{i3, i4 - Np, i1, i2};
-      } else {
-        mn = Move{i4, i3 - Np, i2, i1};
-      }
-      const bool pend = pend_s[0] != 0;
-      const Move mk{pend_s[1], pend_s[2], pend_s[3], pend_s[4]};
-      cta_update_theta(d, t, p, s.x, i1, i2, s.th, s.thp);
-      const int flipsign = (t.subB[i1] ? -1 : 1) * (t.subB[i2] ? -1 : 1);
-      for (int mp = tid; mp < d.n_mp; mp += blockDim.x) s.sgnp[mp] = -s.sgn[mp] * flipsign;
-      __syncthreads();
-      cta_rbm_factors(d, s.thp, s.rbm);
-      __syncthreads();
-      run_pass<KPL>(c, sm, pp, pend, mk, true, mn, &abort_flag);
-      if (status(c)) break;
       if (tid == 0) {
         double re = 0.0, im = 0.0;
         for (int k = 1; k < kWarps; k++) {
@@ -435,10 +551,10 @@ __global__ void __launch_bounds__(kWarps * 32, 1)
           s.dsc[D_PSI0R] = s.dsc[D_PSIPR];
           s.dsc[D_PSI0I] = s.dsc[D_PSIPI];
           pend_s[0] = 1;
-          pend_s[1] = mn.ua;
-          pend_s[2] = mn.db;
-          pend_s[3] = mn.s_up;
-          pend_s[4] = mn.s_dn;
+          pend_s[1] = mv[0];
+          pend_s[2] = mv[1];
+          pend_s[3] = mv[2];
+          pend_s[4] = mv[3];
         }
         if (i0 > 0) naccept++;
         nacc_tmp++;
@@ -466,10 +582,8 @@ __global__ void __launch_bounds__(kWarps * 32, 1)
     __syncthreads();
   }
   if (!status(c) && pend_s[0]) {  // leave Y consistent with the final state
-    Move mk{pend_s[1], pend_s[2], pend_s[3], pend_s[4]};
-    if (tid == 0) pass_issue_first(c, sm, pp);
-    __syncthreads();
-    run_pass<KPL>(c, sm, pp, true, mk, false, none, &abort_flag);
+    const Move mk{pend_s[1], pend_s[2], pend_s[3], pend_s[4]};
+    run_pass<KPL>(c, sm, pp, true, mk, false, &cand_flag, ++pass_id, mv, &abort_flag);
   }
   // every bulk copy of this CTA has landed before the CTA exits (bounded waits)
   if (tid == 0) {
