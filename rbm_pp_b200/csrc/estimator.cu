@@ -21,6 +21,9 @@ struct EstShared {
   double* psib;   // [4N][2] psi(x') accumulators
   int* nap;       // [1]
   double* diag;   // [1]     sum J x x
+  double* P;      // [Np][Np+1]  P(e, j) = XF(d_e, d_j)   (down-down gathers)
+  double* Q;      // [Np][Np+1]  Q(i, a) = XF(u_i, u_a)   (up-up gathers)
+  double* YQ;     // [Np][Np+1]  Y Q
 };
 
 __host__ __device__ __forceinline__ size_t est_layout(const DevDims& d, int nwarps, char* base, WS* w, EstShared* e) {
@@ -36,58 +39,51 @@ __host__ __device__ __forceinline__ size_t est_layout(const DevDims& d, int nwar
   t.psib = (double*)take((size_t)4 * d.N * 16);
   t.nap = (int*)take(16);
   t.diag = (double*)take(16);
+  const size_t tb = (size_t)d.Np * (d.Np + 1) * 8;
+  t.P = (double*)take(tb);
+  t.Q = (double*)take(tb);
+  t.YQ = (double*)take(tb);
   if (e) *e = t;
   return off;
 }
 
-// Ratio for one bond from the shared-memory inverse tile (ld = Np + 1).
-template <int KPL>
-__device__ __forceinline__ double warp_ratio_tile(const DevDims& d, const DevParams& p, const double* T, int qp, const int* idx,
-                                         int ua, int db, int s_up, int s_dn, double* u, double* v) {
-  const int lane = threadIdx.x & 31, Np = d.Np, N = d.N, ld = Np + 1;
-  const double* XFq = p.XF + (size_t)qp * N * N;
-  const double* XFTq = p.XFT + (size_t)qp * N * N;
-  const double c = XFq[(size_t)s_dn * N + s_up];
-  for (int j = lane; j < Np; j += 32) {
-    u[j] = (j == db) ? c : XFq[(size_t)s_dn * N + idx[Np + j]];
-    v[j] = (j == ua) ? c : XFTq[(size_t)s_up * N + idx[j]];
-  }
-  __syncwarp();
-  double acc[KPL];
+// C = A B for n x n row-major shared-memory matrices with leading dimension ld (rows of 2, interleaved
+// columns so that a warp reads consecutive columns of B)
+__device__ __forceinline__ void cta_gemm(int n, int ld, const double* A, const double* B, double* C) {
+  const int nr = (n + 1) / 2, nc = (n + 3) / 4;
+  for (int blk = threadIdx.x; blk < nr * nc; blk += blockDim.x) {
+    const int bi = blk / nc, bj = blk - bi * nc;
+    const int i0 = 2 * bi;
+    double acc[2][4];
 #pragma unroll
-  for (int m = 0; m < KPL; m++) acc[m] = 0.0;
-  for (int j = 0; j < Np; j++) {
-    double uj = u[j];
+    for (int r = 0; r < 2; r++)
 #pragma unroll
-    for (int m = 0; m < KPL; m++) {
-      int k = lane + 32 * m;
-      if (k < Np) acc[m] = fma(uj, T[j * ld + k], acc[m]);
+      for (int q = 0; q < 4; q++) acc[r][q] = 0.0;
+    const bool r1ok = i0 + 1 < n;
+#pragma unroll 2
+    for (int k = 0; k < n; k++) {
+      const double a0 = A[i0 * ld + k], a1 = r1ok ? A[(i0 + 1) * ld + k] : 0.0;
+#pragma unroll
+      for (int q = 0; q < 4; q++) {
+        const int j = bj + q * nc;
+        const double b = (j < n) ? B[k * ld + j] : 0.0;
+        acc[0][q] = fma(a0, b, acc[0][q]);
+        acc[1][q] = fma(a1, b, acc[1][q]);
+      }
     }
-  }
-  double wv = 0.0, sb = 0.0, ra = 0.0, ydbua = 0.0;
 #pragma unroll
-  for (int m = 0; m < KPL; m++) {
-    int k = lane + 32 * m;
-    if (k < Np) {
-      double rho = T[db * ld + k];
-      wv = fma(acc[m], v[k], wv);
-      sb = fma(rho, v[k], sb);
-      if (k == ua) {
-        ra = acc[m];
-        ydbua = rho;
+    for (int q = 0; q < 4; q++) {
+      const int j = bj + q * nc;
+      if (j < n) {
+        C[i0 * ld + j] = acc[0][q];
+        if (r1ok) C[(i0 + 1) * ld + j] = acc[1][q];
       }
     }
   }
-  wv = warp_sum(wv);
-  sb = warp_sum(sb);
-  ra = warp_sum(ra);
-  ydbua = warp_sum(ydbua);
-  __syncwarp();
-  return ra * sb - ydbua * (wv - c);
 }
 
 template <int KPL>
-__global__ void __launch_bounds__(256)
+__global__ void __launch_bounds__(512, 1)
     estimator_kernel(const __grid_constant__ DevDims d, const __grid_constant__ DevTables t,
                      const __grid_constant__ DevParams p, const int8_t* xs, int n, double* out_psi, double* out_hpsi,
                      double* O, int* out_nap, int* out_status, int reweight) {
@@ -96,7 +92,7 @@ __global__ void __launch_bounds__(256)
   __shared__ EstShared e;
   if (threadIdx.x == 0) est_layout(d, blockDim.x >> 5, smem, &s, &e);
   __syncthreads();
-  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, nwarps = blockDim.x >> 5;
+  const int tid = threadIdx.x;
   const int N = d.N, Np = d.Np, ld = Np + 1;
   const int cfgi = blockIdx.x;
   if (cfgi >= n) return;
@@ -149,18 +145,33 @@ __global__ void __launch_bounds__(256)
     if (tid == 0 && out_status) out_status[cfgi] = s.iflag[F_STATUS];
     return;
   }
-  double* u = s.wu + (size_t)warp * Np;
-  double* v = s.wv + (size_t)warp * Np;
   const int off_pp = d.alphar * (N + 1);
   for (int qp = 0; qp < d.n_qp; qp++) {
     const int mp = qp >> 1, sp = qp & 1;
     cta_build_x(d, p, qp, s.idx, s.tile);
+    {
+      const double* XFq = p.XF + (size_t)qp * N * N;
+      for (int i = tid >> 5; i < Np; i += blockDim.x >> 5) {
+        const double* rowP = XFq + (size_t)s.idx[Np + i] * N;
+        const double* rowQ = XFq + (size_t)s.idx[i] * N;
+        for (int j = tid & 31; j < Np; j += 32) {
+          e.P[i * ld + j] = rowP[s.idx[Np + j]];
+          e.Q[i * ld + j] = rowQ[s.idx[j]];
+        }
+      }
+    }
     __syncthreads();
     cta_gauss_jordan(d, s);
     if (s.iflag[F_SINGULAR]) {
       if (tid == 0 && out_status) out_status[cfgi] = ST_SINGULAR;
       return;
     }
+    // Y with the column interchanges applied (into the YQ buffer, which then swaps roles with the tile)
+    for (int a = tid >> 5; a < Np; a += blockDim.x >> 5)
+      for (int b = tid & 31; b < Np; b += 32) e.YQ[a * ld + b] = s.tile[a * ld + s.perm[b]];
+    __syncthreads();
+    double* const Yt = e.YQ;
+    double* const YQb = s.tile;
     const double pfq = (double)d.pf_sign * s.dsc[D_DET];
     const cplx cw = psi_wo_pf(d, t, s.rbm[qp], s.sgn[mp], qp);
     if (tid == 0) {
@@ -168,8 +179,13 @@ __global__ void __launch_bounds__(256)
       s.psi[2 * qp] = cw.re * pfq;
       s.psi[2 * qp + 1] = cw.im * pfq;
     }
-    // local energy: exchange ratios of the antiparallel bonds (calc_phys_quantity.f90:347-373)
-    for (int b = warp; b < nap; b += nwarps) {
+    // local energy: exchange ratios of the antiparallel bonds (calc_phys_quantity.f90:347-373) for all
+    // bonds at once.  With u_b = P(db,:) + du e_db, v_b = Q(:,ua) + dv e_ua (du = c - P(db,db),
+    // dv = c - Q(ua,ua), c = XF(d_db, u_ua)), the entries of u^T Y, Y v and u^T Y v that the ratio
+    // needs are (PY)(db,ua), (YQ)(db,ua), (P YQ)(db,ua) and Y(db,ua).
+    cta_gemm(Np, ld, Yt, e.Q, YQb);
+    __syncthreads();
+    for (int b = tid; b < nap; b += blockDim.x) {
       const int i1 = e.ap[2 * b], i2 = e.ap[2 * b + 1];
       const int i3 = s.cfg[i1], i4 = s.cfg[i2];
       int ua, db, s_up, s_dn;
@@ -184,24 +200,33 @@ __global__ void __launch_bounds__(256)
         s_up = i2;
         s_dn = i1;
       }
-      double R = warp_ratio_tile<KPL>(d, p, s.tile, qp, s.idx, ua, db, s_up, s_dn, u, v);
-      if (lane == 0) {
-        // theta' for this projection (update_theta on the qp's alphar slots) and the cosh product
-        const int s_sign = sp == 0 ? 1 : -1;
-        const int iw1 = t.wmap[(size_t)mp * N + i1], iw2 = t.wmap[(size_t)mp * N + i2];
-        double r = 1.0;
-        for (int f = 0; f < d.alphar; f++) {
-          double th = s.th[qp * d.alphar + f];
-          th = th - 2.0 * p.Wr[(size_t)f * N + iw1] * (double)s.x[i1] * (double)s_sign;
-          th = th - 2.0 * p.Wr[(size_t)f * N + iw2] * (double)s.x[i2] * (double)s_sign;
-          r = r * cosh(th);
-        }
-        int sg = -s.sgn[mp] * (t.subB[i1] ? -1 : 1) * (t.subB[i2] ? -1 : 1);
-        cplx cb = psi_wo_pf(d, t, r, sg, qp);
-        double pn = R * pfq;
-        e.psib[2 * b] += cb.re * pn;
-        e.psib[2 * b + 1] += cb.im * pn;
+      const double c = p.XF[((size_t)qp * N + s_dn) * N + s_up];
+      const double du = c - e.P[db * ld + db], dv = c - e.Q[ua * ld + ua];
+      double py = 0.0, pyq = 0.0;
+      for (int j = 0; j < Np; j++) {
+        const double pj = e.P[db * ld + j];
+        py = fma(pj, Yt[j * ld + ua], py);
+        pyq = fma(pj, YQb[j * ld + ua], pyq);
       }
+      const double y = Yt[db * ld + ua], yq = YQb[db * ld + ua];
+      const double ra = py + du * y, sb = yq + dv * y;
+      const double wv = pyq + du * yq + dv * py + du * dv * y;
+      const double R = ra * sb - y * (wv - c);
+      // theta' for this projection (update_theta on the qp's alphar slots) and the cosh product
+      const int s_sign = sp == 0 ? 1 : -1;
+      const int iw1 = t.wmap[(size_t)mp * N + i1], iw2 = t.wmap[(size_t)mp * N + i2];
+      double r = 1.0;
+      for (int f = 0; f < d.alphar; f++) {
+        double th = s.th[qp * d.alphar + f];
+        th = th - 2.0 * p.Wr[(size_t)f * N + iw1] * (double)s.x[i1] * (double)s_sign;
+        th = th - 2.0 * p.Wr[(size_t)f * N + iw2] * (double)s.x[i2] * (double)s_sign;
+        r = r * cosh(th);
+      }
+      const int sg = -s.sgn[mp] * (t.subB[i1] ? -1 : 1) * (t.subB[i2] ? -1 : 1);
+      const cplx cb = psi_wo_pf(d, t, r, sg, qp);
+      const double pn = R * pfq;
+      e.psib[2 * b] += cb.re * pn;
+      e.psib[2 * b + 1] += cb.im * pn;
     }
     // d Pf / d f_k scatter (slater.f90:140-167, block form)
     if (Orow) {
@@ -209,7 +234,7 @@ __global__ void __launch_bounds__(256)
       const double cc = pfq * d.sp_cc[sp] * cw.re, ss = pfq * d.sp_ss[sp] * cw.re;
       for (int pr = tid; pr < Np * Np; pr += blockDim.x) {
         const int i = pr / Np, j = pr - i * Np;  // i: up electron, j: down electron
-        const double y = s.tile[j * ld + i];    // Y(j, i) = (M^-1)(Np+j, i)
+        const double y = Yt[j * ld + i];        // Y(j, i) = (M^-1)(Np+j, i)
         const int tu = wm[s.idx[i]], td = wm[s.idx[Np + j]];
         double* o1 = Orow + off_pp + t.orb[(size_t)tu * N + td];
         double* o2 = Orow + off_pp + t.orb[(size_t)td * N + tu];
@@ -299,11 +324,12 @@ __global__ void advance_rng_kernel(uint32_t* mt, const int* nap, int ns, int nw,
 }  // namespace
 
 size_t rbmpp_estimator_smem(const DevDims& d, int threads) { return est_layout(d, threads / 32, nullptr, nullptr, nullptr); }
+static const int kEstThreads = 512;
 
 cudaError_t rbmpp_launch_estimator(const DevDims& d, const DevTables& t, const DevParams& p, const int8_t* xs, int n,
                                    double* out_psi, double* out_hpsi, double* O, int* out_nap, int* out_status,
                                    int reweight, cudaStream_t st) {
-  const int threads = 256;
+  const int threads = kEstThreads;
   size_t smem = rbmpp_estimator_smem(d, threads);
   int kpl = (d.Np + 31) / 32;
 #define LAUNCH(K)                                                                                          \

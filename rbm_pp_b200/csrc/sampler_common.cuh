@@ -37,12 +37,12 @@ __device__ __forceinline__ void cta_scratch_all(const SCtx& c, const int* idx, d
     double* Yq = c.Yw + (size_t)qp * Np * Np;
     if (diff) {  // make_sample.f90:106-113
       double mx = 0.0, md = 0.0;
-      for (int e = tid; e < Np * Np; e += blockDim.x) {
-        int a = e / Np, b = e - a * Np;
-        double nv = s.tile[a * ld + b];
-        mx = fmax(mx, fabs(nv));
-        md = fmax(md, fabs(Yq[e] - nv));
-      }
+      for (int a = tid >> 5; a < Np; a += blockDim.x >> 5)
+        for (int b = tid & 31; b < Np; b += 32) {
+          const double nv = s.tile[a * ld + s.perm[b]];
+          mx = fmax(mx, fabs(nv));
+          md = fmax(md, fabs(Yq[a * Np + b] - nv));
+        }
       mx = warp_max(mx);
       md = warp_max(md);
       if ((tid & 31) == 0) {
@@ -60,10 +60,8 @@ __device__ __forceinline__ void cta_scratch_all(const SCtx& c, const int* idx, d
       }
     }
     if (write_y)
-      for (int e = tid; e < Np * Np; e += blockDim.x) {
-        int a = e / Np, b = e - a * Np;
-        Yq[e] = s.tile[a * ld + b];
-      }
+      for (int a = tid >> 5; a < Np; a += blockDim.x >> 5)
+        for (int b = tid & 31; b < Np; b += 32) Yq[a * Np + b] = s.tile[a * ld + s.perm[b]];
     if (tid == 0) pf_out[qp] = (double)d.pf_sign * s.dsc[D_DET];
     __syncthreads();
   }

@@ -488,7 +488,6 @@ __global__ void __launch_bounds__(kWarps * 32, 1)
       if (s.iflag[F_AUX]) make_initial_x(c);
     }
   }
-  const Move none{0, 0, 0, 0};
   int naccept = 0, nacc_tmp = 0, nacc_all = 0;
   for (int i0 = -d.nwarm; i0 <= d.ns && !status(c); i0++) {
     if (nacc_tmp > nfastup) {

@@ -53,6 +53,7 @@ struct WS {
 #define D_PSIPI 5
 #define D_DIFFINV 6
 #define D_DIFFPF 7
+#define D_PIVOT 8
 
 __host__ __device__ __forceinline__ size_t align16(size_t v) { return (v + 15) & ~(size_t)15; }
 
@@ -195,22 +196,23 @@ __device__ __forceinline__ void cta_sign_pp(const DevDims& d, const DevTables& t
 
 // X(i, j) = XF(u_i, d_j) for the current labelling into the padded tile (rows: up electrons).
 __device__ __forceinline__ void cta_build_x(const DevDims& d, const DevParams& p, int qp, const int* idx, double* tile) {
-  const int Np = d.Np, ld = Np + 1;
+  const int Np = d.Np, ld = Np + 1, warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
   const double* XFq = p.XF + (size_t)qp * d.N * d.N;
-  for (int e = threadIdx.x; e < Np * Np; e += blockDim.x) {
-    int i = e / Np, j = e - i * Np;
-    tile[i * ld + j] = XFq[(size_t)idx[i] * d.N + idx[Np + j]];
+  for (int i = warp; i < Np; i += nwarps) {
+    const double* row = XFq + (size_t)idx[i] * d.N;
+    for (int j = lane; j < Np; j += 32) tile[i * ld + j] = row[idx[Np + j]];
   }
 }
 
 // In-place Gauss-Jordan inverse with partial pivoting of the Np x Np tile (the role of
 // dgetrf/dgetri, matrix.f90:155-177) and its determinant (-> Pf through the block identity; the role
-// of dskpfa, matrix.f90:133-151).  After the call the tile holds Y = X^{-1}; dsc[D_DET] = det(X).
-// Sets iflag[F_SINGULAR] when a zero pivot is met.  All threads of the CTA must call it.
+// of dskpfa, matrix.f90:133-151).  After the call column b of Y = X^{-1} is column s.perm[b] of the
+// tile (the row interchanges are not undone in place); dsc[D_DET] = det(X).  Sets iflag[F_SINGULAR]
+// when a zero pivot is met.  All threads of the CTA must call it.
 __device__ __forceinline__ void cta_gauss_jordan(const DevDims& d, const WS& s) {
   const int n = d.Np, ld = n + 1;
   double* T = s.tile;
-  const int tid = threadIdx.x, nt = blockDim.x, warp = tid >> 5, lane = tid & 31;
+  const int tid = threadIdx.x, nt = blockDim.x, warp = tid >> 5, lane = tid & 31, nwarps = nt >> 5;
   if (tid == 0) {
     s.dsc[D_DET] = 1.0;
     s.iflag[F_SINGULAR] = 0;
@@ -238,6 +240,8 @@ __device__ __forceinline__ void cta_gauss_jordan(const DevDims& d, const WS& s) 
       if (lane == 0) {
         s.iflag[F_PIV] = bi;
         s.dsc[D_PVAL] = best;
+        s.dsc[D_PIVOT] = T[bi * ld + k];
+        s.perm[k] = bi;
       }
     }
     __syncthreads();
@@ -250,42 +254,41 @@ __device__ __forceinline__ void cta_gauss_jordan(const DevDims& d, const WS& s) 
       __syncthreads();
       return;
     }
-    if (piv != k)
-      for (int j = tid; j < n; j += nt) {
-        double a = T[k * ld + j];
-        T[k * ld + j] = T[piv * ld + j];
-        T[piv * ld + j] = a;
-      }
-    if (tid == 0) s.perm[k] = piv;
-    __syncthreads();
-    const double pivot = T[k * ld + k];
+    // pivot row (after the interchange) scaled, pivot column saved
+    const double pivot = s.dsc[D_PIVOT];
     for (int j = tid; j < n; j += nt) {
-      s.rowbuf[j] = T[k * ld + j] / pivot;
-      s.colbuf[j] = T[j * ld + k];
+      const double rk = T[piv * ld + j], ck = T[j * ld + k];
+      if (piv != k) T[piv * ld + j] = T[k * ld + j];  // interchange rows k and piv
+      s.rowbuf[j] = rk / pivot;
+      s.colbuf[j] = (j == piv) ? T[k * ld + k] : ck;  // column k after the interchange
     }
     if (tid == 0) s.dsc[D_DET] = (piv != k ? -s.dsc[D_DET] : s.dsc[D_DET]) * pivot;
     __syncthreads();
-    for (int e = tid; e < n * n; e += nt) {
-      int i = e / n, j = e - i * n;
-      double v;
-      if (i == k) v = (j == k) ? 1.0 / pivot : s.rowbuf[j];
-      else if (j == k) v = -s.colbuf[i] / pivot;
-      else v = T[i * ld + j] - s.colbuf[i] * s.rowbuf[j];
-      T[i * ld + j] = v;
+    for (int i = warp; i < n; i += nwarps) {
+      const double ci = s.colbuf[i];
+      for (int j = lane; j < n; j += 32) {
+        double v;
+        if (i == k) v = (j == k) ? 1.0 / pivot : s.rowbuf[j];
+        else if (j == k) v = -ci / pivot;
+        else v = T[i * ld + j] - ci * s.rowbuf[j];
+        T[i * ld + j] = v;
+      }
     }
     __syncthreads();
   }
-  // undo the row interchanges on the columns of the inverse
-  for (int k = n - 1; k >= 0; k--) {
-    int pk = s.perm[k];
-    if (pk != k)
-      for (int i = tid; i < n; i += nt) {
-        double a = T[i * ld + k];
-        T[i * ld + k] = T[i * ld + pk];
-        T[i * ld + pk] = a;
-      }
-    __syncthreads();
+  // column b of the inverse is column src(b) of the tile: compose the interchanges in reverse order
+  if (tid == 0) {
+    int src[RBMPP_MAX_N / 2];
+    for (int b = 0; b < n; b++) src[b] = b;
+    for (int k = n - 1; k >= 0; k--) {
+      const int pk = s.perm[k];
+      const int a = src[k];
+      src[k] = src[pk];
+      src[pk] = a;
+    }
+    for (int b = 0; b < n; b++) s.perm[b] = src[b];
   }
+  __syncthreads();
 }
 
 // RBM cosh products per projection for theta vector th (sub.f90:42-46)
