@@ -1,13 +1,14 @@
 // estimator.cu -- per-configuration estimators (calc_phys_quantity.f90:20-246, 250-302, 306-427) and
-// the adjoint O_k kernel: one CTA per configuration.
+// the adjoint O_k kernel: one CTA per configuration, one warp per Pfaffian projection.
 //
-// For each projection qp the CTA inverts X from scratch in shared memory (the role of calculate_MAll,
-// calc_phys_quantity.f90:85), then
-//   * evaluates the exchange ratio of every antiparallel J1/J2 bond against that inverse
-//     (calc_local_energy_correlation, calc_phys_quantity.f90:338-374), one warp per bond;
-//   * scatters d Pf / d f_k (calculate_derivative_Pfaffian, slater.f90:94-170) times psi_wo_pf into
-//     the configuration's O row (plain read-add-write: for one projection Orbital_Idx maps distinct
-//     electron pairs to distinct parameters when it is injective; atomics otherwise).
+// Each warp owns a padded shared-memory tile and, for its projections qp, inverts X from scratch with
+// warp-level Gauss-Jordan (the role of calculate_MAll, calc_phys_quantity.f90:85), then evaluates the
+// exchange ratio of every antiparallel J1/J2 bond (calc_local_energy_correlation,
+// calc_phys_quantity.f90:338-374) against that inverse.  Bonds are grouped by their up electron ua:
+// with v_ua(i) = XF(u_i, u_ua) and W = Y v_ua (one mat-vec per ua), a bond (ua, db) needs only
+//     r_a = u.Y(:,ua),  s_b = W(db) + dv Y(db,ua),  u^T Y v = u.W + dv r_a,  dv = c - XF(u_ua, u_ua),
+// so the Np^2 work is per up electron, not per bond.  After each round of projections the CTA
+// scatters d Pf / d f_k (calculate_derivative_Pfaffian, slater.f90:94-170) in projection order.
 // The RBM part of O_k (calc_phys_quantity.f90:165-201) is a gather over the inverse translation
 // tables.  Outputs are the raw psi, H psi and d psi/d theta_k, optionally reweighted by
 // 1/(|psi| + shift) as calc_phys_quantity.f90:102-109,221 do.
@@ -15,85 +16,178 @@
 
 namespace {
 
-struct EstShared {
-  int* ap;        // [4N][2] antiparallel bonds (i1, i2)
-  double* apc;    // [4N]    2 J sgn
-  double* psib;   // [4N][2] psi(x') accumulators
-  int* nap;       // [1]
-  double* diag;   // [1]     sum J x x
-  double* P;      // [Np][Np+1]  P(e, j) = XF(d_e, d_j)   (down-down gathers)
-  double* Q;      // [Np][Np+1]  Q(i, a) = XF(u_i, u_a)   (up-up gathers)
-  double* YQ;     // [Np][Np+1]  Y Q
+constexpr int kEstThreads = 256;
+constexpr int kEstWarps = kEstThreads / 32;
+
+struct Est {
+  int* ap;       // [4N][2] antiparallel bonds (i1, i2) in bond_map order
+  double* apc;   // [4N]    2 J sgn
+  int* bua;      // [4N]    up electron of the bond
+  int* bdb;      // [4N]    down electron (local index) of the bond
+  int* order;    // [4N]    bonds sorted by ua
+  int* ustart;   // [Np+1]  CSR offsets into order
+  double* psib;  // [kEstWarps][4N] per-warp partial psi(x') (real projection weights)
+  double* tiles; // [nqw][Np*(Np+1)]
+  int* perm;     // [kEstWarps][Np] column map of each warp's inverse
+  double* W;     // [kEstWarps][Np]
+  double* vp;    // [kEstWarps][Np]  v_ua stored at the tile's column positions
+  double* pfw;   // [n_qp] Pf per projection
+  int* nap;
+  double* diag;
+  int nqw;
 };
 
-__host__ __device__ __forceinline__ size_t est_layout(const DevDims& d, int nwarps, char* base, WS* w, EstShared* e) {
-  size_t off = ws_layout(d, nwarps, base, w);
+__host__ __device__ __forceinline__ size_t est_layout(const DevDims& d, int nqw, char* base, WS* w, Est* e) {
+  size_t off = 0;
   auto take = [&](size_t bytes) -> char* {
     char* p = base ? base + off : nullptr;
     off = align16(off + bytes);
     return p;
   };
-  EstShared t;
-  t.ap = (int*)take((size_t)4 * d.N * 2 * 4);
-  t.apc = (double*)take((size_t)4 * d.N * 8);
-  t.psib = (double*)take((size_t)4 * d.N * 16);
-  t.nap = (int*)take(16);
-  t.diag = (double*)take(16);
-  const size_t tb = (size_t)d.Np * (d.Np + 1) * 8;
-  t.P = (double*)take(tb);
-  t.Q = (double*)take(tb);
-  t.YQ = (double*)take(tb);
-  if (e) *e = t;
+  const int N = d.N, Np = d.Np, NB = 4 * N;
+  WS t;
+  t.mt = nullptr;
+  t.x = (int*)take(N * 4);
+  t.idx = (int*)take(N * 4);
+  t.cfg = (int*)take(N * 4);
+  t.x2 = t.idx2 = t.cfg2 = nullptr;
+  t.th = (double*)take((size_t)d.Mr * 8);
+  t.thp = nullptr;
+  t.sgn = (int*)take(d.n_mp * 4);
+  t.sgnp = nullptr;
+  t.pb = (int*)take(d.n_mp * 4);
+  t.pf = nullptr;
+  t.pfp = nullptr;
+  t.psi = (double*)take((size_t)d.n_qp * 16);
+  t.psip = nullptr;
+  t.rbm = (double*)take((size_t)d.n_qp * 8);
+  t.colbuf = t.rowbuf = nullptr;
+  t.perm = nullptr;
+  t.wA = t.wS = nullptr;
+  t.red = (double*)take(64 * 8);
+  t.iflag = (int*)take(32 * 4);
+  t.dsc = (double*)take(32 * 8);
+  Est x;
+  x.ap = (int*)take((size_t)NB * 2 * 4);
+  x.apc = (double*)take((size_t)NB * 8);
+  x.bua = (int*)take((size_t)NB * 4);
+  x.bdb = (int*)take((size_t)NB * 4);
+  x.order = (int*)take((size_t)NB * 4);
+  x.ustart = (int*)take((size_t)(Np + 1) * 4);
+  x.psib = (double*)take((size_t)kEstWarps * NB * 8);
+  x.perm = (int*)take((size_t)kEstWarps * Np * 4);
+  x.W = (double*)take((size_t)kEstWarps * Np * 8);
+  x.vp = (double*)take((size_t)kEstWarps * Np * 8);
+  x.pfw = (double*)take((size_t)d.n_qp * 8);
+  x.nap = (int*)take(16);
+  x.diag = (double*)take(16);
+  const size_t tile = (size_t)Np * (Np + 1) * 8;
+  size_t tiles_bytes = (size_t)nqw * tile;
+  const size_t signbuf = (size_t)kEstWarps * N * 4;  // sign_PP scratch reuses the tile area
+  if (tiles_bytes < signbuf) tiles_bytes = signbuf;
+  x.tiles = (double*)take(tiles_bytes);
+  x.nqw = nqw;
+  t.tile = x.tiles;
+  t.wu = x.tiles;  // per-warp N-int buffers of cta_sign_pp (used before the projection loop)
+  t.wv = nullptr;
+  if (w) *w = t;
+  if (e) *e = x;
   return off;
 }
 
-// C = A B for n x n row-major shared-memory matrices with leading dimension ld (rows of 2, interleaved
-// columns so that a warp reads consecutive columns of B)
-__device__ __forceinline__ void cta_gemm(int n, int ld, const double* A, const double* B, double* C) {
-  const int nr = (n + 1) / 2, nc = (n + 3) / 4;
-  for (int blk = threadIdx.x; blk < nr * nc; blk += blockDim.x) {
-    const int bi = blk / nc, bj = blk - bi * nc;
-    const int i0 = 2 * bi;
-    double acc[2][4];
-#pragma unroll
-    for (int r = 0; r < 2; r++)
-#pragma unroll
-      for (int q = 0; q < 4; q++) acc[r][q] = 0.0;
-    const bool r1ok = i0 + 1 < n;
-#pragma unroll 2
-    for (int k = 0; k < n; k++) {
-      const double a0 = A[i0 * ld + k], a1 = r1ok ? A[(i0 + 1) * ld + k] : 0.0;
-#pragma unroll
-      for (int q = 0; q < 4; q++) {
-        const int j = bj + q * nc;
-        const double b = (j < n) ? B[k * ld + j] : 0.0;
-        acc[0][q] = fma(a0, b, acc[0][q]);
-        acc[1][q] = fma(a1, b, acc[1][q]);
+// Warp-level Gauss-Jordan inverse with partial pivoting (the role of dgetrf/dgetri, matrix.f90:155-177)
+// of the n x n tile T (leading dimension ld).  Returns det(X) (0 and singular=true on a zero pivot).
+// Column b of X^{-1} is column src[b] of T afterwards (src written to perm).
+template <int KPL>
+__device__ __forceinline__ double warp_gauss_jordan(double* T, int n, int ld, int* perm, bool& singular) {
+  const int lane = threadIdx.x & 31;
+  double det = 1.0;
+  singular = false;
+  for (int k = 0; k < n; k++) {
+    double best = -1.0;
+    int bi = k;
+    for (int i = k + lane; i < n; i += 32) {
+      const double v = fabs(T[i * ld + k]);
+      if (v > best) {
+        best = v;
+        bi = i;
       }
     }
 #pragma unroll
-    for (int q = 0; q < 4; q++) {
-      const int j = bj + q * nc;
+    for (int o = 16; o > 0; o >>= 1) {
+      const double ob = __shfl_xor_sync(0xffffffffu, best, o);
+      const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+      if (ob > best || (ob == best && oi < bi)) {
+        best = ob;
+        bi = oi;
+      }
+    }
+    if (!(best > 0.0)) {
+      singular = true;
+      return 0.0;
+    }
+    const double pivot = T[bi * ld + k];
+    if (lane == 0) perm[k] = bi;
+    __syncwarp();
+    double r[KPL];
+#pragma unroll
+    for (int q = 0; q < KPL; q++) {
+      const int j = lane + 32 * q;
+      r[q] = 0.0;
       if (j < n) {
-        C[i0 * ld + j] = acc[0][q];
-        if (r1ok) C[(i0 + 1) * ld + j] = acc[1][q];
+        const double a = T[k * ld + j], b = T[bi * ld + j];
+        if (bi != k) T[bi * ld + j] = a;
+        r[q] = b / pivot;
       }
     }
+    det = (bi != k ? -det : det) * pivot;
+    __syncwarp();
+    // rows i != k: T(i,j) -= T(i,k) r_j for j != k; column k and row k afterwards
+    for (int i = 0; i < n; i++) {
+      if (i == k) continue;
+      const double f = T[i * ld + k];
+#pragma unroll
+      for (int q = 0; q < KPL; q++) {
+        const int j = lane + 32 * q;
+        if (j < n && j != k) T[i * ld + j] = T[i * ld + j] - f * r[q];
+      }
+    }
+    __syncwarp();
+    for (int i = lane; i < n; i += 32)
+      if (i != k) T[i * ld + k] = -T[i * ld + k] / pivot;
+#pragma unroll
+    for (int q = 0; q < KPL; q++) {
+      const int j = lane + 32 * q;
+      if (j < n) T[k * ld + j] = (j == k) ? 1.0 / pivot : r[q];
+    }
+    __syncwarp();
   }
+  if (lane == 0) {
+    int src[RBMPP_MAX_N / 2];
+    for (int b = 0; b < n; b++) src[b] = b;
+    for (int k = n - 1; k >= 0; k--) {
+      const int pk = perm[k], a = src[k];
+      src[k] = src[pk];
+      src[pk] = a;
+    }
+    for (int b = 0; b < n; b++) perm[b] = src[b];
+  }
+  __syncwarp();
+  return det;
 }
 
 template <int KPL>
-__global__ void __launch_bounds__(512, 1)
+__global__ void __launch_bounds__(kEstThreads, 1)
     estimator_kernel(const __grid_constant__ DevDims d, const __grid_constant__ DevTables t,
                      const __grid_constant__ DevParams p, const int8_t* xs, int n, double* out_psi, double* out_hpsi,
-                     double* O, int* out_nap, int* out_status, int reweight) {
+                     double* O, int* out_nap, int* out_status, int reweight, int nqw) {
   extern __shared__ __align__(16) char smem[];
   __shared__ WS s;
-  __shared__ EstShared e;
-  if (threadIdx.x == 0) est_layout(d, blockDim.x >> 5, smem, &s, &e);
+  __shared__ Est e;
+  if (threadIdx.x == 0) est_layout(d, nqw, smem, &s, &e);
   __syncthreads();
-  const int tid = threadIdx.x;
-  const int N = d.N, Np = d.Np, ld = Np + 1;
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
+  const int N = d.N, Np = d.Np, ld = Np + 1, NB = 4 * N;
   const int cfgi = blockIdx.x;
   if (cfgi >= n) return;
   double* Orow = O ? O + (size_t)cfgi * d.Nv : nullptr;
@@ -101,25 +195,36 @@ __global__ void __launch_bounds__(512, 1)
   for (int i = tid; i < N; i += blockDim.x) s.x[i] = (int)xs[(size_t)cfgi * N + i];
   if (Orow)
     for (int k = tid; k < d.Nv; k += blockDim.x) Orow[k] = 0.0;
+  for (int k = tid; k < kEstWarps * NB; k += blockDim.x) e.psib[k] = 0.0;
   if (tid == 0) s.iflag[F_STATUS] = 0;
   __syncthreads();
   if (tid == 0) {
     int st = x_to_ele(d, s.x, s.idx, s.cfg);
     if (st) s.iflag[F_STATUS] = st;
-    // bond list (bond_map, calc_phys_quantity.f90:382-427) and the diagonal part
+    // bond list (bond_map, calc_phys_quantity.f90:382-427), diagonal part, CSR by up electron
     int na = 0;
     double dg = 0.0;
-    for (int b = 0; b < 4 * N; b++) {
-      int i1 = t.bonds[2 * b], i2 = t.bonds[2 * b + 1];
-      double J = (b < 2 * N) ? d.J1 : d.J2, sg = (b < 2 * N) ? -1.0 : 1.0;
+    for (int a = 0; a <= Np; a++) e.ustart[a] = 0;
+    for (int b = 0; b < NB && !st; b++) {
+      const int i1 = t.bonds[2 * b], i2 = t.bonds[2 * b + 1];
+      const double J = (b < 2 * N) ? d.J1 : d.J2, sg = (b < 2 * N) ? -1.0 : 1.0;
       dg = dg + J * (double)s.x[i1] * (double)s.x[i2];
       if (s.x[i1] != s.x[i2]) {
+        const int i3 = s.cfg[i1], i4 = s.cfg[i2];
+        const int ua = (s.x[i1] == 1) ? i3 : i4, db = ((s.x[i1] == 1) ? i4 : i3) - Np;
         e.ap[2 * na] = i1;
         e.ap[2 * na + 1] = i2;
         e.apc[na] = 2.0 * J * sg;
+        e.bua[na] = ua;
+        e.bdb[na] = db;
+        e.ustart[ua + 1]++;
         na++;
       }
     }
+    for (int a = 0; a < Np; a++) e.ustart[a + 1] += e.ustart[a];
+    int fill[RBMPP_MAX_N / 2];
+    for (int a = 0; a < Np; a++) fill[a] = e.ustart[a];
+    for (int b = 0; b < na; b++) e.order[fill[e.bua[b]]++] = b;
     e.nap[0] = na;
     e.diag[0] = dg;
   }
@@ -129,10 +234,6 @@ __global__ void __launch_bounds__(512, 1)
     return;
   }
   const int nap = e.nap[0];
-  for (int b = tid; b < nap; b += blockDim.x) {
-    e.psib[2 * b] = 0.0;
-    e.psib[2 * b + 1] = 0.0;
-  }
   cta_calc_theta(d, t, p, s.x, s.th);
   cta_sign_pp(d, t, s, s.idx, s.sgn);
   __syncthreads();
@@ -146,108 +247,130 @@ __global__ void __launch_bounds__(512, 1)
     return;
   }
   const int off_pp = d.alphar * (N + 1);
-  for (int qp = 0; qp < d.n_qp; qp++) {
-    const int mp = qp >> 1, sp = qp & 1;
-    cta_build_x(d, p, qp, s.idx, s.tile);
-    {
+  double* psib = e.psib + (size_t)warp * NB;
+  int* src = e.perm + (size_t)warp * Np;
+  double* Wv = e.W + (size_t)warp * Np;
+  double* vp = e.vp + (size_t)warp * Np;
+  bool bad = false;
+  // rounds of nqw projections: warp w < nqw handles qp = round*nqw + w
+  for (int q0 = 0; q0 < d.n_qp; q0 += e.nqw) {
+    const int qp = q0 + warp;
+    double* T = e.tiles + (size_t)warp * Np * ld;
+    if (warp < e.nqw && qp < d.n_qp) {
+      const int mp = qp >> 1, sp = qp & 1;
       const double* XFq = p.XF + (size_t)qp * N * N;
-      for (int i = tid >> 5; i < Np; i += blockDim.x >> 5) {
-        const double* rowP = XFq + (size_t)s.idx[Np + i] * N;
-        const double* rowQ = XFq + (size_t)s.idx[i] * N;
-        for (int j = tid & 31; j < Np; j += 32) {
-          e.P[i * ld + j] = rowP[s.idx[Np + j]];
-          e.Q[i * ld + j] = rowQ[s.idx[j]];
+      const double* XFTq = p.XFT + (size_t)qp * N * N;
+      for (int i = 0; i < Np; i++) {
+        const double* row = XFq + (size_t)s.idx[i] * N;
+        for (int j = lane; j < Np; j += 32) T[i * ld + j] = row[s.idx[Np + j]];
+      }
+      __syncwarp();
+      bool sing;
+      const double det = warp_gauss_jordan<KPL>(T, Np, ld, src, sing);
+      if (sing) bad = true;
+      const double pfq = (double)d.pf_sign * det;
+      const cplx cw = psi_wo_pf(d, t, s.rbm[qp], s.sgn[mp], qp);
+      if (lane == 0) {
+        e.pfw[qp] = pfq;
+        s.psi[2 * qp] = cw.re * pfq;
+        s.psi[2 * qp + 1] = cw.im * pfq;
+      }
+      // exchange ratios, grouped by up electron
+      for (int ua = 0; ua < Np && !sing; ua++) {
+        const int b0 = e.ustart[ua], b1 = e.ustart[ua + 1];
+        if (b0 == b1) continue;
+        const int s_up = s.idx[ua];
+        const int cu = src[ua];
+        // v_ua(i) = XF(u_i, s_up) at the tile's column positions, W = Y v_ua (lane <-> row)
+        for (int i = lane; i < Np; i += 32) vp[src[i]] = XFTq[(size_t)s_up * N + s.idx[i]];
+        __syncwarp();
+        for (int j = lane; j < Np; j += 32) {
+          double a = 0.0;
+#pragma unroll 5
+          for (int k = 0; k < Np; k++) a = fma(T[j * ld + k], vp[k], a);
+          Wv[j] = a;
         }
+        __syncwarp();
+        const double xfuu = XFq[(size_t)s_up * N + s_up];
+        for (int bb = b0; bb < b1; bb++) {
+          const int b = e.order[bb];
+          const int db = e.bdb[b];
+          const int s_dn = s.idx[Np + db];
+          const double c = XFq[(size_t)s_dn * N + s_up];
+          double ra = 0.0, uw = 0.0;
+#pragma unroll
+          for (int q = 0; q < KPL; q++) {
+            const int j = lane + 32 * q;
+            if (j < Np) {
+              const double uj = (j == db) ? c : XFq[(size_t)s_dn * N + s.idx[Np + j]];
+              ra = fma(uj, T[j * ld + cu], ra);
+              uw = fma(uj, Wv[j], uw);
+            }
+          }
+          ra = warp_sum(ra);
+          uw = warp_sum(uw);
+          const double dv = c - xfuu;
+          const double y = T[db * ld + cu];
+          const double sb = Wv[db] + dv * y;
+          const double wv = uw + dv * ra;
+          const double R = ra * sb - y * (wv - c);
+          // cosh product of theta' for this projection (update_theta on the qp's alphar slots)
+          const int i1 = e.ap[2 * b], i2 = e.ap[2 * b + 1];
+          const int iw1 = t.wmap[(size_t)mp * N + i1], iw2 = t.wmap[(size_t)mp * N + i2];
+          const double s_sign = sp == 0 ? 1.0 : -1.0;
+          double ch = 1.0;
+          for (int f = lane; f < d.alphar; f += 32) {
+            double th = s.th[qp * d.alphar + f];
+            th = th - 2.0 * p.Wr[(size_t)f * N + iw1] * (double)s.x[i1] * s_sign;
+            th = th - 2.0 * p.Wr[(size_t)f * N + iw2] * (double)s.x[i2] * s_sign;
+            ch = ch * cosh(th);
+          }
+#pragma unroll
+          for (int o = 16; o > 0; o >>= 1) ch = ch * __shfl_xor_sync(0xffffffffu, ch, o);
+          if (lane == 0) {
+            const int sg = -s.sgn[mp] * (t.subB[i1] ? -1 : 1) * (t.subB[i2] ? -1 : 1);
+            const cplx cb = psi_wo_pf(d, t, ch, sg, qp);
+            psib[b] += cb.re * (R * pfq);
+          }
+        }
+        __syncwarp();
       }
     }
     __syncthreads();
-    cta_gauss_jordan(d, s);
-    if (s.iflag[F_SINGULAR]) {
-      if (tid == 0 && out_status) out_status[cfgi] = ST_SINGULAR;
-      return;
-    }
-    // Y with the column interchanges applied (into the YQ buffer, which then swaps roles with the tile)
-    for (int a = tid >> 5; a < Np; a += blockDim.x >> 5)
-      for (int b = tid & 31; b < Np; b += 32) e.YQ[a * ld + b] = s.tile[a * ld + s.perm[b]];
-    __syncthreads();
-    double* const Yt = e.YQ;
-    double* const YQb = s.tile;
-    const double pfq = (double)d.pf_sign * s.dsc[D_DET];
-    const cplx cw = psi_wo_pf(d, t, s.rbm[qp], s.sgn[mp], qp);
-    if (tid == 0) {
-      s.pf[qp] = pfq;
-      s.psi[2 * qp] = cw.re * pfq;
-      s.psi[2 * qp + 1] = cw.im * pfq;
-    }
-    // local energy: exchange ratios of the antiparallel bonds (calc_phys_quantity.f90:347-373) for all
-    // bonds at once.  With u_b = P(db,:) + du e_db, v_b = Q(:,ua) + dv e_ua (du = c - P(db,db),
-    // dv = c - Q(ua,ua), c = XF(d_db, u_ua)), the entries of u^T Y, Y v and u^T Y v that the ratio
-    // needs are (PY)(db,ua), (YQ)(db,ua), (P YQ)(db,ua) and Y(db,ua).
-    cta_gemm(Np, ld, Yt, e.Q, YQb);
-    __syncthreads();
-    for (int b = tid; b < nap; b += blockDim.x) {
-      const int i1 = e.ap[2 * b], i2 = e.ap[2 * b + 1];
-      const int i3 = s.cfg[i1], i4 = s.cfg[i2];
-      int ua, db, s_up, s_dn;
-      if (s.x[i1] == 1) {
-        ua = i3;
-        db = i4 - Np;
-        s_up = i1;
-        s_dn = i2;
-      } else {
-        ua = i4;
-        db = i3 - Np;
-        s_up = i2;
-        s_dn = i1;
-      }
-      const double c = p.XF[((size_t)qp * N + s_dn) * N + s_up];
-      const double du = c - e.P[db * ld + db], dv = c - e.Q[ua * ld + ua];
-      double py = 0.0, pyq = 0.0;
-      for (int j = 0; j < Np; j++) {
-        const double pj = e.P[db * ld + j];
-        py = fma(pj, Yt[j * ld + ua], py);
-        pyq = fma(pj, YQb[j * ld + ua], pyq);
-      }
-      const double y = Yt[db * ld + ua], yq = YQb[db * ld + ua];
-      const double ra = py + du * y, sb = yq + dv * y;
-      const double wv = pyq + du * yq + dv * py + du * dv * y;
-      const double R = ra * sb - y * (wv - c);
-      // theta' for this projection (update_theta on the qp's alphar slots) and the cosh product
-      const int s_sign = sp == 0 ? 1 : -1;
-      const int iw1 = t.wmap[(size_t)mp * N + i1], iw2 = t.wmap[(size_t)mp * N + i2];
-      double r = 1.0;
-      for (int f = 0; f < d.alphar; f++) {
-        double th = s.th[qp * d.alphar + f];
-        th = th - 2.0 * p.Wr[(size_t)f * N + iw1] * (double)s.x[i1] * (double)s_sign;
-        th = th - 2.0 * p.Wr[(size_t)f * N + iw2] * (double)s.x[i2] * (double)s_sign;
-        r = r * cosh(th);
-      }
-      const int sg = -s.sgn[mp] * (t.subB[i1] ? -1 : 1) * (t.subB[i2] ? -1 : 1);
-      const cplx cb = psi_wo_pf(d, t, r, sg, qp);
-      const double pn = R * pfq;
-      e.psib[2 * b] += cb.re * pn;
-      e.psib[2 * b + 1] += cb.im * pn;
-    }
-    // d Pf / d f_k scatter (slater.f90:140-167, block form)
+    // d Pf / d f_k scatter of this round's projections, in projection order (slater.f90:140-167)
     if (Orow) {
-      const int* wm = t.wmap + (size_t)mp * N;
-      const double cc = pfq * d.sp_cc[sp] * cw.re, ss = pfq * d.sp_ss[sp] * cw.re;
-      for (int pr = tid; pr < Np * Np; pr += blockDim.x) {
-        const int i = pr / Np, j = pr - i * Np;  // i: up electron, j: down electron
-        const double y = Yt[j * ld + i];        // Y(j, i) = (M^-1)(Np+j, i)
-        const int tu = wm[s.idx[i]], td = wm[s.idx[Np + j]];
-        double* o1 = Orow + off_pp + t.orb[(size_t)tu * N + td];
-        double* o2 = Orow + off_pp + t.orb[(size_t)td * N + tu];
-        if (d.orb_injective) {
-          if (cc != 0.0) *o1 = *o1 + y * cc;
-          if (ss != 0.0) *o2 = *o2 + y * ss;
-        } else {
-          if (cc != 0.0) atomicAdd(o1, y * cc);
-          if (ss != 0.0) atomicAdd(o2, y * ss);
+      for (int w = 0; w < e.nqw && q0 + w < d.n_qp; w++) {
+        const int qp = q0 + w, mp = qp >> 1, sp = qp & 1;
+        const double* Tw = e.tiles + (size_t)w * Np * ld;
+        const int* srcw = e.perm + (size_t)w * Np;
+        const int* wm = t.wmap + (size_t)mp * N;
+        const double pfq = e.pfw[qp];
+        const cplx cw = psi_wo_pf(d, t, s.rbm[qp], s.sgn[mp], qp);
+        const double cc = pfq * d.sp_cc[sp] * cw.re, ss = pfq * d.sp_ss[sp] * cw.re;
+        for (int pr = tid; pr < Np * Np; pr += blockDim.x) {
+          const int j = pr / Np, i = pr - j * Np;  // j: down electron, i: up electron
+          const double y = Tw[j * ld + srcw[i]];  // Y(j, i) = (M^-1)(Np+j, i)
+          const int tu = wm[s.idx[i]], td = wm[s.idx[Np + j]];
+          double* o1 = Orow + off_pp + t.orb[(size_t)tu * N + td];
+          double* o2 = Orow + off_pp + t.orb[(size_t)td * N + tu];
+          if (d.orb_injective) {
+            if (cc != 0.0) *o1 = *o1 + y * cc;
+            if (ss != 0.0) *o2 = *o2 + y * ss;
+          } else {
+            if (cc != 0.0) atomicAdd(o1, y * cc);
+            if (ss != 0.0) atomicAdd(o2, y * ss);
+          }
         }
+        __syncthreads();
       }
     }
     __syncthreads();
+  }
+  if (lane == 0 && bad) s.iflag[F_STATUS] = ST_SINGULAR;
+  __syncthreads();
+  if (s.iflag[F_STATUS]) {
+    if (tid == 0 && out_status) out_status[cfgi] = s.iflag[F_STATUS];
+    return;
   }
   // psi(0), H psi
   if (tid == 0) {
@@ -260,8 +383,9 @@ __global__ void __launch_bounds__(512, 1)
     s.dsc[D_PSI0I] = im;
     double hr = e.diag[0] * re, hi = e.diag[0] * im;
     for (int b = 0; b < nap; b++) {
-      hr += e.apc[b] * e.psib[2 * b];
-      hi += e.apc[b] * e.psib[2 * b + 1];
+      double pb = 0.0;
+      for (int w = 0; w < kEstWarps; w++) pb += e.psib[(size_t)w * NB + b];
+      hr += e.apc[b] * pb;
     }
     s.dsc[D_PSIPR] = hr;
     s.dsc[D_PSIPI] = hi;
@@ -321,27 +445,39 @@ __global__ void advance_rng_kernel(uint32_t* mt, const int* nap, int ns, int nw,
   for (int k = 0; k < 625; k++) mt[(size_t)w * 625 + k] = st[k];
 }
 
+int est_tile_warps(const DevDims& d, int max_smem) {
+  for (int q = kEstWarps; q >= 1; q--)
+    if ((long long)est_layout(d, q, nullptr, nullptr, nullptr) <= max_smem) return q;
+  return 0;
+}
+
 }  // namespace
 
-size_t rbmpp_estimator_smem(const DevDims& d, int threads) { return est_layout(d, threads / 32, nullptr, nullptr, nullptr); }
-static const int kEstThreads = 512;
+size_t rbmpp_estimator_smem(const DevDims& d, int threads) {
+  (void)threads;
+  return est_layout(d, 1, nullptr, nullptr, nullptr);
+}
 
 cudaError_t rbmpp_launch_estimator(const DevDims& d, const DevTables& t, const DevParams& p, const int8_t* xs, int n,
                                    double* out_psi, double* out_hpsi, double* O, int* out_nap, int* out_status,
                                    int reweight, cudaStream_t st) {
-  const int threads = kEstThreads;
-  size_t smem = rbmpp_estimator_smem(d, threads);
+  if (n <= 0) return cudaSuccess;
+  int dev = 0, maxsm = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  const int nqw = est_tile_warps(d, maxsm);
+  if (nqw < 1) return cudaErrorInvalidValue;
+  size_t smem = est_layout(d, nqw, nullptr, nullptr, nullptr);
   int kpl = (d.Np + 31) / 32;
 #define LAUNCH(K)                                                                                          \
   do {                                                                                                     \
     cudaError_t e = cudaFuncSetAttribute(estimator_kernel<K>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
                                          (int)smem);                                                       \
     if (e != cudaSuccess) return e;                                                                        \
-    estimator_kernel<K><<<n, threads, smem, st>>>(d, t, p, xs, n, out_psi, out_hpsi, O, out_nap, out_status, \
-                                                  reweight);                                               \
+    estimator_kernel<K><<<n, kEstThreads, smem, st>>>(d, t, p, xs, n, out_psi, out_hpsi, O, out_nap,         \
+                                                      out_status, reweight, nqw);                           \
     return cudaGetLastError();                                                                             \
   } while (0)
-  if (n <= 0) return cudaSuccess;
   if (kpl <= 1) LAUNCH(1);
   if (kpl <= 2) LAUNCH(2);
   if (kpl <= 4) LAUNCH(4);
