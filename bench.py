@@ -28,9 +28,12 @@ ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, ROOT)
 
 METRIC = "MC samples/s and SR steps/s at 10x10 J2=0.5, chosen vs plain FP64, dE/site"
+# DRAM bytes (read + write) that ncu counted for one sampler_stream_kernel launch of the 1-wave 10x10
+# workload, divided by that launch's algorithmic bytes (profiles/sampler_stream_10x10_1wave.md)
+SAMPLER_TRAFFIC_PER_ALG_BYTE = 2.674e12 / 3.1765e12
 
 WORKLOADS = {
-    # translation-symmetric RBM (alpha=4, 400 hidden units per spin parity), 4096 walkers, 65536 samples
+    # 10x10 at scale: translation-symmetric RBM (alpha=4, 100 projections), 4096 walkers, 65536 samples per step
     "j1j2_10x10_trans": dict(L=10, translations=True, alphar=4, orbital="full", walkers=4096, ns=16, J2=0.5),
     # same lattice without translation projection (2 Pfaffian blocks per walker)
     "j1j2_10x10_single": dict(L=10, translations=False, alphar=4, orbital="full", walkers=4096, ns=16, J2=0.5),
@@ -191,6 +194,8 @@ def run_ours(args):
     clk = ClockSampler(torch.cuda.current_device())
     clk.start()
     step_ms, samp_ms, est_ms, sb_ms, solve_ms, acc_all, props, energies = [], [], [], [], [], [], [], []
+    refine = []
+    launches0 = ctx.kernel_launches()
     for _ in range(args.steps):
         rec = runner.step()
         st = ctx.stats()
@@ -202,10 +207,22 @@ def run_ours(args):
         acc_all.append(st["accepts_all"])
         props.append(st["proposals"])
         energies.append(rec["Etot"])
+        refine.append((rec.get("refine_iterations", 0), rec.get("refine_residual", 0.0)))
     torch.cuda.synchronize()
     if world > 1:
         torch.distributed.barrier()
     clocks = clk.stop()
+    launches = ctx.kernel_launches() - launches0
+    # the plain all-FP64 SR path on the same walkers, one step after the timed region (for "chosen vs plain")
+    plain = None
+    if args.precision == "split" and not args.no_plain:
+        runner.precision = capi.SR_FP64
+        prec_rec = runner.step()
+        st = ctx.stats()
+        plain = {"ms_per_step": prec_rec["device_ms"], "sr_steps_per_s": 1e3 / prec_rec["device_ms"],
+                 "s_build_ms": st["sbuild_ms"], "cholesky_solve_ms": st["solve_ms"],
+                 "energy_per_site": prec_rec["Etot"] / (w["L"] ** 2)}
+        runner.precision = prec
     # max over ranks of the device time per step
     t = torch.tensor([float(np.mean(step_ms))], device="cuda")
     if world > 1:
@@ -246,13 +263,18 @@ def run_ours(args):
             "energy_per_site": float(np.mean(energies)) / (w["L"] ** 2),
             "phases_ms": {"make_sample": smp, "estimator": float(np.mean(est_ms)), "s_build": float(np.mean(sb_ms)),
                           "cholesky_solve": float(np.mean(solve_ms))},
-            "roofline": {"kernel": "sampler_kernel (make_sample)", "bound": "hbm", "achieved": achieved,
+            "roofline": {"kernel": "sampler_stream_kernel (make_sample)", "bound": "hbm", "achieved": achieved,
                          "peak": peaks["hbm_gbs"], "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"],
-                         "peak_kind": peak_kind, "traffic": None,
+                         "peak_kind": peak_kind + " (burst copy)",
+                         "traffic": (alg_bytes * SAMPLER_TRAFFIC_PER_ALG_BYTE if SAMPLER_TRAFFIC_PER_ALG_BYTE
+                                     else None),
+                         "traffic_source": "ncu dram bytes / algorithmic bytes of the 1-wave capture, scaled",
                          "algorithmic_bytes": alg_bytes},
             "clocks": clocks,
             "e2e": {"value": e2e_v, "unit": "MC samples/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
-            "gpu_launches": runner.launches_per_step()}
+            "gpu_launches": launches,
+            "sr_refinement": {"iterations": [r[0] for r in refine], "residual": [r[1] for r in refine]},
+            "plain_fp64": plain}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cb = cpu_baseline(w, problem)
         line["cpu_baseline"] = {k: cb[k] for k in ("value", "unit", "cores", "kind", "sample")}
@@ -271,8 +293,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="j1j2_10x10_trans", choices=sorted(WORKLOADS))
-    ap.add_argument("--precision", default="fp64", choices=["fp64", "split"])
+    ap.add_argument("--precision", default="split", choices=["fp64", "split"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-plain", action="store_true", help="skip the extra all-FP64 comparison step")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)

@@ -12,8 +12,8 @@
  *  - Emulated MPI ranks are "walkers": walker w behaves exactly like rank w of the reference
  *    (own MT19937 stream seeded iseed0 + w, own Nfastup, Nsample/Nmpi stored samples).
  *
- * Reference-side binding: INTEGRATION.md shows the Fortran ISO_C_BINDING interface block that
- * replaces the bodies of make_sample, calc_phys_quantity_opt and the SR_pdposv include.
+ * Reference-side binding: a Fortran ISO_C_BINDING interface block over these functions replaces the
+ * bodies of make_sample, calc_phys_quantity_opt and the SR_pdposv include.
  */
 #ifndef RBMPP_H
 #define RBMPP_H
@@ -63,8 +63,10 @@ enum { RBMPP_SR_FP64 = 0, RBMPP_SR_SPLIT_BF16 = 1 };
 typedef struct {
   int iteration;      /* optimisation step (1-based)                                             */
   int precision;      /* RBMPP_SR_FP64: FP64 S build; RBMPP_SR_SPLIT_BF16: 3-term split-BF16 S on the
-                         tensor cores + FP64 Cholesky + iterative refinement against the exact S      */
-  int refine_steps;   /* refinement sweeps for RBMPP_SR_SPLIT_BF16 (2-3)                         */
+                         tensor cores + FP64 Cholesky, refined against the exact S                 */
+  int refine_steps;   /* RBMPP_SR_SPLIT_BF16: at most this many conjugate-gradient iterations on the
+                         exact FP64 S (applied through O), preconditioned by the split-precision
+                         Cholesky factor; they stop at relative residual 1e-13.  0 = no refinement */
   int reserved;
   double delta_tau;   /* RBM.input                                                               */
   double s_factor0;   /* current stabilisation factor (main.f90:439 schedule applied by caller)   */
@@ -77,15 +79,18 @@ typedef struct {
   double lambda;                     /* step norm after the 5/L scaling (SR_pdposv.f90:309)       */
   double lambda_rbm_rbm, lambda_pp_pp, lambda_rbm_pp;
   double delW_max, s_factor, sdiag_av, smat_scaling;
-  double refine_residual;            /* relative residual of the SR solve against the exact S    */
-  int kmax, k_nonzero, nSmat, reserved;
+  double refine_residual;            /* relative residual ||g - S x|| / ||g|| against the exact S
+                                        (RBMPP_SR_SPLIT_BF16 with refinement; 0 otherwise)      */
+  int kmax, k_nonzero, nSmat;
+  int refine_iterations;             /* conjugate-gradient iterations taken                       */
 } rbmpp_sr_out;
 
 /* Lifecycle -------------------------------------------------------------------------------- */
 int rbmpp_create(const rbmpp_dims* dims, rbmpp_ctx** out);
 int rbmpp_destroy(rbmpp_ctx* ctx);
 const char* rbmpp_last_error(const rbmpp_ctx* ctx);
-/* what: 0 = Nv, 1 = Nv_RBM, 2 = Mr, 3 = N_QP_Full, 4 = N, 5 = device bytes held */
+/* what: 0 = Nv, 1 = Nv_RBM, 2 = Mr, 3 = N_QP_Full, 4 = N, 5 = device bytes held,
+ * 6 = kernel launches issued by the library so far (all contexts of the process) */
 int rbmpp_query(const rbmpp_ctx* ctx, int what, long long* value);
 
 /* Tables: W_map(N, 1, N_MP_Trans) (main.f90:94-122; also MP_Trans_Idx, parameter.f90:105-109),
@@ -102,6 +107,10 @@ int rbmpp_set_params(rbmpp_ctx* ctx, const double* Wr, const double* br, const d
 int rbmpp_get_params(rbmpp_ctx* ctx, double* Wr, double* br, double* Slater, double* shift);
 /* Sets mod_main's shift alone (main.f90:451), keeping the other parameters. */
 int rbmpp_set_shift(rbmpp_ctx* ctx, double shift);
+/* Precision of S builds that happen before rbmpp_sr_step names one: rbmpp_measure with Smat != NULL and
+ * rbmpp_exchange_measurement (RBMPP_SR_FP64 default, or RBMPP_SR_SPLIT_BF16).  rbmpp_sr_step builds S
+ * in its own in->precision when no S exists yet.  Replaces the dgemm of calc_phys_quantity.f90:240. */
+int rbmpp_set_s_precision(rbmpp_ctx* ctx, int precision);
 
 /* RNG: walker w (global rank g = walker_offset + w) is seeded sgrnd(iseed0 + g) and skips
  * Nsample*g + 1 draws (main.f90:224-234). */

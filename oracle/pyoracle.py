@@ -55,6 +55,7 @@ def lib():
         L.orc_get_params.argtypes = [P, dp, dp, dp, P]
         L.orc_get_slater_elements.argtypes = [P, dp]
         L.orc_seed.argtypes = [P, C.c_int]
+        L.orc_seed_offset.argtypes = [P, C.c_int, C.c_int]
         L.orc_rank_grnd.argtypes = [P, C.c_int, C.c_int, P]
         L.orc_get_rng_state.argtypes = [P, C.c_int, up, ip]
         L.orc_get_nfastup.argtypes = [P, ip]
@@ -142,8 +143,10 @@ class Oracle:
         lib().orc_get_slater_elements(self.h, out)
         return out.reshape((2 * self.N, 2 * self.N, self.n_qp), order="F")
 
-    def seed(self, iseed0: int):
-        self._chk(lib().orc_seed(self.h, int(iseed0)))
+    def seed(self, iseed0: int, offset: int = 0):
+        """main.f90:224-234 for global ranks offset .. offset + nranks - 1."""
+        self.rank0 = int(offset)
+        self._chk(lib().orc_seed_offset(self.h, int(iseed0), int(offset)))
 
     def rank_grnd(self, rank: int, n: int):
         out = np.zeros(max(n, 1))
@@ -262,9 +265,11 @@ def max_threads():
 class VMCLoop:
     """main.f90:300-455 restated around an Oracle: one call of ``iteration`` is one SR step
     (update_slater_elements, make_sample, calc_phys_quantity_opt, MPI reductions, SR_pdposv,
-    and the s_factor0 / shift bookkeeping of main.f90:439-453)."""
+    and the s_factor0 / shift bookkeeping of main.f90:439-453).  With ``offset`` > 0 the oracle holds
+    the shard of global ranks offset.. and ``allreduce`` (called with scal6, S, g, ov) sums the
+    measurement over the shards, as the MPI_ALLREDUCE calls of main.f90:348-369 do."""
 
-    def __init__(self, orc: Oracle, problem, iseed0: int):
+    def __init__(self, orc: Oracle, problem, iseed0: int, offset: int = 0, allreduce=None):
         self.o = orc
         self.p = problem
         inp = problem.inp
@@ -272,10 +277,13 @@ class VMCLoop:
         self.wf_av_list = [0.0] * 10
         self.shift = 0.0
         self.iteration = 0
-        orc.seed(iseed0)
+        self.allreduce = allreduce
+        orc.seed(iseed0, offset)
         # initialize_parameters (parameter.f90:21-41): rank 0 draws the random RBM init, which W.input
         # (when present) then overrides.
-        u = orc.rank_grnd(0, inp.alphar * (self.o.N + 1))
+        if offset != 0 and problem.Wr is None:
+            raise OracleError("a shard without global rank 0 needs W.input (rank 0's random init is broadcast)")
+        u = orc.rank_grnd(0, inp.alphar * (self.o.N + 1)) if offset == 0 else np.zeros(inp.alphar * (self.o.N + 1))
         br = np.zeros(inp.alphar)
         Wr = np.zeros((self.o.N, inp.alphar))
         k = 0
@@ -297,15 +305,19 @@ class VMCLoop:
         self.iteration += 1
         nacc = o.make_sample(self.iteration == 1)
         m = o.measure(want_S=True)
-        ntot = o.nsample * o.nranks
-        accept_ratio = float(nacc.sum()) / ntot / o.N
-        wf_av = m["wf_av"] / ntot
-        norm = m["norm"]
-        Etot = m["Etot"] / norm
-        Etot2 = m["Etot2"] / norm
-        g = m["gvec"] / norm
-        ov = m["Ovec"] / norm
-        sout, dx, _ = o.sr_step(self.iteration, inp.delta_tau, self.s_factor0, inp.s_cut, Etot, Etot2, m["S"], norm,
+        scal6 = np.array([m["Etot"], m["Etot2"], m["norm"], m["wf_av"], float(nacc.sum()), float(o.nsample * o.nranks)])
+        S, gsum, osum = m["S"], m["gvec"], m["Ovec"]
+        if self.allreduce is not None:
+            scal6, S, gsum, osum = self.allreduce(scal6, S, gsum, osum)
+        ntot = scal6[5]
+        accept_ratio = float(scal6[4]) / ntot / o.N
+        wf_av = scal6[3] / ntot
+        norm = scal6[2]
+        Etot = scal6[0] / norm
+        Etot2 = scal6[1] / norm
+        g = gsum / norm
+        ov = osum / norm
+        sout, dx, _ = o.sr_step(self.iteration, inp.delta_tau, self.s_factor0, inp.s_cut, Etot, Etot2, S, norm,
                                 g, ov)
         self.s_factor0 *= inp.s_factor_scale
         self.wf_av_list = self.wf_av_list[1:] + [wf_av]

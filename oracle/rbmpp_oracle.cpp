@@ -123,6 +123,7 @@ struct Ctx {
   double shift;
   std::vector<double> SE;  // Slater_Elm(2N, 2N, N_QP)                module.f90:55
   std::vector<Rank> ranks;
+  int rank0 = 0;  // global MPI rank of local rank 0 (a shard of the ranks)
   int err;
   char msg[256];
 };
@@ -1022,15 +1023,20 @@ int orc_get_slater_elements(void* h, double* out) {
 }
 
 // main.f90:224-234: every rank seeds sgrnd(iseed0 + rank) and skips Nsample_rank*rank + 1 draws.
-int orc_seed(void* h, int iseed0) {
+// Local rank r is global rank offset + r (the context holds one shard of the ranks).
+int orc_seed_offset(void* h, int iseed0, int offset) {
   Ctx& c = *(Ctx*)h;
+  c.rank0 = offset;
   for (int r = 0; r < c.nranks; r++) {
-    mt_seed(c.ranks[r].rng, (int32_t)(iseed0 + r));
-    long long skip = (long long)c.nsample * r + 1;
+    const int g = offset + r;
+    mt_seed(c.ranks[r].rng, (int32_t)(iseed0 + g));
+    long long skip = (long long)c.nsample * g + 1;
     for (long long i = 0; i < skip; i++) (void)grnd(c.ranks[r].rng);
   }
   return 0;
 }
+
+int orc_seed(void* h, int iseed0) { return orc_seed_offset(h, iseed0, 0); }
 
 int orc_rank_grnd(void* h, int rank, int n, double* out) {
   Ctx& c = *(Ctx*)h;
@@ -1353,7 +1359,7 @@ int orc_sr_step(void* h, const orc_sr_in* in, const double* mat_tmp, double norm
       else lrp += r1;
     }
   lam = std::sqrt(lam);
-  (void)grnd(c.ranks[0].rng);  // :281 (rank 0)
+  if (c.rank0 == 0) (void)grnd(c.ranks[0].rng);  // :281 (rank 0)
   if (std::fabs(lam * lam - lrr - lpp - lrp) > 1e-5) return set_err(c, ORC_E_LAMBDA, "lambda division is wrong");
   lam = lam * 5.0 / (double)c.L;  // :309
   out->lambda = lam;
@@ -1362,7 +1368,7 @@ int orc_sr_step(void* h, const orc_sr_in* in, const double* mat_tmp, double norm
   out->lambda_rbm_pp = lrp;
   if (lam > 1.0)
     for (int k = 0; k < Nv; k++) x[k] = x[k] / lam;
-  (void)grnd(c.ranks[0].rng);  // :313 (rank 0; left-to-right .and.)
+  if (c.rank0 == 0) (void)grnd(c.ranks[0].rng);  // :313 (rank 0; left-to-right .and.)
   for (int k = Nrbm; k < Nv; k++) x[k] = x[k] * scal;  // :325-327
   double delW = 0.0;
   int kmax = -100, knz = 0;

@@ -1,6 +1,7 @@
 """Builds the CUDA library ``librbmpp.so`` in-tree for sm_100a (B200)."""
 from __future__ import annotations
 
+import concurrent.futures
 import os
 import subprocess
 import sys
@@ -8,17 +9,18 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "librbmpp.so")
-SOURCES = ["capi.cu", "sampler.cu", "sampler_stream.cu", "estimator.cu", "linalg.cu"]
+SOURCES = ["capi.cu", "sampler.cu", "sampler_stream.cu", "estimator.cu", "linalg.cu", "gemm_bf16x3.cu"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
          "-Xcompiler", "-O2", "--expt-relaxed-constexpr"]
 
 
 def _stale() -> bool:
-    if not os.path.exists(LIB):
+    if not os.path.exists(LIB) or not os.path.exists(os.path.join(HERE, "rbmpp_driver")):
         return True
-    t = os.path.getmtime(LIB)
-    deps = [os.path.join(CSRC, f) for f in os.listdir(CSRC)] + [os.path.join(HERE, "..", "include", "rbmpp.h")]
+    t = min(os.path.getmtime(LIB), os.path.getmtime(os.path.join(HERE, "rbmpp_driver")))
+    deps = [os.path.join(CSRC, f) for f in os.listdir(CSRC)] + [os.path.join(HERE, "..", "include", "rbmpp.h"),
+                                                                os.path.join(HERE, "driver", "rbmpp_driver.cpp")]
     return any(os.path.getmtime(p) > t for p in deps if os.path.exists(p))
 
 
@@ -27,19 +29,37 @@ def build(force: bool = False, verbose: bool = False, extra: list[str] | None = 
         return LIB
     objdir = os.path.join(HERE, "_build")
     os.makedirs(objdir, exist_ok=True)
-    objs = []
+    objs, cmds = [], []
     for src in SOURCES:
         obj = os.path.join(objdir, src.replace(".cu", ".o"))
-        cmd = [NVCC, *FLAGS, *(extra or []), "-c", os.path.join(CSRC, src), "-o", obj]
-        if verbose:
-            print(" ".join(cmd), flush=True)
-        subprocess.check_call(cmd)
+        cmds.append([NVCC, *FLAGS, *(extra or []), "-c", os.path.join(CSRC, src), "-o", obj])
         objs.append(obj)
+    # one nvcc per source, run side by side (each is single-threaded)
+    with concurrent.futures.ThreadPoolExecutor(max_workers=max(1, min(len(cmds), os.cpu_count() or 1))) as ex:
+        for cmd in cmds:
+            if verbose:
+                print(" ".join(cmd), flush=True)
+        list(ex.map(subprocess.check_call, cmds))
     cmd = [NVCC, "-gencode", "arch=compute_100a,code=sm_100a", "-shared", "-o", LIB, *objs, "-lcuda"]
     if verbose:
         print(" ".join(cmd), flush=True)
     subprocess.check_call(cmd)
+    build_driver(verbose)
     return LIB
+
+
+DRIVER_SRC = os.path.join(HERE, "driver", "rbmpp_driver.cpp")
+DRIVER = os.path.join(HERE, "rbmpp_driver")
+
+
+def build_driver(verbose: bool = False) -> str:
+    """The C++ main.f90 host program, linked against librbmpp.so (found next to it at run time)."""
+    cmd = ["g++", "-O2", "-std=c++17", "-Wall", DRIVER_SRC, "-o", DRIVER, "-L" + HERE, "-lrbmpp",
+           "-Wl,-rpath,$ORIGIN"]
+    if verbose:
+        print(" ".join(cmd), flush=True)
+    subprocess.check_call(cmd)
+    return DRIVER
 
 
 if __name__ == "__main__":

@@ -20,7 +20,7 @@ EXPORTS = ["rbmpp_create", "rbmpp_destroy", "rbmpp_last_error", "rbmpp_query", "
            "rbmpp_set_params", "rbmpp_get_params", "rbmpp_seed_walkers", "rbmpp_rank0_grnd", "rbmpp_make_sample",
            "rbmpp_get_samples", "rbmpp_set_samples", "rbmpp_measure", "rbmpp_measure_energy", "rbmpp_sr_step",
            "rbmpp_iteration", "rbmpp_eval_configs", "rbmpp_get_stats", "rbmpp_exchange_measurement",
-           "rbmpp_set_shift", "rbmpp_get_walker_state"]
+           "rbmpp_set_shift", "rbmpp_get_walker_state", "rbmpp_set_s_precision"]
 
 SR_FP64 = 0
 SR_SPLIT_BF16 = 1
@@ -43,7 +43,7 @@ class SrOut(C.Structure):
                 ("lambda_pp_pp", C.c_double), ("lambda_rbm_pp", C.c_double), ("delW_max", C.c_double),
                 ("s_factor", C.c_double), ("sdiag_av", C.c_double), ("smat_scaling", C.c_double),
                 ("refine_residual", C.c_double), ("kmax", C.c_int), ("k_nonzero", C.c_int), ("nSmat", C.c_int),
-                ("reserved", C.c_int)]
+                ("refine_iterations", C.c_int)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_ if k != "reserved"}
@@ -84,6 +84,7 @@ def lib():
         L.rbmpp_exchange_measurement.argtypes = [P, C.c_int, P, P, P, P]
         L.rbmpp_set_shift.argtypes = [P, C.c_double]
         L.rbmpp_get_walker_state.argtypes = [P, P, P]
+        L.rbmpp_set_s_precision.argtypes = [P, C.c_int]
         _lib = L
     return _lib
 
@@ -134,6 +135,12 @@ class Context:
     def _chk(self, rc):
         if rc != 0:
             raise RbmppError(rc, lib().rbmpp_last_error(self.h).decode())
+
+    def kernel_launches(self) -> int:
+        """Kernel launches the library has issued so far (process-wide counter)."""
+        v = C.c_longlong()
+        lib().rbmpp_query(self.h, 6, C.byref(v))
+        return v.value
 
     def device_bytes(self) -> int:
         v = C.c_longlong()
@@ -196,7 +203,7 @@ class Context:
         self._chk(lib().rbmpp_measure_energy(self.h, _p(scal)))
         return dict(Etot=scal[0], Etot2=scal[1], norm=scal[2], wf_av=scal[3])
 
-    def sr_step(self, iteration, delta_tau, s_factor0, s_cut, precision=SR_FP64, refine_steps=3):
+    def sr_step(self, iteration, delta_tau, s_factor0, s_cut, precision=SR_FP64, refine_steps=50):
         sin = SrIn(iteration, precision, refine_steps, 0, delta_tau, s_factor0, s_cut)
         sout = SrOut()
         dx = np.zeros(self.Nv)
@@ -213,6 +220,9 @@ class Context:
         out = np.zeros(self.nw, dtype=np.int32)
         self._chk(lib().rbmpp_get_walker_state(self.h, _p(out), None))
         return out
+
+    def set_s_precision(self, precision):
+        self._chk(lib().rbmpp_set_s_precision(self.h, int(precision)))
 
     def set_shift(self, shift):
         self._chk(lib().rbmpp_set_shift(self.h, float(shift)))

@@ -4,6 +4,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -41,6 +42,11 @@ cudaError_t rbmpp_add_diag(int, double*, double, cudaStream_t);
 cudaError_t rbmpp_rowcol_absmax(int, const double*, const int*, int, double*, cudaStream_t);
 cudaError_t rbmpp_sample_scalars(int, const double*, int, const double*, double, double*, double*, double*,
                                  cudaStream_t);
+void rbmpp_bf16x3_pads(int, int, int*, int*);
+int rbmpp_syrk_bf16x3(int, int, const double*, void*, void*, int*, double*, double*, cudaStream_t);
+
+static std::atomic<long long> g_launches{0};
+void rbmpp_note_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 
 namespace {
 
@@ -117,8 +123,8 @@ struct rbmpp_ctx {
   double *d_O = nullptr, *d_psiS = nullptr, *d_eloc = nullptr, *d_a = nullptr, *d_b = nullptr, *d_acc4 = nullptr;
   int *d_nap = nullptr, *d_estat = nullptr;
   double *d_gvec = nullptr, *d_Ovec = nullptr, *d_S = nullptr, *d_part = nullptr, *d_vec = nullptr;
-  double *d_tmp_ns = nullptr;
-  int* d_info = nullptr;
+  double *d_tmp_ns = nullptr, *d_rv = nullptr;
+  int *d_info = nullptr, *d_err = nullptr;
   void *d_hi = nullptr, *d_lo = nullptr;
   int ldk = 0;
   float* d_Sf = nullptr;
@@ -134,6 +140,9 @@ struct rbmpp_ctx {
   cudaEvent_t ev[12] = {};
   double stats[8] = {0};
   int stream_stages = 0;  // > 0: TMA-streamed sampler with this many stages
+  // S of the current measurement: built lazily in the precision the SR step asks for
+  bool S_valid = false, S_reduced = false;
+  int S_prec = RBMPP_SR_FP64, meas_prec = RBMPP_SR_FP64;
 };
 
 namespace {
@@ -193,6 +202,7 @@ int upload_params(rbmpp_ctx* c) {
   }
   CK(cudaMemcpyAsync(c->d_slater, c->slater.data(), sizeof(double) * d.n_slater, cudaMemcpyHostToDevice, c->st));
   long long tot = (long long)d.n_qp * d.N * d.N;
+  rbmpp_note_launch();
   build_xf_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, c->st>>>(d.N, d.n_mp, c->d_wmap, c->d_orb, c->d_slater,
                                                                       d.sp_cc[0], d.sp_ss[0], d.sp_cc[1], d.sp_ss[1],
                                                                       c->d_XF, c->d_XFT);
@@ -222,6 +232,77 @@ int ensure_measure_buffers(rbmpp_ctx* c) {
   if ((r = dalloc(c, &c->d_S, (size_t)d.Nv * d.Nv))) return r;
   if ((r = dalloc(c, &c->d_part, (size_t)2 * 64 * d.Nv))) return r;
   if ((r = dalloc(c, &c->d_info, 4))) return r;
+  if ((r = dalloc(c, &c->d_err, 4))) return r;
+  if ((r = dalloc(c, &c->d_rv, (size_t)2 * d.Nv))) return r;
+  return 0;
+}
+
+// S_raw = sum over samples of O O^T (the dgemm of calc_phys_quantity.f90:240) for the current
+// measurement, in FP64 or as split-BF16 products on the tensor cores (exact FP64 diagonal).
+int build_S(rbmpp_ctx* c, int prec) {
+  if (c->S_valid && c->S_prec == prec) return 0;
+  if (c->S_reduced)
+    return fail(c, RBMPP_E_STATE, "S was loaded by exchange_measurement in precision %d; cannot rebuild in %d",
+                c->S_prec, prec);
+  const DevDims& d = c->d;
+  CK(cudaEventRecord(c->ev[5], c->st));
+  if (prec == RBMPP_SR_FP64) {
+    CK(rbmpp_syrk_ot_o(d.Nv, c->ns_tot, c->d_O, c->d_S, c->st));
+  } else if (prec == RBMPP_SR_SPLIT_BF16) {
+    if (!c->d_hi) {
+      int kp = 0, np = 0;
+      rbmpp_bf16x3_pads(c->ns_tot, d.Nv, &kp, &np);
+      const size_t bytes = (size_t)kp * np * 2;
+      cudaError_t e = cudaMalloc(&c->d_hi, bytes);
+      if (!e) e = cudaMalloc(&c->d_lo, bytes);
+      if (e) return fail(c, RBMPP_E_CUDA, "cudaMalloc(split-BF16 operands, 2 x %zu bytes): %s", bytes,
+                         cudaGetErrorString(e));
+      c->bytes += 2 * bytes;
+    }
+    const int r = rbmpp_syrk_bf16x3(c->ns_tot, d.Nv, c->d_O, c->d_hi, c->d_lo, c->d_err, c->d_S, c->d_part, c->st);
+    if (r == 1) return fail(c, RBMPP_E_CUDA, "cuTensorMapEncodeTiled unavailable from the driver");
+    if (r) return fail(c, RBMPP_E_CUDA, "split-BF16 S build: %s", cudaGetErrorString((cudaError_t)(r - 100)));
+    CK(rbmpp_symmetrize(d.Nv, c->d_S, c->st));
+  } else {
+    return fail(c, RBMPP_E_ARG, "unknown S precision %d", prec);
+  }
+  CK(cudaEventRecord(c->ev[6], c->st));
+  CK(cudaStreamSynchronize(c->st));
+  if (prec == RBMPP_SR_SPLIT_BF16) {
+    int err = 0;
+    CK(cudaMemcpy(&err, c->d_err, sizeof(int), cudaMemcpyDeviceToHost));
+    if (err) return fail(c, RBMPP_E_TIMEOUT, "split-BF16 S build: a bounded device wait ran out");
+  }
+  float ms = 0.f;
+  CK(cudaEventElapsedTime(&ms, c->ev[5], c->ev[6]));
+  c->stats[3] = ms;
+  c->S_valid = true;
+  c->S_prec = prec;
+  return 0;
+}
+
+// y = A x with A = D (S_raw / norm - ov ov^T) D + sigma I, D = diag(1 on the RBM block, scal on the
+// Pfaffian block): the conditioned S of SR_pdposv.f90:4-170 applied exactly in FP64 through O
+// (S_raw x = O^T (O x)), without forming S.
+int apply_S_exact(rbmpp_ctx* c, const std::vector<double>& x, const std::vector<double>& ov, double norm, double scal,
+                  double sigma, std::vector<double>& y) {
+  const int Nv = c->d.Nv, Nrbm = c->d.Nv_rbm;
+  std::vector<double> y1(Nv), y2(Nv);
+  double ovy = 0.0;
+  for (int k = 0; k < Nv; k++) {
+    y1[k] = k < Nrbm ? x[k] : x[k] * scal;
+    ovy += ov[k] * y1[k];
+  }
+  CK(cudaMemcpyAsync(c->d_rv, y1.data(), sizeof(double) * Nv, cudaMemcpyHostToDevice, c->st));
+  CK(rbmpp_gemv_o(c->ns_tot, Nv, c->d_O, c->d_rv, c->d_tmp_ns, c->st));
+  CK(rbmpp_gemv_ot(c->ns_tot, Nv, c->d_O, c->d_tmp_ns, nullptr, c->d_rv + Nv, nullptr, c->d_part, 64, c->st));
+  CK(cudaMemcpyAsync(y2.data(), c->d_rv + Nv, sizeof(double) * Nv, cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  y.assign(Nv, 0.0);
+  for (int k = 0; k < Nv; k++) {
+    const double v = y2[k] / norm - ov[k] * ovy;
+    y[k] = (k < Nrbm ? v : v * scal) + sigma * x[k];
+  }
   return 0;
 }
 
@@ -372,7 +453,7 @@ int rbmpp_destroy(rbmpp_ctx* c) {
                   c->d_XF, c->d_XFT, c->W.x, c->W.idx, c->W.cfg, c->W.th, c->W.sgn, c->W.pf, c->W.psi, c->W.Y,
                   c->W.mt, c->W.nfastup, c->W.naccept, c->W.nacc_all, c->W.status, c->W.xs, c->W.pfs, c->W.psis, c->d_O, c->d_psiS,
                   c->d_eloc, c->d_a, c->d_b, c->d_tmp_ns, c->d_acc4, c->d_nap, c->d_estat, c->d_gvec, c->d_Ovec,
-                  c->d_vec, c->d_S, c->d_part, c->d_info, c->d_hi, c->d_lo, c->d_Sf};
+                  c->d_vec, c->d_S, c->d_part, c->d_info, c->d_err, c->d_rv, c->d_hi, c->d_lo, c->d_Sf};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   for (auto& e : c->ev)
@@ -393,6 +474,7 @@ int rbmpp_query(const rbmpp_ctx* c, int what, long long* v) {
     case 3: *v = c->d.n_qp; break;
     case 4: *v = c->d.N; break;
     case 5: *v = (long long)c->bytes; break;
+    case 6: *v = g_launches.load(std::memory_order_relaxed); break;
     default: return RBMPP_E_ARG;
   }
   return 0;
@@ -464,6 +546,7 @@ int rbmpp_get_params(rbmpp_ctx* c, double* Wr, double* br, double* slater, doubl
 
 int rbmpp_seed_walkers(rbmpp_ctx* c, int iseed0) {
   if (!c) return RBMPP_E_ARG;
+  rbmpp_note_launch();
   seed_kernel<<<(c->d.nw + 63) / 64, 64, 0, c->st>>>(c->W.mt, c->d.nw, iseed0, c->d.ns, c->dims.walker_offset);
   CK(cudaGetLastError());
   CK(cudaStreamSynchronize(c->st));
@@ -476,6 +559,7 @@ int rbmpp_rank0_grnd(rbmpp_ctx* c, int n, double* out) {
   if (n == 0) return 0;
   double* d_out = nullptr;
   CK(cudaMalloc(&d_out, sizeof(double) * n));
+  rbmpp_note_launch();
   draw_kernel<<<1, 1, 0, c->st>>>(c->W.mt, n, d_out);
   cudaError_t e = cudaGetLastError();
   if (e == cudaSuccess) e = cudaMemcpyAsync(out, d_out, sizeof(double) * n, cudaMemcpyDeviceToHost, c->st);
@@ -525,6 +609,7 @@ int rbmpp_get_samples(rbmpp_ctx* c, int* x, double* psi, double* pf) {
   if (x) {
     int* dx = nullptr;
     CK(cudaMalloc(&dx, sizeof(int) * nx));
+    rbmpp_note_launch();
     i8_to_int_kernel<<<(unsigned)((nx + 255) / 256), 256, 0, c->st>>>(c->W.xs, dx, nx);
     cudaError_t e = cudaMemcpyAsync(x, dx, sizeof(int) * nx, cudaMemcpyDeviceToHost, c->st);
     if (e == cudaSuccess) e = cudaStreamSynchronize(c->st);
@@ -544,6 +629,7 @@ int rbmpp_set_samples(rbmpp_ctx* c, const int* x) {
   CK(cudaMalloc(&dx, sizeof(int) * nx));
   cudaError_t e = cudaMemcpyAsync(dx, x, sizeof(int) * nx, cudaMemcpyHostToDevice, c->st);
   if (e == cudaSuccess) {
+    rbmpp_note_launch();
     int_to_i8_kernel<<<(unsigned)((nx + 255) / 256), 256, 0, c->st>>>(dx, c->W.xs, nx);
     e = cudaGetLastError();
   }
@@ -558,6 +644,8 @@ static int measure_common(rbmpp_ctx* c, bool with_o) {
   const DevDims& d = c->d;
   int r = ensure_measure_buffers(c);
   if (r) return r;
+  c->S_valid = false;
+  c->S_reduced = false;
   c->d.shift = c->shift;
   CK(cudaEventRecord(c->ev[2], c->st));
   CK(rbmpp_launch_estimator(c->d, tables(c), params(c), c->W.xs, c->ns_tot, c->d_psiS, c->d_eloc,
@@ -589,17 +677,15 @@ int rbmpp_measure(rbmpp_ctx* c, double* scal, double* gvec, double* Ovec, double
   if (r) return r;
   CK(cudaEventRecord(c->ev[4], c->st));
   CK(rbmpp_gemv_ot(c->ns_tot, d.Nv, c->d_O, c->d_a, c->d_b, c->d_gvec, c->d_Ovec, c->d_part, 64, c->st));
-  CK(cudaEventRecord(c->ev[5], c->st));
-  CK(rbmpp_syrk_ot_o(d.Nv, c->ns_tot, c->d_O, c->d_S, c->st));
-  CK(cudaEventRecord(c->ev[6], c->st));
+  CK(cudaEventRecord(c->ev[11], c->st));
   CK(cudaStreamSynchronize(c->st));
   {
-    float a1 = 0.f, a2 = 0.f;
-    CK(cudaEventElapsedTime(&a1, c->ev[4], c->ev[5]));
-    CK(cudaEventElapsedTime(&a2, c->ev[5], c->ev[6]));
+    float a1 = 0.f;
+    CK(cudaEventElapsedTime(&a1, c->ev[4], c->ev[11]));
     c->stats[2] = a1;
-    c->stats[3] = a2;
   }
+  // S itself is built when it is first needed (here if Smat is wanted, else by exchange or SR step)
+  if (Smat && (r = build_S(c, c->meas_prec))) return r;
   if (scal) std::memcpy(scal, c->meas_scal, sizeof(double) * 4);
   if (gvec) CK(cudaMemcpy(gvec, c->d_gvec, sizeof(double) * d.Nv, cudaMemcpyDeviceToHost));
   if (Ovec) CK(cudaMemcpy(Ovec, c->d_Ovec, sizeof(double) * d.Nv, cudaMemcpyDeviceToHost));
@@ -636,6 +722,7 @@ int rbmpp_eval_configs(rbmpp_ctx* c, int n, const int* x, double* psi, double* h
   if (!e) e = cudaMalloc(&dst, sizeof(int) * n);
   if (!e) e = cudaMemcpyAsync(dx, x, sizeof(int) * nx, cudaMemcpyHostToDevice, c->st);
   if (!e) {
+    rbmpp_note_launch();
     int_to_i8_kernel<<<(unsigned)((nx + 255) / 256), 256, 0, c->st>>>(dx, dx8, nx);
     e = cudaGetLastError();
   }
@@ -661,9 +748,19 @@ int rbmpp_eval_configs(rbmpp_ctx* c, int n, const int* x, double* psi, double* h
 int rbmpp_sr_step(rbmpp_ctx* c, const rbmpp_sr_in* in, rbmpp_sr_out* out, double* dx_out) {
   if (!c || !in || !out) return RBMPP_E_ARG;
   if (!c->measured) return fail(c, RBMPP_E_STATE, "sr_step before measure");
-  if (in->precision != RBMPP_SR_FP64) return fail(c, RBMPP_E_ARG, "unknown SR precision %d", in->precision);
+  if (in->precision != RBMPP_SR_FP64 && in->precision != RBMPP_SR_SPLIT_BF16)
+    return fail(c, RBMPP_E_ARG, "unknown SR precision %d", in->precision);
   const DevDims& d = c->d;
   const int Nv = d.Nv, Nrbm = d.Nv_rbm, N = d.N;
+  const bool refine = in->precision == RBMPP_SR_SPLIT_BF16 && in->refine_steps > 0;
+  if (refine && c->n_samples_total != (double)c->ns_tot)
+    return fail(c, RBMPP_E_ARG,
+                "split-BF16 refinement applies S through this context's samples only; with a measurement reduced "
+                "over several contexts use refine_steps = 0");
+  {
+    int r = build_S(c, in->precision);
+    if (r) return r;
+  }
   std::memset(out, 0, sizeof(*out));
   const double norm = c->meas_scal[2];
   const double ntot = c->n_samples_total;
@@ -791,22 +888,77 @@ int rbmpp_sr_step(rbmpp_ctx* c, const rbmpp_sr_in* in, rbmpp_sr_out* out, double
   if (info != 0) return fail(c, RBMPP_E_CHOL, "info (pdposv): %d", info);
   CK(rbmpp_potrs_upper(Nv, c->d_S, d_x, c->st));
   CK(cudaEventRecord(c->ev[8], c->st));
-  // lambda = sqrt(x^T S x) = ||U x|| and its block split (:251-277)
   std::vector<double> x(Nv), ux(Nv), xr(Nv, 0.0), xp(Nv, 0.0);
   CK(cudaMemcpyAsync(x.data(), d_x, sizeof(double) * Nv, cudaMemcpyDeviceToHost, c->st));
-  CK(rbmpp_trmv_upper(Nv, c->d_S, d_x, d_y, c->st));
-  CK(cudaMemcpyAsync(ux.data(), d_y, sizeof(double) * Nv, cudaMemcpyDeviceToHost, c->st));
   CK(cudaStreamSynchronize(c->st));
-  {
-    float ms = 0.f;
-    CK(cudaEventElapsedTime(&ms, c->ev[7], c->ev[8]));
-    c->stats[4] = ms;
-  }
-  double lam2 = 0.0;
-  for (int k = 0; k < Nv; k++) lam2 += ux[k] * ux[k];
-  for (int k = 0; k < Nv; k++) (k < Nrbm ? xr[k] : xp[k]) = x[k];
-  double lrr = 0, lpp = 0;
-  {
+  const double sigma = sdiag * s_factor;
+  double lam2 = 0.0, lrr = 0.0, lpp = 0.0;
+  if (refine) {
+    // the split-precision solve refined against the exact FP64 S (applied through O): conjugate
+    // gradients on A x = g preconditioned by the Cholesky factor of the split-precision S, started
+    // from the split solve; stops at relative residual 1e-13 or after refine_steps iterations
+    auto precond = [&](const std::vector<double>& rr, std::vector<double>& zz) -> int {
+      CK(cudaMemcpyAsync(d_y, rr.data(), sizeof(double) * Nv, cudaMemcpyHostToDevice, c->st));
+      CK(rbmpp_potrs_upper(Nv, c->d_S, d_y, c->st));
+      zz.resize(Nv);
+      CK(cudaMemcpyAsync(zz.data(), d_y, sizeof(double) * Nv, cudaMemcpyDeviceToHost, c->st));
+      CK(cudaStreamSynchronize(c->st));
+      return 0;
+    };
+    auto dot = [&](const std::vector<double>& a, const std::vector<double>& b) {
+      double t = 0.0;
+      for (int k = 0; k < Nv; k++) t += a[k] * b[k];
+      return t;
+    };
+    const double gn = std::sqrt(dot(g, g));
+    std::vector<double> ax, res(Nv), zv, pv, ap;
+    int r = apply_S_exact(c, x, ov, norm, scal, sigma, ax);
+    if (r) return r;
+    for (int k = 0; k < Nv; k++) res[k] = g[k] - ax[k];
+    if ((r = precond(res, zv))) return r;
+    pv = zv;
+    double rz = dot(res, zv);
+    int it = 0;
+    for (; it < in->refine_steps && gn > 0.0 && std::sqrt(dot(res, res)) > 1e-13 * gn; it++) {
+      if ((r = apply_S_exact(c, pv, ov, norm, scal, sigma, ap))) return r;
+      const double pap = dot(pv, ap);
+      if (!(pap > 0.0)) break;
+      const double alpha = rz / pap;
+      for (int k = 0; k < Nv; k++) {
+        x[k] += alpha * pv[k];
+        res[k] -= alpha * ap[k];
+      }
+      if ((r = precond(res, zv))) return r;
+      const double rz1 = dot(res, zv), beta = rz1 / rz;
+      rz = rz1;
+      for (int k = 0; k < Nv; k++) pv[k] = zv[k] + beta * pv[k];
+    }
+    out->refine_iterations = it;
+    // lambda^2 = x^T A x and its block split (:251-277) with the exact A
+    for (int k = 0; k < Nv; k++) (k < Nrbm ? xr[k] : xp[k]) = x[k];
+    std::vector<double> axr, axp;
+    r = apply_S_exact(c, xr, ov, norm, scal, sigma, axr);
+    if (!r) r = apply_S_exact(c, xp, ov, norm, scal, sigma, axp);
+    if (r) return r;
+    for (int k = 0; k < Nv; k++) {
+      lrr += xr[k] * axr[k];
+      lpp += xp[k] * axp[k];
+      lam2 += x[k] * (axr[k] + axp[k]);
+    }
+    // true residual of the final x
+    double rn = 0.0;
+    for (int k = 0; k < Nv; k++) {
+      const double t = g[k] - (axr[k] + axp[k]);
+      rn += t * t;
+    }
+    out->refine_residual = gn > 0.0 ? std::sqrt(rn) / gn : 0.0;
+  } else {
+    // lambda = sqrt(x^T S x) = ||U x|| and its block split (:251-277)
+    CK(rbmpp_trmv_upper(Nv, c->d_S, d_x, d_y, c->st));
+    CK(cudaMemcpyAsync(ux.data(), d_y, sizeof(double) * Nv, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    for (int k = 0; k < Nv; k++) lam2 += ux[k] * ux[k];
+    for (int k = 0; k < Nv; k++) (k < Nrbm ? xr[k] : xp[k]) = x[k];
     CK(cudaMemcpyAsync(d_y, xr.data(), sizeof(double) * Nv, cudaMemcpyHostToDevice, c->st));
     CK(rbmpp_trmv_upper(Nv, c->d_S, d_y, d_diag, c->st));
     CK(cudaMemcpyAsync(ux.data(), d_diag, sizeof(double) * Nv, cudaMemcpyDeviceToHost, c->st));
@@ -817,6 +969,11 @@ int rbmpp_sr_step(rbmpp_ctx* c, const rbmpp_sr_in* in, rbmpp_sr_out* out, double
     CK(cudaMemcpyAsync(ux.data(), d_diag, sizeof(double) * Nv, cudaMemcpyDeviceToHost, c->st));
     CK(cudaStreamSynchronize(c->st));
     for (int k = 0; k < Nv; k++) lpp += ux[k] * ux[k];
+  }
+  {
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, c->ev[7], c->ev[8]));
+    c->stats[4] = ms;
   }
   double lrp = lam2 - lrr - lpp;
   double lam = std::sqrt(lam2);
@@ -875,6 +1032,7 @@ int rbmpp_sr_step(rbmpp_ctx* c, const rbmpp_sr_in* in, rbmpp_sr_out* out, double
   out->nSmat = nS;
   if (dx_out) std::memcpy(dx_out, x.data(), sizeof(double) * Nv);
   c->measured = false;  // S was factorised in place
+  c->S_valid = false;
   return upload_params(c);
 }
 
@@ -884,14 +1042,23 @@ int rbmpp_exchange_measurement(rbmpp_ctx* c, int direction, double* d_S, double*
   const int Nv = c->d.Nv;
   const size_t nS = (size_t)Nv * Nv * sizeof(double), nV = (size_t)Nv * sizeof(double);
   if (direction == 0) {
-    if (d_S) CK(cudaMemcpyAsync(d_S, c->d_S, nS, cudaMemcpyDeviceToDevice, c->st));
+    if (d_S) {
+      int r = build_S(c, c->meas_prec);
+      if (r) return r;
+      CK(cudaMemcpyAsync(d_S, c->d_S, nS, cudaMemcpyDeviceToDevice, c->st));
+    }
     if (d_g) CK(cudaMemcpyAsync(d_g, c->d_gvec, nV, cudaMemcpyDeviceToDevice, c->st));
     if (d_ov) CK(cudaMemcpyAsync(d_ov, c->d_Ovec, nV, cudaMemcpyDeviceToDevice, c->st));
     for (int k = 0; k < 4; k++) scal6[k] = c->meas_scal[k];
     scal6[4] = (double)c->naccept_total;
     scal6[5] = c->n_samples_total;
   } else {
-    if (d_S) CK(cudaMemcpyAsync(c->d_S, d_S, nS, cudaMemcpyDeviceToDevice, c->st));
+    if (d_S) {
+      CK(cudaMemcpyAsync(c->d_S, d_S, nS, cudaMemcpyDeviceToDevice, c->st));
+      c->S_valid = true;
+      c->S_reduced = true;
+      c->S_prec = c->meas_prec;
+    }
     if (d_g) CK(cudaMemcpyAsync(c->d_gvec, d_g, nV, cudaMemcpyDeviceToDevice, c->st));
     if (d_ov) CK(cudaMemcpyAsync(c->d_Ovec, d_ov, nV, cudaMemcpyDeviceToDevice, c->st));
     for (int k = 0; k < 4; k++) c->meas_scal[k] = scal6[k];
@@ -899,6 +1066,14 @@ int rbmpp_exchange_measurement(rbmpp_ctx* c, int direction, double* d_S, double*
     c->n_samples_total = scal6[5];
   }
   CK(cudaStreamSynchronize(c->st));
+  return 0;
+}
+
+int rbmpp_set_s_precision(rbmpp_ctx* c, int precision) {
+  if (!c) return RBMPP_E_ARG;
+  if (precision != RBMPP_SR_FP64 && precision != RBMPP_SR_SPLIT_BF16)
+    return fail(c, RBMPP_E_ARG, "unknown S precision %d", precision);
+  c->meas_prec = precision;
   return 0;
 }
 
@@ -916,6 +1091,9 @@ int rbmpp_iteration(rbmpp_ctx* c, int precision, double delta_tau, double s_fact
     c->s_factor0 = s_factor0_initial;
     c->s_factor_init = true;
   }
+  if (precision != RBMPP_SR_FP64 && precision != RBMPP_SR_SPLIT_BF16)
+    return fail(c, RBMPP_E_ARG, "unknown SR precision %d", precision);
+  c->meas_prec = precision;
   c->iteration++;
   CK(cudaEventRecord(c->ev[9], c->st));
   int r = rbmpp_make_sample(c, c->iteration == 1 ? 1 : 0, nullptr, nullptr);
@@ -926,7 +1104,7 @@ int rbmpp_iteration(rbmpp_ctx* c, int precision, double delta_tau, double s_fact
   std::memset(&in, 0, sizeof(in));
   in.iteration = c->iteration;
   in.precision = precision;
-  in.refine_steps = 3;
+  in.refine_steps = 50;
   in.delta_tau = delta_tau;
   in.s_factor0 = c->s_factor0;
   in.s_cut = s_cut;

@@ -15,6 +15,10 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+// Counts every kernel launch the library issues (process-wide); defined in capi.cu, read through
+// rbmpp_query(ctx, 6, ...).
+void rbmpp_note_launch();
+
 #define RBMPP_MAX_N 512
 #define RBMPP_MAX_KPL 8  // columns per lane in the warp streaming loops: Np <= 256
 

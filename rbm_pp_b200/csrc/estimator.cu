@@ -474,7 +474,7 @@ cudaError_t rbmpp_launch_estimator(const DevDims& d, const DevTables& t, const D
     cudaError_t e = cudaFuncSetAttribute(estimator_kernel<K>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
                                          (int)smem);                                                       \
     if (e != cudaSuccess) return e;                                                                        \
-    estimator_kernel<K><<<n, kEstThreads, smem, st>>>(d, t, p, xs, n, out_psi, out_hpsi, O, out_nap,         \
+    rbmpp_note_launch(); estimator_kernel<K><<<n, kEstThreads, smem, st>>>(d, t, p, xs, n, out_psi, out_hpsi, O, out_nap,         \
                                                       out_status, reweight, nqw);                           \
     return cudaGetLastError();                                                                             \
   } while (0)
@@ -487,6 +487,7 @@ cudaError_t rbmpp_launch_estimator(const DevDims& d, const DevTables& t, const D
 }
 
 cudaError_t rbmpp_launch_advance_rng(uint32_t* mt, const int* nap, int ns, int nw, int extra, cudaStream_t st) {
+  rbmpp_note_launch();
   advance_rng_kernel<<<(nw + 63) / 64, 64, 0, st>>>(mt, nap, ns, nw, extra);
   return cudaGetLastError();
 }

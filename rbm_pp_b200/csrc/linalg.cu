@@ -5,6 +5,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+void rbmpp_note_launch();  // capi.cu: counts kernel launches
+
 namespace {
 
 // C(i, j) = alpha * sum_k A(k, i) B(k, j) + beta * C(i, j) on upper-triangular 128 x 128 tiles.
@@ -353,16 +355,19 @@ __global__ void sample_scalars_kernel(int ns, const double* psi, int psi_stride,
 cudaError_t rbmpp_syrk_ot_o(int nv, int ns, const double* O, double* S, cudaStream_t st) {
   int nt = (nv + BM - 1) / BM;
   int ntiles = nt * (nt + 1) / 2;
+  rbmpp_note_launch();
   gemm_atb_upper<false><<<ntiles, 256, 0, st>>>(nv, ns, O, nv, 1, 1.0, 0.0, S, nv, 0);
   cudaError_t e = cudaGetLastError();
   if (e) return e;
   dim3 g((nv + 31) / 32, (nv + 31) / 32);
+  rbmpp_note_launch();
   symmetrize_kernel<<<g, dim3(32, 8), 0, st>>>(nv, S);
   return cudaGetLastError();
 }
 
 cudaError_t rbmpp_symmetrize(int n, double* S, cudaStream_t st) {
   dim3 g((n + 31) / 32, (n + 31) / 32);
+  rbmpp_note_launch();
   symmetrize_kernel<<<g, dim3(32, 8), 0, st>>>(n, S);
   return cudaGetLastError();
 }
@@ -371,12 +376,15 @@ cudaError_t rbmpp_symmetrize(int n, double* S, cudaStream_t st) {
 cudaError_t rbmpp_potrf_upper(int n, double* A, int* d_info, cudaStream_t st) {
   cudaMemsetAsync(d_info, 0, sizeof(int), st);
   for (int k0 = 0; k0 < n; k0 += NB) {
+    rbmpp_note_launch();
     potrf_diag_kernel<<<1, 256, 0, st>>>(n, A, n, k0, d_info);
     int rest = n - (k0 + NB);
     if (rest > 0) {
       int blocks = min(1024, (rest + 7) / 8);
+      rbmpp_note_launch();
       trsm_panel_kernel<<<blocks, 256, 0, st>>>(n, A, n, k0);
       int nt = (rest + BM - 1) / BM;
+      rbmpp_note_launch();
       gemm_atb_upper<true><<<nt * (nt + 1) / 2, 256, 0, st>>>(n, NB, A + k0, 1, n, -1.0, 1.0, A, n, k0 + NB);
     }
   }
@@ -386,19 +394,28 @@ cudaError_t rbmpp_potrf_upper(int n, double* A, int* d_info, cudaStream_t st) {
 // b <- A^{-1} b with A = U^T U (upper factor in A)
 cudaError_t rbmpp_potrs_upper(int n, const double* A, double* b, cudaStream_t st) {
   for (int k0 = 0; k0 < n; k0 += NB) {
+    rbmpp_note_launch();
     trsv_diag_kernel<<<1, 32, 0, st>>>(n, A, n, b, k0, 1);
     int rest = n - (k0 + NB);
-    if (rest > 0) trsv_update_kernel<<<(rest + 255) / 256, 256, 0, st>>>(n, A, n, b, k0, 1);
+    if (rest > 0) {
+      rbmpp_note_launch();
+      trsv_update_kernel<<<(rest + 255) / 256, 256, 0, st>>>(n, A, n, b, k0, 1);
+    }
   }
   int last = ((n - 1) / NB) * NB;
   for (int k0 = last; k0 >= 0; k0 -= NB) {
+    rbmpp_note_launch();
     trsv_diag_kernel<<<1, 32, 0, st>>>(n, A, n, b, k0, 0);
-    if (k0 > 0) trsv_update_kernel<<<(k0 + 255) / 256, 256, 0, st>>>(n, A, n, b, k0, 0);
+    if (k0 > 0) {
+      rbmpp_note_launch();
+      trsv_update_kernel<<<(k0 + 255) / 256, 256, 0, st>>>(n, A, n, b, k0, 0);
+    }
   }
   return cudaGetLastError();
 }
 
 cudaError_t rbmpp_trmv_upper(int n, const double* A, const double* x, double* y, cudaStream_t st) {
+  rbmpp_note_launch();
   trmv_upper_kernel<<<(n * 32 + 255) / 256, 256, 0, st>>>(n, A, n, x, y);
   return cudaGetLastError();
 }
@@ -408,47 +425,59 @@ cudaError_t rbmpp_gemv_ot(int ns, int nv, const double* O, const double* c0, con
                           double* out1, double* part, int nparts, cudaStream_t st) {
   int chunk = (ns + nparts - 1) / nparts;
   dim3 g((nv + 127) / 128, nparts);
+  rbmpp_note_launch();
   gemv_ot_partial<<<g, 128, 0, st>>>(ns, nv, O, c0, c1, chunk, part, c1 ? part + (long long)nparts * nv : nullptr);
+  rbmpp_note_launch();
   sum_parts<<<(nv + 255) / 256, 256, 0, st>>>(nv, nparts, part, out0);
-  if (c1) sum_parts<<<(nv + 255) / 256, 256, 0, st>>>(nv, nparts, part + (long long)nparts * nv, out1);
+  if (c1) {
+    rbmpp_note_launch();
+    sum_parts<<<(nv + 255) / 256, 256, 0, st>>>(nv, nparts, part + (long long)nparts * nv, out1);
+  }
   return cudaGetLastError();
 }
 
 cudaError_t rbmpp_gemv_o(int ns, int nv, const double* O, const double* x, double* y, cudaStream_t st) {
+  rbmpp_note_launch();
   gemv_o_kernel<<<(ns * 32 + 255) / 256, 256, 0, st>>>(ns, nv, O, x, y);
   return cudaGetLastError();
 }
 
 cudaError_t rbmpp_sr_form(int n, double* S, double norm, const double* ov, cudaStream_t st) {
   long long tot = (long long)n * n;
+  rbmpp_note_launch();
   sr_form_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(n, S, norm, ov);
   return cudaGetLastError();
 }
 
 cudaError_t rbmpp_sr_scale(int n, int nrbm, double* S, double f, cudaStream_t st) {
   long long tot = (long long)n * n;
+  rbmpp_note_launch();
   sr_scale_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(n, nrbm, S, f);
   return cudaGetLastError();
 }
 
 cudaError_t rbmpp_get_diag(int n, const double* S, double* d, cudaStream_t st) {
+  rbmpp_note_launch();
   get_diag_kernel<<<(n + 255) / 256, 256, 0, st>>>(n, S, d);
   return cudaGetLastError();
 }
 
 cudaError_t rbmpp_add_diag(int n, double* S, double v, cudaStream_t st) {
+  rbmpp_note_launch();
   add_diag_kernel<<<(n + 255) / 256, 256, 0, st>>>(n, S, v);
   return cudaGetLastError();
 }
 
 cudaError_t rbmpp_rowcol_absmax(int n, const double* S, const int* list, int nlist, double* out, cudaStream_t st) {
   if (nlist <= 0) return cudaSuccess;
+  rbmpp_note_launch();
   rowcol_absmax_kernel<<<nlist, 256, 0, st>>>(n, S, list, nlist, out);
   return cudaGetLastError();
 }
 
 cudaError_t rbmpp_sample_scalars(int ns, const double* psi, int psi_stride, const double* eloc, double shift,
                                  double* a, double* b, double* acc4, cudaStream_t st) {
+  rbmpp_note_launch();
   sample_scalars_kernel<<<1, 256, 0, st>>>(ns, psi, psi_stride, eloc, shift, a, b, acc4);
   return cudaGetLastError();
 }

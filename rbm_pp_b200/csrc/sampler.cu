@@ -333,7 +333,7 @@ cudaError_t rbmpp_launch_sampler(const DevDims& d, const DevTables& t, const Dev
     cudaError_t e = cudaFuncSetAttribute(sampler_kernel<K>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
                                          (int)smem);                                                     \
     if (e != cudaSuccess) return e;                                                                      \
-    sampler_kernel<K><<<d.nw, threads, smem, st>>>(d, t, p, W, first);                                   \
+    rbmpp_note_launch(); sampler_kernel<K><<<d.nw, threads, smem, st>>>(d, t, p, W, first);                                   \
     return cudaGetLastError();                                                                           \
   } while (0)
   if (kpl <= 1) LAUNCH(1);

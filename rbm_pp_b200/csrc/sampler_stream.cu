@@ -632,7 +632,7 @@ cudaError_t rbmpp_launch_sampler_stream(const DevDims& d, const DevTables& t, co
     cudaError_t e = cudaFuncSetAttribute(sampler_stream_kernel<K>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
                                          (int)smem);                                                            \
     if (e != cudaSuccess) return e;                                                                             \
-    sampler_stream_kernel<K><<<d.nw, kWarps * 32, smem, stream>>>(d, t, p, W, first, st);                       \
+    rbmpp_note_launch(); sampler_stream_kernel<K><<<d.nw, kWarps * 32, smem, stream>>>(d, t, p, W, first, st);                       \
     return cudaGetLastError();                                                                                  \
   } while (0)
   if (kpl <= 1) LAUNCH(1);

@@ -33,6 +33,15 @@ class Bookkeeping:
         return wf * 0.001 / float(self.N) / float(self.N)
 
 
+def allreduce_measurement(S, g, ov, scal6, group=None):
+    """The MPI_ALLREDUCE(SUM) calls of main.f90:348-369, in place on torch tensors: the partial S
+    matrix, gvec, Ovec and scal6 = (Etot, Etot2, norm, wf_av, naccept, n_samples) of every rank.
+    NCCL over NVLink for CUDA tensors; the same call runs over gloo for CPU tensors."""
+    import torch.distributed as dist
+    for t in (S, g, ov, scal6):
+        dist.all_reduce(t, op=dist.ReduceOp.SUM, group=group)
+
+
 def reduce_measurement(parts):
     """Host-side reference of the cross-rank sum: parts is a list of (scal6, S, g, ov)."""
     scal = np.sum([p[0] for p in parts], axis=0)
@@ -60,15 +69,6 @@ class SRRunner:
         self.book = Bookkeeping(inp, ctx.N)
         self._bufs = None
 
-    def launches_per_step(self) -> int:
-        """Kernel launches of one SR step (sampler, estimator, RNG advance, reductions, GEMV, S build,
-        SR element-wise kernels, blocked Cholesky and solves, Slater-element rebuild)."""
-        nv = self.ctx.Nv
-        nb = (nv + 63) // 64
-        potrf = nb + 2 * (nb - 1)
-        potrs = 2 * nb + 2 * (nb - 1)
-        return 1 + 1 + 1 + 1 + 3 + 2 + 1 + 2 + 1 + 1 + 1 + 1 + potrf + potrs + 3 + 1
-
     def step(self):
         import torch
         inp = self.p.inp
@@ -77,7 +77,6 @@ class SRRunner:
             rec = out.as_dict()
             rec["device_ms"] = self.ctx.stats()["iteration_ms"]
             return rec
-        import torch.distributed as dist
         self.iteration += 1
         ev0 = torch.cuda.Event(enable_timing=True)
         ev1 = torch.cuda.Event(enable_timing=True)
@@ -94,8 +93,7 @@ class SRRunner:
         torch.cuda.synchronize()
         self.ctx.exchange_measurement(0, S.data_ptr(), g.data_ptr(), ov.data_ptr(), scal)
         sc = torch.tensor(scal, dtype=torch.float64, device="cuda")
-        for t in (S, g, ov, sc):
-            dist.all_reduce(t)
+        allreduce_measurement(S, g, ov, sc)
         torch.cuda.synchronize()
         scal = sc.cpu().numpy()
         self.ctx.exchange_measurement(1, S.data_ptr(), g.data_ptr(), ov.data_ptr(), scal)

@@ -1,0 +1,86 @@
+"""The C++ main.f90 host program (rbm_pp_b200/rbmpp_driver) over the C ABI.
+
+CPU: its readers of RBM.input, sym_info.txt, orbitalidx.def, zqp_orbital_initial.dat and W.input agree
+with the Python readers on files written in the reference's formats.
+GPU: a short optimisation run (Nstep = 3, Nav = 2, 8 emulated ranks) reproduces the oracle's energies,
+averaged parameters and final-energy measurement (main.f90:300-575) on the same seed.
+"""
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from rbm_pp_b200 import build
+from rbm_pp_b200 import formats as fm
+
+
+def _driver():
+    build.build()
+    return build.DRIVER
+
+
+@pytest.mark.parametrize("trans,orbital", [(False, "full"), (True, "sublattice2")])
+def test_driver_reads_reference_inputs(tmp_path, trans, orbital):
+    p = fm.synthetic_problem(4, translations=trans, alphar=2, orbital=orbital, nsample=64, seed=3)
+    fm.write_problem(str(tmp_path), p)
+    out = subprocess.run([_driver(), "--dir", str(tmp_path), "--walkers", "8", "--check-inputs"],
+                         capture_output=True, text=True, timeout=60)
+    assert out.returncode == 0, out.stderr
+    t = out.stdout.split()
+    kv = {t[i]: t[i + 1] for i in range(0, len(t) - 1, 2)}
+    q = fm.read_problem(str(tmp_path))
+    assert int(kv["N"]) == 16 and int(kv["ns"]) == 8 and int(kv["alphar"]) == 2
+    assert int(kv["n_mp"]) == q.sym.n_mp and int(kv["n_slater"]) == q.n_slater
+    assert int(kv["W.input"]) == 1
+    assert abs(float(kv["mean|f|"]) - 0.25) < 1e-12
+    assert int(kv["W_map(1,last)"]) == int(q.sym.W_map[0, -1])
+    assert int(kv["orbital_idx(N,N)"]) == int(q.orbital_idx[-1, -1])
+
+
+def test_driver_rejects_bad_walker_split(tmp_path):
+    p = fm.synthetic_problem(4, translations=False, alphar=1, nsample=64, seed=3)
+    fm.write_problem(str(tmp_path), p)
+    out = subprocess.run([_driver(), "--dir", str(tmp_path), "--walkers", "7", "--check-inputs"],
+                         capture_output=True, text=True, timeout=60)
+    assert out.returncode != 0 and "multiple of --walkers" in out.stderr
+
+
+@pytest.mark.gpu
+def test_driver_run_matches_oracle(tmp_path):
+    import pyoracle as po
+    nw, ns, nstep, nav, seed = 8, 8, 3, 2, 4242
+    p = fm.synthetic_problem(4, translations=False, alphar=1, nsample=nw * ns, seed=17, Nstep=nstep, Nav=nav)
+    fm.write_problem(str(tmp_path), p)
+    out = subprocess.run([_driver(), "--dir", str(tmp_path), "--walkers", str(nw), "--seed", str(seed)],
+                         capture_output=True, text=True, timeout=600)
+    assert out.returncode == 0, out.stderr + out.stdout
+    got = np.loadtxt(os.path.join(tmp_path, "Energy_vs_Iteration.txt"))
+    # oracle: the same loop (VMCLoop restates main.f90:300-455), then the averaging and final energy
+    o = po.Oracle(p, nranks=nw, nsample_per_rank=ns, nthreads=4)
+    loop = po.VMCLoop(o, p, iseed0=seed)
+    acc = None
+    shift_av = 0.0
+    for it in range(1, nstep + 1):
+        shift_now = loop.shift
+        rec = loop.iteration_step()
+        assert abs(got[it - 1, 1] - rec["Etot"]) <= 1e-9 * abs(rec["Etot"]), (it, got[it - 1, 1], rec["Etot"])
+        if it > nstep - nav:
+            br, Wr, sl, _ = o.get_params()
+            shift_av += shift_now
+            acc = (br, Wr, sl) if acc is None else (acc[0] + br, acc[1] + Wr, acc[2] + sl)
+    br, Wr, sl = (a / nav for a in acc)
+    q = fm.read_W(os.path.join(tmp_path, "optimized_W.txt"), 16, 1)
+    assert np.allclose(q[0], br, rtol=1e-9, atol=1e-13) and np.allclose(q[1], Wr, rtol=1e-9, atol=1e-13)
+    f = fm.read_zqp(os.path.join(tmp_path, "zqp_orbital_opt.dat"), p.n_slater, rescale=False)
+    assert np.allclose(f, sl, rtol=1e-9, atol=1e-13)
+    o.set_params(br, Wr, sl, shift_av / nav)
+    o.make_sample(True)
+    for _ in range(2):
+        o.make_sample(False)
+    fin = np.loadtxt(os.path.join(tmp_path, "energy_after_opt.txt"))
+    for it in range(nav):
+        o.make_sample(False)
+        m = o.measure_energy()
+        E = m["Etot"] / m["norm"]
+        assert abs(fin[it, 1] - E) <= 1e-8 * abs(E), (it, fin[it, 1], E)
