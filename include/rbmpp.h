@@ -166,6 +166,17 @@ int rbmpp_get_walker_state(const rbmpp_ctx* ctx, int* nfastup, int* naccept_all)
  * (Ovec_loc_x before reweighting, calc_phys_quantity.f90:115-220).  Any output may be NULL. */
 int rbmpp_eval_configs(rbmpp_ctx* ctx, int n, const int* x, double* psi, double* hpsi, double* O);
 
+/* rbmpp_eval_configs without any device allocation.  No counterpart in the reference: it exists for
+ * callers that can't call cudaMalloc/cudaFree, such as a host code whose own pool allocator holds the
+ * GPU's memory, or a loop that must not be stalled by cudaFree's device-wide wait.
+ * x, psi, hpsi, O have the layouts of rbmpp_eval_configs but are DEVICE pointers on the context's
+ * device, owned by the caller (psi, hpsi, O may be NULL).  Scratch comes from one fixed array of
+ * about 2 MiB in the library's device image: at most 4096 configurations per call (more returns
+ * RBMPP_E_ARG).  The first call on a device looks up that array's device address; make that first
+ * call before any stream capture.  All calls share the array, so calls whose GPU work overlaps race:
+ * issue them one at a time.  Returns after the results are complete on the device. */
+int rbmpp_eval_configs_noalloc(rbmpp_ctx* ctx, int n, const int* d_x, double* d_psi, double* d_hpsi, double* d_O);
+
 #ifdef __cplusplus
 }
 #endif

@@ -20,7 +20,8 @@ EXPORTS = ["rbmpp_create", "rbmpp_destroy", "rbmpp_last_error", "rbmpp_query", "
            "rbmpp_set_params", "rbmpp_get_params", "rbmpp_seed_walkers", "rbmpp_rank0_grnd", "rbmpp_make_sample",
            "rbmpp_get_samples", "rbmpp_set_samples", "rbmpp_measure", "rbmpp_measure_energy", "rbmpp_sr_step",
            "rbmpp_iteration", "rbmpp_eval_configs", "rbmpp_get_stats", "rbmpp_exchange_measurement",
-           "rbmpp_set_shift", "rbmpp_get_walker_state", "rbmpp_set_s_precision"]
+           "rbmpp_set_shift", "rbmpp_get_walker_state", "rbmpp_eval_configs_noalloc",
+           "rbmpp_set_s_precision"]
 
 SR_FP64 = 0
 SR_SPLIT_BF16 = 1
@@ -84,6 +85,7 @@ def lib():
         L.rbmpp_exchange_measurement.argtypes = [P, C.c_int, P, P, P, P]
         L.rbmpp_set_shift.argtypes = [P, C.c_double]
         L.rbmpp_get_walker_state.argtypes = [P, P, P]
+        L.rbmpp_eval_configs_noalloc.argtypes = [P, C.c_int, P, P, P, P]
         L.rbmpp_set_s_precision.argtypes = [P, C.c_int]
         _lib = L
     return _lib
@@ -252,6 +254,13 @@ class Context:
         if O is not None:
             out["O"] = O.reshape(n, self.Nv)
         return out
+
+    def eval_configs_noalloc(self, n: int, d_x: int, d_psi: int, d_hpsi: int, d_O: int):
+        """rbmpp_eval_configs_noalloc on caller-owned device buffers (integer device addresses, 0 for
+        an output that is not wanted); the library allocates nothing for this call."""
+        self._chk(lib().rbmpp_eval_configs_noalloc(self.h, int(n), C.c_void_p(d_x or None),
+                                                   C.c_void_p(d_psi or None), C.c_void_p(d_hpsi or None),
+                                                   C.c_void_p(d_O or None)))
 
 
 def initial_params(ctx: Context, problem):

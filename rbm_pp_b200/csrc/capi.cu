@@ -10,6 +10,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -1142,3 +1143,99 @@ int rbmpp_get_stats(const rbmpp_ctx* c, double* out, int n) {
 }
 
 }  // extern "C"
+
+// ===================================================================================================
+// rbmpp_eval_configs_noalloc: rbmpp_eval_configs for callers that must not allocate device memory.
+//
+// rbmpp_eval_configs allocates and frees device buffers on every call.  Some callers can't allow that:
+// a host code whose own pool allocator has reserved the GPU's memory up front (a cudaMalloc from the
+// library would then fail, or fragment the pool), or a loop that must not stall other streams (cudaFree
+// waits for all work on the device).  This entry point takes the configurations and the results in
+// device memory that the caller owns.  Its only scratch, the int8 copy of the configurations and one
+// status word per configuration, lives in the fixed array below, which is part of the library's device
+// image: every GPU that loads the library holds it until the process exits.
+//
+// Every call shares that array, and it keeps what the last call wrote.  The status words are written
+// for every configuration of the call and the error word is cleared at the start of each call, so no
+// stale value is read; but two calls whose work overlaps on the GPU (two contexts on one device driven
+// from two host threads, say) race on the array.
+// ===================================================================================================
+namespace {
+
+constexpr int kNoAllocMaxConfigs = 4096;                                        // configurations per call
+constexpr size_t kNoAllocX8 = (size_t)kNoAllocMaxConfigs * RBMPP_MAX_N;         // int8 spins: 2 MiB
+constexpr size_t kNoAllocStatus = kNoAllocX8;                                   // offset of the status words
+constexpr size_t kNoAllocBad = kNoAllocStatus + 4 * (size_t)kNoAllocMaxConfigs;  // offset of the error word
+constexpr size_t kNoAllocBytes = kNoAllocBad + 256;
+
+static __device__ __align__(256) unsigned char g_eval_scratch[kNoAllocBytes];
+
+// Device address of g_eval_scratch on each device, looked up on the first call there.
+std::mutex g_noalloc_mu;
+void* g_noalloc_addr[64] = {};
+
+// Records n - i for the first configuration i whose status is non-zero (atomicMax keeps the smallest i).
+__global__ void first_bad_kernel(const int* status, int n, int* bad) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n && status[i] != 0) atomicMax(bad, n - i);
+}
+
+int noalloc_run(rbmpp_ctx* c, int n, const int* d_x, double* d_psi, double* d_hpsi, double* d_O) {
+  const int dev = c->dims.device;
+  unsigned char* base = nullptr;
+  {
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_addr[dev]) {
+      void* p = nullptr;
+      cudaError_t e = cudaGetSymbolAddress(&p, g_eval_scratch);
+      if (e != cudaSuccess || !p)
+        return fail(c, RBMPP_E_CUDA, "cudaGetSymbolAddress(g_eval_scratch) on device %d: %s", dev,
+                    cudaGetErrorString(e));
+      g_noalloc_addr[dev] = p;
+    }
+    base = (unsigned char*)g_noalloc_addr[dev];
+  }
+  int8_t* x8 = (int8_t*)base;
+  int* status = (int*)(base + kNoAllocStatus);
+  int* bad = (int*)(base + kNoAllocBad);
+  const long long nx = (long long)n * c->d.N;
+  CK(cudaMemsetAsync(bad, 0, sizeof(int), c->st));
+  rbmpp_note_launch();
+  int_to_i8_kernel<<<(unsigned)((nx + 255) / 256), 256, 0, c->st>>>(d_x, x8, nx);
+  CK(cudaGetLastError());
+  CK(rbmpp_launch_estimator(c->d, tables(c), params(c), x8, n, d_psi, d_hpsi, d_O, nullptr, status, 0, c->st));
+  rbmpp_note_launch();
+  first_bad_kernel<<<(n + 255) / 256, 256, 0, c->st>>>(status, n, bad);
+  CK(cudaGetLastError());
+  int hbad = 0;
+  CK(cudaMemcpyAsync(&hbad, bad, sizeof(int), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  if (hbad) {
+    const int i = n - hbad;
+    int code = 0;
+    CK(cudaMemcpy(&code, status + i, sizeof(int), cudaMemcpyDeviceToHost));
+    return fail(c, code, "eval_configs_noalloc failed on configuration %d (code %d)", i, code);
+  }
+  return 0;
+}
+
+}  // namespace
+
+extern "C" int rbmpp_eval_configs_noalloc(rbmpp_ctx* c, int n, const int* d_x, double* d_psi, double* d_hpsi,
+                                          double* d_O) {
+  if (!c || n < 0 || (n > 0 && !d_x)) return fail(c, RBMPP_E_ARG, "eval_configs_noalloc: bad arguments");
+  if (n > kNoAllocMaxConfigs)
+    return fail(c, RBMPP_E_ARG, "eval_configs_noalloc: n = %d configurations exceeds the fixed scratch limit of %d",
+                n, kNoAllocMaxConfigs);
+  if (c->dims.device < 0 || c->dims.device >= 64)
+    return fail(c, RBMPP_E_ARG, "eval_configs_noalloc: device ordinal %d outside 0..63", c->dims.device);
+  if (!c->params_set) return fail(c, RBMPP_E_STATE, "set_params must come first");
+  if (n == 0) return 0;
+  // the scratch address and every launch belong to the context's device: make it current for the call
+  int prev = -1;
+  CK(cudaGetDevice(&prev));
+  if (prev != c->dims.device) CK(cudaSetDevice(c->dims.device));
+  const int r = noalloc_run(c, n, d_x, d_psi, d_hpsi, d_O);
+  if (prev != c->dims.device) cudaSetDevice(prev);
+  return r;
+}
