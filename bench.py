@@ -38,6 +38,8 @@ WORKLOADS = {
     # same lattice without translation projection (2 Pfaffian blocks per walker)
     "j1j2_10x10_single": dict(L=10, translations=False, alphar=4, orbital="full", walkers=4096, ns=16, J2=0.5),
     "j1j2_6x6_trans_small": dict(L=6, translations=True, alphar=2, orbital="full", walkers=256, ns=16, J2=0.5),
+    # 10x10 without translation projection, 16384 samples: a few-GB profiling case of the S build (Nv = 10404)
+    "j1j2_10x10_single_16k": dict(L=10, translations=False, alphar=4, orbital="full", walkers=1024, ns=16, J2=0.5),
     # one wave of walkers (one per SM), one stored sample each: the profiling case of the 10x10 kernels
     "j1j2_10x10_trans_1wave": dict(L=10, translations=True, alphar=4, orbital="full", walkers=148, ns=1, J2=0.5),
 }
