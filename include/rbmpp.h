@@ -81,6 +81,9 @@ typedef struct {
   double delW_max, s_factor, sdiag_av, smat_scaling;
   double refine_residual;            /* relative residual ||g - S x|| / ||g|| against the exact S
                                         (RBMPP_SR_SPLIT_BF16 with refinement; 0 otherwise)      */
+  double precond_shift;              /* extra diagonal added to the split-precision S before its
+                                        Cholesky when S + shift was not positive definite at
+                                        working precision (0 when none was needed)              */
   int kmax, k_nonzero, nSmat;
   int refine_iterations;             /* conjugate-gradient iterations taken                       */
 } rbmpp_sr_out;

@@ -43,7 +43,7 @@ class SrOut(C.Structure):
                 ("accept_ratio", C.c_double), ("lambda_", C.c_double), ("lambda_rbm_rbm", C.c_double),
                 ("lambda_pp_pp", C.c_double), ("lambda_rbm_pp", C.c_double), ("delW_max", C.c_double),
                 ("s_factor", C.c_double), ("sdiag_av", C.c_double), ("smat_scaling", C.c_double),
-                ("refine_residual", C.c_double), ("kmax", C.c_int), ("k_nonzero", C.c_int), ("nSmat", C.c_int),
+                ("refine_residual", C.c_double), ("precond_shift", C.c_double), ("kmax", C.c_int), ("k_nonzero", C.c_int), ("nSmat", C.c_int),
                 ("refine_iterations", C.c_int)]
 
     def as_dict(self):

@@ -126,6 +126,7 @@ struct rbmpp_ctx {
   double *d_gvec = nullptr, *d_Ovec = nullptr, *d_S = nullptr, *d_part = nullptr, *d_vec = nullptr;
   double *d_tmp_ns = nullptr, *d_rv = nullptr;
   int *d_info = nullptr, *d_err = nullptr;
+  double* d_Sb = nullptr;  // copy of the shifted split-precision S (preconditioner retries)
   void *d_hi = nullptr, *d_lo = nullptr;
   int ldk = 0;
   float* d_Sf = nullptr;
@@ -454,7 +455,7 @@ int rbmpp_destroy(rbmpp_ctx* c) {
                   c->d_XF, c->d_XFT, c->W.x, c->W.idx, c->W.cfg, c->W.th, c->W.sgn, c->W.pf, c->W.psi, c->W.Y,
                   c->W.mt, c->W.nfastup, c->W.naccept, c->W.nacc_all, c->W.status, c->W.xs, c->W.pfs, c->W.psis, c->d_O, c->d_psiS,
                   c->d_eloc, c->d_a, c->d_b, c->d_tmp_ns, c->d_acc4, c->d_nap, c->d_estat, c->d_gvec, c->d_Ovec,
-                  c->d_vec, c->d_S, c->d_part, c->d_info, c->d_err, c->d_rv, c->d_hi, c->d_lo, c->d_Sf};
+                  c->d_vec, c->d_S, c->d_part, c->d_info, c->d_err, c->d_rv, c->d_hi, c->d_lo, c->d_Sf, c->d_Sb};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   for (auto& e : c->ev)
@@ -881,9 +882,29 @@ int rbmpp_sr_step(rbmpp_ctx* c, const rbmpp_sr_in* in, rbmpp_sr_out* out, double
   CK(rbmpp_launch_advance_rng(c->W.mt, nullptr, 0, d.nw, 1, c->st));
   // pdposv('U') :232 -> Cholesky of the upper triangle + solve
   CK(cudaEventRecord(c->ev[7], c->st));
-  CK(rbmpp_potrf_upper(Nv, c->d_S, c->d_info, c->st));
+  const size_t s_bytes = (size_t)Nv * Nv * sizeof(double);
+  if (in->precision == RBMPP_SR_SPLIT_BF16) {
+    // the split-precision factor only preconditions the refinement on the exact S: if the split S plus the
+    // reference's shift is not positive definite at working precision, factor it with a larger diagonal
+    if (!c->d_Sb) {
+      cudaError_t e = cudaMalloc(&c->d_Sb, s_bytes);
+      if (e) return fail(c, RBMPP_E_CUDA, "cudaMalloc(S backup, %zu bytes): %s", s_bytes, cudaGetErrorString(e));
+      c->bytes += s_bytes;
+    }
+    CK(cudaMemcpyAsync(c->d_Sb, c->d_S, s_bytes, cudaMemcpyDeviceToDevice, c->st));
+  }
   int info = 0;
-  CK(cudaMemcpyAsync(&info, c->d_info, sizeof(int), cudaMemcpyDeviceToHost, c->st));
+  double tau = 0.0;
+  for (int attempt = 0;; attempt++) {
+    CK(rbmpp_potrf_upper(Nv, c->d_S, c->d_info, c->st));
+    CK(cudaMemcpyAsync(&info, c->d_info, sizeof(int), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    if (info == 0 || in->precision != RBMPP_SR_SPLIT_BF16 || in->refine_steps <= 0 || attempt == 12) break;
+    tau = tau == 0.0 ? sdiag * s_factor : 4.0 * tau;
+    CK(cudaMemcpyAsync(c->d_S, c->d_Sb, s_bytes, cudaMemcpyDeviceToDevice, c->st));
+    CK(rbmpp_add_diag(Nv, c->d_S, tau, c->st));
+  }
+  out->precond_shift = tau;
   CK(cudaMemcpyAsync(d_x, g.data(), sizeof(double) * Nv, cudaMemcpyHostToDevice, c->st));
   CK(cudaStreamSynchronize(c->st));
   if (info != 0) return fail(c, RBMPP_E_CHOL, "info (pdposv): %d", info);
