@@ -24,7 +24,6 @@ struct Stream {
   double* stage;  // [ST][Np*Np]; also the Gauss-Jordan tile outside passes
   uint64_t* full;
   uint64_t* empty;
-  int* dirty;
   double* wU0;  // [kWarps][Np] gathered row / column of the deferred exchange
   double* wV0;
   double* wS;   // [kWarps][Np] Y v of the deferred exchange
@@ -48,7 +47,6 @@ __host__ __device__ __forceinline__ size_t stream_layout(const DevDims& d, int S
   t.stage = (double*)take(stage_bytes > gj ? stage_bytes : gj, 128);
   t.full = (uint64_t*)take(8 * (size_t)ST, 8);
   t.empty = (uint64_t*)take(8 * (size_t)ST, 8);
-  t.dirty = (int*)take(4 * (size_t)ST, 4);
   t.wU0 = (double*)take((size_t)kWarps * d.Np * 8, 16);
   t.wV0 = (double*)take((size_t)kWarps * d.Np * 8, 16);
   t.wS = (double*)take((size_t)kWarps * d.Np * 8, 16);
@@ -62,6 +60,14 @@ struct Move {
   int ua, db, s_up, s_dn;  // up electron, down electron (local index), their sites before the move
 };
 
+// Tile math is templated on KPL (columns per lane) and NP: NP > 0 is the block size Np known at compile time
+// (the even-L lattices 4x4 .. 10x10 have Np = 8, 18, 32, 50), so loops unroll fully and tile addresses
+// become immediate offsets; NP = 0 reads Np from the dimensions.
+template <int NP>
+__device__ __forceinline__ int np_of(const DevDims& d) {
+  return NP > 0 ? NP : d.Np;
+}
+
 // Lane-held gathers of one exchange for one projection: u = new row ua of X, v = new column db of X,
 // c = their shared corner (the gathers of pfupdate_two.f90:48-52 in block form).
 template <int KPL>
@@ -69,10 +75,10 @@ struct UV {
   double u[KPL], v[KPL], c;
 };
 
-template <int KPL>
+template <int KPL, int NP>
 __device__ __forceinline__ void gather_regs(const DevDims& d, const DevParams& p, int qp, const int* idx,
                                             const Move& m, UV<KPL>& g) {
-  const int lane = threadIdx.x & 31, Np = d.Np, N = d.N;
+  const int lane = threadIdx.x & 31, Np = np_of<NP>(d), N = d.N;
   const double* XFq = p.XF + (size_t)qp * N * N;
   const double* XFTq = p.XFT + (size_t)qp * N * N;
   g.c = __ldg(XFq + (size_t)m.s_dn * N + m.s_up);
@@ -88,13 +94,13 @@ __device__ __forceinline__ void gather_regs(const DevDims& d, const DevParams& p
   }
 }
 
-template <int KPL>
+template <int KPL, int NP>
 __device__ __forceinline__ double store_regs(const DevDims& d, const Move& m, const UV<KPL>& g, double* u, double* v) {
-  const int lane = threadIdx.x & 31;
+  const int lane = threadIdx.x & 31, Np = np_of<NP>(d);
 #pragma unroll
   for (int q = 0; q < KPL; q++) {
     const int j = lane + 32 * q;
-    if (j < d.Np) {
+    if (j < Np) {
       u[j] = (j == m.db) ? g.c : g.u[q];
       v[j] = (j == m.ua) ? g.c : g.v[q];
     }
@@ -102,33 +108,76 @@ __device__ __forceinline__ double store_regs(const DevDims& d, const Move& m, co
   return g.c;
 }
 
-// Deferred rank-2 update of the tile for an accepted exchange (the algebra of pfupdate_two.f90:113-224
-// in block form): Y' = Y - A B^T / R1 - s1 t1^T / R2, with A = Y e_ua, B = u^T Y - e_ua^T,
-// s1 = Y v - A (u^T Y v - c)/R1 - e_db, t1 = e_db^T Y - Y(db,ua) B^T / R1, R2 = R / R1.
-template <int KPL>
-__device__ __forceinline__ void warp_apply_update(const DevDims& d, double* Y, const Move& m, double c, const double* u,
-                                                  const double* v, double* S, double* A) {
-  const int lane = threadIdx.x & 31, Np = d.Np;
-  double acc[KPL], rho[KPL];
+// acc[q] = (u^T Y)_k for the lane's columns k = lane + 32 q, as two interleaved FMA chains (even and odd
+// rows) so consecutive FMAs do not wait on each other.
+template <int KPL, int NP>
+__device__ __forceinline__ void col_sums(const double* Y, const double* u, int Np, double (&acc)[KPL]) {
+  const int lane = threadIdx.x & 31;
+  double a1[KPL];
 #pragma unroll
-  for (int q = 0; q < KPL; q++) acc[q] = 0.0;
-#pragma unroll 5
-  for (int j = 0; j < Np; j++) {
-    const double uj = u[j];
+  for (int q = 0; q < KPL; q++) acc[q] = a1[q] = 0.0;
+  constexpr int UNR = NP > 0 ? NP / 2 : 4;
+#pragma unroll UNR
+  for (int j = 0; j + 1 < Np; j += 2) {
+    const double u0 = u[j], u1 = u[j + 1];
 #pragma unroll
     for (int q = 0; q < KPL; q++) {
       const int k = lane + 32 * q;
-      if (k < Np) acc[q] = fma(uj, Y[j * Np + k], acc[q]);
+      if (k < Np) {
+        acc[q] = fma(u0, Y[j * Np + k], acc[q]);
+        a1[q] = fma(u1, Y[(j + 1) * Np + k], a1[q]);
+      }
     }
   }
-  for (int j = lane; j < Np; j += 32) {  // row sums, lane <-> row
-    double a = 0.0;
-#pragma unroll 5
-    for (int k = 0; k < Np; k++) a = fma(Y[j * Np + k], v[k], a);
-    S[j] = a;
+  if (Np & 1) {
+    const int j = Np - 1;
+#pragma unroll
+    for (int q = 0; q < KPL; q++) {
+      const int k = lane + 32 * q;
+      if (k < Np) acc[q] = fma(u[j], Y[j * Np + k], acc[q]);
+    }
+  }
+#pragma unroll
+  for (int q = 0; q < KPL; q++) acc[q] += a1[q];
+}
+
+// value of acc at column k0, taken from the lane that owns it (valid on all lanes)
+template <int KPL>
+__device__ __forceinline__ double lane_pick(const double (&acc)[KPL], int k0) {
+  double mine = 0.0;
+#pragma unroll
+  for (int q = 0; q < KPL; q++)
+    if (q == (k0 >> 5)) mine = acc[q];
+  return __shfl_sync(0xffffffffu, mine, k0 & 31);
+}
+
+// Deferred rank-2 update of the tile for an accepted exchange (the algebra of pfupdate_two.f90:113-224
+// in block form): Y' = Y - A B^T / R1 - s1 t1^T / R2, with A = Y e_ua, B = u^T Y - e_ua^T,
+// s1 = Y v - A (u^T Y v - c)/R1 - e_db, t1 = e_db^T Y - Y(db,ua) B^T / R1, R2 = R / R1.
+template <int KPL, int NP>
+__device__ __forceinline__ void warp_apply_update(const DevDims& d, double* Y, const Move& m, double c, const double* u,
+                                                  const double* v, double* S, double* A) {
+  const int lane = threadIdx.x & 31, Np = np_of<NP>(d);
+  double acc[KPL], rho[KPL];
+  col_sums<KPL, NP>(Y, u, Np, acc);
+  // row sums S = Y v, lane <-> row; each lane starts its row at a different column so the 64-bit
+  // shared loads of a half-warp fall in distinct banks
+  constexpr int UNR = NP > 0 ? NP / 2 : 4;
+  for (int j = lane; j < Np; j += 32) {
+    double a0 = 0.0, a1 = 0.0;
+    int k = j % Np;
+#pragma unroll UNR
+    for (int kk = 0; kk + 1 < Np; kk += 2) {
+      const int k1 = (k + 1 == Np) ? 0 : k + 1;
+      a0 = fma(Y[j * Np + k], v[k], a0);
+      a1 = fma(Y[j * Np + k1], v[k1], a1);
+      k = (k1 + 1 == Np) ? 0 : k1 + 1;
+    }
+    if (Np & 1) a0 = fma(Y[j * Np + k], v[k], a0);
+    S[j] = a0 + a1;
     A[j] = Y[j * Np + m.ua];
   }
-  double wv = 0.0, ra = 0.0, ydbua = 0.0;
+  double wv = 0.0;
 #pragma unroll
   for (int q = 0; q < KPL; q++) {
     const int k = lane + 32 * q;
@@ -136,15 +185,11 @@ __device__ __forceinline__ void warp_apply_update(const DevDims& d, double* Y, c
     if (k < Np) {
       rho[q] = Y[m.db * Np + k];
       wv = fma(acc[q], v[k], wv);
-      if (k == m.ua) {
-        ra = acc[q];
-        ydbua = rho[q];
-      }
     }
   }
+  const double ra = lane_pick<KPL>(acc, m.ua);
+  const double ydbua = Y[m.db * Np + m.ua];
   wv = warp_sum(wv);
-  ra = warp_sum(ra);
-  ydbua = warp_sum(ydbua);
   __syncwarp();
   const double R1 = ra, R = ra * S[m.db] - ydbua * (wv - c);
   const double inv_r1 = 1.0 / R1, r1_over_r = R1 / R, wc = (wv - c) * inv_r1;
@@ -156,7 +201,8 @@ __device__ __forceinline__ void warp_apply_update(const DevDims& d, double* Y, c
     bk[q] = B * inv_r1;
     tk[q] = (rho[q] - ydbua * B * inv_r1) * r1_over_r;
   }
-#pragma unroll 4
+  constexpr int UNR2 = NP > 0 ? NP : 4;
+#pragma unroll UNR2
   for (int j = 0; j < Np; j++) {
     const double Aj = A[j];
     const double s1 = S[j] - Aj * wc - (j == m.db ? 1.0 : 0.0);
@@ -170,40 +216,28 @@ __device__ __forceinline__ void warp_apply_update(const DevDims& d, double* Y, c
 }
 
 // Ratio R = (u^T Y)_ua (Y v)_db - Y(db,ua) (u^T Y v - c) on the shared-memory tile
-template <int KPL>
+template <int KPL, int NP>
 __device__ __forceinline__ double warp_tile_ratio(const DevDims& d, const double* Y, const Move& m, double c,
                                                   const double* u, const double* v) {
-  const int lane = threadIdx.x & 31, Np = d.Np;
+  const int lane = threadIdx.x & 31, Np = np_of<NP>(d);
   double acc[KPL];
-#pragma unroll
-  for (int q = 0; q < KPL; q++) acc[q] = 0.0;
-#pragma unroll 5
-  for (int j = 0; j < Np; j++) {
-    const double uj = u[j];
-#pragma unroll
-    for (int q = 0; q < KPL; q++) {
-      const int k = lane + 32 * q;
-      if (k < Np) acc[q] = fma(uj, Y[j * Np + k], acc[q]);
-    }
-  }
-  double wv = 0.0, sb = 0.0, ra = 0.0, ydbua = 0.0;
+  col_sums<KPL, NP>(Y, u, Np, acc);
+  double wv = 0.0, sb = 0.0;
 #pragma unroll
   for (int q = 0; q < KPL; q++) {
     const int k = lane + 32 * q;
     if (k < Np) {
-      const double rho = Y[m.db * Np + k];
       wv = fma(acc[q], v[k], wv);
-      sb = fma(rho, v[k], sb);
-      if (k == m.ua) {
-        ra = acc[q];
-        ydbua = rho;
-      }
+      sb = fma(Y[m.db * Np + k], v[k], sb);
     }
   }
-  wv = warp_sum(wv);
-  sb = warp_sum(sb);
-  ra = warp_sum(ra);
-  ydbua = warp_sum(ydbua);
+  const double ra = lane_pick<KPL>(acc, m.ua);
+  const double ydbua = Y[m.db * Np + m.ua];
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    wv += __shfl_xor_sync(0xffffffffu, wv, o);
+    sb += __shfl_xor_sync(0xffffffffu, sb, o);
+  }
   return ra * sb - ydbua * (wv - c);
 }
 
@@ -212,14 +246,10 @@ struct Pipe {
   int last_issued[16];  // per stage: last tile index loaded (thread 0 only), -1 if none
 };
 
-__device__ __forceinline__ void bulk_wait_older_than_8() { asm volatile("cp.async.bulk.wait_group 8;" ::: "memory"); }
-
-// producer (thread 0): first min(ST, n_qp) loads of a pass.  Stores of the previous pass for these
-// projections completed long ago unless the pass is short.
+// producer (thread 0): first min(ST, n_qp) loads of a pass.  Every store of the previous pass has
+// completed: the consumer that issued it waited for it before the pass-ending barrier.
 __device__ __forceinline__ void pass_issue_first(const SCtx& c, const Stream& sm, Pipe& pp) {
   const int n = c.d.n_qp, n0 = n < sm.ST ? n : sm.ST;
-  if (n < 2 * sm.ST) bulk_wait_all();
-  else bulk_wait_older_than_8();
   fence_proxy_async_global();
   const size_t NN = (size_t)c.d.Np * c.d.Np;
   for (int t = 0; t < n0; t++) {
@@ -231,42 +261,19 @@ __device__ __forceinline__ void pass_issue_first(const SCtx& c, const Stream& sm
   }
 }
 
-// producer (thread 0): refill the ring for the rest of the pass and store released modified tiles
+// producer (thread 0): refill each stage as soon as its consumer releases it
 __device__ __forceinline__ bool pass_produce(const SCtx& c, const Stream& sm, Pipe& pp, volatile int* abort_flag) {
   const int n = c.d.n_qp, ST = sm.ST;
   const size_t NN = (size_t)c.d.Np * c.d.Np;
-  bool waited_tail = false;
   for (int t = ST; t < n; t++) {
     uint32_t T = pp.T0 + t, Tp = T - ST;
     int s = (int)(T % ST);
     if (!mbar_wait(&sm.empty[s], (Tp / ST) & 1u)) return false;
-    if (sm.dirty[s]) {
-      bulk_store(c.Yw + (size_t)(t - ST) * NN, sm.stage + (size_t)s * NN, sm.tile_bytes);
-      bulk_commit();
-      bulk_wait_read_all();
-      sm.dirty[s] = 0;
-    }
     if (*abort_flag) return false;
-    if (!waited_tail && t >= n - ST) {  // these projections were stored at the end of the previous pass
-      bulk_wait_all();
-      fence_proxy_async_global();
-      waited_tail = true;
-    }
     mbar_arrive_expect_tx(&sm.full[s], sm.tile_bytes);
     bulk_load(sm.stage + (size_t)s * NN, c.Yw + (size_t)t * NN, sm.tile_bytes, &sm.full[s]);
     pp.last_issued[s] = (int)T;
   }
-  for (int t = (n > ST ? n - ST : 0); t < n; t++) {
-    uint32_t T = pp.T0 + t;
-    int s = (int)(T % ST);
-    if (!mbar_wait(&sm.empty[s], (T / ST) & 1u)) return false;
-    if (sm.dirty[s]) {
-      bulk_store(c.Yw + (size_t)t * NN, sm.stage + (size_t)s * NN, sm.tile_bytes);
-      bulk_commit();
-      sm.dirty[s] = 0;
-    }
-  }
-  bulk_wait_read_all();
   return true;
 }
 
@@ -323,7 +330,7 @@ __device__ __forceinline__ void control_propose(const SCtx& c, volatile int* can
 }
 
 // consumers: deferred update (pend) and/or proposal ratio (prop) per tile
-template <int KPL>
+template <int KPL, int NP>
 __device__ __forceinline__ bool pass_consume(const SCtx& c, const Stream& sm, const Pipe& pp, bool pend,
                                              const Move& mk, bool prop, volatile int* cand_flag, int pass_id,
                                              const int* mv, double& pre, double& pim, volatile int* abort_flag) {
@@ -341,22 +348,23 @@ __device__ __forceinline__ bool pass_consume(const SCtx& c, const Stream& sm, co
   Move mn{0, 0, 0, 0};
   bool have_move = false;
   int t = warp - 1;
-  if (pend && t < n) gather_regs<KPL>(d, c.p, t, s.idx, mk, gk);
+  bool stored = false;
+  if (pend && t < n) gather_regs<KPL, NP>(d, c.p, t, s.idx, mk, gk);
   for (; t < n; t += kConsumers) {
     const uint32_t T = pp.T0 + t;
     const int st = (int)(T % sm.ST);
     const int tn = t + kConsumers;
     double ck = 0.0;
     if (pend) {
-      ck = store_regs<KPL>(d, mk, gk, U0, V0);
-      if (tn < n) gather_regs<KPL>(d, c.p, tn, s.idx, mk, gk);
+      ck = store_regs<KPL, NP>(d, mk, gk, U0, V0);
+      if (tn < n) gather_regs<KPL, NP>(d, c.p, tn, s.idx, mk, gk);
     }
     __syncwarp();
     if (*abort_flag) return false;
     if (!mbar_wait(&sm.full[st], (T / sm.ST) & 1u)) return false;
     double* Y = sm.stage + (size_t)st * NN;
     if (pend) {
-      warp_apply_update<KPL>(d, Y, mk, ck, U0, V0, S0, A0);
+      warp_apply_update<KPL, NP>(d, Y, mk, ck, U0, V0, S0, A0);
       fence_proxy_async_smem();
     }
     if (prop) {
@@ -375,12 +383,12 @@ __device__ __forceinline__ bool pass_consume(const SCtx& c, const Stream& sm, co
         if (!ok || status(c)) return false;
         mn = Move{mv[0], mv[1], mv[2], mv[3]};
         have_move = true;
-        gather_regs<KPL>(d, c.p, t, s.idx, mn, gn);
+        gather_regs<KPL, NP>(d, c.p, t, s.idx, mn, gn);
       }
-      const double cn = store_regs<KPL>(d, mn, gn, u, v);
+      const double cn = store_regs<KPL, NP>(d, mn, gn, u, v);
       __syncwarp();
-      if (tn < n) gather_regs<KPL>(d, c.p, tn, s.idx, mn, gn);
-      const double R = warp_tile_ratio<KPL>(d, Y, mn, cn, u, v);
+      if (tn < n) gather_regs<KPL, NP>(d, c.p, tn, s.idx, mn, gn);
+      const double R = warp_tile_ratio<KPL, NP>(d, Y, mn, cn, u, v);
       if (lane == 0) {
         const double pfn = R * s.pf[t];
         s.pfp[t] = pfn;
@@ -393,16 +401,26 @@ __device__ __forceinline__ bool pass_consume(const SCtx& c, const Stream& sm, co
     }
     __syncwarp();
     if (lane == 0) {
-      if (pend) sm.dirty[st] = 1;
+      if (pend) {  // write the updated tile back; the stage is released once the copy has read it
+        bulk_store(c.Yw + (size_t)t * NN, Y, sm.tile_bytes);
+        bulk_commit();
+        bulk_wait_read_all();
+        stored = true;
+      }
       mbar_arrive(&sm.empty[st]);
     }
   }
+  if (lane == 0 && stored) {  // the next pass reloads these tiles: their stores must have landed
+    bulk_wait_all();
+    fence_proxy_async_global();
+  }
+  __syncwarp();
   return true;
 }
 
 // One pass over all projections (all threads).  prop: evaluate a new proposal (control warp draws
 // it); pend: apply the deferred update of the previously accepted exchange mk.
-template <int KPL>
+template <int KPL, int NP>
 __device__ __forceinline__ void run_pass(const SCtx& c, const Stream& sm, Pipe& pp, bool pend, const Move& mk,
                                          bool prop, volatile int* cand_flag, int pass_id, int* mv,
                                          volatile int* abort_flag) {
@@ -415,11 +433,12 @@ __device__ __forceinline__ void run_pass(const SCtx& c, const Stream& sm, Pipe& 
     if (prop) control_propose(c, cand_flag, pass_id, mv);
     if (lane == 0 && !status(c)) ok = pass_produce(c, sm, pp, abort_flag);
   } else {
-    ok = pass_consume<KPL>(c, sm, pp, pend, mk, prop, cand_flag, pass_id, mv, pre, pim, abort_flag);
+    ok = pass_consume<KPL, NP>(c, sm, pp, pend, mk, prop, cand_flag, pass_id, mv, pre, pim, abort_flag);
   }
   if (!ok) {
     *abort_flag = 1;
     if (!status(c)) status(c) = ST_TIMEOUT;
+    bulk_wait_all();  // this thread's stores in flight, if any
   }
   if (lane == 0 && warp > 0) {
     c.s.red[warp] = pre;
@@ -438,7 +457,7 @@ __device__ __forceinline__ void drain(const SCtx& c) {
   __syncthreads();
 }
 
-template <int KPL>
+template <int KPL, int NP>
 __global__ void __launch_bounds__(kWarps * 32, 1)
     sampler_stream_kernel(const __grid_constant__ DevDims d, const __grid_constant__ DevTables t,
                           const __grid_constant__ DevParams p, const __grid_constant__ DevWalkers W, int first,
@@ -455,7 +474,6 @@ __global__ void __launch_bounds__(kWarps * 32, 1)
     for (int k = 0; k < ST; k++) {
       mbar_init(&sm.full[k], 1);
       mbar_init(&sm.empty[k], 1);
-      sm.dirty[k] = 0;
     }
     fence_mbar_init();
     pend_s[0] = 0;
@@ -493,7 +511,7 @@ __global__ void __launch_bounds__(kWarps * 32, 1)
     if (nacc_tmp > nfastup) {
       if (pend_s[0]) {  // apply the deferred update before the drift check
         const Move mk{pend_s[1], pend_s[2], pend_s[3], pend_s[4]};
-        run_pass<KPL>(c, sm, pp, true, mk, false, &cand_flag, ++pass_id, mv, &abort_flag);
+        run_pass<KPL, NP>(c, sm, pp, true, mk, false, &cand_flag, ++pass_id, mv, &abort_flag);
         if (tid == 0) pend_s[0] = 0;
       }
       drain(c);
@@ -514,7 +532,7 @@ __global__ void __launch_bounds__(kWarps * 32, 1)
       }
       const bool pend = pend_s[0] != 0;
       const Move mk{pend_s[1], pend_s[2], pend_s[3], pend_s[4]};
-      run_pass<KPL>(c, sm, pp, pend, mk, true, &cand_flag, ++pass_id, mv, &abort_flag);
+      run_pass<KPL, NP>(c, sm, pp, pend, mk, true, &cand_flag, ++pass_id, mv, &abort_flag);
       if (status(c)) break;
       const int i1 = s.iflag[F_I1], i2 = s.iflag[F_I2];
       const int i3 = s.cfg[i1], i4 = s.cfg[i2];
@@ -582,14 +600,13 @@ __global__ void __launch_bounds__(kWarps * 32, 1)
   }
   if (!status(c) && pend_s[0]) {  // leave Y consistent with the final state
     const Move mk{pend_s[1], pend_s[2], pend_s[3], pend_s[4]};
-    run_pass<KPL>(c, sm, pp, true, mk, false, &cand_flag, ++pass_id, mv, &abort_flag);
+    run_pass<KPL, NP>(c, sm, pp, true, mk, false, &cand_flag, ++pass_id, mv, &abort_flag);
   }
   // every bulk copy of this CTA has landed before the CTA exits (bounded waits)
-  if (tid == 0) {
+  if (tid == 0)
     for (int k = 0; k < sm.ST && k < 16; k++)
       if (pp.last_issued[k] >= 0) (void)mbar_wait(&sm.full[k], ((uint32_t)pp.last_issued[k] / sm.ST) & 1u);
-    bulk_wait_all();
-  }
+  bulk_wait_all();
   __syncthreads();
   for (int k = tid; k < 625; k += blockDim.x) W.mt[(size_t)w * 625 + k] = s.mt[k];
   for (int i = tid; i < N; i += blockDim.x) {
@@ -627,16 +644,23 @@ cudaError_t rbmpp_launch_sampler_stream(const DevDims& d, const DevTables& t, co
                                         int first, int st, cudaStream_t stream) {
   size_t smem = rbmpp_stream_smem(d, st);
   int kpl = (d.Np + 31) / 32;
-#define LAUNCH(K)                                                                                               \
-  do {                                                                                                          \
-    cudaError_t e = cudaFuncSetAttribute(sampler_stream_kernel<K>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
-                                         (int)smem);                                                            \
-    if (e != cudaSuccess) return e;                                                                             \
-    rbmpp_note_launch(); sampler_stream_kernel<K><<<d.nw, kWarps * 32, smem, stream>>>(d, t, p, W, first, st);                       \
-    return cudaGetLastError();                                                                                  \
+#define LAUNCH(K, NPC)                                                                                        \
+  do {                                                                                                        \
+    cudaError_t e = cudaFuncSetAttribute(sampler_stream_kernel<K, NPC>,                                       \
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);             \
+    if (e != cudaSuccess) return e;                                                                           \
+    rbmpp_note_launch(); sampler_stream_kernel<K, NPC><<<d.nw, kWarps * 32, smem, stream>>>(d, t, p, W, first, st); \
+    return cudaGetLastError();                                                                                \
   } while (0)
-  if (kpl <= 1) LAUNCH(1);
-  if (kpl <= 2) LAUNCH(2);
+  switch (d.Np) {  // block sizes of the even-L lattices with a compile-time specialisation
+    case 8: LAUNCH(1, 8);
+    case 18: LAUNCH(1, 18);
+    case 32: LAUNCH(1, 32);
+    case 50: LAUNCH(2, 50);
+    default: break;
+  }
+  if (kpl <= 1) LAUNCH(1, 0);
+  if (kpl <= 2) LAUNCH(2, 0);
 #undef LAUNCH
   return cudaErrorInvalidValue;
 }

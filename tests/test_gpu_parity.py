@@ -125,7 +125,8 @@ def test_sr_iterations_stay_in_lockstep():
     g.close()
 
 
-@pytest.mark.parametrize("L,trans,alphar,nw,ns", [(4, True, 1, 4, 8), (6, True, 2, 3, 4)])
+@pytest.mark.parametrize("L,trans,alphar,nw,ns", [(4, True, 1, 4, 8), (6, True, 2, 3, 4), (8, True, 2, 4, 2),
+                                                  (10, True, 4, 8, 1)])
 def test_stream_and_direct_samplers_agree(L, trans, alphar, nw, ns, monkeypatch):
     """The TMA-streamed sampler (deferred updates) and the direct sampler (immediate updates) give the
     same chains and the same stored amplitudes to rounding."""
