@@ -1,37 +1,41 @@
 // sampler_stream.cu -- Metropolis sampler that streams each walker's projections through shared memory
 // with TMA bulk copies (make_sample.f90:4-240, same RNG order as sampler.cu).
 //
-// One CTA per walker: warp 0 is the control warp (its lane 0 draws the random numbers and issues every
-// bulk copy; the warp evaluates theta' and the cosh products of the proposal), warps 1..8 consume tiles.  A tile is one projection's Y = X^{-1} (Np x Np FP64, row
-// major).  Every proposal is one pass over the n_qp tiles through an ST-stage ring:
-//   producer:  cp.async.bulk global->shared (mbarrier complete_tx), and after the consumer releases a
-//              modified tile, cp.async.bulk shared->global before the stage is refilled;
-//   consumer:  applies the deferred rank-2 update of the previously accepted exchange (if any) to the
-//              tile in place, then evaluates the determinant ratio of the current proposal on it.
-// So a proposal costs one read of Y and an accepted move one write: the algorithmic minimum
-// (pfupdate_two.f90 reads InvM once per ratio and rewrites it per accepted move).
-// The first tiles of a pass are requested before the candidate is drawn, and the consumers apply the
-// deferred update while the control warp draws the candidate, which hides the serial part of a proposal.
+// One CTA per walker.  Warp 0 is the control warp: its lane 0 draws every random number and issues the
+// bulk loads, and the warp evaluates theta' and the cosh products of the proposal.  Warps 1..14 are seven
+// pairs of consumers.  A tile is one projection's Y = X^{-1} (Np x Np FP64, row major), and each pair
+// works on one tile at a time, each warp of the pair on half of its rows.  Every proposal is one pass over
+// the n_qp tiles through an ST-stage ring:
+//   producer:  cp.async.bulk global->shared (mbarrier complete_tx) into a stage as soon as it is released;
+//   pair:      applies the deferred rank-2 update of the previously accepted exchange (if any) to the tile
+//              in place, evaluates the determinant ratio of the current proposal on it, writes an updated
+//              tile back with cp.async.bulk shared->global, and releases the stage.
+// The halves combine only vectors and scalars (partial column sums, row db, the ratio's terms) through
+// shared memory at two pair barriers per tile.  A proposal costs one read of Y and an accepted move one
+// write: the algorithmic minimum (pfupdate_two.f90 reads InvM once per ratio and rewrites it per accepted
+// move).  The first tiles of a pass are requested before the candidate is drawn, and the pairs apply the
+// deferred update while the control warp draws the candidate.
 #include "sampler_common.cuh"
 
 namespace {
 
-constexpr int kWarps = 9;  // warp 0: control (RNG, candidate, theta', producer); warps 1..8: consumers
-constexpr int kConsumers = kWarps - 1;
+constexpr int kPairs = 7;
+constexpr int kWarps = 1 + 2 * kPairs;  // warp 0: control (RNG, candidate, theta', producer); 1..14: pairs
 #define ST_TIMEOUT 22
 
 struct Stream {
   double* stage;  // [ST][Np*Np]; also the Gauss-Jordan tile outside passes
   uint64_t* full;
   uint64_t* empty;
-  double* wU0;  // [kWarps][Np] gathered row / column of the deferred exchange
-  double* wV0;
-  double* wS;   // [kWarps][Np] Y v of the deferred exchange
-  double* wA;   // [kWarps][Np] column ua of Y
+  double* pS;     // [kPairs][Np] row sums Y v of the deferred exchange (each half writes its rows)
+  double* pA;     // [kPairs][Np] column ua of Y
+  double* pscal;  // [kPairs][2 slots][2 halves][4] ratio terms of each half
   int ST;
   uint32_t tile_bytes;
 };
 
+// Per-warp vectors come from the walker workspace: wu = u of the proposal, wA = u and wv = v of the
+// deferred exchange, wS = this warp's partial column sums.
 __host__ __device__ __forceinline__ size_t stream_layout(const DevDims& d, int ST, char* base, WS* w, Stream* st) {
   size_t off = ws_layout(d, kWarps, base, w, false);
   auto take = [&](size_t bytes, size_t align) -> char* {
@@ -47,10 +51,9 @@ __host__ __device__ __forceinline__ size_t stream_layout(const DevDims& d, int S
   t.stage = (double*)take(stage_bytes > gj ? stage_bytes : gj, 128);
   t.full = (uint64_t*)take(8 * (size_t)ST, 8);
   t.empty = (uint64_t*)take(8 * (size_t)ST, 8);
-  t.wU0 = (double*)take((size_t)kWarps * d.Np * 8, 16);
-  t.wV0 = (double*)take((size_t)kWarps * d.Np * 8, 16);
-  t.wS = (double*)take((size_t)kWarps * d.Np * 8, 16);
-  t.wA = (double*)take((size_t)kWarps * d.Np * 8, 16);
+  t.pS = (double*)take((size_t)kPairs * d.Np * 8, 16);
+  t.pA = (double*)take((size_t)kPairs * d.Np * 8, 16);
+  t.pscal = (double*)take((size_t)kPairs * 16 * 8, 16);
   if (w) w->tile = t.stage;
   if (st) *st = t;
   return off;
@@ -108,17 +111,36 @@ __device__ __forceinline__ double store_regs(const DevDims& d, const Move& m, co
   return g.c;
 }
 
-// acc[q] = (u^T Y)_k for the lane's columns k = lane + 32 q, as two interleaved FMA chains (even and odd
-// rows) so consecutive FMAs do not wait on each other.
+// Rows [r0, r1) of half h of a pair: the first (Np+1)/2 rows, or the rest.
+__device__ __forceinline__ void half_rows(int Np, int h, int& r0, int& r1) {
+  const int m = (Np + 1) >> 1;
+  r0 = h ? m : 0;
+  r1 = h ? Np : m;
+}
+
+// Barrier of the two warps of pair g (named barrier 1 + g, 64 threads) that also returns, on every thread,
+// whether any thread of the pair passed a non-zero flag: both warps take the same branch afterwards.
+__device__ __forceinline__ bool pair_sync_or(int g, bool flag) {
+  uint32_t out;
+  asm volatile(
+      "{\n .reg .pred p, q;\n setp.ne.u32 q, %1, 0;\n bar.red.or.pred p, %2, 64, q;\n selp.u32 %0, 1, 0, p;\n}\n"
+      : "=r"(out)
+      : "r"((uint32_t)flag), "r"(1 + g)
+      : "memory");
+  return out != 0;
+}
+
+// acc[q] = sum over rows r0 .. r0+nr-1 of u_j Y[j][k], k = lane + 32 q, as two interleaved FMA chains
 template <int KPL, int NP>
-__device__ __forceinline__ void col_sums(const double* Y, const double* u, int Np, double (&acc)[KPL]) {
+__device__ __forceinline__ void col_sums_rows(const double* Y, const double* u, int Np, int r0, int nr,
+                                              double (&acc)[KPL]) {
   const int lane = threadIdx.x & 31;
   double a1[KPL];
 #pragma unroll
   for (int q = 0; q < KPL; q++) acc[q] = a1[q] = 0.0;
-  constexpr int UNR = NP > 0 ? NP / 2 : 4;
-#pragma unroll UNR
-  for (int j = 0; j + 1 < Np; j += 2) {
+#pragma unroll 4
+  for (int jj = 0; jj + 1 < nr; jj += 2) {
+    const int j = r0 + jj;
     const double u0 = u[j], u1 = u[j + 1];
 #pragma unroll
     for (int q = 0; q < KPL; q++) {
@@ -129,8 +151,8 @@ __device__ __forceinline__ void col_sums(const double* Y, const double* u, int N
       }
     }
   }
-  if (Np & 1) {
-    const int j = Np - 1;
+  if (nr & 1) {
+    const int j = r0 + nr - 1;
 #pragma unroll
     for (int q = 0; q < KPL; q++) {
       const int k = lane + 32 * q;
@@ -151,47 +173,72 @@ __device__ __forceinline__ double lane_pick(const double (&acc)[KPL], int k0) {
   return __shfl_sync(0xffffffffu, mine, k0 & 31);
 }
 
-// Deferred rank-2 update of the tile for an accepted exchange (the algebra of pfupdate_two.f90:113-224
-// in block form): Y' = Y - A B^T / R1 - s1 t1^T / R2, with A = Y e_ua, B = u^T Y - e_ua^T,
-// s1 = Y v - A (u^T Y v - c)/R1 - e_db, t1 = e_db^T Y - Y(db,ua) B^T / R1, R2 = R / R1.
+// rows counted by half h; a compile-time constant for even NP
+template <int NP>
+__device__ __forceinline__ int half_count(int r0, int r1) {
+  return (NP > 0 && (NP & 1) == 0) ? NP / 2 : r1 - r0;
+}
+
+// Half h of the deferred rank-2 update of a tile for an accepted exchange (the algebra of
+// pfupdate_two.f90:113-224 in block form): Y' = Y - A B^T / R1 - s1 t1^T / R2, with A = Y e_ua,
+// B = u^T Y - e_ua^T, s1 = Y v - A (u^T Y v - c)/R1 - e_db, t1 = e_db^T Y - Y(db,ua) B^T / R1, R2 = R / R1.
+// Each half forms its rows' part of u^T Y, Y v and A, the pair exchanges them at one barrier, and each half
+// rewrites its own rows.  bad enters as this warp's failure flag and leaves as the pair's (uniform).
 template <int KPL, int NP>
-__device__ __forceinline__ void warp_apply_update(const DevDims& d, double* Y, const Move& m, double c, const double* u,
-                                                  const double* v, double* S, double* A) {
+__device__ __forceinline__ bool update_half(const DevDims& d, double* Y, const Move& m, double c, const double* u,
+                                            const double* v, int g, int h, double* my_acc, const double* other_acc,
+                                            double* pS, double* pA, bool bad) {
   const int lane = threadIdx.x & 31, Np = np_of<NP>(d);
-  double acc[KPL], rho[KPL];
-  col_sums<KPL, NP>(Y, u, Np, acc);
-  // row sums S = Y v, lane <-> row; each lane starts its row at a different column so the 64-bit
-  // shared loads of a half-warp fall in distinct banks
-  constexpr int UNR = NP > 0 ? NP / 2 : 4;
-  for (int j = lane; j < Np; j += 32) {
-    double a0 = 0.0, a1 = 0.0;
-    int k = j % Np;
-#pragma unroll UNR
-    for (int kk = 0; kk + 1 < Np; kk += 2) {
-      const int k1 = (k + 1 == Np) ? 0 : k + 1;
-      a0 = fma(Y[j * Np + k], v[k], a0);
-      a1 = fma(Y[j * Np + k1], v[k1], a1);
-      k = (k1 + 1 == Np) ? 0 : k1 + 1;
+  int r0, r1;
+  half_rows(Np, h, r0, r1);
+  const int nr = half_count<NP>(r0, r1);
+  double accp[KPL], rho[KPL];
+  double ydbua = 0.0;
+  if (!bad) {
+    col_sums_rows<KPL, NP>(Y, u, Np, r0, nr, accp);
+    // this half's row sums S = Y v (lane <-> row; each lane starts at its own column so the 64-bit shared
+    // loads of a half-warp fall in distinct banks) and its part of column ua
+    const int j = r0 + lane;
+    if (lane < nr) {
+      double a0 = 0.0, a1 = 0.0;
+      int k = j;
+#pragma unroll 5
+      for (int kk = 0; kk + 1 < Np; kk += 2) {
+        const int k1 = (k + 1 == Np) ? 0 : k + 1;
+        a0 = fma(Y[j * Np + k], v[k], a0);
+        a1 = fma(Y[j * Np + k1], v[k1], a1);
+        k = (k1 + 1 == Np) ? 0 : k1 + 1;
+      }
+      if (Np & 1) a0 = fma(Y[j * Np + k], v[k], a0);
+      pS[j] = a0 + a1;
+      pA[j] = Y[j * Np + m.ua];
     }
-    if (Np & 1) a0 = fma(Y[j * Np + k], v[k], a0);
-    S[j] = a0 + a1;
-    A[j] = Y[j * Np + m.ua];
+#pragma unroll
+    for (int q = 0; q < KPL; q++) {
+      const int k = lane + 32 * q;
+      rho[q] = 0.0;
+      if (k < Np) {
+        rho[q] = Y[m.db * Np + k];  // row db, read before either half rewrites it
+        my_acc[k] = accp[q];
+      }
+    }
+    ydbua = Y[m.db * Np + m.ua];
   }
-  double wv = 0.0;
+  if (pair_sync_or(g, bad)) return true;
+  double acc[KPL], wv = 0.0;
 #pragma unroll
   for (int q = 0; q < KPL; q++) {
     const int k = lane + 32 * q;
-    rho[q] = 0.0;
+    acc[q] = 0.0;
     if (k < Np) {
-      rho[q] = Y[m.db * Np + k];
+      const double o = other_acc[k];
+      acc[q] = h == 0 ? accp[q] + o : o + accp[q];  // both halves form acc_0 + acc_1
       wv = fma(acc[q], v[k], wv);
     }
   }
   const double ra = lane_pick<KPL>(acc, m.ua);
-  const double ydbua = Y[m.db * Np + m.ua];
   wv = warp_sum(wv);
-  __syncwarp();
-  const double R1 = ra, R = ra * S[m.db] - ydbua * (wv - c);
+  const double R1 = ra, R = ra * pS[m.db] - ydbua * (wv - c);
   const double inv_r1 = 1.0 / R1, r1_over_r = R1 / R, wc = (wv - c) * inv_r1;
   double bk[KPL], tk[KPL];
 #pragma unroll
@@ -201,11 +248,11 @@ __device__ __forceinline__ void warp_apply_update(const DevDims& d, double* Y, c
     bk[q] = B * inv_r1;
     tk[q] = (rho[q] - ydbua * B * inv_r1) * r1_over_r;
   }
-  constexpr int UNR2 = NP > 0 ? NP : 4;
-#pragma unroll UNR2
-  for (int j = 0; j < Np; j++) {
-    const double Aj = A[j];
-    const double s1 = S[j] - Aj * wc - (j == m.db ? 1.0 : 0.0);
+#pragma unroll 5
+  for (int jj = 0; jj < nr; jj++) {
+    const int j = r0 + jj;
+    const double Aj = pA[j];
+    const double s1 = pS[j] - Aj * wc - (j == m.db ? 1.0 : 0.0);
 #pragma unroll
     for (int q = 0; q < KPL; q++) {
       const int k = lane + 32 * q;
@@ -213,32 +260,45 @@ __device__ __forceinline__ void warp_apply_update(const DevDims& d, double* Y, c
     }
   }
   __syncwarp();
+  return false;
 }
 
-// Ratio R = (u^T Y)_ua (Y v)_db - Y(db,ua) (u^T Y v - c) on the shared-memory tile
+// Half h's terms of the ratio R = (u^T Y)_ua (Y v)_db - Y(db,ua) (u^T Y v - c): its rows' part of u^T Y v
+// and of (u^T Y)_ua, and, from the half that holds row db, (Y v)_db and Y(db,ua).  v comes from the
+// lane's registers (columns lane + 32 q).  Lane 0 writes them to scal[0..3].
 template <int KPL, int NP>
-__device__ __forceinline__ double warp_tile_ratio(const DevDims& d, const double* Y, const Move& m, double c,
-                                                  const double* u, const double* v) {
+__device__ __forceinline__ void ratio_half(const DevDims& d, const double* Y, const Move& m, double c, const double* u,
+                                           const UV<KPL>& g, int h, double* scal) {
   const int lane = threadIdx.x & 31, Np = np_of<NP>(d);
+  int r0, r1;
+  half_rows(Np, h, r0, r1);
   double acc[KPL];
-  col_sums<KPL, NP>(Y, u, Np, acc);
+  col_sums_rows<KPL, NP>(Y, u, Np, r0, half_count<NP>(r0, r1), acc);
+  const bool owner = m.db >= r0 && m.db < r1;
   double wv = 0.0, sb = 0.0;
 #pragma unroll
   for (int q = 0; q < KPL; q++) {
     const int k = lane + 32 * q;
     if (k < Np) {
-      wv = fma(acc[q], v[k], wv);
-      sb = fma(Y[m.db * Np + k], v[k], sb);
+      const double vk = (k == m.ua) ? c : g.v[q];
+      wv = fma(acc[q], vk, wv);
+      if (owner) sb = fma(Y[m.db * Np + k], vk, sb);
     }
   }
   const double ra = lane_pick<KPL>(acc, m.ua);
-  const double ydbua = Y[m.db * Np + m.ua];
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) {
     wv += __shfl_xor_sync(0xffffffffu, wv, o);
     sb += __shfl_xor_sync(0xffffffffu, sb, o);
   }
-  return ra * sb - ydbua * (wv - c);
+  if (lane == 0) {
+    scal[0] = wv;
+    scal[1] = ra;
+    if (owner) {
+      scal[2] = sb;
+      scal[3] = Y[m.db * Np + m.ua];
+    }
+  }
 }
 
 struct Pipe {
@@ -329,7 +389,9 @@ __device__ __forceinline__ void control_propose(const SCtx& c, volatile int* can
   if (lane == 0) *cand_flag = pass_id;
 }
 
-// consumers: deferred update (pend) and/or proposal ratio (prop) per tile
+// Pairs: deferred update (pend) and/or proposal ratio (prop) per tile.  Pair g takes tiles g, g + kPairs, ...
+// Every warp of a pair reaches the same pair barriers in the same order, and a failure (a bounded wait that
+// ran out, an abort) is agreed at those barriers, so both warps leave together.
 template <int KPL, int NP>
 __device__ __forceinline__ bool pass_consume(const SCtx& c, const Stream& sm, const Pipe& pp, bool pend,
                                              const Move& mk, bool prop, volatile int* cand_flag, int pass_id,
@@ -337,37 +399,41 @@ __device__ __forceinline__ bool pass_consume(const SCtx& c, const Stream& sm, co
   const DevDims& d = c.d;
   const WS& s = c.s;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, Np = d.Np, n = d.n_qp;
+  const int cw = warp - 1, g = cw >> 1, h = cw & 1, partner = 1 + 2 * g + (1 - h);
   const size_t NN = (size_t)Np * Np;
-  double* U0 = sm.wU0 + (size_t)warp * Np;
-  double* V0 = sm.wV0 + (size_t)warp * Np;
-  double* S0 = sm.wS + (size_t)warp * Np;
-  double* A0 = sm.wA + (size_t)warp * Np;
   double* u = s.wu + (size_t)warp * Np;
-  double* v = s.wv + (size_t)warp * Np;
+  double* U0 = s.wA + (size_t)warp * Np;
+  double* V0 = s.wv + (size_t)warp * Np;
+  double* my_acc = s.wS + (size_t)warp * Np;
+  const double* other_acc = s.wS + (size_t)partner * Np;
+  double* pS = sm.pS + (size_t)g * Np;
+  double* pA = sm.pA + (size_t)g * Np;
+  double* pscal = sm.pscal + (size_t)g * 16;
   UV<KPL> gk, gn;
   Move mn{0, 0, 0, 0};
-  bool have_move = false;
-  int t = warp - 1;
-  bool stored = false;
+  bool have_move = false, stored = false;
+  int slot = 0;
+  int t = g;
   if (pend && t < n) gather_regs<KPL, NP>(d, c.p, t, s.idx, mk, gk);
-  for (; t < n; t += kConsumers) {
+  for (; t < n; t += kPairs) {
     const uint32_t T = pp.T0 + t;
     const int st = (int)(T % sm.ST);
-    const int tn = t + kConsumers;
+    const int tn = t + kPairs;
     double ck = 0.0;
     if (pend) {
       ck = store_regs<KPL, NP>(d, mk, gk, U0, V0);
       if (tn < n) gather_regs<KPL, NP>(d, c.p, tn, s.idx, mk, gk);
     }
     __syncwarp();
-    if (*abort_flag) return false;
-    if (!mbar_wait(&sm.full[st], (T / sm.ST) & 1u)) return false;
+    bool bad = (*abort_flag != 0) || !mbar_wait(&sm.full[st], (T / sm.ST) & 1u);
     double* Y = sm.stage + (size_t)st * NN;
     if (pend) {
-      warp_apply_update<KPL, NP>(d, Y, mk, ck, U0, V0, S0, A0);
+      if (update_half<KPL, NP>(d, Y, mk, ck, U0, V0, g, h, my_acc, other_acc, pS, pA, bad)) return false;
       fence_proxy_async_smem();
     }
-    if (prop) {
+    double* sc = pscal + slot * 8 + h * 4;
+    double cn = 0.0;
+    if (prop && !bad) {
       if (!have_move) {
         bool ok = false;
         for (int it = 0; it < (1 << 24); it++) {
@@ -380,27 +446,36 @@ __device__ __forceinline__ bool pass_consume(const SCtx& c, const Stream& sm, co
         }
         __syncwarp();
         __threadfence_block();
-        if (!ok || status(c)) return false;
-        mn = Move{mv[0], mv[1], mv[2], mv[3]};
-        have_move = true;
-        gather_regs<KPL, NP>(d, c.p, t, s.idx, mn, gn);
+        if (!ok || status(c)) bad = true;
+        if (!bad) {
+          mn = Move{mv[0], mv[1], mv[2], mv[3]};
+          have_move = true;
+          gather_regs<KPL, NP>(d, c.p, t, s.idx, mn, gn);
+        }
       }
-      const double cn = store_regs<KPL, NP>(d, mn, gn, u, v);
-      __syncwarp();
-      if (tn < n) gather_regs<KPL, NP>(d, c.p, tn, s.idx, mn, gn);
-      const double R = warp_tile_ratio<KPL, NP>(d, Y, mn, cn, u, v);
-      if (lane == 0) {
-        const double pfn = R * s.pf[t];
-        s.pfp[t] = pfn;
-        cplx cw = psi_wo_pf(d, c.t, s.rbm[t], s.sgnp[t >> 1], t);
-        s.psip[2 * t] = cw.re * pfn;
-        s.psip[2 * t + 1] = cw.im * pfn;
-        pre += cw.re * pfn;
-        pim += cw.im * pfn;
+      if (!bad) {
+        cn = store_regs<KPL, NP>(d, mn, gn, u, V0);
+        __syncwarp();
+        ratio_half<KPL, NP>(d, Y, mn, cn, u, gn, h, sc);
+        if (tn < n) gather_regs<KPL, NP>(d, c.p, tn, s.idx, mn, gn);
       }
     }
-    __syncwarp();
-    if (lane == 0) {
+    if (pair_sync_or(g, bad)) return false;
+    if (h == 0 && lane == 0) {
+      if (prop) {
+        const double* s0 = pscal + slot * 8;
+        const double* s1 = s0 + 4;
+        const double* so = (mn.db < ((Np + 1) >> 1)) ? s0 : s1;
+        const double wv = s0[0] + s1[0], ra = s0[1] + s1[1];
+        const double R = ra * so[2] - so[3] * (wv - cn);
+        const double pfn = R * s.pf[t];
+        s.pfp[t] = pfn;
+        cplx cw2 = psi_wo_pf(d, c.t, s.rbm[t], s.sgnp[t >> 1], t);
+        s.psip[2 * t] = cw2.re * pfn;
+        s.psip[2 * t + 1] = cw2.im * pfn;
+        pre += cw2.re * pfn;
+        pim += cw2.im * pfn;
+      }
       if (pend) {  // write the updated tile back; the stage is released once the copy has read it
         bulk_store(c.Yw + (size_t)t * NN, Y, sm.tile_bytes);
         bulk_commit();
@@ -409,6 +484,7 @@ __device__ __forceinline__ bool pass_consume(const SCtx& c, const Stream& sm, co
       }
       mbar_arrive(&sm.empty[st]);
     }
+    slot ^= 1;
   }
   if (lane == 0 && stored) {  // the next pass reloads these tiles: their stores must have landed
     bulk_wait_all();
