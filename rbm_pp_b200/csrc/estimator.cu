@@ -95,88 +95,7 @@ __host__ __device__ __forceinline__ size_t est_layout(const DevDims& d, int nqw,
   return off;
 }
 
-// Warp-level Gauss-Jordan inverse with partial pivoting (the role of dgetrf/dgetri, matrix.f90:155-177)
-// of the n x n tile T (leading dimension ld).  Returns det(X) (0 and singular=true on a zero pivot).
-// Column b of X^{-1} is column src[b] of T afterwards (src written to perm).
-template <int KPL>
-__device__ __forceinline__ double warp_gauss_jordan(double* T, int n, int ld, int* perm, bool& singular) {
-  const int lane = threadIdx.x & 31;
-  double det = 1.0;
-  singular = false;
-  for (int k = 0; k < n; k++) {
-    double best = -1.0;
-    int bi = k;
-    for (int i = k + lane; i < n; i += 32) {
-      const double v = fabs(T[i * ld + k]);
-      if (v > best) {
-        best = v;
-        bi = i;
-      }
-    }
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-      const double ob = __shfl_xor_sync(0xffffffffu, best, o);
-      const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
-      if (ob > best || (ob == best && oi < bi)) {
-        best = ob;
-        bi = oi;
-      }
-    }
-    if (!(best > 0.0)) {
-      singular = true;
-      return 0.0;
-    }
-    const double pivot = T[bi * ld + k];
-    if (lane == 0) perm[k] = bi;
-    __syncwarp();
-    double r[KPL];
-#pragma unroll
-    for (int q = 0; q < KPL; q++) {
-      const int j = lane + 32 * q;
-      r[q] = 0.0;
-      if (j < n) {
-        const double a = T[k * ld + j], b = T[bi * ld + j];
-        if (bi != k) T[bi * ld + j] = a;
-        r[q] = b / pivot;
-      }
-    }
-    det = (bi != k ? -det : det) * pivot;
-    __syncwarp();
-    // rows i != k: T(i,j) -= T(i,k) r_j for j != k; column k and row k afterwards
-    for (int i = 0; i < n; i++) {
-      if (i == k) continue;
-      const double f = T[i * ld + k];
-#pragma unroll
-      for (int q = 0; q < KPL; q++) {
-        const int j = lane + 32 * q;
-        if (j < n && j != k) T[i * ld + j] = T[i * ld + j] - f * r[q];
-      }
-    }
-    __syncwarp();
-    for (int i = lane; i < n; i += 32)
-      if (i != k) T[i * ld + k] = -T[i * ld + k] / pivot;
-#pragma unroll
-    for (int q = 0; q < KPL; q++) {
-      const int j = lane + 32 * q;
-      if (j < n) T[k * ld + j] = (j == k) ? 1.0 / pivot : r[q];
-    }
-    __syncwarp();
-  }
-  if (lane == 0) {
-    int src[RBMPP_MAX_N / 2];
-    for (int b = 0; b < n; b++) src[b] = b;
-    for (int k = n - 1; k >= 0; k--) {
-      const int pk = perm[k], a = src[k];
-      src[k] = src[pk];
-      src[pk] = a;
-    }
-    for (int b = 0; b < n; b++) perm[b] = src[b];
-  }
-  __syncwarp();
-  return det;
-}
-
-template <int KPL>
+template <int KPL, int NP>
 __global__ void __launch_bounds__(kEstThreads, 1)
     estimator_kernel(const __grid_constant__ DevDims d, const __grid_constant__ DevTables t,
                      const __grid_constant__ DevParams p, const int8_t* xs, int n, double* out_psi, double* out_hpsi,
@@ -187,7 +106,7 @@ __global__ void __launch_bounds__(kEstThreads, 1)
   if (threadIdx.x == 0) est_layout(d, nqw, smem, &s, &e);
   __syncthreads();
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  const int N = d.N, Np = d.Np, ld = Np + 1, NB = 4 * N;
+  const int N = d.N, Np = NP > 0 ? NP : d.Np, ld = Np + 1, NB = 4 * N;
   const int cfgi = blockIdx.x;
   if (cfgi >= n) return;
   double* Orow = O ? O + (size_t)cfgi * d.Nv : nullptr;
@@ -266,7 +185,7 @@ __global__ void __launch_bounds__(kEstThreads, 1)
       }
       __syncwarp();
       bool sing;
-      const double det = warp_gauss_jordan<KPL>(T, Np, ld, src, sing);
+      const double det = warp_gj<KPL, NP>(T, Np, src, sing);
       if (sing) bad = true;
       const double pfq = (double)d.pf_sign * det;
       const cplx cw = psi_wo_pf(d, t, s.rbm[qp], s.sgn[mp], qp);
@@ -300,11 +219,12 @@ __global__ void __launch_bounds__(kEstThreads, 1)
           double ra = 0.0, uw = 0.0;
 #pragma unroll
           for (int q = 0; q < KPL; q++) {
-            const int j = lane + 32 * q;
+            const int j = lane + 32 * q, jc = j < Np ? j : Np - 1;  // in-tile index for every lane
+            const double tj = T[jc * ld + cu], wj = Wv[jc];
             if (j < Np) {
               const double uj = (j == db) ? c : XFq[(size_t)s_dn * N + s.idx[Np + j]];
-              ra = fma(uj, T[j * ld + cu], ra);
-              uw = fma(uj, Wv[j], uw);
+              ra = fma(uj, tj, ra);
+              uw = fma(uj, wj, uw);
             }
           }
           ra = warp_sum(ra);
@@ -469,19 +389,27 @@ cudaError_t rbmpp_launch_estimator(const DevDims& d, const DevTables& t, const D
   if (nqw < 1) return cudaErrorInvalidValue;
   size_t smem = est_layout(d, nqw, nullptr, nullptr, nullptr);
   int kpl = (d.Np + 31) / 32;
-#define LAUNCH(K)                                                                                          \
+#define LAUNCH(K, NPC)                                                                                     \
   do {                                                                                                     \
-    cudaError_t e = cudaFuncSetAttribute(estimator_kernel<K>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
+    cudaError_t e = cudaFuncSetAttribute(estimator_kernel<K, NPC>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
                                          (int)smem);                                                       \
     if (e != cudaSuccess) return e;                                                                        \
-    rbmpp_note_launch(); estimator_kernel<K><<<n, kEstThreads, smem, st>>>(d, t, p, xs, n, out_psi, out_hpsi, O, out_nap,         \
-                                                      out_status, reweight, nqw);                           \
+    rbmpp_note_launch();                                                                                   \
+    estimator_kernel<K, NPC><<<n, kEstThreads, smem, st>>>(d, t, p, xs, n, out_psi, out_hpsi, O, out_nap,   \
+                                                           out_status, reweight, nqw);                      \
     return cudaGetLastError();                                                                             \
   } while (0)
-  if (kpl <= 1) LAUNCH(1);
-  if (kpl <= 2) LAUNCH(2);
-  if (kpl <= 4) LAUNCH(4);
-  if (kpl <= 8) LAUNCH(8);
+  switch (d.Np) {  // block sizes of the even-L lattices with a compile-time specialisation
+    case 8: LAUNCH(1, 8);
+    case 18: LAUNCH(1, 18);
+    case 32: LAUNCH(1, 32);
+    case 50: LAUNCH(2, 50);
+    default: break;
+  }
+  if (kpl <= 1) LAUNCH(1, 0);
+  if (kpl <= 2) LAUNCH(2, 0);
+  if (kpl <= 4) LAUNCH(4, 0);
+  if (kpl <= 8) LAUNCH(8, 0);
 #undef LAUNCH
   return cudaErrorInvalidValue;
 }

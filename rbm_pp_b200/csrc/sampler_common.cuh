@@ -14,13 +14,93 @@ struct SCtx {
   int w;
   const WS& s;  // pointer table kept in shared memory
   double* Yw;   // this walker's Y
+  // Optional: par_ntile >= 2 tiles of Np x (Np + 1) doubles at par_tiles let one warp per tile invert
+  // projections in parallel during from-scratch recomputes (the streaming sampler's stage area).
+  double* par_tiles;
+  int par_ntile;
 };
 
 __device__ __forceinline__ int& status(const SCtx& c) { return c.s.iflag[F_STATUS]; }
 
+// Scratch inverse of every projection, one warp per projection on its own tile (warps 1..par_ntile):
+// the same results as the CTA-wide path below, which inverts one projection at a time.
+template <int KPL, int NP>
+__device__ __forceinline__ void warp_scratch_all(const SCtx& c, const int* idx, double* pf_out, bool write_y,
+                                                 bool diff) {
+  const DevDims& d = c.d;
+  const WS& s = c.s;
+  const int Np = NP > 0 ? NP : d.Np, ld = Np + 1, N = d.N;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, wk = warp - 1;
+  double wratio = -1.0;
+  bool sing_any = false;
+  if (wk >= 0 && wk < c.par_ntile) {
+    double* T = c.par_tiles + (size_t)wk * Np * ld;
+    int* perm = (int*)(s.wS + (size_t)warp * Np);
+    for (int qp = wk; qp < d.n_qp && !sing_any; qp += c.par_ntile) {
+      const double* XFq = c.p.XF + (size_t)qp * N * N;
+      for (int i = 0; i < Np; i++) {
+        const double* row = XFq + (size_t)idx[i] * N;
+        for (int j = lane; j < Np; j += 32) T[i * ld + j] = row[idx[Np + j]];
+      }
+      __syncwarp();
+      bool sing;
+      const double det = warp_gj<KPL, NP>(T, Np, perm, sing);
+      if (sing) {
+        sing_any = true;
+        break;
+      }
+      double* Yq = c.Yw + (size_t)qp * Np * Np;
+      if (diff) {  // make_sample.f90:106-113
+        double mx = 0.0, md = 0.0;
+        for (int a = 0; a < Np; a++)
+          for (int b = lane; b < Np; b += 32) {
+            const double nv = T[a * ld + perm[b]];
+            mx = fmax(mx, fabs(nv));
+            md = fmax(md, fabs(Yq[a * Np + b] - nv));
+          }
+        mx = warp_max(mx);
+        md = warp_max(md);
+        wratio = fmax(wratio, md / mx);
+      }
+      if (write_y)
+        for (int a = 0; a < Np; a++)
+          for (int b = lane; b < Np; b += 32) Yq[a * Np + b] = T[a * ld + perm[b]];
+      if (lane == 0) pf_out[qp] = (double)d.pf_sign * det;
+      __syncwarp();
+    }
+  }
+  if (lane == 0) {
+    s.red[warp] = wratio;
+    s.red[32 + warp] = sing_any ? 1.0 : 0.0;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    double di = -1.0;
+    bool sg = false;
+    for (int w = 1; w <= c.par_ntile; w++) {
+      di = fmax(di, s.red[w]);
+      if (s.red[32 + w] != 0.0) sg = true;
+    }
+    if (sg) status(c) = ST_SINGULAR;
+    s.dsc[D_DIFFINV] = di;
+  }
+  // generic writes of Y / of the shared tiles before later bulk (async-proxy) copies touch them
+  if (write_y) fence_proxy_async_global();
+  fence_proxy_async_smem();
+  __syncthreads();
+}
+
 // Scratch inverse of every projection for labelling idx: writes Y (when write_y) and pf_out.
 // When diff is requested, also computes the reference's drift measures against the stored Y / pf.
+// KPL > 0 selects the warp-parallel path when the context provides tiles for it.
+template <int KPL = 0, int NP = 0>
 __device__ __forceinline__ void cta_scratch_all(const SCtx& c, const int* idx, double* pf_out, bool write_y, bool diff) {
+  if constexpr (KPL > 0) {
+    if (c.par_ntile >= 2) {
+      warp_scratch_all<KPL, NP>(c, idx, pf_out, write_y, diff);
+      return;
+    }
+  }
   const DevDims& d = c.d;
   const WS& s = c.s;
   const int Np = d.Np, ld = Np + 1, tid = threadIdx.x;
@@ -73,6 +153,7 @@ __device__ __forceinline__ void cta_scratch_all(const SCtx& c, const int* idx, d
 }
 
 // calc_theta, x_to_Ele_Idx, calculate_MAll, sign_PP, calc_amplitude (make_sample.f90:54-60 / :345-350)
+template <int KPL = 0, int NP = 0>
 __device__ __forceinline__ void full_state(const SCtx& c) {
   const WS& s = c.s;
   cta_calc_theta(c.d, c.t, c.p, s.x, s.th);
@@ -82,7 +163,7 @@ __device__ __forceinline__ void full_state(const SCtx& c) {
   }
   __syncthreads();
   if (status(c)) return;
-  cta_scratch_all(c, s.idx, s.pf, true, false);
+  cta_scratch_all<KPL, NP>(c, s.idx, s.pf, true, false);
   if (status(c)) return;
   cta_sign_pp(c.d, c.t, s, s.idx, s.sgn);
   __syncthreads();
@@ -95,6 +176,7 @@ __device__ __forceinline__ void full_state(const SCtx& c) {
 }
 
 // make_initial_x make_sample.f90:298-362
+template <int KPL = 0, int NP = 0>
 __device__ __forceinline__ void make_initial_x(const SCtx& c) {
   const WS& s = c.s;
   for (int it1 = 0; it1 < 1000000; it1++) {
@@ -116,7 +198,7 @@ __device__ __forceinline__ void make_initial_x(const SCtx& c) {
     }
     __syncthreads();
     if (status(c)) return;
-    full_state(c);
+    full_state<KPL, NP>(c);
     if (status(c)) return;
     if (hypot(s.dsc[D_PSI0R], s.dsc[D_PSI0I]) > 1e-300) return;
   }
@@ -125,6 +207,7 @@ __device__ __forceinline__ void make_initial_x(const SCtx& c) {
 }
 
 // Nfastup checkpoint make_sample.f90:74-128
+template <int KPL = 0, int NP = 0>
 __device__ __forceinline__ void checkpoint(const SCtx& c, int& nfastup) {
   const DevDims& d = c.d;
   const WS& s = c.s;
@@ -153,7 +236,7 @@ __device__ __forceinline__ void checkpoint(const SCtx& c, int& nfastup) {
   // old Pf kept in pfp for the drift measure
   for (int qp = threadIdx.x; qp < d.n_qp; qp += blockDim.x) s.pfp[qp] = s.pf[qp];
   __syncthreads();
-  cta_scratch_all(c, s.idx, s.pf, true, true);
+  cta_scratch_all<KPL, NP>(c, s.idx, s.pf, true, true);
   if (status(c)) return;
   cta_amplitude(d, c.t, s, s.th, s.pf, s.sgn, s.psi, D_PSI0R);
   if (threadIdx.x == 0) {
@@ -177,6 +260,7 @@ __device__ __forceinline__ void checkpoint(const SCtx& c, int& nfastup) {
 }
 
 // Global spin flip make_sample.f90:135-158 (RNG check already drawn by the caller).
+template <int KPL = 0, int NP = 0>
 __device__ __forceinline__ void global_flip(const SCtx& c) {
   const DevDims& d = c.d;
   const WS& s = c.s;
@@ -189,7 +273,7 @@ __device__ __forceinline__ void global_flip(const SCtx& c) {
   }
   __syncthreads();
   if (status(c)) return;
-  cta_scratch_all(c, s.idx2, s.pfp, false, false);  // Pf of the flipped configuration
+  cta_scratch_all<KPL, NP>(c, s.idx2, s.pfp, false, false);  // Pf of the flipped configuration
   if (status(c)) return;
   cta_sign_pp(d, c.t, s, s.idx2, s.sgnp);
   __syncthreads();
@@ -223,7 +307,7 @@ __device__ __forceinline__ void global_flip(const SCtx& c) {
     s.dsc[D_PSI0I] = s.dsc[D_PSIPI];
   }
   __syncthreads();
-  cta_scratch_all(c, s.idx, s.pf, true, false);  // Tmp_Inv_M of the accepted flipped state
+  cta_scratch_all<KPL, NP>(c, s.idx, s.pf, true, false);  // Tmp_Inv_M of the accepted flipped state
 }
 
 

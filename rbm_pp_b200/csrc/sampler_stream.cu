@@ -120,10 +120,13 @@ __device__ __forceinline__ void half_rows(int Np, int h, int& r0, int& r1) {
 
 // Barrier of the two warps of pair g (named barrier 1 + g, 64 threads) that also returns, on every thread,
 // whether any thread of the pair passed a non-zero flag: both warps take the same branch afterwards.
+// The warp is reconverged first and the barrier is the non-aligned form, which counts threads one by one,
+// so lanes that arrive from a divergent branch (lane 0's bookkeeping) are counted exactly once.
 __device__ __forceinline__ bool pair_sync_or(int g, bool flag) {
+  __syncwarp();
   uint32_t out;
   asm volatile(
-      "{\n .reg .pred p, q;\n setp.ne.u32 q, %1, 0;\n bar.red.or.pred p, %2, 64, q;\n selp.u32 %0, 1, 0, p;\n}\n"
+      "{\n .reg .pred p, q;\n setp.ne.u32 q, %1, 0;\n barrier.red.or.pred p, %2, 64, q;\n selp.u32 %0, 1, 0, p;\n}\n"
       : "=r"(out)
       : "r"((uint32_t)flag), "r"(1 + g)
       : "memory");
@@ -557,7 +560,13 @@ __global__ void __launch_bounds__(kWarps * 32, 1)
     cand_flag = -1;
   }
   __syncthreads();
-  const SCtx c{d, t, p, W, (int)blockIdx.x, ws, W.Y + (size_t)blockIdx.x * d.n_qp * d.Np * d.Np};
+  // from-scratch recomputes invert up to kWarps - 1 projections in parallel, one per tile of the stage area
+  const size_t gj_tile = (size_t)d.Np * (d.Np + 1) * 8;
+  const size_t area = (size_t)sm.ST * sm.tile_bytes > gj_tile ? (size_t)sm.ST * sm.tile_bytes : gj_tile;
+  int ntile = (int)(area / gj_tile);
+  ntile = ntile < kWarps - 1 ? ntile : kWarps - 1;
+  const SCtx c{d, t, p, W, (int)blockIdx.x, ws, W.Y + (size_t)blockIdx.x * d.n_qp * d.Np * d.Np, sm.stage,
+               ntile >= 2 ? ntile : 0};
   const WS& s = ws;
   const int w = c.w, N = d.N;
   Pipe pp;
@@ -571,15 +580,15 @@ __global__ void __launch_bounds__(kWarps * 32, 1)
   int nfastup = W.nfastup[w];
 
   if (first) {
-    make_initial_x(c);
+    make_initial_x<KPL, NP>(c);
   } else {
     for (int i = tid; i < N; i += blockDim.x) s.x[i] = W.xs[((size_t)w * d.ns + (d.ns - 1)) * N + i];
     __syncthreads();
-    full_state(c);
+    full_state<KPL, NP>(c);
     if (!status(c)) {
       if (tid == 0) s.iflag[F_AUX] = grnd(s.mt) < 0.05;
       __syncthreads();
-      if (s.iflag[F_AUX]) make_initial_x(c);
+      if (s.iflag[F_AUX]) make_initial_x<KPL, NP>(c);
     }
   }
   int naccept = 0, nacc_tmp = 0, nacc_all = 0;
@@ -592,7 +601,7 @@ __global__ void __launch_bounds__(kWarps * 32, 1)
       }
       drain(c);
       if (status(c)) break;
-      checkpoint(c, nfastup);
+      checkpoint<KPL, NP>(c, nfastup);
       if (status(c)) break;
       nacc_tmp = 0;
     }
@@ -601,7 +610,7 @@ __global__ void __launch_bounds__(kWarps * 32, 1)
       __syncthreads();
       if (s.iflag[F_FLIP]) {
         drain(c);
-        global_flip(c);
+        global_flip<KPL, NP>(c);
         if (status(c)) break;
         if (tid == 0 && s.iflag[F_ACCEPT]) pend_s[0] = 0;  // Y recomputed for the flipped state
         __syncthreads();
@@ -702,16 +711,13 @@ __global__ void __launch_bounds__(kWarps * 32, 1)
 
 // Stage count and shared memory of the streaming sampler; 0 when it does not apply.
 int rbmpp_stream_stages(const DevDims& d, int max_smem) {
+  // One stage per pair (or per projection when there are fewer): the tiles that reuse a stage within a
+  // pass then belong to the same pair, so a pair never waits on a stage two loads ahead of it, where the
+  // mbarrier's phase parity could not tell the two loads apart.  No fallback to fewer stages: the
+  // direct sampler takes shapes whose stages do not fit.
   if (d.Np > 64) return 0;
-  const size_t tile = (size_t)8 * d.Np * d.Np;
-  int st = d.n_qp < 8 ? d.n_qp : 8;
-  while (st >= 1) {
-    size_t need = stream_layout(d, st, nullptr, nullptr, nullptr);
-    if ((long long)need <= max_smem) return st;
-    st--;
-  }
-  (void)tile;
-  return 0;
+  const int st = d.n_qp < kPairs ? d.n_qp : kPairs;
+  return (long long)stream_layout(d, st, nullptr, nullptr, nullptr) <= max_smem ? st : 0;
 }
 
 size_t rbmpp_stream_smem(const DevDims& d, int st) { return stream_layout(d, st, nullptr, nullptr, nullptr); }

@@ -332,3 +332,115 @@ __device__ __forceinline__ void cta_amplitude(const DevDims& d, const DevTables&
   }
   __syncthreads();
 }
+
+// Warp-level Gauss-Jordan inverse with partial pivoting (the role of dgetrf/dgetri, matrix.f90:155-177) of
+// the n x n tile T with leading dimension n + 1 (n = NP when NP > 0, a compile-time size; otherwise n_rt).
+// Returns det(X) (0 and singular = true on a zero pivot).  Column b of X^{-1} is column perm[b] of T
+// afterwards.  The pivot column is held in registers (rows lane + 32 p) and broadcast by shuffles, so the
+// elimination's loads do not wait on its stores.  Lanes past the last row or column load from a clamped,
+// in-tile index (and discard the value): the compiler may issue a guarded shared load unconditionally,
+// and a tile can end at the end of the block's shared memory.
+template <int KPL, int NP>
+__device__ __forceinline__ double warp_gj(double* T, int n_rt, int* perm, bool& singular) {
+  const int n = NP > 0 ? NP : n_rt, ld = n + 1;
+  const int lane = threadIdx.x & 31;
+  double det = 1.0;
+  singular = false;
+  for (int k = 0; k < n; k++) {
+    double fc[KPL];
+    double best = -1.0;
+    int bi = k;
+#pragma unroll
+    for (int p = 0; p < KPL; p++) {
+      const int i = lane + 32 * p;
+      const double tv = T[(i < n ? i : n - 1) * ld + k];
+      fc[p] = (i < n) ? tv : 0.0;
+      if (i >= k && i < n) {
+        const double v = fabs(fc[p]);
+        if (v > best) {
+          best = v;
+          bi = i;
+        }
+      }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      const double ob = __shfl_xor_sync(0xffffffffu, best, o);
+      const int oi = __shfl_xor_sync(0xffffffffu, bi, o);
+      if (ob > best || (ob == best && oi < bi)) {
+        best = ob;
+        bi = oi;
+      }
+    }
+    if (!(best > 0.0)) {
+      singular = true;
+      return 0.0;
+    }
+    // T(bi, k) and T(k, k) from their lanes
+    double pv = 0.0, fkk = 0.0;
+#pragma unroll
+    for (int p = 0; p < KPL; p++) {
+      if (p == (bi >> 5)) pv = fc[p];
+      if (p == (k >> 5)) fkk = fc[p];
+    }
+    const double pivot = __shfl_sync(0xffffffffu, pv, bi & 31);
+    fkk = __shfl_sync(0xffffffffu, fkk, k & 31);
+    if (lane == 0) perm[k] = bi;
+    double r[KPL];
+#pragma unroll
+    for (int q = 0; q < KPL; q++) {
+      const int j = lane + 32 * q, jc = j < n ? j : n - 1;
+      const double a = T[k * ld + jc], b = T[bi * ld + jc];
+      r[q] = 0.0;
+      if (j < n) {
+        if (bi != k) T[bi * ld + j] = a;
+        r[q] = b / pivot;
+      }
+    }
+    det = (bi != k ? -det : det) * pivot;
+    __syncwarp();
+    // rows i != k: T(i,j) -= f_i r_j for j != k, with f_i = T(i,k) after the interchange
+#pragma unroll
+    for (int p = 0; p < KPL; p++) {
+#pragma unroll 8
+      for (int l = 0; l < 32; l++) {
+        const int i = 32 * p + l;
+        if (i >= n) break;
+        double f = __shfl_sync(0xffffffffu, fc[p], l);
+        if (i == bi) f = fkk;
+        if (i != k) {
+#pragma unroll
+          for (int q = 0; q < KPL; q++) {
+            const int j = lane + 32 * q;
+            const double t = T[i * ld + (j < n ? j : n - 1)];
+            if (j < n && j != k) T[i * ld + j] = t - f * r[q];
+          }
+        }
+      }
+    }
+    __syncwarp();
+#pragma unroll
+    for (int p = 0; p < KPL; p++) {
+      const int i = lane + 32 * p;
+      if (i < n && i != k) T[i * ld + k] = -((i == bi) ? fkk : fc[p]) / pivot;
+    }
+#pragma unroll
+    for (int q = 0; q < KPL; q++) {
+      const int j = lane + 32 * q;
+      if (j < n) T[k * ld + j] = (j == k) ? 1.0 / pivot : r[q];
+    }
+    __syncwarp();
+  }
+  if (lane == 0) {  // source column of each column of the inverse: undo the interchanges in reverse
+    int src[RBMPP_MAX_N / 2];
+    for (int b = 0; b < n; b++) src[b] = b;
+    for (int k = n - 1; k >= 0; k--) {
+      const int pk = perm[k], a = src[k];
+      src[k] = src[pk];
+      src[pk] = a;
+    }
+    for (int b = 0; b < n; b++) perm[b] = src[b];
+  }
+  __syncwarp();
+  return det;
+}
