@@ -171,6 +171,70 @@ def run_reference(args):
     return 0
 
 
+BATCH_LS = (12, 14, 16, 18)
+BATCH_J2 = (0.40, 0.45, 0.50, 0.55, 0.60)
+
+
+def run_batch(args):
+    """Batched sampling over lattices L = 12..18 crossed with J2/J1 = 0.40..0.60 (1024 walkers each,
+    alpha = 2, no translation projection, N_QP = 2): one persistent launch per make_sample, launch shape
+    and walker order picked by the autotuner.  Reports aggregate MC samples/s of the batched launch and,
+    for comparison, each instance's MC samples/s when launched alone."""
+    import torch
+    from rbm_pp_b200 import capi
+    from rbm_pp_b200 import formats as fm
+    torch.cuda.set_device(0)
+    walkers, ns = (1024, 4) if args.workload == "batch_l12_18" else (64, 2)
+    ctxs, meta = [], []
+    for L in BATCH_LS:
+        for J2 in BATCH_J2:
+            p = fm.synthetic_problem(L, translations=False, alphar=2, orbital="full", nsample=walkers * ns,
+                                     seed=100 + L, J2=J2)
+            g = capi.Context(p, n_walkers=walkers, nsample_per_walker=ns)
+            g.set_params(p.br, p.Wr, p.slater, 0.0)
+            g.seed(4000 + 10 * L + int(100 * J2))
+            ctxs.append(g)
+            meta.append((L, J2))
+    b = capi.Batch(ctxs)
+    threads, order, probe_ms = b.tune()
+    b.make_sample(True)
+    for _ in range(max(0, args.warmup - 1)):
+        b.make_sample(False)
+    clk = ClockSampler(0)
+    clk.start()
+    ms = []
+    for _ in range(args.steps):
+        b.make_sample(False)
+        ms.append(ctxs[0].stats()["sampler_ms"])
+    clocks = clk.stop()
+    batch_ms = float(np.mean(ms))
+    total_samples = walkers * ns * len(ctxs)
+    # each instance alone (same direct sampler), one make_sample each
+    os.environ["RBMPP_SAMPLER"] = "direct"
+    alone = []
+    for g, (L, J2) in zip(ctxs, meta):
+        g.make_sample(False)
+        t = g.stats()["sampler_ms"]
+        alone.append({"L": L, "J2": J2, "ms": t, "samples_per_s": walkers * ns / (t * 1e-3)})
+    os.environ.pop("RBMPP_SAMPLER", None)
+    line = {"metric": "MC samples/s, batched lattices L=12..18 x J2/J1=0.40..0.60 in one launch",
+            "value": total_samples / (batch_ms * 1e-3), "unit": "MC samples/s", "n_gpus": 1, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": batch_ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded, reference file shapes)",
+            "config": {"workload": args.workload, "instances": len(ctxs), "walkers_per_instance": walkers,
+                       "samples_per_walker": ns, "alphar": 2, "n_qp": 2,
+                       "tuned": {"threads": threads, "order": ["context-major", "round-robin",
+                                                                "longest-first"][order],
+                                 "probe_ms": probe_ms}},
+            "unbatched_sum_ms": float(sum(a["ms"] for a in alone)),
+            "per_instance_alone": alone, "clocks": clocks}
+    print(json.dumps(line), flush=True)
+    b.close()
+    for g in ctxs:
+        g.close()
+    return 0
+
+
 def run_ours(args):
     import torch
     rank, world, local = _rank_env()
@@ -294,13 +358,16 @@ def main():
     ap.add_argument("--steps", type=int, default=2)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--workload", default="j1j2_10x10_trans", choices=sorted(WORKLOADS))
+    ap.add_argument("--workload", default="j1j2_10x10_trans",
+                    choices=sorted(WORKLOADS) + ["batch_l12_18", "batch_l12_18_small"])
     ap.add_argument("--precision", default="split", choices=["fp64", "split"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true", help="skip the extra all-FP64 comparison step")
     args = ap.parse_args()
     if args.impl == "reference":
         return run_reference(args)
+    if args.workload.startswith("batch_"):
+        return run_batch(args)
     return run_ours(args)
 
 

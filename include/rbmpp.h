@@ -169,6 +169,24 @@ int rbmpp_get_walker_state(const rbmpp_ctx* ctx, int* nfastup, int* naccept_all)
  * (Ovec_loc_x before reweighting, calc_phys_quantity.f90:115-220).  Any output may be NULL. */
 int rbmpp_eval_configs(rbmpp_ctx* ctx, int n, const int* x, double* psi, double* hpsi, double* O);
 
+/* Batched sampling: one persistent launch over the walkers of several contexts on one device (different
+ * lattice sizes L, couplings J1/J2 and parameters; the Pfaffian block size may differ per context).  No
+ * counterpart in the reference, which runs one lattice per job.  Each context keeps its own walkers,
+ * random streams and stored samples, exactly as its own rbmpp_make_sample would produce them. */
+typedef struct rbmpp_batch rbmpp_batch;
+int rbmpp_batch_create(rbmpp_ctx* const* ctxs, int n, rbmpp_batch** out);
+int rbmpp_batch_destroy(rbmpp_batch* b);
+const char* rbmpp_batch_last_error(const rbmpp_batch* b);
+/* Autotuner: times probe launches (up to 8 walkers per context, 2 sweeps) for each block size in
+ * {128, 256, 512} threads, measures every context's per-walker cost, and picks the block size and walker
+ * order (context-major, round robin, or longest-first) with the smallest predicted makespan.  Call after
+ * seeding and before the first rbmpp_batch_make_sample; the probed walkers' random streams and Nfastup
+ * are restored.  Outputs (nullable): threads, order (0, 1, 2), probe time in ms of the chosen shape. */
+int rbmpp_batch_tune(rbmpp_batch* b, int* threads, int* order, double* probe_ms);
+/* make_sample (make_sample.f90:4-240) for every walker of every context in one launch;
+ * naccept_total: per-context accepted moves of the stored sweeps (n values) or NULL. */
+int rbmpp_batch_make_sample(rbmpp_batch* b, int first_iteration, long long* naccept_total);
+
 /* rbmpp_eval_configs without any device allocation.  No counterpart in the reference: it exists for
  * callers that can't call cudaMalloc/cudaFree, such as a host code whose own pool allocator holds the
  * GPU's memory, or a loop that must not be stalled by cudaFree's device-wide wait.

@@ -21,7 +21,8 @@ EXPORTS = ["rbmpp_create", "rbmpp_destroy", "rbmpp_last_error", "rbmpp_query", "
            "rbmpp_get_samples", "rbmpp_set_samples", "rbmpp_measure", "rbmpp_measure_energy", "rbmpp_sr_step",
            "rbmpp_iteration", "rbmpp_eval_configs", "rbmpp_get_stats", "rbmpp_exchange_measurement",
            "rbmpp_set_shift", "rbmpp_get_walker_state", "rbmpp_eval_configs_noalloc",
-           "rbmpp_set_s_precision"]
+           "rbmpp_set_s_precision", "rbmpp_batch_create", "rbmpp_batch_destroy", "rbmpp_batch_last_error",
+           "rbmpp_batch_tune", "rbmpp_batch_make_sample"]
 
 SR_FP64 = 0
 SR_SPLIT_BF16 = 1
@@ -87,6 +88,12 @@ def lib():
         L.rbmpp_get_walker_state.argtypes = [P, P, P]
         L.rbmpp_eval_configs_noalloc.argtypes = [P, C.c_int, P, P, P, P]
         L.rbmpp_set_s_precision.argtypes = [P, C.c_int]
+        L.rbmpp_batch_create.argtypes = [P, C.c_int, C.POINTER(P)]
+        L.rbmpp_batch_destroy.argtypes = [P]
+        L.rbmpp_batch_last_error.restype = C.c_char_p
+        L.rbmpp_batch_last_error.argtypes = [P]
+        L.rbmpp_batch_tune.argtypes = [P, P, P, P]
+        L.rbmpp_batch_make_sample.argtypes = [P, C.c_int, P]
         _lib = L
     return _lib
 
@@ -261,6 +268,40 @@ class Context:
         self._chk(lib().rbmpp_eval_configs_noalloc(self.h, int(n), C.c_void_p(d_x or None),
                                                    C.c_void_p(d_psi or None), C.c_void_p(d_hpsi or None),
                                                    C.c_void_p(d_O or None)))
+
+
+class Batch:
+    """One launch of make_sample over several contexts (rbmpp_batch_*)."""
+
+    def __init__(self, contexts):
+        self.ctxs = list(contexts)
+        arr = (C.c_void_p * len(self.ctxs))(*[c.h.value for c in self.ctxs])
+        h = C.c_void_p()
+        rc = lib().rbmpp_batch_create(C.cast(arr, C.c_void_p), len(self.ctxs), C.byref(h))
+        self.h = h
+        self._chk(rc)
+
+    def _chk(self, rc):
+        if rc != 0:
+            raise RbmppError(rc, lib().rbmpp_batch_last_error(self.h).decode())
+
+    def tune(self):
+        th, order, ms = C.c_int(), C.c_int(), C.c_double()
+        self._chk(lib().rbmpp_batch_tune(self.h, C.byref(th), C.byref(order), C.byref(ms)))
+        return th.value, order.value, ms.value
+
+    def make_sample(self, first: bool):
+        out = np.zeros(len(self.ctxs), dtype=np.int64)
+        self._chk(lib().rbmpp_batch_make_sample(self.h, 1 if first else 0, _p(out)))
+        return out
+
+    def close(self):
+        if getattr(self, "h", None):
+            lib().rbmpp_batch_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        self.close()
 
 
 def initial_params(ctx: Context, problem):

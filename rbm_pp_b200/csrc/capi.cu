@@ -142,6 +142,7 @@ struct rbmpp_ctx {
   cudaEvent_t ev[12] = {};
   double stats[8] = {0};
   int stream_stages = 0;  // > 0: TMA-streamed sampler with this many stages
+  bool est_fits = true;   // the estimator's workspace fits in shared memory
   // S of the current measurement: built lazily in the precision the SR step asks for
   bool S_valid = false, S_reduced = false;
   int S_prec = RBMPP_SR_FP64, meas_prec = RBMPP_SR_FP64;
@@ -378,10 +379,14 @@ int rbmpp_create(const rbmpp_dims* dims, rbmpp_ctx** out) {
   if (e != cudaSuccess) return fail(c, RBMPP_E_CUDA, "cudaSetDevice: %s", cudaGetErrorString(e));
   CK(cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking));
   for (auto& e : c->ev) CK(cudaEventCreate(&e));
-  size_t smem = std::max(rbmpp_sampler_smem(d, 256), rbmpp_estimator_smem(d, 256));
   int maxsm = 0;
   CK(cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, dims->device));
-  if ((long long)smem > maxsm) return fail(c, RBMPP_E_ARG, "shared-memory workspace %zu B exceeds %d B", smem, maxsm);
+  // large blocks (N/2 > ~120): the direct sampler's Gauss-Jordan tile moves to a per-walker global scratch
+  if ((long long)rbmpp_sampler_smem(d, 256) > maxsm) d.gj_global = 1;
+  if ((long long)rbmpp_sampler_smem(d, 256) > maxsm)
+    return fail(c, RBMPP_E_ARG, "sampler workspace %zu B exceeds %d B of shared memory", rbmpp_sampler_smem(d, 256),
+                maxsm);
+  c->est_fits = (long long)rbmpp_estimator_smem(d, 256) <= maxsm;
   c->stream_stages = rbmpp_stream_stages(d, maxsm);
   if (getenv("RBMPP_SAMPLER") && std::string(getenv("RBMPP_SAMPLER")) == "direct") c->stream_stages = 0;
   int r;
@@ -415,6 +420,7 @@ int rbmpp_create(const rbmpp_dims* dims, rbmpp_ctx** out) {
   if ((r = dalloc(c, &W.xs, nw * ns * N))) return r;
   if ((r = dalloc(c, &W.pfs, nw * ns * d.n_qp))) return r;
   if ((r = dalloc(c, &W.psis, nw * ns * (d.n_qp + 1) * 2))) return r;
+  if (d.gj_global && (r = dalloc(c, &W.gj, nw * (size_t)d.Np * (d.Np + 1)))) return r;
   std::vector<int> nf(nw, std::min(100, N * 2));  // main.f90:309
   CK(cudaMemcpy(W.nfastup, nf.data(), sizeof(int) * nw, cudaMemcpyHostToDevice));
   // sublattice and bonds: define_sublattice (interface_for_PP.f90:110-136), bond_map (:382-427)
@@ -453,7 +459,7 @@ int rbmpp_destroy(rbmpp_ctx* c) {
   if (!c) return 0;
   void* ptrs[] = {c->d_wmap, c->d_winv, c->d_orb, c->d_bonds, c->d_subB, c->d_para, c->d_Wr, c->d_br, c->d_slater,
                   c->d_XF, c->d_XFT, c->W.x, c->W.idx, c->W.cfg, c->W.th, c->W.sgn, c->W.pf, c->W.psi, c->W.Y,
-                  c->W.mt, c->W.nfastup, c->W.naccept, c->W.nacc_all, c->W.status, c->W.xs, c->W.pfs, c->W.psis, c->d_O, c->d_psiS,
+                  c->W.mt, c->W.nfastup, c->W.naccept, c->W.nacc_all, c->W.status, c->W.xs, c->W.pfs, c->W.psis, c->W.gj, c->d_O, c->d_psiS,
                   c->d_eloc, c->d_a, c->d_b, c->d_tmp_ns, c->d_acc4, c->d_nap, c->d_estat, c->d_gvec, c->d_Ovec,
                   c->d_vec, c->d_S, c->d_part, c->d_info, c->d_err, c->d_rv, c->d_hi, c->d_lo, c->d_Sf, c->d_Sb};
   for (void* p : ptrs)
@@ -644,6 +650,8 @@ int rbmpp_set_samples(rbmpp_ctx* c, const int* x) {
 
 static int measure_common(rbmpp_ctx* c, bool with_o) {
   const DevDims& d = c->d;
+  if (!c->est_fits)
+    return fail(c, RBMPP_E_ARG, "the estimator's workspace for N/2 = %d exceeds the shared memory of one block", d.Np);
   int r = ensure_measure_buffers(c);
   if (r) return r;
   c->S_valid = false;
@@ -709,6 +717,9 @@ int rbmpp_eval_configs(rbmpp_ctx* c, int n, const int* x, double* psi, double* h
   if (!c || n < 0 || !x) return RBMPP_E_ARG;
   if (!c->params_set) return fail(c, RBMPP_E_STATE, "set_params must come first");
   if (n == 0) return 0;
+  if (!c->est_fits)
+    return fail(c, RBMPP_E_ARG, "the estimator's workspace for N/2 = %d exceeds the shared memory of one block",
+                c->d.Np);
   const DevDims& d = c->d;
   int* dx = nullptr;
   int8_t* dx8 = nullptr;
@@ -1160,6 +1171,291 @@ int rbmpp_get_walker_state(const rbmpp_ctx* cc, int* nfastup, int* nacc_all) {
 int rbmpp_get_stats(const rbmpp_ctx* c, double* out, int n) {
   if (!c || !out || n < 0) return RBMPP_E_ARG;
   for (int k = 0; k < n && k < 8; k++) out[k] = c->stats[k];
+  return 0;
+}
+
+}  // extern "C"
+
+// ===================================================================================================
+// Batched make_sample: several contexts (lattice sizes, couplings, parameter sets) on one device sampled
+// by one persistent launch of the direct sampler, with the launch shape and the walker order chosen by a
+// measuring autotuner.
+// ===================================================================================================
+cudaError_t rbmpp_launch_sampler_batch(const BatchInst*, const int2*, int, int, int, int, size_t, long long*,
+                                       cudaStream_t);
+int rbmpp_batch_occupancy(int, int, size_t);
+
+struct rbmpp_batch {
+  std::vector<rbmpp_ctx*> ctx;
+  std::vector<int> off;  // first block of each context in context-major order
+  int total = 0, kpl = 1, threads = 256, order = 0, nsm = 0;
+  size_t smem[3] = {0, 0, 0};  // dynamic shared memory for 128, 256, 512 threads
+  std::vector<double> cost;    // per-walker cost of each context (model, then measured)
+  BatchInst* d_inst = nullptr;
+  int2* d_sched = nullptr;
+  long long* d_cycles = nullptr;
+  cudaEvent_t ev[2] = {};
+  std::string err;
+};
+
+namespace {
+
+int bfail(rbmpp_batch* b, int code, const char* fmt, ...) {
+  char buf[512];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  if (b) b->err = buf;
+  return code;
+}
+
+#define BCK(call)                                                                                  \
+  do {                                                                                             \
+    cudaError_t e_ = (call);                                                                       \
+    if (e_ != cudaSuccess) return bfail(b, RBMPP_E_CUDA, "%s: %s", #call, cudaGetErrorString(e_)); \
+  } while (0)
+
+int thr_index(int threads) { return threads == 128 ? 0 : threads == 256 ? 1 : 2; }
+
+// Block order of the whole batch.  0: context after context; 1: round robin over contexts;
+// 2: longest walkers first (by the per-walker cost), the list-scheduling order that bounds the makespan.
+std::vector<int2> make_schedule(const rbmpp_batch* b, int order) {
+  std::vector<int2> s;
+  s.reserve(b->total);
+  const int n = (int)b->ctx.size();
+  if (order == 0) {
+    for (int k = 0; k < n; k++)
+      for (int w = 0; w < b->ctx[k]->d.nw; w++) s.push_back(make_int2(k, w));
+  } else if (order == 1) {
+    int wmax = 0;
+    for (auto* c : b->ctx) wmax = std::max(wmax, c->d.nw);
+    for (int w = 0; w < wmax; w++)
+      for (int k = 0; k < n; k++)
+        if (w < b->ctx[k]->d.nw) s.push_back(make_int2(k, w));
+  } else {
+    std::vector<int> ks(n);
+    for (int k = 0; k < n; k++) ks[k] = k;
+    std::stable_sort(ks.begin(), ks.end(), [&](int a, int c2) { return b->cost[a] > b->cost[c2]; });
+    int wmax = 0;
+    for (auto* c : b->ctx) wmax = std::max(wmax, c->d.nw);
+    // contexts of (nearly) equal cost interleave, which spreads each context's walkers over the SMs
+    for (int w = 0; w < wmax; w++)
+      for (int k : ks)
+        if (w < b->ctx[k]->d.nw) s.push_back(make_int2(k, w));
+    std::stable_sort(s.begin(), s.end(), [&](const int2& a, const int2& c2) { return b->cost[a.x] > b->cost[c2.x]; });
+  }
+  return s;
+}
+
+// Makespan of a block order under greedy list scheduling on `slots` identical block slots.
+double makespan(const std::vector<int2>& sched, const std::vector<double>& cost, int slots) {
+  std::vector<double> load(std::max(1, slots), 0.0);
+  for (const int2& j : sched) {
+    auto it = std::min_element(load.begin(), load.end());
+    *it += cost[j.x];
+  }
+  return *std::max_element(load.begin(), load.end());
+}
+
+int upload_insts(rbmpp_batch* b, const std::vector<DevDims>* dims_override) {
+  std::vector<BatchInst> h(b->ctx.size());
+  for (size_t k = 0; k < b->ctx.size(); k++) {
+    rbmpp_ctx* c = b->ctx[k];
+    c->d.shift = c->shift;
+    h[k].d = dims_override ? (*dims_override)[k] : c->d;
+    h[k].t = tables(c);
+    h[k].p = params(c);
+    h[k].W = c->W;
+  }
+  BCK(cudaMemcpy(b->d_inst, h.data(), sizeof(BatchInst) * h.size(), cudaMemcpyHostToDevice));
+  return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int rbmpp_batch_create(rbmpp_ctx* const* ctxs, int n, rbmpp_batch** out) {
+  if (!ctxs || n < 1 || !out) return RBMPP_E_ARG;
+  rbmpp_batch* b = new rbmpp_batch();
+  *out = b;
+  int dev = -1;
+  for (int k = 0; k < n; k++) {
+    rbmpp_ctx* c = ctxs[k];
+    if (!c) return bfail(b, RBMPP_E_ARG, "context %d is null", k);
+    if (!c->tables_set || !c->params_set) return bfail(b, RBMPP_E_STATE, "context %d: tables and params first", k);
+    if (dev < 0) dev = c->dims.device;
+    if (c->dims.device != dev) return bfail(b, RBMPP_E_ARG, "contexts on different devices");
+    b->ctx.push_back(c);
+    b->off.push_back(b->total);
+    b->total += c->d.nw;
+    b->kpl = std::max(b->kpl, (c->d.Np + 31) / 32);
+    // cost model until measured: proposals x (Y bytes read per proposal + the per-proposal fixed work)
+    const double sweeps = (double)(c->d.nwarm + c->d.ns + 1);
+    b->cost.push_back(sweeps * c->d.N * ((double)c->d.n_qp * c->d.Np * c->d.Np + 64.0 * c->d.N));
+  }
+  BCK(cudaSetDevice(dev));
+  int maxsm = 0;
+  BCK(cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+  BCK(cudaDeviceGetAttribute(&b->nsm, cudaDevAttrMultiProcessorCount, dev));
+  const int opts[3] = {128, 256, 512};
+  for (int i = 0; i < 3; i++) {
+    size_t m = 0;
+    for (auto* c : b->ctx) m = std::max(m, rbmpp_sampler_smem(c->d, opts[i]));
+    b->smem[i] = (long long)m <= maxsm ? m : 0;
+  }
+  if (!b->smem[1] && !b->smem[0]) return bfail(b, RBMPP_E_ARG, "sampler workspace exceeds shared memory");
+  b->threads = b->smem[1] ? 256 : 128;
+  BCK(cudaMalloc(&b->d_inst, sizeof(BatchInst) * n));
+  BCK(cudaMalloc(&b->d_sched, sizeof(int2) * b->total));
+  BCK(cudaMalloc(&b->d_cycles, sizeof(long long) * b->total));
+  for (auto& e : b->ev) BCK(cudaEventCreate(&e));
+  b->order = 2;
+  std::vector<int2> sched = make_schedule(b, b->order);
+  BCK(cudaMemcpy(b->d_sched, sched.data(), sizeof(int2) * sched.size(), cudaMemcpyHostToDevice));
+  return 0;
+}
+
+int rbmpp_batch_destroy(rbmpp_batch* b) {
+  if (!b) return 0;
+  if (b->d_inst) cudaFree(b->d_inst);
+  if (b->d_sched) cudaFree(b->d_sched);
+  if (b->d_cycles) cudaFree(b->d_cycles);
+  for (auto& e : b->ev)
+    if (e) cudaEventDestroy(e);
+  delete b;
+  return 0;
+}
+
+const char* rbmpp_batch_last_error(const rbmpp_batch* b) { return b ? b->err.c_str() : "null batch"; }
+
+int rbmpp_batch_tune(rbmpp_batch* b, int* threads_out, int* order_out, double* probe_ms) {
+  if (!b) return RBMPP_E_ARG;
+  const int n = (int)b->ctx.size();
+  for (auto* c : b->ctx) {
+    if (!c->seeded) return bfail(b, RBMPP_E_STATE, "seed every context before tuning");
+    if (c->sampled) return bfail(b, RBMPP_E_STATE, "tune before the first batched make_sample");
+  }
+  // probe: up to 8 walkers of each context, 2 sweeps from a fresh configuration (first_iteration)
+  std::vector<int2> probe;
+  std::vector<DevDims> pd(n);
+  for (int k = 0; k < n; k++) {
+    pd[k] = b->ctx[k]->d;
+    pd[k].nwarm = 1;
+    pd[k].ns = 0;
+    for (int w = 0; w < std::min(8, b->ctx[k]->d.nw); w++) probe.push_back(make_int2(k, w));
+  }
+  // the probed walkers' random streams and Nfastup are saved and restored
+  std::vector<std::vector<uint32_t>> mt(n);
+  std::vector<std::vector<int>> nf(n);
+  for (int k = 0; k < n; k++) {
+    rbmpp_ctx* c = b->ctx[k];
+    const int m = std::min(8, c->d.nw);
+    mt[k].resize((size_t)m * 625);
+    nf[k].resize(m);
+    BCK(cudaMemcpy(mt[k].data(), c->W.mt, sizeof(uint32_t) * mt[k].size(), cudaMemcpyDeviceToHost));
+    BCK(cudaMemcpy(nf[k].data(), c->W.nfastup, sizeof(int) * m, cudaMemcpyDeviceToHost));
+  }
+  int r = upload_insts(b, &pd);
+  if (r) return r;
+  cudaStream_t st = b->ctx[0]->st;
+  BCK(cudaMemcpy(b->d_sched, probe.data(), sizeof(int2) * probe.size(), cudaMemcpyHostToDevice));
+  const int opts[3] = {128, 256, 512};
+  double best_est = 1e300, best_ms = 0.0;
+  int best_thr = b->threads, best_order = b->order;
+  std::vector<double> best_cost = b->cost;
+  for (int i = 0; i < 3; i++) {
+    if (!b->smem[i]) continue;
+    const int occ = rbmpp_batch_occupancy(b->kpl, opts[i], b->smem[i]);
+    if (occ < 1) continue;
+    BCK(cudaEventRecord(b->ev[0], st));
+    BCK(rbmpp_launch_sampler_batch(b->d_inst, b->d_sched, (int)probe.size(), 1, b->kpl, opts[i], b->smem[i],
+                                   b->d_cycles, st));
+    BCK(cudaEventRecord(b->ev[1], st));
+    BCK(cudaStreamSynchronize(st));
+    float ms = 0.f;
+    BCK(cudaEventElapsedTime(&ms, b->ev[0], b->ev[1]));
+    std::vector<long long> cyc(probe.size());
+    BCK(cudaMemcpy(cyc.data(), b->d_cycles, sizeof(long long) * cyc.size(), cudaMemcpyDeviceToHost));
+    // per-walker cost of a full make_sample: probe cycles per sweep x sweeps of the real call
+    std::vector<double> cost(n, 0.0);
+    std::vector<int> cnt(n, 0);
+    for (size_t j = 0; j < probe.size(); j++) {
+      cost[probe[j].x] += (double)cyc[j];
+      cnt[probe[j].x]++;
+    }
+    for (int k = 0; k < n; k++)
+      cost[k] = cnt[k] ? cost[k] / cnt[k] / 2.0 * (double)(b->ctx[k]->d.nwarm + b->ctx[k]->d.ns + 1) : 0.0;
+    const std::vector<double> keep = b->cost;
+    b->cost = cost;
+    for (int order = 0; order < 3; order++) {
+      const double est = makespan(make_schedule(b, order), cost, b->nsm * occ);
+      if (est < best_est) {
+        best_est = est;
+        best_thr = opts[i];
+        best_order = order;
+        best_ms = ms;
+        best_cost = cost;
+      }
+    }
+    b->cost = keep;
+  }
+  for (int k = 0; k < n; k++) {
+    rbmpp_ctx* c = b->ctx[k];
+    BCK(cudaMemcpy(c->W.mt, mt[k].data(), sizeof(uint32_t) * mt[k].size(), cudaMemcpyHostToDevice));
+    BCK(cudaMemcpy(c->W.nfastup, nf[k].data(), sizeof(int) * nf[k].size(), cudaMemcpyHostToDevice));
+  }
+  b->threads = best_thr;
+  b->order = best_order;
+  b->cost = best_cost;
+  std::vector<int2> sched = make_schedule(b, b->order);
+  BCK(cudaMemcpy(b->d_sched, sched.data(), sizeof(int2) * sched.size(), cudaMemcpyHostToDevice));
+  if (threads_out) *threads_out = b->threads;
+  if (order_out) *order_out = b->order;
+  if (probe_ms) *probe_ms = best_ms;
+  return 0;
+}
+
+int rbmpp_batch_make_sample(rbmpp_batch* b, int first, long long* naccept_total) {
+  if (!b) return RBMPP_E_ARG;
+  for (size_t k = 0; k < b->ctx.size(); k++) {
+    rbmpp_ctx* c = b->ctx[k];
+    if (!c->params_set || !c->seeded) return bfail(b, RBMPP_E_STATE, "context %zu: set_params and seed first", k);
+    if (!first && !c->sampled) return bfail(b, RBMPP_E_STATE, "context %zu: make_sample(first=0) before any sample", k);
+    BCK(cudaStreamSynchronize(c->st));
+  }
+  int r = upload_insts(b, nullptr);
+  if (r) return r;
+  cudaStream_t st = b->ctx[0]->st;
+  const int ti = thr_index(b->threads);
+  BCK(cudaEventRecord(b->ev[0], st));
+  BCK(rbmpp_launch_sampler_batch(b->d_inst, b->d_sched, b->total, first ? 1 : 0, b->kpl, b->threads, b->smem[ti],
+                                 nullptr, st));
+  BCK(cudaEventRecord(b->ev[1], st));
+  BCK(cudaStreamSynchronize(st));
+  float ms = 0.f;
+  BCK(cudaEventElapsedTime(&ms, b->ev[0], b->ev[1]));
+  for (size_t k = 0; k < b->ctx.size(); k++) {
+    rbmpp_ctx* c = b->ctx[k];
+    const int nw = c->d.nw;
+    std::vector<int> stv(nw), na(nw), naa(nw);
+    BCK(cudaMemcpy(stv.data(), c->W.status, sizeof(int) * nw, cudaMemcpyDeviceToHost));
+    for (int w = 0; w < nw; w++)
+      if (stv[w]) return bfail(b, stv[w], "context %zu walker %d: make_sample failed (code %d)", k, w, stv[w]);
+    BCK(cudaMemcpy(na.data(), c->W.naccept, sizeof(int) * nw, cudaMemcpyDeviceToHost));
+    BCK(cudaMemcpy(naa.data(), c->W.nacc_all, sizeof(int) * nw, cudaMemcpyDeviceToHost));
+    long long tot = 0, tot_all = 0;
+    for (int v : na) tot += v;
+    for (int v : naa) tot_all += v;
+    c->stats[0] = ms;
+    c->stats[5] = (double)tot_all;
+    c->stats[6] = (double)nw * (double)(c->d.nwarm + c->d.ns + 1) * (double)c->d.nupdate;
+    c->naccept_total = tot;
+    c->sampled = true;
+    c->measured = false;
+    if (naccept_total) naccept_total[k] = tot;
+  }
   return 0;
 }
 

@@ -27,6 +27,7 @@ struct DevDims {
   int nw, ns, nupdate, nwarm;
   int orb_injective;  // Orbital_Idx is injective within each spin block for one projection
   int pf_sign;        // (-1)^{Np(Np-1)/2}
+  int gj_global;      // the direct sampler's Gauss-Jordan tile lives in DevWalkers::gj (too large for SMEM)
   double J1, J2, shift;
   double sp_cc[2], sp_cs[2], sp_ss[2], para_sp[2];
 };
@@ -64,6 +65,15 @@ struct DevWalkers {
   int8_t* xs;      // [w][s][N]
   double* pfs;     // [w][s][n_qp]
   double* psis;    // [w][s][n_qp+1][2]
+  double* gj;      // [w][Np][Np+1] Gauss-Jordan scratch when DevDims::gj_global, else null
+};
+
+// One context of a batched launch (several lattices / couplings in one kernel)
+struct BatchInst {
+  DevDims d;
+  DevTables t;
+  DevParams p;
+  DevWalkers W;
 };
 
 // ---- status codes (same numbering as include/rbmpp.h) ----

@@ -146,18 +146,21 @@ __device__ __forceinline__ void warp_update(const DevDims& d, double* Yq, int ua
   __syncwarp();
 }
 
+// make_sample for walker w of one context, by the whole CTA
 template <int KPL>
-__global__ void __launch_bounds__(256, 1)
-    sampler_kernel(const __grid_constant__ DevDims d, const __grid_constant__ DevTables t,
-                   const __grid_constant__ DevParams p, const __grid_constant__ DevWalkers W, int first) {
+__device__ __forceinline__ void sampler_body(const DevDims& d, const DevTables& t, const DevParams& p,
+                                             const DevWalkers& W, const int w, const int first) {
   extern __shared__ __align__(16) char smem[];
   __shared__ WS ws;
-  if (threadIdx.x == 0) ws_layout(d, blockDim.x >> 5, smem, &ws);
+  if (threadIdx.x == 0) {
+    ws_layout(d, blockDim.x >> 5, smem, &ws);
+    if (d.gj_global) ws.tile = W.gj + (size_t)w * d.Np * (d.Np + 1);
+  }
   __syncthreads();
-  const SCtx c{d, t, p, W, (int)blockIdx.x, ws, W.Y + (size_t)blockIdx.x * d.n_qp * d.Np * d.Np};
+  const SCtx c{d, t, p, W, w, ws, W.Y + (size_t)w * d.n_qp * d.Np * d.Np};
   const WS& s = ws;
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, nwarps = blockDim.x >> 5;
-  const int w = c.w, N = d.N, Np = d.Np;
+  const int N = d.N, Np = d.Np;
 
   for (int k = tid; k < 625; k += blockDim.x) s.mt[k] = W.mt[(size_t)w * 625 + k];
   if (tid == 0) status(c) = 0;
@@ -318,9 +321,65 @@ __global__ void __launch_bounds__(256, 1)
   }
 }
 
+template <int KPL>
+__global__ void __launch_bounds__(256, 1)
+    sampler_kernel(const __grid_constant__ DevDims d, const __grid_constant__ DevTables t,
+                   const __grid_constant__ DevParams p, const __grid_constant__ DevWalkers W, int first) {
+  sampler_body<KPL>(d, t, p, W, (int)blockIdx.x, first);
+}
+
 }  // namespace
 
-// Host launcher ------------------------------------------------------------------------------------
+// ---- one launch over the walkers of several contexts ----------------------------------------------
+// Block b runs walker sched[b].y of context sched[b].x, with that context's dimensions, tables,
+// parameters and walker arrays copied to shared memory first.
+namespace {
+
+template <int KPL, int THREADS>
+__global__ void __launch_bounds__(THREADS, 1)
+    sampler_batch_kernel(const BatchInst* __restrict__ inst, const int2* __restrict__ sched, int first,
+                         long long* __restrict__ cycles) {
+  __shared__ BatchInst bi;
+  const int2 job = sched[blockIdx.x];
+  if (threadIdx.x == 0) bi = inst[job.x];
+  __syncthreads();
+  const long long c0 = clock64();
+  sampler_body<KPL>(bi.d, bi.t, bi.p, bi.W, job.y, first);
+  if (cycles && threadIdx.x == 0) cycles[blockIdx.x] = clock64() - c0;
+}
+
+}  // namespace
+
+// Host launchers -----------------------------------------------------------------------------------
+// sched: n_blocks (context, walker) pairs; kpl: columns per lane covering the largest block size;
+// threads: 128, 256 or 512; smem: dynamic shared memory for the largest context; cycles: per-block
+// SM cycles (nullable).
+cudaError_t rbmpp_launch_sampler_batch(const BatchInst* inst, const int2* sched, int n_blocks, int first, int kpl,
+                                       int threads, size_t smem, long long* cycles, cudaStream_t st) {
+#define BLAUNCH(K, TH)                                                                                      \
+  do {                                                                                                      \
+    cudaError_t e = cudaFuncSetAttribute(sampler_batch_kernel<K, TH>,                                       \
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);           \
+    if (e != cudaSuccess) return e;                                                                         \
+    rbmpp_note_launch();                                                                                    \
+    sampler_batch_kernel<K, TH><<<n_blocks, TH, smem, st>>>(inst, sched, first, cycles);                    \
+    return cudaGetLastError();                                                                              \
+  } while (0)
+#define BTHREADS(K)                     \
+  do {                                  \
+    if (threads == 128) BLAUNCH(K, 128); \
+    if (threads == 256) BLAUNCH(K, 256); \
+    if (threads == 512) BLAUNCH(K, 512); \
+  } while (0)
+  if (kpl <= 1) BTHREADS(1);
+  if (kpl <= 2) BTHREADS(2);
+  if (kpl <= 4) BTHREADS(4);
+  if (kpl <= 8) BTHREADS(8);
+#undef BTHREADS
+#undef BLAUNCH
+  return cudaErrorInvalidValue;
+}
+
 size_t rbmpp_sampler_smem(const DevDims& d, int threads) { return ws_layout(d, threads / 32, nullptr, nullptr); }
 
 cudaError_t rbmpp_launch_sampler(const DevDims& d, const DevTables& t, const DevParams& p, const DevWalkers& W,
@@ -342,4 +401,32 @@ cudaError_t rbmpp_launch_sampler(const DevDims& d, const DevTables& t, const Dev
   if (kpl <= 8) LAUNCH(8);
 #undef LAUNCH
   return cudaErrorInvalidValue;
+}
+
+// Resident blocks per SM of the batched sampler for a launch shape (0 if it cannot launch).
+int rbmpp_batch_occupancy(int kpl, int threads, size_t smem) {
+  int nb = 0;
+  cudaError_t e = cudaErrorInvalidValue;
+#define BOCC(K, TH)                                                                                              \
+  do {                                                                                                           \
+    if (cudaFuncSetAttribute(sampler_batch_kernel<K, TH>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) \
+        != cudaSuccess)                                                                                          \
+      return 0;                                                                                                  \
+    e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb, sampler_batch_kernel<K, TH>, TH, smem);             \
+    return e == cudaSuccess ? nb : 0;                                                                            \
+  } while (0)
+#define BOT(K)                          \
+  do {                                  \
+    if (threads == 128) BOCC(K, 128);   \
+    if (threads == 256) BOCC(K, 256);   \
+    if (threads == 512) BOCC(K, 512);   \
+  } while (0)
+  if (kpl <= 1) BOT(1);
+  if (kpl <= 2) BOT(2);
+  if (kpl <= 4) BOT(4);
+  if (kpl <= 8) BOT(8);
+#undef BOT
+#undef BOCC
+  (void)e;
+  return 0;
 }

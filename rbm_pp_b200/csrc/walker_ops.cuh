@@ -85,7 +85,7 @@ __host__ __device__ __forceinline__ size_t ws_layout(const DevDims& d, int nwarp
   t.psi = (double*)take(d.n_qp * 16);
   t.psip = (double*)take(d.n_qp * 16);
   t.rbm = (double*)take(d.n_qp * 8);
-  t.tile = own_tile ? (double*)take((size_t)Np * (Np + 1) * 8) : nullptr;
+  t.tile = (own_tile && !d.gj_global) ? (double*)take((size_t)Np * (Np + 1) * 8) : nullptr;
   t.colbuf = (double*)take(Np * 8);
   t.rowbuf = (double*)take(Np * 8);
   t.perm = (int*)take(Np * 4);
