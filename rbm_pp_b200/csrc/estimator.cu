@@ -7,8 +7,12 @@
 // calc_phys_quantity.f90:338-374) against that inverse.  Bonds are grouped by their up electron ua:
 // with v_ua(i) = XF(u_i, u_ua) and W = Y v_ua (one mat-vec per ua), a bond (ua, db) needs only
 //     r_a = u.Y(:,ua),  s_b = W(db) + dv Y(db,ua),  u^T Y v = u.W + dv r_a,  dv = c - XF(u_ua, u_ua),
-// so the Np^2 work is per up electron, not per bond.  After each round of projections the CTA
-// scatters d Pf / d f_k (calculate_derivative_Pfaffian, slater.f90:94-170) in projection order.
+// so the Np^2 work is per up electron, not per bond.  The up to eight bonds of one up electron gather
+// their rows u together and reduce their dot products together; W and the needed column of Y stay in
+// registers (lane <-> row) and reach other lanes by shuffles.  A warp first stores every bond's ratio,
+// then weighs the bonds lane-parallel (cosh products of the moved spins, calc_phys_quantity.f90:338-374)
+// into per-lane sums of sum_b 2 J sgn psi(x'_b).  After each round of projections the CTA scatters
+// d Pf / d f_k (calculate_derivative_Pfaffian, slater.f90:94-170) in projection order.
 // The RBM part of O_k (calc_phys_quantity.f90:165-201) is a gather over the inverse translation
 // tables.  Outputs are the raw psi, H psi and d psi/d theta_k, optionally reweighted by
 // 1/(|psi| + shift) as calc_phys_quantity.f90:102-109,221 do.
@@ -26,10 +30,9 @@ struct Est {
   int* bdb;      // [4N]    down electron (local index) of the bond
   int* order;    // [4N]    bonds sorted by ua
   int* ustart;   // [Np+1]  CSR offsets into order
-  double* psib;  // [kEstWarps][4N] per-warp partial psi(x') (real projection weights)
+  double* Rb;    // [kEstWarps][4N] per-warp exchange ratios of the current projection
   double* tiles; // [nqw][Np*(Np+1)]
   int* perm;     // [kEstWarps][Np] column map of each warp's inverse
-  double* W;     // [kEstWarps][Np]
   double* vp;    // [kEstWarps][Np]  v_ua stored at the tile's column positions
   double* pfw;   // [n_qp] Pf per projection
   int* nap;
@@ -74,9 +77,8 @@ __host__ __device__ __forceinline__ size_t est_layout(const DevDims& d, int nqw,
   x.bdb = (int*)take((size_t)NB * 4);
   x.order = (int*)take((size_t)NB * 4);
   x.ustart = (int*)take((size_t)(Np + 1) * 4);
-  x.psib = (double*)take((size_t)kEstWarps * NB * 8);
+  x.Rb = (double*)take((size_t)kEstWarps * NB * 8);
   x.perm = (int*)take((size_t)kEstWarps * Np * 4);
-  x.W = (double*)take((size_t)kEstWarps * Np * 8);
   x.vp = (double*)take((size_t)kEstWarps * Np * 8);
   x.pfw = (double*)take((size_t)d.n_qp * 8);
   x.nap = (int*)take(16);
@@ -114,7 +116,6 @@ __global__ void __launch_bounds__(kEstThreads, 1)
   for (int i = tid; i < N; i += blockDim.x) s.x[i] = (int)xs[(size_t)cfgi * N + i];
   if (Orow)
     for (int k = tid; k < d.Nv; k += blockDim.x) Orow[k] = 0.0;
-  for (int k = tid; k < kEstWarps * NB; k += blockDim.x) e.psib[k] = 0.0;
   if (tid == 0) s.iflag[F_STATUS] = 0;
   __syncthreads();
   if (tid == 0) {
@@ -166,11 +167,17 @@ __global__ void __launch_bounds__(kEstThreads, 1)
     return;
   }
   const int off_pp = d.alphar * (N + 1);
-  double* psib = e.psib + (size_t)warp * NB;
+  double* Rw = e.Rb + (size_t)warp * NB;
   int* src = e.perm + (size_t)warp * Np;
-  double* Wv = e.W + (size_t)warp * Np;
   double* vp = e.vp + (size_t)warp * Np;
+  int jc[KPL];
+#pragma unroll
+  for (int q = 0; q < KPL; q++) {
+    const int j = lane + 32 * q;
+    jc[q] = j < Np ? j : Np - 1;  // in-tile index for every lane
+  }
   bool bad = false;
+  double hacc = 0.0;  // this lane's share of sum_b 2 J sgn psi(x'_b)
   // rounds of nqw projections: warp w < nqw handles qp = round*nqw + w
   for (int q0 = 0; q0 < d.n_qp; q0 += e.nqw) {
     const int qp = q0 + warp;
@@ -179,13 +186,9 @@ __global__ void __launch_bounds__(kEstThreads, 1)
       const int mp = qp >> 1, sp = qp & 1;
       const double* XFq = p.XF + (size_t)qp * N * N;
       const double* XFTq = p.XFT + (size_t)qp * N * N;
-      for (int i = 0; i < Np; i++) {
-        const double* row = XFq + (size_t)s.idx[i] * N;
-        for (int j = lane; j < Np; j += 32) T[i * ld + j] = row[s.idx[Np + j]];
-      }
-      __syncwarp();
+      warp_gather_tile<KPL, NP, 8>(T, XFq, s.idx, Np, N);
       bool sing;
-      const double det = warp_gj<KPL, NP>(T, Np, src, sing);
+      const double det = warp_gj<KPL, NP, (KPL <= 2 ? 16 : (KPL <= 4 ? 8 : 4))>(T, Np, src, sing);
       if (sing) bad = true;
       const double pfq = (double)d.pf_sign * det;
       const cplx cw = psi_wo_pf(d, t, s.rbm[qp], s.sgn[mp], qp);
@@ -194,67 +197,129 @@ __global__ void __launch_bounds__(kEstThreads, 1)
         s.psi[2 * qp] = cw.re * pfq;
         s.psi[2 * qp + 1] = cw.im * pfq;
       }
+      // down-electron sites of this lane's rows (the columns of every u row)
+      int dsite[KPL];
+#pragma unroll
+      for (int q = 0; q < KPL; q++) dsite[q] = s.idx[Np + jc[q]];
       // exchange ratios, grouped by up electron
       for (int ua = 0; ua < Np && !sing; ua++) {
         const int b0 = e.ustart[ua], b1 = e.ustart[ua + 1];
         if (b0 == b1) continue;
         const int s_up = s.idx[ua];
         const int cu = src[ua];
-        // v_ua(i) = XF(u_i, s_up) at the tile's column positions, W = Y v_ua (lane <-> row)
-        for (int i = lane; i < Np; i += 32) vp[src[i]] = XFTq[(size_t)s_up * N + s.idx[i]];
-        __syncwarp();
-        for (int j = lane; j < Np; j += 32) {
-          double a = 0.0;
-#pragma unroll 5
-          for (int k = 0; k < Np; k++) a = fma(T[j * ld + k], vp[k], a);
-          Wv[j] = a;
-        }
-        __syncwarp();
-        const double xfuu = XFq[(size_t)s_up * N + s_up];
-        for (int bb = b0; bb < b1; bb++) {
-          const int b = e.order[bb];
-          const int db = e.bdb[b];
-          const int s_dn = s.idx[Np + db];
-          const double c = XFq[(size_t)s_dn * N + s_up];
-          double ra = 0.0, uw = 0.0;
+        double vv[KPL];
 #pragma unroll
-          for (int q = 0; q < KPL; q++) {
-            const int j = lane + 32 * q, jc = j < Np ? j : Np - 1;  // in-tile index for every lane
-            const double tj = T[jc * ld + cu], wj = Wv[jc];
-            if (j < Np) {
-              const double uj = (j == db) ? c : XFq[(size_t)s_dn * N + s.idx[Np + j]];
-              ra = fma(uj, tj, ra);
-              uw = fma(uj, wj, uw);
+        for (int q = 0; q < KPL; q++) vv[q] = XFTq[(size_t)s_up * N + s.idx[jc[q]]];
+        const double xfuu = XFq[(size_t)s_up * N + s_up];
+        constexpr int MB = KPL <= 2 ? 8 : (KPL <= 4 ? 4 : 2);  // a site lies on 4 J1 and 4 J2 bonds
+        for (int c0 = b0; c0 < b1; c0 += MB) {
+          const int m = b1 - c0 < MB ? b1 - c0 : MB;
+          // rows u of the m bonds: u_j = XF(s_dn, down site j), gathered before any use
+          double uu[MB][KPL], cb[MB];
+          int bv[MB], dbv[MB];
+#pragma unroll
+          for (int t2 = 0; t2 < MB; t2++) {
+            bv[t2] = 0;
+            dbv[t2] = 0;
+            cb[t2] = 0.0;
+#pragma unroll
+            for (int q = 0; q < KPL; q++) uu[t2][q] = 0.0;
+            if (t2 < m) {
+              const int b = e.order[c0 + t2], db = e.bdb[b];
+              const double* urow = XFq + (size_t)s.idx[Np + db] * N;
+              bv[t2] = b;
+              dbv[t2] = db;
+              cb[t2] = urow[s_up];
+#pragma unroll
+              for (int q = 0; q < KPL; q++) uu[t2][q] = urow[dsite[q]];
             }
           }
-          ra = warp_sum(ra);
-          uw = warp_sum(uw);
-          const double dv = c - xfuu;
-          const double y = T[db * ld + cu];
-          const double sb = Wv[db] + dv * y;
-          const double wv = uw + dv * ra;
-          const double R = ra * sb - y * (wv - c);
-          // cosh product of theta' for this projection (update_theta on the qp's alphar slots)
-          const int i1 = e.ap[2 * b], i2 = e.ap[2 * b + 1];
-          const int iw1 = t.wmap[(size_t)mp * N + i1], iw2 = t.wmap[(size_t)mp * N + i2];
-          const double s_sign = sp == 0 ? 1.0 : -1.0;
-          double ch = 1.0;
-          for (int f = lane; f < d.alphar; f += 32) {
-            double th = s.th[qp * d.alphar + f];
-            th = th - 2.0 * p.Wr[(size_t)f * N + iw1] * (double)s.x[i1] * s_sign;
-            th = th - 2.0 * p.Wr[(size_t)f * N + iw2] * (double)s.x[i2] * s_sign;
-            ch = ch * cosh(th);
+          if (c0 == b0) {
+            // v_ua(i) = XF(u_i, s_up) at the tile's column positions, W = Y v_ua (lane <-> row)
+#pragma unroll
+            for (int q = 0; q < KPL; q++)
+              if (lane + 32 * q < Np) vp[src[lane + 32 * q]] = vv[q];
+            __syncwarp();
+          }
+          double wv[KPL], tj[KPL];
+#pragma unroll
+          for (int q = 0; q < KPL; q++) {
+            double a0 = 0.0, a1 = 0.0;
+            const double* Tr = T + jc[q] * ld;
+#pragma unroll 5
+            for (int k = 0; k + 1 < Np; k += 2) {
+              a0 = fma(Tr[k], vp[k], a0);
+              a1 = fma(Tr[k + 1], vp[k + 1], a1);
+            }
+            if (Np & 1) a0 = fma(Tr[Np - 1], vp[Np - 1], a0);
+            wv[q] = a0 + a1;
+            tj[q] = Tr[cu];
+          }
+          double ra[MB], uw[MB];
+#pragma unroll
+          for (int t2 = 0; t2 < MB; t2++) {
+            ra[t2] = 0.0;
+            uw[t2] = 0.0;
+#pragma unroll
+            for (int q = 0; q < KPL; q++)
+              if (lane + 32 * q < Np) {
+                const double uj = (lane + 32 * q == dbv[t2]) ? cb[t2] : uu[t2][q];
+                ra[t2] = fma(uj, tj[q], ra[t2]);
+                uw[t2] = fma(uj, wv[q], uw[t2]);
+              }
           }
 #pragma unroll
-          for (int o = 16; o > 0; o >>= 1) ch = ch * __shfl_xor_sync(0xffffffffu, ch, o);
-          if (lane == 0) {
-            const int sg = -s.sgn[mp] * (t.subB[i1] ? -1 : 1) * (t.subB[i2] ? -1 : 1);
-            const cplx cb = psi_wo_pf(d, t, ch, sg, qp);
-            psib[b] += cb.re * (R * pfq);
-          }
+          for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+            for (int t2 = 0; t2 < MB; t2++)
+              if (t2 < m) {
+                ra[t2] += __shfl_xor_sync(0xffffffffu, ra[t2], o);
+                uw[t2] += __shfl_xor_sync(0xffffffffu, uw[t2], o);
+              }
+#pragma unroll
+          for (int t2 = 0; t2 < MB; t2++)
+            if (t2 < m) {
+              const int db = dbv[t2];
+              double yq = 0.0, wq = 0.0;
+#pragma unroll
+              for (int q = 0; q < KPL; q++)
+                if (q == (db >> 5)) {
+                  yq = tj[q];
+                  wq = wv[q];
+                }
+              const double y = __shfl_sync(0xffffffffu, yq, db & 31);  // Y(db, ua)
+              const double wdb = __shfl_sync(0xffffffffu, wq, db & 31);
+              const double c = cb[t2];
+              const double dv = c - xfuu;
+              const double sb = wdb + dv * y;
+              const double wvv = uw[t2] + dv * ra[t2];
+              if (lane == 0) Rw[bv[t2]] = ra[t2] * sb - y * (wvv - c);
+            }
         }
         __syncwarp();
       }
+      __syncwarp();
+      // weigh every bond: cosh product of theta' for this projection (update_theta on the qp's alphar slots)
+      if (!sing) {
+        const int* wm = t.wmap + (size_t)mp * N;
+        const double s_sign = sp == 0 ? 1.0 : -1.0;
+        for (int b = lane; b < nap; b += 32) {
+          const int i1 = e.ap[2 * b], i2 = e.ap[2 * b + 1];
+          const int iw1 = wm[i1], iw2 = wm[i2];
+          const double x1 = (double)s.x[i1], x2 = (double)s.x[i2];
+          double ch = 1.0;
+          for (int f = 0; f < d.alphar; f++) {
+            double th = s.th[qp * d.alphar + f];
+            th = th - 2.0 * p.Wr[(size_t)f * N + iw1] * x1 * s_sign;
+            th = th - 2.0 * p.Wr[(size_t)f * N + iw2] * x2 * s_sign;
+            ch = ch * cosh(th);
+          }
+          const int sg = -s.sgn[mp] * (t.subB[i1] ? -1 : 1) * (t.subB[i2] ? -1 : 1);
+          const cplx cbw = psi_wo_pf(d, t, ch, sg, qp);
+          hacc = hacc + e.apc[b] * (cbw.re * (Rw[b] * pfq));
+        }
+      }
+      __syncwarp();
     }
     __syncthreads();
     // d Pf / d f_k scatter of this round's projections, in projection order (slater.f90:140-167)
@@ -267,18 +332,42 @@ __global__ void __launch_bounds__(kEstThreads, 1)
         const double pfq = e.pfw[qp];
         const cplx cw = psi_wo_pf(d, t, s.rbm[qp], s.sgn[mp], qp);
         const double cc = pfq * d.sp_cc[sp] * cw.re, ss = pfq * d.sp_ss[sp] * cw.re;
-        for (int pr = tid; pr < Np * Np; pr += blockDim.x) {
-          const int j = pr / Np, i = pr - j * Np;  // j: down electron, i: up electron
-          const double y = Tw[j * ld + srcw[i]];  // Y(j, i) = (M^-1)(Np+j, i)
-          const int tu = wm[s.idx[i]], td = wm[s.idx[Np + j]];
-          double* o1 = Orow + off_pp + t.orb[(size_t)tu * N + td];
-          double* o2 = Orow + off_pp + t.orb[(size_t)td * N + tu];
-          if (d.orb_injective) {
-            if (cc != 0.0) *o1 = *o1 + y * cc;
-            if (ss != 0.0) *o2 = *o2 + y * ss;
-          } else {
-            if (cc != 0.0) atomicAdd(o1, y * cc);
-            if (ss != 0.0) atomicAdd(o2, y * ss);
+        const int npr = Np * Np;
+        if (d.orb_injective) {
+          // every (up, down) pair of one projection has its own two targets, so a thread may load the
+          // targets of SB pairs before it stores any of them
+          constexpr int SB = 8;
+          for (int pr0 = tid; pr0 < npr; pr0 += SB * kEstThreads) {
+            double y[SB], v1[SB], v2[SB];
+            int a1[SB], a2[SB];
+#pragma unroll
+            for (int u = 0; u < SB; u++) {
+              const int pr = pr0 + u * kEstThreads, prc = pr < npr ? pr : npr - 1;
+              const int j = prc / Np, i = prc - j * Np;  // j: down electron, i: up electron
+              y[u] = Tw[j * ld + srcw[i]];               // Y(j, i) = (M^-1)(Np+j, i)
+              const int tu = wm[s.idx[i]], td = wm[s.idx[Np + j]];
+              a1[u] = off_pp + t.orb[(size_t)tu * N + td];
+              a2[u] = off_pp + t.orb[(size_t)td * N + tu];
+            }
+#pragma unroll
+            for (int u = 0; u < SB; u++) {
+              v1[u] = cc != 0.0 ? Orow[a1[u]] : 0.0;
+              v2[u] = ss != 0.0 ? Orow[a2[u]] : 0.0;
+            }
+#pragma unroll
+            for (int u = 0; u < SB; u++)
+              if (pr0 + u * kEstThreads < npr) {
+                if (cc != 0.0) Orow[a1[u]] = v1[u] + y[u] * cc;
+                if (ss != 0.0) Orow[a2[u]] = v2[u] + y[u] * ss;
+              }
+          }
+        } else {
+          for (int pr = tid; pr < npr; pr += blockDim.x) {
+            const int j = pr / Np, i = pr - j * Np;
+            const double y = Tw[j * ld + srcw[i]];
+            const int tu = wm[s.idx[i]], td = wm[s.idx[Np + j]];
+            if (cc != 0.0) atomicAdd(Orow + off_pp + t.orb[(size_t)tu * N + td], y * cc);
+            if (ss != 0.0) atomicAdd(Orow + off_pp + t.orb[(size_t)td * N + tu], y * ss);
           }
         }
         __syncthreads();
@@ -287,6 +376,8 @@ __global__ void __launch_bounds__(kEstThreads, 1)
     __syncthreads();
   }
   if (lane == 0 && bad) s.iflag[F_STATUS] = ST_SINGULAR;
+  hacc = warp_sum(hacc);
+  if (lane == 0) s.red[warp] = hacc;
   __syncthreads();
   if (s.iflag[F_STATUS]) {
     if (tid == 0 && out_status) out_status[cfgi] = s.iflag[F_STATUS];
@@ -302,11 +393,7 @@ __global__ void __launch_bounds__(kEstThreads, 1)
     s.dsc[D_PSI0R] = re;
     s.dsc[D_PSI0I] = im;
     double hr = e.diag[0] * re, hi = e.diag[0] * im;
-    for (int b = 0; b < nap; b++) {
-      double pb = 0.0;
-      for (int w = 0; w < kEstWarps; w++) pb += e.psib[(size_t)w * NB + b];
-      hr += e.apc[b] * pb;
-    }
+    for (int w = 0; w < kEstWarps; w++) hr += s.red[w];
     s.dsc[D_PSIPR] = hr;
     s.dsc[D_PSIPI] = hi;
     if (out_nap) out_nap[cfgi] = nap;

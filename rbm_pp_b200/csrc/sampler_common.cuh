@@ -37,12 +37,7 @@ __device__ __forceinline__ void warp_scratch_all(const SCtx& c, const int* idx, 
     double* T = c.par_tiles + (size_t)wk * Np * ld;
     int* perm = (int*)(s.wS + (size_t)warp * Np);
     for (int qp = wk; qp < d.n_qp && !sing_any; qp += c.par_ntile) {
-      const double* XFq = c.p.XF + (size_t)qp * N * N;
-      for (int i = 0; i < Np; i++) {
-        const double* row = XFq + (size_t)idx[i] * N;
-        for (int j = lane; j < Np; j += 32) T[i * ld + j] = row[idx[Np + j]];
-      }
-      __syncwarp();
+      warp_gather_tile<KPL, NP, 8>(T, c.p.XF + (size_t)qp * N * N, idx, Np, N);
       bool sing;
       const double det = warp_gj<KPL, NP>(T, Np, perm, sing);
       if (sing) {

@@ -333,17 +333,59 @@ __device__ __forceinline__ void cta_amplitude(const DevDims& d, const DevTables&
   __syncthreads();
 }
 
+// Warp-level gather of the n x n block X(i, j) = XF(idx[i], idx[n + j]) into the tile T (leading dimension
+// n + 1), lane <-> column.  Rows go in batches of B whose loads are all issued before any of their stores:
+// the compiler cannot move a global load past a shared store it cannot prove disjoint, so a row-at-a-time
+// loop would wait one L2 round trip per row.
+template <int KPL, int NP, int B>
+__device__ __forceinline__ void warp_gather_tile(double* T, const double* XFq, const int* idx, int n_rt, int N) {
+  const int n = NP > 0 ? NP : n_rt, ld = n + 1;
+  const int lane = threadIdx.x & 31;
+  int col[KPL];
+#pragma unroll
+  for (int q = 0; q < KPL; q++) {
+    const int j = lane + 32 * q;
+    col[q] = idx[n + (j < n ? j : n - 1)];
+  }
+  for (int i0 = 0; i0 < n; i0 += B) {
+    double v[B][KPL];
+#pragma unroll
+    for (int ii = 0; ii < B; ii++) {
+      const int i = i0 + ii;
+      const double* row = XFq + (size_t)idx[i < n ? i : n - 1] * N;
+#pragma unroll
+      for (int q = 0; q < KPL; q++) v[ii][q] = row[col[q]];
+    }
+#pragma unroll
+    for (int ii = 0; ii < B; ii++) {
+      const int i = i0 + ii;
+#pragma unroll
+      for (int q = 0; q < KPL; q++)
+        if (i < n && lane + 32 * q < n) T[i * ld + lane + 32 * q] = v[ii][q];
+    }
+  }
+  __syncwarp();
+}
+
 // Warp-level Gauss-Jordan inverse with partial pivoting (the role of dgetrf/dgetri, matrix.f90:155-177) of
 // the n x n tile T with leading dimension n + 1 (n = NP when NP > 0, a compile-time size; otherwise n_rt).
 // Returns det(X) (0 and singular = true on a zero pivot).  Column b of X^{-1} is column perm[b] of T
-// afterwards.  The pivot column is held in registers (rows lane + 32 p) and broadcast by shuffles, so the
-// elimination's loads do not wait on its stores.  Lanes past the last row or column load from a clamped,
-// in-tile index (and discard the value): the compiler may issue a guarded shared load unconditionally,
-// and a tile can end at the end of the block's shared memory.
-template <int KPL, int NP>
+// afterwards.  The pivot column is held in registers (rows lane + 32 p) and broadcast by shuffles.  The
+// elimination runs over batches of B rows, loading every row of a batch before storing any, so a step
+// waits a shared-memory round trip per batch rather than per row.  Lanes past the last row or column load
+// from a clamped, in-tile index (and discard the value): the compiler may issue a guarded shared load
+// unconditionally, and a tile can end at the end of the block's shared memory.
+template <int KPL, int NP, int B = 8>
 __device__ __forceinline__ double warp_gj(double* T, int n_rt, int* perm, bool& singular) {
+  static_assert(32 % B == 0, "row batches must tile a 32-row group");
   const int n = NP > 0 ? NP : n_rt, ld = n + 1;
   const int lane = threadIdx.x & 31;
+  int jc[KPL];
+#pragma unroll
+  for (int q = 0; q < KPL; q++) {
+    const int j = lane + 32 * q;
+    jc[q] = j < n ? j : n - 1;
+  }
   double det = 1.0;
   singular = false;
   for (int k = 0; k < n; k++) {
@@ -389,8 +431,8 @@ __device__ __forceinline__ double warp_gj(double* T, int n_rt, int* perm, bool& 
     double r[KPL];
 #pragma unroll
     for (int q = 0; q < KPL; q++) {
-      const int j = lane + 32 * q, jc = j < n ? j : n - 1;
-      const double a = T[k * ld + jc], b = T[bi * ld + jc];
+      const int j = lane + 32 * q;
+      const double a = T[k * ld + jc[q]], b = T[bi * ld + jc[q]];
       r[q] = 0.0;
       if (j < n) {
         if (bi != k) T[bi * ld + j] = a;
@@ -400,22 +442,38 @@ __device__ __forceinline__ double warp_gj(double* T, int n_rt, int* perm, bool& 
     det = (bi != k ? -det : det) * pivot;
     __syncwarp();
     // rows i != k: T(i,j) -= f_i r_j for j != k, with f_i = T(i,k) after the interchange
+    auto batch = [&](const int p, const int l0, const double fcp) {
+      double tv[B][KPL];
 #pragma unroll
-    for (int p = 0; p < KPL; p++) {
-#pragma unroll 8
-      for (int l = 0; l < 32; l++) {
-        const int i = 32 * p + l;
-        if (i >= n) break;
-        double f = __shfl_sync(0xffffffffu, fc[p], l);
+      for (int ii = 0; ii < B; ii++) {
+        const int i = 32 * p + l0 + ii, ic = i < n ? i : n - 1;
+#pragma unroll
+        for (int q = 0; q < KPL; q++) tv[ii][q] = T[ic * ld + jc[q]];
+      }
+#pragma unroll
+      for (int ii = 0; ii < B; ii++) {
+        const int i = 32 * p + l0 + ii;
+        double f = __shfl_sync(0xffffffffu, fcp, l0 + ii);
         if (i == bi) f = fkk;
-        if (i != k) {
+        if (i < n && i != k) {
 #pragma unroll
           for (int q = 0; q < KPL; q++) {
             const int j = lane + 32 * q;
-            const double t = T[i * ld + (j < n ? j : n - 1)];
-            if (j < n && j != k) T[i * ld + j] = t - f * r[q];
+            if (j < n && j != k) T[i * ld + j] = tv[ii][q] - f * r[q];
           }
         }
+      }
+    };
+#pragma unroll
+    for (int p = 0; p < KPL; p++) {
+      if (32 * p >= n) break;
+      if constexpr (NP > 0) {
+#pragma unroll
+        for (int l0 = 0; l0 < 32; l0 += B)
+          if (32 * p + l0 < n) batch(p, l0, fc[p]);
+      } else {
+#pragma unroll 1
+        for (int l0 = 0; l0 < 32 && 32 * p + l0 < n; l0 += B) batch(p, l0, fc[p]);
       }
     }
     __syncwarp();
@@ -431,16 +489,18 @@ __device__ __forceinline__ double warp_gj(double* T, int n_rt, int* perm, bool& 
     }
     __syncwarp();
   }
-  if (lane == 0) {  // source column of each column of the inverse: undo the interchanges in reverse
-    int src[RBMPP_MAX_N / 2];
-    for (int b = 0; b < n; b++) src[b] = b;
+  // Source column of each column of the inverse: undo the interchanges in reverse, in place.  When step k
+  // is undone, positions > k already hold source columns and positions < k are untouched (perm[k'] >= k').
+  if (lane == 0)
     for (int k = n - 1; k >= 0; k--) {
-      const int pk = perm[k], a = src[k];
-      src[k] = src[pk];
-      src[pk] = a;
+      const int pk = perm[k];
+      if (pk != k) {
+        perm[k] = perm[pk];
+        perm[pk] = k;
+      } else {
+        perm[k] = k;
+      }
     }
-    for (int b = 0; b < n; b++) perm[b] = src[b];
-  }
   __syncwarp();
   return det;
 }
