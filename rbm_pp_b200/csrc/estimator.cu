@@ -8,8 +8,9 @@
 // with v_ua(i) = XF(u_i, u_ua) and W = Y v_ua (one mat-vec per ua), a bond (ua, db) needs only
 //     r_a = u.Y(:,ua),  s_b = W(db) + dv Y(db,ua),  u^T Y v = u.W + dv r_a,  dv = c - XF(u_ua, u_ua),
 // so the Np^2 work is per up electron, not per bond.  The up to eight bonds of one up electron gather
-// their rows u together and reduce their dot products together; W and the needed column of Y stay in
-// registers (lane <-> row) and reach other lanes by shuffles.  A warp first stores every bond's ratio,
+// their rows u together and reduce their 16 dot products in one transposed butterfly; lane t then
+// finishes bond t.  W and the needed column of Y stay in registers (lane <-> row) and reach other lanes
+// by shuffles.  A warp first stores every bond's ratio,
 // then weighs the bonds lane-parallel (cosh products of the moved spins, calc_phys_quantity.f90:338-374)
 // into per-lane sums of sum_b 2 J sgn psi(x'_b).  After each round of projections the CTA scatters
 // d Pf / d f_k (calculate_derivative_Pfaffian, slater.f90:94-170) in projection order.
@@ -95,6 +96,30 @@ __host__ __device__ __forceinline__ size_t est_layout(const DevDims& d, int nqw,
   if (w) *w = t;
   if (e) *e = x;
   return off;
+}
+
+// Sums NV values (a power of two, at most 32) over the warp together.  Each halving level trades half of
+// the values with the partner lane, so the NV sums take NV - 1 + 5 - log2(NV) shuffles instead of 5 NV.
+// Returns the warp total of value lane >> (5 - log2(NV)); v is overwritten.
+template <int NV>
+__device__ __forceinline__ double warp_transpose_sum(double (&v)[NV], int lane) {
+  constexpr int L2 = NV >= 32 ? 5 : NV >= 16 ? 4 : NV >= 8 ? 3 : NV >= 4 ? 2 : NV >= 2 ? 1 : 0;
+  static_assert((1 << L2) == NV && NV <= 32, "NV must be a power of two <= 32");
+#pragma unroll
+  for (int lev = 0; lev < L2; lev++) {
+    const int h = NV >> (lev + 1), o = 16 >> lev;
+    const bool hi = (lane & o) != 0;
+#pragma unroll
+    for (int i = 0; i < h; i++) {
+      const double keep = hi ? v[h + i] : v[i];
+      const double give = hi ? v[i] : v[h + i];
+      v[i] = keep + __shfl_xor_sync(0xffffffffu, give, o);
+    }
+  }
+  double r = v[0];
+#pragma unroll
+  for (int o = 16 >> L2; o > 0; o >>= 1) r += __shfl_xor_sync(0xffffffffu, r, o);
+  return r;
 }
 
 template <int KPL, int NP>
@@ -212,28 +237,38 @@ __global__ void __launch_bounds__(kEstThreads, 1)
         for (int q = 0; q < KPL; q++) vv[q] = XFTq[(size_t)s_up * N + s.idx[jc[q]]];
         const double xfuu = XFq[(size_t)s_up * N + s_up];
         constexpr int MB = KPL <= 2 ? 8 : (KPL <= 4 ? 4 : 2);  // a site lies on 4 J1 and 4 J2 bonds
+        constexpr int NV = 2 * MB, SH = MB == 8 ? 1 : (MB == 4 ? 2 : 3);  // value v ends in lane v << SH
         for (int c0 = b0; c0 < b1; c0 += MB) {
           const int m = b1 - c0 < MB ? b1 - c0 : MB;
+          // bond t of the chunk in lane t: its index, down electron, down site and X'(ua, db) = XF(s_dn, s_up)
+          int b_l = 0, db_l = 0, sdn_l = 0;
+          double c_l = 0.0;
+          if (lane < m) {
+            b_l = e.order[c0 + lane];
+            db_l = e.bdb[b_l];
+            sdn_l = s.idx[Np + db_l];
+            c_l = XFq[(size_t)sdn_l * N + s_up];
+          }
           // rows u of the m bonds: u_j = XF(s_dn, down site j), gathered before any use
           double uu[MB][KPL], cb[MB];
-          int bv[MB], dbv[MB];
+          int dbv[MB];
 #pragma unroll
           for (int t2 = 0; t2 < MB; t2++) {
-            bv[t2] = 0;
-            dbv[t2] = 0;
+            dbv[t2] = -1;
             cb[t2] = 0.0;
 #pragma unroll
             for (int q = 0; q < KPL; q++) uu[t2][q] = 0.0;
             if (t2 < m) {
-              const int b = e.order[c0 + t2], db = e.bdb[b];
-              const double* urow = XFq + (size_t)s.idx[Np + db] * N;
-              bv[t2] = b;
-              dbv[t2] = db;
-              cb[t2] = urow[s_up];
+              const int sdn = __shfl_sync(0xffffffffu, sdn_l, t2);
+              dbv[t2] = __shfl_sync(0xffffffffu, db_l, t2);
+              const double* urow = XFq + (size_t)sdn * N;
 #pragma unroll
               for (int q = 0; q < KPL; q++) uu[t2][q] = urow[dsite[q]];
             }
           }
+#pragma unroll
+          for (int t2 = 0; t2 < MB; t2++)
+            if (t2 < m) cb[t2] = __shfl_sync(0xffffffffu, c_l, t2);
           if (c0 == b0) {
             // v_ua(i) = XF(u_i, s_up) at the tile's column positions, W = Y v_ua (lane <-> row)
 #pragma unroll
@@ -255,46 +290,40 @@ __global__ void __launch_bounds__(kEstThreads, 1)
             wv[q] = a0 + a1;
             tj[q] = Tr[cu];
           }
-          double ra[MB], uw[MB];
+          // partial sums: val[t] = u_t . Y(:, ua), val[MB + t] = u_t . W
+          double val[NV];
 #pragma unroll
           for (int t2 = 0; t2 < MB; t2++) {
-            ra[t2] = 0.0;
-            uw[t2] = 0.0;
+            val[t2] = 0.0;
+            val[MB + t2] = 0.0;
 #pragma unroll
             for (int q = 0; q < KPL; q++)
               if (lane + 32 * q < Np) {
                 const double uj = (lane + 32 * q == dbv[t2]) ? cb[t2] : uu[t2][q];
-                ra[t2] = fma(uj, tj[q], ra[t2]);
-                uw[t2] = fma(uj, wv[q], uw[t2]);
+                val[t2] = fma(uj, tj[q], val[t2]);
+                val[MB + t2] = fma(uj, wv[q], val[MB + t2]);
               }
           }
+          const double tot = warp_transpose_sum<NV>(val, lane);
+          // lane t < m finishes bond t
+          const double ra = __shfl_sync(0xffffffffu, tot, (lane << SH) & 31);
+          const double uw = __shfl_sync(0xffffffffu, tot, ((MB + lane) << SH) & 31);
+          double y = 0.0, wdb = 0.0;
 #pragma unroll
-          for (int o = 16; o > 0; o >>= 1)
-#pragma unroll
-            for (int t2 = 0; t2 < MB; t2++)
-              if (t2 < m) {
-                ra[t2] += __shfl_xor_sync(0xffffffffu, ra[t2], o);
-                uw[t2] += __shfl_xor_sync(0xffffffffu, uw[t2], o);
-              }
-#pragma unroll
-          for (int t2 = 0; t2 < MB; t2++)
-            if (t2 < m) {
-              const int db = dbv[t2];
-              double yq = 0.0, wq = 0.0;
-#pragma unroll
-              for (int q = 0; q < KPL; q++)
-                if (q == (db >> 5)) {
-                  yq = tj[q];
-                  wq = wv[q];
-                }
-              const double y = __shfl_sync(0xffffffffu, yq, db & 31);  // Y(db, ua)
-              const double wdb = __shfl_sync(0xffffffffu, wq, db & 31);
-              const double c = cb[t2];
-              const double dv = c - xfuu;
-              const double sb = wdb + dv * y;
-              const double wvv = uw[t2] + dv * ra[t2];
-              if (lane == 0) Rw[bv[t2]] = ra[t2] * sb - y * (wvv - c);
+          for (int q = 0; q < KPL; q++) {
+            const double a = __shfl_sync(0xffffffffu, tj[q], db_l & 31);   // Y(db, ua)
+            const double w = __shfl_sync(0xffffffffu, wv[q], db_l & 31);   // W(db)
+            if (q == (db_l >> 5)) {
+              y = a;
+              wdb = w;
             }
+          }
+          if (lane < m) {
+            const double dv = c_l - xfuu;
+            const double sb = wdb + dv * y;
+            const double wvv = uw + dv * ra;
+            Rw[b_l] = ra * sb - y * (wvv - c_l);
+          }
         }
         __syncwarp();
       }

@@ -39,7 +39,7 @@ __device__ __forceinline__ void warp_scratch_all(const SCtx& c, const int* idx, 
     for (int qp = wk; qp < d.n_qp && !sing_any; qp += c.par_ntile) {
       warp_gather_tile<KPL, NP, 8>(T, c.p.XF + (size_t)qp * N * N, idx, Np, N);
       bool sing;
-      const double det = warp_gj<KPL, NP>(T, Np, perm, sing);
+      const double det = warp_gj<KPL, NP, 4>(T, Np, perm, sing);
       if (sing) {
         sing_any = true;
         break;

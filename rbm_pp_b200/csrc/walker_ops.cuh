@@ -370,9 +370,9 @@ __device__ __forceinline__ void warp_gather_tile(double* T, const double* XFq, c
 // Warp-level Gauss-Jordan inverse with partial pivoting (the role of dgetrf/dgetri, matrix.f90:155-177) of
 // the n x n tile T with leading dimension n + 1 (n = NP when NP > 0, a compile-time size; otherwise n_rt).
 // Returns det(X) (0 and singular = true on a zero pivot).  Column b of X^{-1} is column perm[b] of T
-// afterwards.  The pivot column is held in registers (rows lane + 32 p) and broadcast by shuffles.  The
-// elimination runs over batches of B rows, loading every row of a batch before storing any, so a step
-// waits a shared-memory round trip per batch rather than per row.  Lanes past the last row or column load
+// afterwards.  The pivot search holds the pivot column in registers (rows lane + 32 p).  The elimination
+// runs over batches of B rows, loading every row of a batch (and its multiplier) before storing any, so a
+// step waits a shared-memory round trip per batch rather than per row.  Lanes past the last row or column load
 // from a clamped, in-tile index (and discard the value): the compiler may issue a guarded shared load
 // unconditionally, and a tile can end at the end of the block's shared memory.
 template <int KPL, int NP, int B = 8>
@@ -442,24 +442,25 @@ __device__ __forceinline__ double warp_gj(double* T, int n_rt, int* perm, bool& 
     det = (bi != k ? -det : det) * pivot;
     __syncwarp();
     // rows i != k: T(i,j) -= f_i r_j for j != k, with f_i = T(i,k) after the interchange
-    auto batch = [&](const int p, const int l0, const double fcp) {
-      double tv[B][KPL];
+    // The multiplier of row i is T(i, k) read back from the tile: a broadcast load, issued with the
+    // batch's other loads.  After the interchange row bi holds the old row k, so T(bi, k) = fkk.
+    auto batch = [&](const int p, const int l0) {
+      double tv[B][KPL], fv[B];
 #pragma unroll
       for (int ii = 0; ii < B; ii++) {
         const int i = 32 * p + l0 + ii, ic = i < n ? i : n - 1;
+        fv[ii] = T[ic * ld + k];
 #pragma unroll
         for (int q = 0; q < KPL; q++) tv[ii][q] = T[ic * ld + jc[q]];
       }
 #pragma unroll
       for (int ii = 0; ii < B; ii++) {
         const int i = 32 * p + l0 + ii;
-        double f = __shfl_sync(0xffffffffu, fcp, l0 + ii);
-        if (i == bi) f = fkk;
         if (i < n && i != k) {
 #pragma unroll
           for (int q = 0; q < KPL; q++) {
             const int j = lane + 32 * q;
-            if (j < n && j != k) T[i * ld + j] = tv[ii][q] - f * r[q];
+            if (j < n && j != k) T[i * ld + j] = tv[ii][q] - fv[ii] * r[q];
           }
         }
       }
@@ -470,10 +471,10 @@ __device__ __forceinline__ double warp_gj(double* T, int n_rt, int* perm, bool& 
       if constexpr (NP > 0) {
 #pragma unroll
         for (int l0 = 0; l0 < 32; l0 += B)
-          if (32 * p + l0 < n) batch(p, l0, fc[p]);
+          if (32 * p + l0 < n) batch(p, l0);
       } else {
 #pragma unroll 1
-        for (int l0 = 0; l0 < 32 && 32 * p + l0 < n; l0 += B) batch(p, l0, fc[p]);
+        for (int l0 = 0; l0 < 32 && 32 * p + l0 < n; l0 += B) batch(p, l0);
       }
     }
     __syncwarp();
