@@ -30,7 +30,7 @@ sys.path.insert(0, ROOT)
 METRIC = "MC samples/s and SR steps/s at 10x10 J2=0.5, chosen vs plain FP64, dE/site"
 # DRAM bytes (read + write) that ncu counted for one sampler_stream_kernel launch of the 1-wave 10x10
 # workload, divided by that launch's algorithmic bytes (profiles/sampler_stream_10x10_1wave.md)
-SAMPLER_TRAFFIC_PER_ALG_BYTE = 2.674e12 / 3.1765e12
+SAMPLER_TRAFFIC_PER_ALG_BYTE = (2.0798e12 + 0.6537e12) / 3.1765e12
 
 WORKLOADS = {
     # 10x10 at scale: translation-symmetric RBM (alpha=4, 100 projections), 4096 walkers, 65536 samples per step
