@@ -42,6 +42,8 @@ WORKLOADS = {
     "j1j2_10x10_single_16k": dict(L=10, translations=False, alphar=4, orbital="full", walkers=1024, ns=16, J2=0.5),
     # one wave of walkers (one per SM), one stored sample each: the profiling case of the 10x10 kernels
     "j1j2_10x10_trans_1wave": dict(L=10, translations=True, alphar=4, orbital="full", walkers=148, ns=1, J2=0.5),
+    # correlation measurement (the Calc_Correlation program) of 16384 samples on the 10x10 translation-symmetric state
+    "corr_10x10_trans": dict(L=10, translations=True, alphar=4, orbital="full", walkers=4096, ns=4, J2=0.5),
 }
 
 
@@ -235,6 +237,82 @@ def run_batch(args):
     return 0
 
 
+def corr_flops_per_sample(w):
+    """Algorithmic FP64 flops of one correlation-measured sample, per projection: the scratch inverse
+    (2 Np^3), one mat-vec W = Y v per up electron (2 Np^3) and two dot products of length Np per
+    up-down pair (4 Np^3)."""
+    np_ = w["L"] ** 2 // 2
+    n_qp = 2 * (w["L"] ** 2 if w["translations"] else 1)
+    return n_qp * 8.0 * np_ ** 3
+
+
+def run_corr(args):
+    """The correlation measurement of the Calc_Correlation program (Chi_sp for every site pair, Chi_vbs
+    per bond type, energy scalars) on the stored samples of one make_sample, through the C ABI."""
+    import torch
+    from rbm_pp_b200 import capi
+    torch.cuda.set_device(0)
+    w = WORKLOADS[args.workload]
+    problem = make_problem(w)
+    g = capi.Context(problem, n_walkers=w["walkers"], nsample_per_walker=w["ns"])
+    g.set_params(problem.br, problem.Wr, problem.slater, 0.0)
+    g.seed(2024)
+    g.make_sample(True)
+    launches0 = g.kernel_launches()
+    for _ in range(args.warmup):
+        g.measure_correlation()
+    clk = ClockSampler(0)
+    clk.start()
+    kern, wall = [], []
+    launches0 = g.kernel_launches()
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        m = g.measure_correlation()
+        wall.append(time.perf_counter() - t0)
+        kern.append(g.stats()["estimator_ms"])
+    clocks = clk.stop()
+    launches = g.kernel_launches() - launches0
+    n = w["walkers"] * w["ns"]
+    wall_s = float(np.mean(wall))
+    kern_ms = float(np.mean(kern))
+    flops = corr_flops_per_sample(w) * n
+    achieved = flops / (kern_ms * 1e-3) / 1e12
+    nchi = w["L"] ** 2 * (w["L"] ** 2 + 1) // 2
+    line = {"metric": "correlation-measured samples/s at 10x10 J2=0.5 (Chi_sp over all site pairs, Chi_vbs)",
+            "value": n / wall_s, "unit": "samples/s", "n_gpus": 1, "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": wall_s * 1e3, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64", "data": "synthetic (seeded, reference file shapes)",
+            "config": {"workload": args.workload, "L": w["L"], "walkers": w["walkers"], "samples_per_step": n,
+                       "alphar": w["alphar"], "n_qp": 2 * (w["L"] ** 2 if w["translations"] else 1),
+                       "l2": "per-sample rows larger than L2"},
+            "kernel_ms": kern_ms,
+            "roofline": {"kernel": "correlation_kernel", "bound": "fp64", "achieved": achieved, "peak": 40.0,
+                         "unit": "TFLOP/s", "frac": achieved / 40.0,
+                         "peak_kind": "nominal FP64 (no measured FP64 peak on this pool)", "traffic": None,
+                         "algorithmic_flops": flops},
+            "energy_per_site": m["Etot"] / m["norm"] / w["L"] ** 2, "clocks": clocks, "gpu_launches": launches,
+            "e2e": {"value": n / wall_s, "unit": "samples/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 8 * (5 + 6 * nchi)}}
+    if not args.no_cpu_baseline:
+        sys.path.insert(0, os.path.join(ROOT, "oracle"))
+        import pyoracle as po
+        cores = os.cpu_count() or 1
+        threads = min(cores, 64, po.max_threads() if po.max_threads() > 0 else cores)
+        o = po.Oracle(problem, nranks=threads, nsample_per_rank=1, nthreads=threads)
+        o.set_params(problem.br, problem.Wr, problem.slater, 0.0)
+        o.seed(777)
+        o.make_sample(True)
+        t0 = time.perf_counter()
+        o.measure_correlation()
+        dt = time.perf_counter() - t0
+        line["cpu_baseline"] = {"value": threads / dt, "unit": "samples/s", "cores": threads, "kind": "port",
+                                "sample": f"oracle correlation measurement of {threads} samples (one per thread) "
+                                          f"in {dt:.1f} s"}
+    print(json.dumps(line), flush=True)
+    g.close()
+    return 0
+
+
 def run_ours(args):
     import torch
     rank, world, local = _rank_env()
@@ -368,6 +446,8 @@ def main():
         return run_reference(args)
     if args.workload.startswith("batch_"):
         return run_batch(args)
+    if args.workload.startswith("corr_"):
+        return run_corr(args)
     return run_ours(args)
 
 

@@ -136,6 +136,15 @@ int rbmpp_set_samples(rbmpp_ctx* ctx, const int* x_sample);
 int rbmpp_measure(rbmpp_ctx* ctx, double* scal, double* gvec, double* Ovec, double* Smat);
 /* calc_phys_quantity_after_opt (calc_phys_quantity.f90:250-302): scal = {Etot, Etot2, norm, wf_av}. */
 int rbmpp_measure_energy(rbmpp_ctx* ctx, double* scal);
+/* calc_phys_quantity_after_opt of the Calc_Correlation program (Calc_Correlation/calc_phys_quantity.f90:264-344,
+ * with calc_local_energy_correlation :348-424 and calc_local_correlation :477-550) over all walkers, summed as
+ * the MPI_REDUCE calls of Calc_Correlation/main.f90:553-581 (before division by norm):
+ * scal = {Etot, Etot2, norm, wf_av, Re wf_sgn}; chi_sp = Chi_sp(2, Nchi) (SzSz, exchange part) and
+ * chi_vbs = Chi_vbs(Nchi, 4) (bond types (1,0), (0,1), (1,1), (1,-1)), column-major, Nchi = N (N + 1) / 2,
+ * pair i0 = i2 (i2 - 1) / 2 + i1 for 1 <= i1 <= i2 <= N.  Any pointer may be NULL.  Each walker's stream
+ * advances by one draw per sample, antiparallel bond and antiparallel site pair, as the reference's
+ * amplitude calls do (sub.f90:72). */
+int rbmpp_measure_correlation(rbmpp_ctx* ctx, double* scal, double* chi_sp, double* chi_vbs);
 
 /* Cross-GPU reduction of the measurement (the MPI_ALLREDUCE calls of main.f90:348-369).
  * direction 0: copy this context's sums into caller DEVICE buffers d_S (Nv*Nv), d_g, d_ov (Nv) and

@@ -64,6 +64,7 @@ def lib():
         L.orc_set_samples.argtypes = [P, ip]
         L.orc_measure.argtypes = [P, dp, dp, dp, P, P, P, C.c_int]
         L.orc_measure_energy.argtypes = [P, dp, C.c_int]
+        L.orc_measure_correlation.argtypes = [P, dp, dp, dp, C.c_int]
         L.orc_eval_configs.argtypes = [P, C.c_int, ip, P, P, P, P]
         L.orc_proposal_pf.argtypes = [P, ip, C.c_int, C.c_int, dp, dp]
         L.orc_sr_step.argtypes = [P, C.POINTER(SrIn), dp, C.c_double, dp, dp, C.POINTER(SrOut), P]
@@ -203,6 +204,16 @@ class Oracle:
         scal = np.zeros(4)
         self._chk(lib().orc_measure_energy(self.h, scal, self.nthreads))
         return dict(Etot=scal[0], Etot2=scal[1], norm=scal[2], wf_av=scal[3])
+
+    def measure_correlation(self):
+        """Calc_Correlation's calc_phys_quantity_after_opt: scalars, Chi_sp (2, Nchi), Chi_vbs (Nchi, 4)."""
+        nchi = self.N * (self.N + 1) // 2
+        scal = np.zeros(5)
+        sp = np.zeros(2 * nchi)
+        vb = np.zeros(4 * nchi)
+        self._chk(lib().orc_measure_correlation(self.h, scal, sp, vb, self.nthreads))
+        return dict(Etot=scal[0], Etot2=scal[1], norm=scal[2], wf_av=scal[3], wf_sgn=scal[4],
+                    chi_sp=sp.reshape((2, nchi), order="F"), chi_vbs=vb.reshape((nchi, 4), order="F"))
 
     def eval_configs(self, x, want_h=True, want_O=False):
         x = np.ascontiguousarray(x, dtype=np.int32)

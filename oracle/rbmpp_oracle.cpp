@@ -1228,6 +1228,149 @@ int orc_measure_energy(void* h, double* scal, int nthreads) {
   return 0;
 }
 
+// ------------------------------------------------------------------------------------------------
+// Correlation measurement of the Calc_Correlation program (Calc_Correlation/calc_phys_quantity.f90):
+// calc_local_energy_correlation :348-424 (local energy and SdotS per bond), calc_local_correlation
+// :477-550 (SzSz and exchange parts for every site pair i1 <= i2) and their accumulation in
+// calc_phys_quantity_after_opt :264-344.  Pair index i0 = i2 (i2 - 1) / 2 + i1 (1-based, i1 <= i2).
+// Every exchanged amplitude consumes one draw (sub.f90:72), in the reference's loop order.
+// ------------------------------------------------------------------------------------------------
+struct ExchangeBuf {
+  std::vector<double> thp, tpf, va, vb;
+  std::vector<int> tidx, tsgn;
+  std::vector<cplx> psip, psipw;
+  explicit ExchangeBuf(const Ctx& c)
+      : thp(c.Mr), tpf(c.n_qp), va(c.N), vb(c.N), tidx(c.N), tsgn(c.n_mp), psip(c.n_qp + 1), psipw(c.n_qp) {}
+};
+
+// psi(x') for the exchange of the antiparallel spins on sites i1, i2 (0-based), as in
+// calc_local_correlation :507-533.
+static cplx exchange_psi(const Ctx& c, const int* x, const double* th, const int* idx, const int* cfg,
+                         const int* sgn, const double* pf, const double* inv, MT& rng, int i1, int i2, ExchangeBuf& b) {
+  const int N = c.N;
+  for (int j = 0; j < c.Mr; j++) b.thp[j] = th[j];
+  update_theta(c, x, i1, i2, b.thp.data());
+  const int i3 = cfg[i1], i4 = cfg[i2];
+  for (int i = 0; i < N; i++) b.tidx[i] = idx[i];
+  b.tidx[i3] = i2;
+  b.tidx[i4] = i1;
+  for (int qp = 0; qp < c.n_qp; qp++)
+    b.tpf[qp] = new_pf_two_qp(c, qp, i3, i4, b.tidx.data(), &inv[(size_t)N * N * qp], pf[qp], b.va.data(), b.vb.data());
+  for (int mp = 0; mp < c.n_mp; mp++) {
+    int s = -sgn[mp];
+    if (c.subB[i1]) s = -s;
+    if (c.subB[i2]) s = -s;
+    b.tsgn[mp] = s;
+  }
+  amplitude(c, b.thp.data(), b.tpf.data(), b.tsgn.data(), b.psipw.data(), b.psip.data(), rng);
+  return b.psip[0];
+}
+
+// One stored sample: psi(0), Eloc_x (before reweighting), SdotS(N, 4) (before reweighting) and
+// Chi_loc_x(2, Nchi).
+static int corr_sample(const Ctx& c, const int* x, MT& rng, cplx& psi0, cplx& eloc, cplx* sdots, cplx* chi) {
+  const int N = c.N;
+  std::vector<double> th(c.Mr), pf(c.n_qp), inv((size_t)N * N * c.n_qp);
+  std::vector<int> idx(N), cfg(N), sgn(c.n_mp);
+  std::vector<cplx> psi(c.n_qp + 1), psiw(c.n_qp);
+  ExchangeBuf b(c);
+  calc_theta(c, x, th.data());
+  if (x_to_ele(c, x, idx.data(), cfg.data())) return ORC_E_CONFIG;
+  int e = calc_mall(c, idx.data(), pf.data(), inv.data(), true);
+  if (e) return e;
+  if (sign_pp(c, idx.data(), sgn.data())) return ORC_E_SIGN;
+  amplitude(c, th.data(), pf.data(), sgn.data(), psiw.data(), psi.data(), rng);
+  psi0 = psi[0];
+  // calc_local_energy_correlation :364-421
+  eloc = 0.0;
+  for (int k = 0; k < 4 * N; k++) sdots[k] = 0.0;
+  for (int i0 = 1; i0 <= 4; i0++) {
+    const double J = (i0 <= 2) ? c.J1 : c.J2, sg = (i0 <= 2) ? -1.0 : 1.0;
+    for (int i1 = 0; i1 < N; i1++) {
+      const int i2 = bond_map(c, i0, i1);
+      cplx& sd = sdots[i1 + (size_t)N * (i0 - 1)];
+      eloc = eloc + J * (double)x[i1] * (double)x[i2] * psi0;
+      sd = sd + (double)x[i1] * (double)x[i2] * psi0;
+      if (x[i1] != x[i2]) {
+        const cplx pp = exchange_psi(c, x, th.data(), idx.data(), cfg.data(), sgn.data(), pf.data(), inv.data(), rng,
+                                     i1, i2, b);
+        eloc = eloc + 2.0 * J * sg * pp;
+        sd = sd + 2.0 * sg * pp;
+      }
+    }
+  }
+  // calc_local_correlation :495-547
+  size_t i0 = 0;
+  for (int i2 = 0; i2 < N; i2++)
+    for (int i1 = 0; i1 <= i2; i1++, i0++) {
+      chi[2 * i0] = (double)x[i1] * (double)x[i2] * psi0;
+      chi[2 * i0 + 1] = (i1 == i2) ? psi0 : cplx(0.0);
+      if (x[i1] != x[i2]) {
+        const cplx pp = exchange_psi(c, x, th.data(), idx.data(), cfg.data(), sgn.data(), pf.data(), inv.data(), rng,
+                                     i1, i2, b);
+        double sgs = 1.0;
+        if (c.subB[i1]) sgs = -sgs;
+        if (c.subB[i2]) sgs = -sgs;
+        chi[2 * i0 + 1] = sgs * pp;
+      }
+    }
+  return 0;
+}
+
+// calc_phys_quantity_after_opt of the Calc_Correlation program (:264-344) over all ranks, summed in rank
+// order like the MPI_REDUCE calls of Calc_Correlation/main.f90:553-581 (before the division by norm):
+// scal = Etot, Etot2, norm, wf_av, Re wf_sgn; chi_sp = Chi_sp(2, Nchi); chi_vbs = Chi_vbs(Nchi, 4)
+// (Fortran column-major).
+int orc_measure_correlation(void* h, double* scal, double* chi_sp, double* chi_vbs, int nthreads) {
+  Ctx& c = *(Ctx*)h;
+  const int N = c.N;
+  const size_t nchi = (size_t)N * (N + 1) / 2;
+  std::vector<double> rs((size_t)c.nranks * 5, 0.0), rsp((size_t)c.nranks * 2 * nchi, 0.0),
+      rvb((size_t)c.nranks * 4 * nchi, 0.0);
+  std::vector<int> errs(c.nranks, 0);
+#pragma omp parallel for schedule(dynamic, 1) num_threads(nthreads > 0 ? nthreads : 1)
+  for (int r = 0; r < c.nranks; r++) {
+    std::vector<cplx> sd((size_t)4 * N), chi(2 * nchi);
+    double* S = &rs[(size_t)5 * r];
+    double* sp = &rsp[(size_t)2 * nchi * r];
+    double* vb = &rvb[(size_t)4 * nchi * r];
+    for (int s = 0; s < c.nsample; s++) {
+      cplx psi0, E;
+      int e = corr_sample(c, &c.ranks[r].x_sample[(size_t)N * s], c.ranks[r].rng, psi0, E, sd.data(), chi.data());
+      if (e) {
+        errs[r] = e;
+        break;
+      }
+      const double w = 1.0 / (std::abs(psi0) + c.shift);
+      E = E * w;
+      S[0] += w * std::real(std::conj(psi0) * E);
+      S[1] += std::real(std::conj(E) * E);
+      S[2] += (std::abs(psi0) * w) * (std::abs(psi0) * w);
+      S[3] += std::abs(psi0);
+      S[4] += std::real(psi0 / std::abs(psi0));
+      for (auto& v : sd) v = v * w;
+      for (int i3 = 0; i3 < 4; i3++) {
+        size_t i0 = 0;
+        for (int i2 = 0; i2 < N; i2++)
+          for (int i1 = 0; i1 <= i2; i1++, i0++)
+            vb[i0 + nchi * i3] += std::real(std::conj(sd[i1 + (size_t)N * i3]) * sd[i2 + (size_t)N * i3]);
+      }
+      for (size_t k = 0; k < 2 * nchi; k++) sp[k] += w * w * std::real(std::conj(psi0) * chi[k]);
+    }
+  }
+  for (int r = 0; r < c.nranks; r++)
+    if (errs[r]) return set_err(c, errs[r], "calc_phys_quantity_after_opt (correlation) failed");
+  for (int k = 0; k < 5; k++) scal[k] = 0.0;
+  for (size_t k = 0; k < 2 * nchi; k++) chi_sp[k] = 0.0;
+  for (size_t k = 0; k < 4 * nchi; k++) chi_vbs[k] = 0.0;
+  for (int r = 0; r < c.nranks; r++) {
+    for (int k = 0; k < 5; k++) scal[k] += rs[(size_t)5 * r + k];
+    for (size_t k = 0; k < 2 * nchi; k++) chi_sp[k] += rsp[(size_t)2 * nchi * r + k];
+    for (size_t k = 0; k < 4 * nchi; k++) chi_vbs[k] += rvb[(size_t)4 * nchi * r + k];
+  }
+  return 0;
+}
+
 // Per-configuration evaluation for tests: psi (N_QP+1 complex), raw H psi (complex), raw dpsi/dtheta
 // (Nv complex).  Uses a private RNG (the amplitude draws do not affect values).
 int orc_eval_configs(void* h, int n, const int* x, double* psi, double* hpsi, double* Oraw, double* pf) {

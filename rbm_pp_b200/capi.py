@@ -22,7 +22,7 @@ EXPORTS = ["rbmpp_create", "rbmpp_destroy", "rbmpp_last_error", "rbmpp_query", "
            "rbmpp_iteration", "rbmpp_eval_configs", "rbmpp_get_stats", "rbmpp_exchange_measurement",
            "rbmpp_set_shift", "rbmpp_get_walker_state", "rbmpp_eval_configs_noalloc",
            "rbmpp_set_s_precision", "rbmpp_batch_create", "rbmpp_batch_destroy", "rbmpp_batch_last_error",
-           "rbmpp_batch_tune", "rbmpp_batch_make_sample"]
+           "rbmpp_batch_tune", "rbmpp_batch_make_sample", "rbmpp_measure_correlation"]
 
 SR_FP64 = 0
 SR_SPLIT_BF16 = 1
@@ -79,6 +79,7 @@ def lib():
         L.rbmpp_set_samples.argtypes = [P, P]
         L.rbmpp_measure.argtypes = [P, P, P, P, P]
         L.rbmpp_measure_energy.argtypes = [P, P]
+        L.rbmpp_measure_correlation.argtypes = [P, P, P, P]
         L.rbmpp_sr_step.argtypes = [P, C.POINTER(SrIn), C.POINTER(SrOut), P]
         L.rbmpp_iteration.argtypes = [P, C.c_int, C.c_double, C.c_double, C.c_double, C.c_double, C.POINTER(SrOut)]
         L.rbmpp_eval_configs.argtypes = [P, C.c_int, P, P, P, P]
@@ -211,6 +212,16 @@ class Context:
         scal = np.zeros(4)
         self._chk(lib().rbmpp_measure_energy(self.h, _p(scal)))
         return dict(Etot=scal[0], Etot2=scal[1], norm=scal[2], wf_av=scal[3])
+
+    def measure_correlation(self):
+        """Calc_Correlation's calc_phys_quantity_after_opt: scalars, Chi_sp (2, Nchi), Chi_vbs (Nchi, 4)."""
+        nchi = self.N * (self.N + 1) // 2
+        scal = np.zeros(5)
+        sp = np.zeros(2 * nchi)
+        vb = np.zeros(4 * nchi)
+        self._chk(lib().rbmpp_measure_correlation(self.h, _p(scal), _p(sp), _p(vb)))
+        return dict(Etot=scal[0], Etot2=scal[1], norm=scal[2], wf_av=scal[3], wf_sgn=scal[4],
+                    chi_sp=sp.reshape((2, nchi), order="F"), chi_vbs=vb.reshape((nchi, 4), order="F"))
 
     def sr_step(self, iteration, delta_tau, s_factor0, s_cut, precision=SR_FP64, refine_steps=50):
         sin = SrIn(iteration, precision, refine_steps, 0, delta_tau, s_factor0, s_cut)

@@ -45,6 +45,11 @@ cudaError_t rbmpp_sample_scalars(int, const double*, int, const double*, double,
                                  cudaStream_t);
 void rbmpp_bf16x3_pads(int, int, int*, int*);
 int rbmpp_syrk_bf16x3(int, int, const double*, void*, void*, int*, double*, double*, cudaStream_t);
+int rbmpp_correlation_fits(const DevDims&, int);
+cudaError_t rbmpp_launch_correlation(const DevDims&, const DevTables&, const DevParams&, const int8_t*, int, double*,
+                                     double*, double*, double*, int*, int*, cudaStream_t);
+cudaError_t rbmpp_fill(double*, long long, double, cudaStream_t);
+cudaError_t rbmpp_gemm_atb_upper(int, int, const double*, long long, long long, double*, long long, cudaStream_t);
 
 static std::atomic<long long> g_launches{0};
 void rbmpp_note_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
@@ -127,6 +132,9 @@ struct rbmpp_ctx {
   double *d_tmp_ns = nullptr, *d_rv = nullptr;
   int *d_info = nullptr, *d_err = nullptr;
   double* d_Sb = nullptr;  // copy of the shifted split-precision S (preconditioner retries)
+  // correlation measurement: per-sample rows (2 Nchi + 1), w SdotS rows (4N), ones, Chi_vbs blocks, sums
+  double *d_crow = nullptr, *d_csd = nullptr, *d_cones = nullptr, *d_cvbs = nullptr, *d_cpart = nullptr,
+         *d_csum = nullptr;
   void *d_hi = nullptr, *d_lo = nullptr;
   int ldk = 0;
   float* d_Sf = nullptr;
@@ -461,7 +469,8 @@ int rbmpp_destroy(rbmpp_ctx* c) {
                   c->d_XF, c->d_XFT, c->W.x, c->W.idx, c->W.cfg, c->W.th, c->W.sgn, c->W.pf, c->W.psi, c->W.Y,
                   c->W.mt, c->W.nfastup, c->W.naccept, c->W.nacc_all, c->W.status, c->W.xs, c->W.pfs, c->W.psis, c->W.gj, c->d_O, c->d_psiS,
                   c->d_eloc, c->d_a, c->d_b, c->d_tmp_ns, c->d_acc4, c->d_nap, c->d_estat, c->d_gvec, c->d_Ovec,
-                  c->d_vec, c->d_S, c->d_part, c->d_info, c->d_err, c->d_rv, c->d_hi, c->d_lo, c->d_Sf, c->d_Sb};
+                  c->d_vec, c->d_S, c->d_part, c->d_info, c->d_err, c->d_rv, c->d_hi, c->d_lo, c->d_Sf, c->d_Sb,
+                  c->d_crow, c->d_csd, c->d_cones, c->d_cvbs, c->d_cpart, c->d_csum};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   for (auto& e : c->ev)
@@ -710,6 +719,81 @@ int rbmpp_measure_energy(rbmpp_ctx* c, double* scal) {
   int r = measure_common(c, false);
   if (r) return r;
   if (scal) std::memcpy(scal, c->meas_scal, sizeof(double) * 4);
+  return 0;
+}
+
+// Calc_Correlation/calc_phys_quantity.f90:264-344 over the stored samples.  The per-sample rows are summed
+// over samples by fixed partitions (rbmpp_gemv_ot with unit weights) and Chi_vbs(., t) = sum_s sdr sdr^T
+// by the FP64 upper-triangle GEMM, so the sums do not depend on scheduling.
+int rbmpp_measure_correlation(rbmpp_ctx* c, double* scal, double* chi_sp, double* chi_vbs) {
+  if (!c) return RBMPP_E_ARG;
+  if (!c->sampled) return fail(c, RBMPP_E_STATE, "measure before make_sample");
+  const DevDims& d = c->d;
+  int dev = 0, maxsm = 0;
+  CK(cudaGetDevice(&dev));
+  CK(cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev));
+  if (rbmpp_correlation_fits(d, maxsm) < 1)
+    return fail(c, RBMPP_E_ARG, "the correlation workspace for N/2 = %d exceeds the shared memory of one block", d.Np);
+  int r = ensure_measure_buffers(c);
+  if (r) return r;
+  const size_t nchi = (size_t)d.N * (d.N + 1) / 2, lr = 2 * nchi + 1;
+  const int nparts = 64;
+  if (!c->d_crow) {
+    if ((r = dalloc(c, &c->d_crow, (size_t)c->ns_tot * lr))) return r;
+    if ((r = dalloc(c, &c->d_csd, (size_t)c->ns_tot * 4 * d.N))) return r;
+    if ((r = dalloc(c, &c->d_cones, (size_t)c->ns_tot))) return r;
+    if ((r = dalloc(c, &c->d_cvbs, (size_t)4 * d.N * d.N))) return r;
+    if ((r = dalloc(c, &c->d_cpart, (size_t)nparts * lr))) return r;
+    if ((r = dalloc(c, &c->d_csum, lr))) return r;
+    CK(rbmpp_fill(c->d_cones, c->ns_tot, 1.0, c->st));
+  }
+  c->S_valid = false;
+  c->S_reduced = false;
+  c->d.shift = c->shift;
+  CK(cudaEventRecord(c->ev[2], c->st));
+  CK(rbmpp_launch_correlation(c->d, tables(c), params(c), c->W.xs, c->ns_tot, c->d_psiS, c->d_eloc, c->d_crow,
+                              c->d_csd, c->d_nap, c->d_estat, c->st));
+  CK(cudaEventRecord(c->ev[3], c->st));
+  CK(cudaStreamSynchronize(c->st));
+  {
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, c->ev[2], c->ev[3]));
+    c->stats[1] = ms;
+  }
+  r = check_walker_status(c, c->d_estat, c->ns_tot, "calc_phys_quantity_after_opt (correlation)");
+  if (r) return r;
+  CK(rbmpp_sample_scalars(c->ns_tot, c->d_psiS, (d.n_qp + 1) * 2, c->d_eloc, c->shift, c->d_a, c->d_b, c->d_acc4,
+                          c->st));
+  CK(rbmpp_gemv_ot(c->ns_tot, (int)lr, c->d_crow, c->d_cones, nullptr, c->d_csum, nullptr, c->d_cpart, nparts, c->st));
+  for (int t = 0; t < 4; t++)
+    CK(rbmpp_gemm_atb_upper(d.N, c->ns_tot, c->d_csd + (size_t)t * d.N, 4LL * d.N, 1, c->d_cvbs + (size_t)t * d.N * d.N,
+                            d.N, c->st));
+  // one amplitude draw per sample, per antiparallel bond and per antiparallel site pair (N/2 x N/2 of them)
+  CK(rbmpp_launch_advance_rng(c->W.mt, c->d_nap, d.ns, d.nw, d.ns * d.Np * d.Np, c->st));
+  std::vector<double> sums(lr), vbs((size_t)4 * d.N * d.N);
+  double s4[4];
+  CK(cudaMemcpyAsync(s4, c->d_acc4, sizeof(double) * 4, cudaMemcpyDeviceToHost, c->st));
+  CK(cudaMemcpyAsync(sums.data(), c->d_csum, sizeof(double) * lr, cudaMemcpyDeviceToHost, c->st));
+  CK(cudaMemcpyAsync(vbs.data(), c->d_cvbs, sizeof(double) * vbs.size(), cudaMemcpyDeviceToHost, c->st));
+  CK(cudaStreamSynchronize(c->st));
+  std::memcpy(c->meas_scal, s4, sizeof(s4));
+  c->n_samples_total = (double)d.nw * (double)d.ns;
+  if (scal) {
+    std::memcpy(scal, s4, sizeof(s4));
+    scal[4] = sums[2 * nchi];
+  }
+  if (chi_sp)
+    for (size_t i0 = 0; i0 < nchi; i0++) {
+      chi_sp[2 * i0] = sums[i0];
+      chi_sp[2 * i0 + 1] = sums[nchi + i0];
+    }
+  if (chi_vbs)
+    for (int t = 0; t < 4; t++) {
+      const double* C = vbs.data() + (size_t)t * d.N * d.N;  // column-major, upper triangle
+      size_t i0 = 0;
+      for (int i2 = 0; i2 < d.N; i2++)
+        for (int i1 = 0; i1 <= i2; i1++, i0++) chi_vbs[i0 + nchi * t] = C[i1 + (size_t)d.N * i2];
+    }
   return 0;
 }
 

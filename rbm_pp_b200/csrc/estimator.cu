@@ -98,30 +98,6 @@ __host__ __device__ __forceinline__ size_t est_layout(const DevDims& d, int nqw,
   return off;
 }
 
-// Sums NV values (a power of two, at most 32) over the warp together.  Each halving level trades half of
-// the values with the partner lane, so the NV sums take NV - 1 + 5 - log2(NV) shuffles instead of 5 NV.
-// Returns the warp total of value lane >> (5 - log2(NV)); v is overwritten.
-template <int NV>
-__device__ __forceinline__ double warp_transpose_sum(double (&v)[NV], int lane) {
-  constexpr int L2 = NV >= 32 ? 5 : NV >= 16 ? 4 : NV >= 8 ? 3 : NV >= 4 ? 2 : NV >= 2 ? 1 : 0;
-  static_assert((1 << L2) == NV && NV <= 32, "NV must be a power of two <= 32");
-#pragma unroll
-  for (int lev = 0; lev < L2; lev++) {
-    const int h = NV >> (lev + 1), o = 16 >> lev;
-    const bool hi = (lane & o) != 0;
-#pragma unroll
-    for (int i = 0; i < h; i++) {
-      const double keep = hi ? v[h + i] : v[i];
-      const double give = hi ? v[i] : v[h + i];
-      v[i] = keep + __shfl_xor_sync(0xffffffffu, give, o);
-    }
-  }
-  double r = v[0];
-#pragma unroll
-  for (int o = 16 >> L2; o > 0; o >>= 1) r += __shfl_xor_sync(0xffffffffu, r, o);
-  return r;
-}
-
 template <int KPL, int NP>
 __global__ void __launch_bounds__(kEstThreads, 1)
     estimator_kernel(const __grid_constant__ DevDims d, const __grid_constant__ DevTables t,

@@ -365,6 +365,15 @@ cudaError_t rbmpp_syrk_ot_o(int nv, int ns, const double* O, double* S, cudaStre
   return cudaGetLastError();
 }
 
+// C(i, j) = sum_k A(k, i) A(k, j) for i <= j (upper triangle, column-major C), A(k, i) = A[k sk + i si]
+cudaError_t rbmpp_gemm_atb_upper(int n, int K, const double* A, long long sk, long long si, double* C, long long ldc,
+                                 cudaStream_t st) {
+  int nt = (n + BM - 1) / BM;
+  rbmpp_note_launch();
+  gemm_atb_upper<false><<<nt * (nt + 1) / 2, 256, 0, st>>>(n, K, A, sk, si, 1.0, 0.0, C, ldc, 0);
+  return cudaGetLastError();
+}
+
 cudaError_t rbmpp_symmetrize(int n, double* S, cudaStream_t st) {
   dim3 g((n + 31) / 32, (n + 31) / 32);
   rbmpp_note_launch();
