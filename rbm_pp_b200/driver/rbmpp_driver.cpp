@@ -14,8 +14,13 @@
 // MPI ranks are the library's walkers: --walkers W emulates Nmpi = W ranks on one GPU, each with
 // Nsample/Nmpi stored samples and the seeding rule of main.f90:224-235.
 //
+// With --correlation the final measurement follows the Calc_Correlation program instead
+// (Calc_Correlation/main.f90:498-600): shift = 0 for a first make_sample, shift = 1e-5 times the mean |psi|
+// of its samples, 7 more make_samples, then Nav rounds of make_sample + rbmpp_measure_correlation, each
+// writing Chi_sp / norm to fort.<60000+it> and Chi_vbs / norm to fort.<70000+it> in the reference's formats.
+//
 // Usage: rbmpp_driver [--dir D] [--walkers W] [--seed S] [--precision fp64|split] [--device G]
-//                     [--nstep N] [--check-inputs]
+//                     [--nstep N] [--correlation] [--check-inputs]
 // --check-inputs parses and validates the inputs, prints a summary and exits without touching a GPU.
 #include <chrono>
 #include <cmath>
@@ -244,7 +249,7 @@ int main(int argc, char** argv) {
   std::string dir = ".", prec = "fp64";
   int walkers = 1, device = 0, nstep_override = -1;
   long long seed = -1;
-  bool check_only = false;
+  bool check_only = false, correlation = false;
   for (int i = 1; i < argc; i++) {
     std::string a = argv[i];
     auto next = [&]() -> std::string {
@@ -258,6 +263,7 @@ int main(int argc, char** argv) {
     else if (a == "--device") device = std::atoi(next().c_str());
     else if (a == "--nstep") nstep_override = std::atoi(next().c_str());
     else if (a == "--check-inputs") check_only = true;
+    else if (a == "--correlation") correlation = true;
     else die("unknown argument " + a);
   }
   Inputs in;
@@ -363,16 +369,54 @@ int main(int argc, char** argv) {
   write_zqp(dir + "/zqp_orbital_opt.dat", sl_av);
 
   // final energy (:486-575): warm up, then Nav measurements
-  lib.ck(rbmpp_make_sample(lib.c, 1, nullptr, nullptr), "make_sample");
-  for (int it = 0; it < 2; it++) lib.ck(rbmpp_make_sample(lib.c, 0, nullptr, nullptr), "make_sample");
+  const size_t nchi = (size_t)N * (N + 1) / 2;
+  std::vector<double> chi_sp, chi_vbs;
+  if (correlation) {  // Calc_Correlation/main.f90:498-527
+    chi_sp.resize(2 * nchi);
+    chi_vbs.resize(4 * nchi);
+    lib.ck(rbmpp_set_shift(lib.c, 0.0), "set_shift");
+    lib.ck(rbmpp_make_sample(lib.c, 1, nullptr, nullptr), "make_sample");
+    std::vector<double> psi((size_t)2 * (in.n_mp * 2 + 1) * ns * walkers);
+    lib.ck(rbmpp_get_samples(lib.c, nullptr, psi.data(), nullptr), "get_samples");
+    double wf = 0.0;
+    for (long long k = 0; k < (long long)ns * walkers; k++) {
+      const double* q = psi.data() + (size_t)2 * (in.n_mp * 2 + 1) * k;
+      wf += std::hypot(q[0], q[1]);
+    }
+    wf /= (double)ns * walkers;
+    lib.ck(rbmpp_set_shift(lib.c, wf * 1e-5), "set_shift");
+    std::printf("wf_av, shift =%15.5E%15.5E\n", wf, wf * 1e-5);
+    for (int it = 0; it < 7; it++) lib.ck(rbmpp_make_sample(lib.c, 0, nullptr, nullptr), "make_sample");
+  } else {
+    lib.ck(rbmpp_make_sample(lib.c, 1, nullptr, nullptr), "make_sample");
+    for (int it = 0; it < 2; it++) lib.ck(rbmpp_make_sample(lib.c, 0, nullptr, nullptr), "make_sample");
+  }
   FILE* fa = std::fopen((dir + "/energy_after_opt.txt").c_str(), "w");
   if (!fa) die("cannot write energy_after_opt.txt");
   std::vector<double> e1, e2;
   for (int it = 1; it <= in.Nav; it++) {
     long long nacc = 0;
     lib.ck(rbmpp_make_sample(lib.c, 0, nullptr, &nacc), "make_sample");
-    double sc[4];
-    lib.ck(rbmpp_measure_energy(lib.c, sc), "measure_energy");
+    double sc[5];
+    if (correlation) {
+      lib.ck(rbmpp_measure_correlation(lib.c, sc, chi_sp.data(), chi_vbs.data()), "measure_correlation");
+      // Calc_Correlation/main.f90:572-581 (divided by norm) and :596-607 (unit 60000+it, 70000+it)
+      FILE* f6 = std::fopen((dir + "/fort." + std::to_string(60000 + it)).c_str(), "w");
+      FILE* f7 = std::fopen((dir + "/fort." + std::to_string(70000 + it)).c_str(), "w");
+      if (!f6 || !f7) die("cannot write the correlation files");
+      std::fprintf(f6, "# chi index,  SzSz,  SpSm\n");
+      for (size_t i = 0; i < nchi; i++)
+        std::fprintf(f6, "%6zu%25.15f%25.15f\n", i + 1, chi_sp[2 * i] / sc[2], chi_sp[2 * i + 1] / sc[2]);
+      std::fprintf(f7, "# chi index, <SSSS> for (1,0), (0,1), (1,1), (1,-1)\n");
+      for (size_t i = 0; i < nchi; i++)
+        std::fprintf(f7, "%6zu%25.15f%25.15f%25.15f%25.15f\n", i + 1, chi_vbs[i] / sc[2], chi_vbs[i + nchi] / sc[2],
+                     chi_vbs[i + 2 * nchi] / sc[2], chi_vbs[i + 3 * nchi] / sc[2]);
+      std::fclose(f6);
+      std::fclose(f7);
+      std::printf("   wf_sgn               :%20.10f\n", sc[4] / ((double)ns * walkers));
+    } else {
+      lib.ck(rbmpp_measure_energy(lib.c, sc), "measure_energy");
+    }
     const double E = sc[0] / sc[2], E2 = sc[1] / sc[2];
     const double acc = (double)nacc / ((double)ns * walkers) / (double)N;
     std::printf("Iteration (Energy Measuement) :%6d\n   total energy         :%20.10f\n"

@@ -84,3 +84,39 @@ def test_driver_run_matches_oracle(tmp_path):
         m = o.measure_energy()
         E = m["Etot"] / m["norm"]
         assert abs(fin[it, 1] - E) <= 1e-8 * abs(E), (it, fin[it, 1], E)
+
+
+@pytest.mark.gpu
+def test_driver_correlation_files(tmp_path):
+    """--correlation: Calc_Correlation's final measurement writes fort.<60000+it> (Chi_sp / norm) and
+    fort.<70000+it> (Chi_vbs / norm).  Each round obeys Chi_sp(1, ii) = Chi_sp(2, ii) = 1 and the bond sum
+    rule E = sum_b J_b (Chi_sp(1, b) + 2 Chi_sp(2, b)) against its own line of energy_after_opt.txt."""
+    L, nw, ns, nav = 4, 8, 4, 2
+    p = fm.synthetic_problem(L, translations=False, alphar=1, nsample=nw * ns, seed=19, Nstep=2, Nav=nav, J2=0.5)
+    fm.write_problem(str(tmp_path), p)
+    out = subprocess.run([_driver(), "--dir", str(tmp_path), "--walkers", str(nw), "--seed", "99", "--correlation"],
+                         capture_output=True, text=True, timeout=600)
+    assert out.returncode == 0, out.stderr + out.stdout
+    fin = np.loadtxt(os.path.join(tmp_path, "energy_after_opt.txt"))
+    N = L * L
+    nchi = N * (N + 1) // 2
+
+    def pair(a, b):
+        a, b = min(a, b), max(a, b)
+        return b * (b + 1) // 2 + a
+
+    bonds = []
+    for t in range(4):
+        for i1 in range(N):
+            ix, iy = divmod(i1, L)
+            dx, dy = ((1, 0), (0, 1), (1, 1), (1, -1))[t]
+            bonds.append((t, i1, ((ix + dx) % L) * L + (iy + dy) % L))
+    J = (p.inp.J1, p.inp.J1, p.inp.J2, p.inp.J2)
+    for it in range(1, nav + 1):
+        sp = np.loadtxt(os.path.join(tmp_path, f"fort.{60000 + it}"), comments="#")
+        vb = np.loadtxt(os.path.join(tmp_path, f"fort.{70000 + it}"), comments="#")
+        assert sp.shape == (nchi, 3) and vb.shape == (nchi, 5)
+        diag = [pair(i, i) for i in range(N)]
+        assert np.allclose(sp[diag, 1], 1.0, rtol=1e-12) and np.allclose(sp[diag, 2], 1.0, rtol=1e-12)
+        e = sum(J[t] * (sp[pair(a, b), 1] + 2.0 * sp[pair(a, b), 2]) for t, a, b in bonds)
+        assert abs(e - fin[it - 1, 1]) <= 1e-9 * abs(fin[it - 1, 1]), (it, e, fin[it - 1, 1])
