@@ -7,10 +7,10 @@
 // first (one warp-level Gauss-Jordan per projection, as in the estimator).  Then warp w takes the up
 // electrons ua = w, w + 8, ... over every projection of the round: one mat-vec W = Y v_ua per (ua, qp), and
 // for each chunk of eight down electrons their rows u are gathered together, the sixteen dot products
-// u.Y(:,ua) and u.W are reduced in one transposed butterfly, and lane t finishes pair (ua, db_t): the
-// block-form ratio, the cosh product of the exchanged spins' theta', the projection weight.  psi(x') of
-// pair (ua, db) accumulates in shared memory, written only by the warp that owns ua, in projection order,
-// so the sums are deterministic.
+// u.Y(:,ua) and u.W are reduced in one transposed butterfly, and lane t forms the block-form ratio of
+// pair (ua, db_t).  Then one lane per pair applies the cosh product of the exchanged spins' theta' and the
+// projection weight.  psi(x') of pair (ua, db) accumulates in shared memory, written only by the warp that
+// owns ua, in projection order, so the sums are deterministic.
 //
 // Per sample the CTA then writes, for a deterministic reduction over samples afterwards:
 //   row[i0]            = w^2 psi(0) x_i1 x_i2 psi(0)                 (Chi_sp(1, i0) term)
@@ -32,6 +32,7 @@ struct Cor {
   double* psx;    // [Np][Np] psi(x') of the exchange of up electron ua and down electron db
   int* perm;      // [kCorWarps][Np] column map of each projection's inverse
   double* vp;     // [kCorWarps][Np] v_ua at the tile's column positions
+  double* rb;     // [kCorWarps][Np] ratios of one up electron's pairs, one projection
   double* bsum;   // [4N] J_t SdotS of every bond (unweighted), summed in bond order by thread 0
   double* tiles;  // [nqw][Np*(Np+1)]
   int nqw;
@@ -72,6 +73,7 @@ __host__ __device__ __forceinline__ size_t cor_layout(const DevDims& d, int nqw,
   x.psx = (double*)take((size_t)Np * Np * 8);
   x.perm = (int*)take((size_t)kCorWarps * Np * 4);
   x.vp = (double*)take((size_t)kCorWarps * Np * 8);
+  x.rb = (double*)take((size_t)kCorWarps * Np * 8);
   x.bsum = (double*)take((size_t)4 * N * 8);
   const size_t tile = (size_t)Np * (Np + 1) * 8;
   size_t tiles_bytes = (size_t)nqw * tile;
@@ -138,6 +140,7 @@ __global__ void __launch_bounds__(kCorThreads, 1)
     dsite[q] = s.idx[Np + jc[q]];
   }
   double* vp = e.vp + (size_t)warp * Np;
+  double* rb = e.rb + (size_t)warp * Np;
   for (int q0 = 0; q0 < d.n_qp; q0 += e.nqw) {
     // inversions of this round's projections, one warp each
     if (warp < e.nqw && q0 + warp < d.n_qp) {
@@ -256,23 +259,28 @@ __global__ void __launch_bounds__(kCorThreads, 1)
             const double dv = c_l - xfuu;
             const double sb = wdb + dv * y;
             const double wvv = uw + dv * ra;
-            const double R = ra * sb - y * (wvv - c_l);
-            // theta' of the exchange on sites (min, max) (update_theta, RBM.f90:95-148), this projection
-            const int i1 = s_up < sdn_l ? s_up : sdn_l, i2 = s_up < sdn_l ? sdn_l : s_up;
-            const int iw1 = s_up < sdn_l ? iwu : wm[sdn_l], iw2 = s_up < sdn_l ? wm[sdn_l] : iwu;
-            const double x1 = s_up < sdn_l ? x_up : -x_up, x2 = -x1;
-            double ch = 1.0;
-            for (int f = 0; f < d.alphar; f++) {
-              double th = s.th[qp * d.alphar + f];
-              th = th - 2.0 * p.Wr[(size_t)f * N + iw1] * x1 * s_sign;
-              th = th - 2.0 * p.Wr[(size_t)f * N + iw2] * x2 * s_sign;
-              ch = ch * cosh(th);
-            }
-            const int sg = -s.sgn[mp] * (t.subB[i1] ? -1 : 1) * (t.subB[i2] ? -1 : 1);
-            const cplx cbw = psi_wo_pf(d, t, ch, sg, qp);
-            double& acc = e.psx[(size_t)ua * Np + db_l];
-            acc = acc + cbw.re * (R * pfq);
+            rb[db_l] = ra * sb - y * (wvv - c_l);
           }
+        }
+        __syncwarp();
+        // weights of the exchanged configurations, one pair per lane: the cosh product of theta' on the
+        // sites (min, max) (update_theta, RBM.f90:95-148) for this projection, the sign and projection factor
+        for (int db = lane; db < Np; db += 32) {
+          const int sdn = s.idx[Np + db];
+          const int i1 = s_up < sdn ? s_up : sdn, i2 = s_up < sdn ? sdn : s_up;
+          const int iw1 = s_up < sdn ? iwu : wm[sdn], iw2 = s_up < sdn ? wm[sdn] : iwu;
+          const double x1 = s_up < sdn ? x_up : -x_up, x2 = -x1;
+          double ch = 1.0;
+          for (int f = 0; f < d.alphar; f++) {
+            double th = s.th[qp * d.alphar + f];
+            th = th - 2.0 * p.Wr[(size_t)f * N + iw1] * x1 * s_sign;
+            th = th - 2.0 * p.Wr[(size_t)f * N + iw2] * x2 * s_sign;
+            ch = ch * cosh(th);
+          }
+          const int sg = -s.sgn[mp] * (t.subB[i1] ? -1 : 1) * (t.subB[i2] ? -1 : 1);
+          const cplx cbw = psi_wo_pf(d, t, ch, sg, qp);
+          double& acc = e.psx[(size_t)ua * Np + db];
+          acc = acc + cbw.re * (rb[db] * pfq);
         }
         __syncwarp();  // vp is rewritten for the next projection
       }
