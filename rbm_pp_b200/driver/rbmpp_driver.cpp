@@ -219,11 +219,60 @@ void write_W(const std::string& path, int N, int alphar, const std::vector<doubl
   std::fclose(f);
 }
 
+// Fortran edit descriptor Ew.d: a sign, "0.", d significant digits, then E+xx (or +xxx without the E for
+// exponents beyond 99), right-justified in w columns.
+std::string fort_e(double v, int w, int d) {
+  char m[64];
+  std::snprintf(m, sizeof(m), "%.*E", d - 1, v);  // [-]D.DDDE[+-]XX with d significant digits
+  std::string s(m);
+  const bool neg = s[0] == '-';
+  if (neg) s = s.substr(1);
+  const size_t ep = s.find('E');
+  std::string digits = s.substr(0, 1) + s.substr(2, ep - 2);
+  int e = std::atoi(s.c_str() + ep + 1);
+  if (v != 0.0) e += 1;
+  char ex[16];
+  if (std::abs(e) <= 99)
+    std::snprintf(ex, sizeof(ex), "E%c%02d", e < 0 ? '-' : '+', std::abs(e));
+  else
+    std::snprintf(ex, sizeof(ex), "%c%03d", e < 0 ? '-' : '+', std::abs(e));
+  std::string out = std::string(neg ? "-" : "") + "0." + digits + ex;
+  if ((int)out.size() < w) out = std::string(w - out.size(), ' ') + out;
+  return out;
+}
+
 void write_zqp(const std::string& path, const std::vector<double>& sl) {  // parameter.f90:266-275
   FILE* f = std::fopen(path.c_str(), "w");
   if (!f) die("cannot write " + path);
   std::fprintf(f, "\n Slater%10d\n\n\n\n", (int)sl.size());
-  for (size_t k = 0; k < sl.size(); k++) std::fprintf(f, "%5d%25.15E%25.15E\n", (int)k, sl[k], 0.0);
+  for (size_t k = 0; k < sl.size(); k++)
+    std::fprintf(f, "%5d%s%s\n", (int)k, fort_e(sl[k], 25, 15).c_str(), fort_e(0.0, 25, 15).c_str());
+  std::fclose(f);
+}
+
+// The input echoes of write_initial_parameters (parameter.f90:177-207): chk_orbitalidx.def,
+// chk_qptransidx.def (MP_Trans_Idx = W_map, parameter.f90:107) and chk_zqp_orbital_opt.dat.
+// The list-directed integers are written in a 12-column field.
+void write_input_checks(const std::string& dir, const Inputs& in) {
+  const int N = in.N;
+  FILE* f = std::fopen((dir + "/chk_orbitalidx.def").c_str(), "w");
+  if (!f) die("cannot write chk_orbitalidx.def");
+  std::fprintf(f, "%12d\n", in.n_slater);
+  for (int i1 = 0; i1 < N; i1++)
+    for (int i2 = 0; i2 < N; i2++)
+      std::fprintf(f, "%5d%7d%7d\n", i1, i2, in.orbital_idx[i1 + (size_t)N * i2] - 1);
+  std::fclose(f);
+  f = std::fopen((dir + "/chk_qptransidx.def").c_str(), "w");
+  if (!f) die("cannot write chk_qptransidx.def");
+  std::fprintf(f, "%12d\n", in.n_mp);
+  for (int mp = 0; mp < in.n_mp; mp++) std::fprintf(f, "%3d%20.12f%20.12f\n", mp + 1, in.para[2 * mp], in.para[2 * mp + 1]);
+  for (int mp = 0; mp < in.n_mp; mp++)
+    for (int i = 0; i < N; i++) std::fprintf(f, "%5d%7d%7d\n", mp + 1, i + 1, in.W_map[i + (size_t)N * mp]);
+  std::fclose(f);
+  f = std::fopen((dir + "/chk_zqp_orbital_opt.dat").c_str(), "w");
+  if (!f) die("cannot write chk_zqp_orbital_opt.dat");
+  std::fprintf(f, "# N_Slater%10d\n", in.n_slater);
+  for (int k = 0; k < in.n_slater; k++) std::fprintf(f, "%4d%s\n", k, fort_e(in.slater[k], 25, 15).c_str());
   std::fclose(f);
 }
 
@@ -284,6 +333,7 @@ int main(int argc, char** argv) {
                 "mean|f| %.15f W_map(1,last) %d orbital_idx(N,N) %d\n",
                 in.L, N, in.Nsample, walkers, ns, in.alphar, in.Nstep, in.Nav, in.n_mp, in.n_slater, in.have_W ? 1 : 0,
                 fabs_av, in.W_map[(size_t)N * (in.n_mp - 1)], in.orbital_idx[(size_t)N * N - 1]);
+    write_input_checks(dir, in);
     return 0;
   }
   const int precision = prec == "split" ? RBMPP_SR_SPLIT_BF16 : RBMPP_SR_FP64;
@@ -326,7 +376,10 @@ int main(int argc, char** argv) {
     br = in.br;
     Wr = in.Wr;
   }
+  // write_initial_parameters (parameter.f90:148-234); rank 4's sub_initial_W.txt is the same content
   write_W(dir + "/initial_W.txt", N, in.alphar, br, Wr);
+  write_W(dir + "/sub_initial_W.txt", N, in.alphar, br, Wr);
+  write_input_checks(dir, in);
   std::vector<double> sl = in.slater;
   lib.ck(rbmpp_set_params(lib.c, Wr.data(), br.data(), nullptr, nullptr, sl.data(), 0.0), "set_params");
 
@@ -367,6 +420,8 @@ int main(int argc, char** argv) {
   lib.ck(rbmpp_set_params(lib.c, Wr_av.data(), br_av.data(), nullptr, nullptr, sl_av.data(), shift_av), "set_params");
   write_W(dir + "/optimized_W.txt", N, in.alphar, br_av, Wr_av);
   write_zqp(dir + "/zqp_orbital_opt.dat", sl_av);
+  write_W(dir + "/sub_optimized_W.txt", N, in.alphar, br_av, Wr_av);  // rank 3's copies (parameter.f90:280-311)
+  write_zqp(dir + "/sub_zqp_orbital_opt.dat", sl_av);
 
   // final energy (:486-575): warm up, then Nav measurements
   const size_t nchi = (size_t)N * (N + 1) / 2;

@@ -120,3 +120,34 @@ def test_driver_correlation_files(tmp_path):
         assert np.allclose(sp[diag, 1], 1.0, rtol=1e-12) and np.allclose(sp[diag, 2], 1.0, rtol=1e-12)
         e = sum(J[t] * (sp[pair(a, b), 1] + 2.0 * sp[pair(a, b), 2]) for t, a, b in bonds)
         assert abs(e - fin[it - 1, 1]) <= 1e-9 * abs(fin[it - 1, 1]), (it, e, fin[it - 1, 1])
+
+
+def test_driver_writes_input_checks(tmp_path):
+    """chk_orbitalidx.def, chk_qptransidx.def and chk_zqp_orbital_opt.dat (parameter.f90:177-207) echo the
+    inputs the driver read, in the reference's record layout and Fortran E format."""
+    p = fm.synthetic_problem(4, translations=True, alphar=1, nsample=16, seed=8)
+    fm.write_problem(str(tmp_path), p)
+    out = subprocess.run([_driver(), "--dir", str(tmp_path), "--walkers", "2", "--check-inputs"],
+                         capture_output=True, text=True, timeout=60)
+    assert out.returncode == 0, out.stderr
+    q = fm.read_problem(str(tmp_path))
+    N = 16
+    lines = open(os.path.join(tmp_path, "chk_orbitalidx.def")).read().splitlines()
+    assert int(lines[0]) == q.n_slater
+    rows = np.array([[int(v) for v in ln.split()] for ln in lines[1:]])
+    assert rows.shape == (N * N, 3)
+    assert np.array_equal(rows[:, 2].reshape(N, N), q.orbital_idx - 1)  # i1 outer, i2 inner
+    lines = open(os.path.join(tmp_path, "chk_qptransidx.def")).read().splitlines()
+    n_mp = int(lines[0])
+    assert n_mp == q.sym.n_mp
+    para = np.array([[float(v) for v in ln.split()[1:]] for ln in lines[1:1 + n_mp]])
+    assert np.allclose(para[:, 0] + 1j * para[:, 1], q.sym.para_mp, atol=1e-12)
+    idx = np.array([[int(v) for v in ln.split()] for ln in lines[1 + n_mp:]])
+    assert np.array_equal(idx[:, 2].reshape(n_mp, N).T, q.sym.W_map)
+    lines = open(os.path.join(tmp_path, "chk_zqp_orbital_opt.dat")).read().splitlines()
+    assert lines[0].split()[-1] == str(q.n_slater)
+    vals = [ln[4:].strip() for ln in lines[1:]]
+    assert all(v.lstrip("-").startswith("0.") and "E" in v for v in vals)
+    f = np.array([float(v) for v in vals])
+    assert np.allclose(f, q.slater, rtol=1e-14, atol=0)
+    assert abs(np.abs(f).mean() - 0.25) < 1e-12
