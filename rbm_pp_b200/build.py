@@ -16,11 +16,11 @@ FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std
 
 
 def _stale() -> bool:
-    if not os.path.exists(LIB) or not os.path.exists(os.path.join(HERE, "rbmpp_driver")):
+    if not os.path.exists(LIB) or not os.path.exists(DRIVER) or not os.path.exists(POST):
         return True
-    t = min(os.path.getmtime(LIB), os.path.getmtime(os.path.join(HERE, "rbmpp_driver")))
+    t = min(os.path.getmtime(LIB), os.path.getmtime(DRIVER), os.path.getmtime(POST))
     deps = [os.path.join(CSRC, f) for f in os.listdir(CSRC)] + [os.path.join(HERE, "..", "include", "rbmpp.h"),
-                                                                os.path.join(HERE, "driver", "rbmpp_driver.cpp")]
+                                                                DRIVER_SRC, POST_SRC]
     return any(os.path.getmtime(p) > t for p in deps if os.path.exists(p))
 
 
@@ -50,6 +50,8 @@ def build(force: bool = False, verbose: bool = False, extra: list[str] | None = 
 
 DRIVER_SRC = os.path.join(HERE, "driver", "rbmpp_driver.cpp")
 DRIVER = os.path.join(HERE, "rbmpp_driver")
+POST_SRC = os.path.join(HERE, "driver", "rbmpp_post_process.cpp")
+POST = os.path.join(HERE, "rbmpp_post_process")
 
 
 def build_driver(verbose: bool = False) -> str:
@@ -59,7 +61,17 @@ def build_driver(verbose: bool = False) -> str:
     if verbose:
         print(" ".join(cmd), flush=True)
     subprocess.check_call(cmd)
+    build_post_process(verbose)
     return DRIVER
+
+
+def build_post_process(verbose: bool = False) -> str:
+    """The host-only C++ correlation post-processing program (no GPU, no library)."""
+    cmd = ["g++", "-O2", "-std=c++17", "-Wall", POST_SRC, "-o", POST]
+    if verbose:
+        print(" ".join(cmd), flush=True)
+    subprocess.check_call(cmd)
+    return POST
 
 
 if __name__ == "__main__":
