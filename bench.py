@@ -29,8 +29,11 @@ sys.path.insert(0, ROOT)
 
 METRIC = "MC samples/s and SR steps/s at 10x10 J2=0.5, chosen vs plain FP64, dE/site"
 # DRAM bytes (read + write) that ncu counted for one sampler_stream_kernel launch of the 1-wave 10x10
-# workload, divided by that launch's algorithmic bytes (profiles/sampler_stream_10x10_1wave.md)
+# workload (one walker per SM, one stored sample), divided by that launch's algorithmic bytes
 SAMPLER_TRAFFIC_PER_ALG_BYTE = (2.0798e12 + 0.6537e12) / 3.1765e12
+# wall-clock budget of one bench process: the plain all-FP64 twin trajectory gets as many of the K steps as fit
+PAIR_BUDGET_S = 1450.0
+T_START = time.perf_counter()
 
 WORKLOADS = {
     # 10x10 at scale: translation-symmetric RBM (alpha=4, 100 projections), 4096 walkers, 65536 samples per step
@@ -118,55 +121,60 @@ def measured_peaks():
 
 
 def cpu_baseline(w, problem, max_threads=None):
-    """The oracle (a line-by-line CPU restatement of the reference's make_sample and
-    calc_phys_quantity_opt) on the host cores: one walker per thread, Nsample = 1 per walker
-    (30 warm-up + 2 sweeps, then one measured sample), scaled to the workload's MC samples/s."""
+    """The oracle (a line-by-line CPU restatement of the reference's make_sample and calc_phys_quantity_opt)
+    on the host cores, one walker per thread, each walker a complete make_sample of the workload (warm-up plus
+    every stored sweep) and the measurement of all its samples.  The rate (stored samples per second) needs no
+    extrapolation; only the time of a whole step is scaled by the walker count."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import pyoracle as po
     cores = os.cpu_count() or 1
     threads = min(cores, max_threads or 64, po.max_threads() if po.max_threads() > 0 else cores)
-    o = po.Oracle(problem, nranks=threads, nsample_per_rank=1, nthreads=threads)
+    walkers, ns = w["walkers"], w["ns"]
+    o = po.Oracle(problem, nranks=threads, nsample_per_rank=ns, nthreads=threads)
     o.set_params(problem.br, problem.Wr, problem.slater, 0.0)
     o.seed(777)
     t0 = time.perf_counter()
     o.make_sample(True)
     t1 = time.perf_counter()
-    o.measure(want_S=False)
+    m = o.measure(want_S=False)
     t2 = time.perf_counter()
-    sweeps = 30 + 1 + 1
-    t_sweep = (t1 - t0) / sweeps  # per walker (walkers run in parallel, one per thread)
-    t_sample = (t2 - t1) / 1.0
-    walkers, ns = w["walkers"], w["ns"]
-    t_walker = (max(30, ns // 100) + ns + 1) * t_sweep + ns * t_sample
-    t_step = t_walker * walkers / threads
-    return {"value": walkers * ns / t_step, "unit": "MC samples/s", "cores": threads, "kind": "port",
-            "sample": (f"oracle make_sample+measure, {threads} walkers x 1 stored sample (32 sweeps each) on "
-                       f"{threads} threads in {t2 - t0:.1f} s; scaled to {walkers} walkers x {ns} samples "
-                       f"(sweep {t_sweep:.3f} s, measured sample {t_sample:.3f} s per walker)"),
-           "sr_steps_per_s_est_without_S": 1.0 / t_step}
+    t_sample = t2 - t0
+    return {"value": threads * ns / t_sample, "unit": "MC samples/s", "cores": threads, "kind": "port",
+            "sample": (f"oracle make_sample ({max(30, ns // 100)} + {ns} sweeps) and measure of {threads} walkers x "
+                       f"{ns} stored samples, one walker per thread, in {t_sample:.1f} s (sampling {t1 - t0:.1f} s, "
+                       f"measurement {t2 - t1:.1f} s); a {walkers}-walker step would take "
+                       f"{t_sample * walkers / threads:.0f} s"),
+            "measured_s": t_sample, "step_s_extrapolated": t_sample * walkers / threads,
+            "energy_per_site": m["Etot"] / m["norm"] / (w["L"] ** 2)}
 
 
 def run_reference(args):
+    """The reference arm: the oracle port on the host cores, each step one complete sample of the workload
+    (threads walkers, full make_sample + measurement); warm-up is one such step (the CPU has nothing to warm
+    beyond that)."""
     rank, world, _ = _rank_env()
     if rank != 0:
         return 0
     w = WORKLOADS[args.workload]
     problem = make_problem(w)
-    for _ in range(args.warmup):
-        pass  # host code has no device warm-up; each timed step is a bounded sample
-    vals = []
+    for _ in range(min(args.warmup, 1)):
+        cpu_baseline(w, problem)
+    vals, meas = [], []
     info = None
     for _ in range(args.steps):
         info = cpu_baseline(w, problem)
         vals.append(info["value"])
+        meas.append(info["measured_s"])
     v = float(np.median(vals))
     ms = w["walkers"] * w["ns"] / v * 1e3
     line = {"impl": "reference", "metric": METRIC, "value": v, "unit": "MC samples/s", "n_gpus": args.gpus,
-            "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+            "steps": args.steps, "warmup": min(args.warmup, 1), "ms_per_step": ms, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "config": {"workload": args.workload, "L": w["L"], "walkers": w["walkers"],
                        "samples_per_step": w["walkers"] * w["ns"], "alphar": w["alphar"],
                        "n_mp_trans": w["L"] ** 2 if w["translations"] else 1, "J2": w["J2"]},
+            "measured_s_per_step": meas,
+            "ms_per_step_basis": "the measured complete walkers, scaled by walker count to the full step",
             "cpu_baseline": {k: info[k] for k in ("value", "unit", "cores", "kind", "sample")},
             "e2e": {"value": v, "unit": "MC samples/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
@@ -329,44 +337,48 @@ def run_ours(args):
     ctx = capi.Context(problem, n_walkers=w["walkers"], nsample_per_walker=w["ns"], device=local,
                        walker_offset=rank * w["walkers"])
     runner = rdist.SRRunner(ctx, problem, iseed0=12345, precision=prec, world=world, rank=rank)
-    inp = problem.inp
     for _ in range(args.warmup):
         runner.step()
     torch.cuda.synchronize()
+    # the plain all-FP64 twin continues from the same state (walkers, streams, parameters, bookkeeping)
+    twin = None
+    if world == 1 and args.precision == "split" and not args.no_plain:
+        twin = capi.Context(problem, n_walkers=w["walkers"], nsample_per_walker=w["ns"], device=local,
+                            walker_offset=0)
+        twin.copy_state_from(ctx)
     if world > 1:
         torch.distributed.barrier()
     clk = ClockSampler(torch.cuda.current_device())
     clk.start()
-    step_ms, samp_ms, est_ms, sb_ms, solve_ms, acc_all, props, energies = [], [], [], [], [], [], [], []
-    refine = []
+    step_ms, samp_ms, est_ms, sb_ms, solve_ms, ref_ms, acc_all, props, energies = [], [], [], [], [], [], [], [], []
+    refine, e2e_ms = [], []
     launches0 = ctx.kernel_launches()
+    br, Wr, sl, sh = ctx.get_params()
+    h2d = d2h = br.nbytes + Wr.nbytes + sl.nbytes + 8
     for _ in range(args.steps):
+        # end to end through the public API: the step's parameters in from host buffers, its energy and the new
+        # parameters back to the host; the device time of the same step is `value`'s
+        t0 = time.perf_counter()
+        ctx.set_params(br, Wr, sl, sh)
         rec = runner.step()
+        br, Wr, sl, sh = ctx.get_params()
+        e2e_ms.append((time.perf_counter() - t0) * 1e3)
         st = ctx.stats()
         step_ms.append(rec["device_ms"])
         samp_ms.append(st["sampler_ms"])
         est_ms.append(st["estimator_ms"])
         sb_ms.append(st["sbuild_ms"])
         solve_ms.append(st["solve_ms"])
+        ref_ms.append(st["refine_ms"])
         acc_all.append(st["accepts_all"])
         props.append(st["proposals"])
         energies.append(rec["Etot"])
-        refine.append((rec.get("refine_iterations", 0), rec.get("refine_residual", 0.0)))
+        refine.append((rec.get("refine_iterations", 0), rec.get("refine_residual", 0.0), st["cholesky_attempts"]))
     torch.cuda.synchronize()
     if world > 1:
         torch.distributed.barrier()
     clocks = clk.stop()
     launches = ctx.kernel_launches() - launches0
-    # the plain all-FP64 SR path on the same walkers, one step after the timed region (for "chosen vs plain")
-    plain = None
-    if args.precision == "split" and not args.no_plain:
-        runner.precision = capi.SR_FP64
-        prec_rec = runner.step()
-        st = ctx.stats()
-        plain = {"ms_per_step": prec_rec["device_ms"], "sr_steps_per_s": 1e3 / prec_rec["device_ms"],
-                 "s_build_ms": st["sbuild_ms"], "cholesky_solve_ms": st["solve_ms"],
-                 "energy_per_site": prec_rec["Etot"] / (w["L"] ** 2)}
-        runner.precision = prec
     # max over ranks of the device time per step
     t = torch.tensor([float(np.mean(step_ms))], device="cuda")
     if world > 1:
@@ -374,19 +386,31 @@ def run_ours(args):
     ms = float(t.item())
     samples_per_step = w["walkers"] * w["ns"] * world
     value = samples_per_step / (ms * 1e-3)
-    # end to end through the public API with host buffers: parameters in, parameters + energy out
-    e2e_ms = []
-    h2d = d2h = 0
-    for _ in range(max(1, min(args.steps, 2))):
-        t0 = time.perf_counter()
-        br, Wr, sl, sh = ctx.get_params()
-        d2h = (br.nbytes + Wr.nbytes + sl.nbytes + 8)
-        ctx.set_params(br, Wr, sl, sh)
-        h2d = (br.nbytes + Wr.nbytes + sl.nbytes + 8)
-        rec = runner.step()
-        br, Wr, sl, sh = ctx.get_params()
-        e2e_ms.append((time.perf_counter() - t0) * 1e3)
     e2e_v = samples_per_step / (float(np.mean(e2e_ms)) * 1e-3)
+    # the twin: the same steps with the plain all-FP64 S build and Cholesky solve, as many as the budget allows
+    plain = None
+    if twin is not None:
+        left = PAIR_BUDGET_S - (time.perf_counter() - T_START) - (120.0 if not args.no_cpu_baseline else 0.0)
+        n_pair = int(max(1, min(args.steps, left // (ms * 1.05e-3))))
+        trunner = rdist.SRRunner.attach(twin, problem, capi.SR_FP64)
+        pe, pms, psr = [], [], []
+        for _ in range(n_pair):
+            prec_rec = trunner.step()
+            stp = twin.stats()
+            pe.append(prec_rec["Etot"])
+            pms.append(prec_rec["device_ms"])
+            psr.append(stp["sbuild_ms"] + stp["solve_ms"] + stp["refine_ms"])
+        chosen_sr = [a + b + c for a, b, c in zip(sb_ms, solve_ms, ref_ms)]
+        de = [abs(a - b) / (w["L"] ** 2) for a, b in zip(energies, pe)]
+        plain = {"paired_steps": n_pair, "ms_per_step": float(np.mean(pms)),
+                 "sr_steps_per_s": 1e3 / float(np.mean(pms)),
+                 "energy_per_site": [e / (w["L"] ** 2) for e in pe],
+                 "sr_phase_ms": float(np.mean(psr)),
+                 "sr_phase_speedup_chosen_vs_plain": float(np.mean(psr)) / float(np.mean(chosen_sr[:n_pair])),
+                 "delta_e_per_site": {"per_step": de, "max": float(max(de)), "mean": float(np.mean(de)),
+                                      "of_the_mean": abs(float(np.mean(energies[:n_pair])) - float(np.mean(pe)))
+                                      / (w["L"] ** 2)}}
+        twin.close()
     peaks, peak_kind = measured_peaks()
     Np = (w["L"] ** 2) // 2
     n_qp = 2 * (w["L"] ** 2 if w["translations"] else 1)
@@ -404,9 +428,10 @@ def run_ours(args):
                        "l2": "inputs larger than L2 (Y %.1f GB, O %.1f GB per GPU)" % (
                            w["walkers"] * n_qp * Np * Np * 8 / 1e9, samples_per_step / world * ctx.Nv * 8 / 1e9)},
             "sr_steps_per_s": 1e3 / ms,
-            "energy_per_site": float(np.mean(energies)) / (w["L"] ** 2),
+            "energy_per_site": [e / (w["L"] ** 2) for e in energies],
             "phases_ms": {"make_sample": smp, "estimator": float(np.mean(est_ms)), "s_build": float(np.mean(sb_ms)),
-                          "cholesky_solve": float(np.mean(solve_ms))},
+                          "cholesky_solve": float(np.mean(solve_ms)), "refinement": float(np.mean(ref_ms)),
+                          "sr_phase": float(np.mean(sb_ms)) + float(np.mean(solve_ms)) + float(np.mean(ref_ms))},
             "roofline": {"kernel": "sampler_stream_kernel (make_sample)", "bound": "hbm", "achieved": achieved,
                          "peak": peaks["hbm_gbs"], "unit": "GB/s", "frac": achieved / peaks["hbm_gbs"],
                          "peak_kind": peak_kind + " (burst copy)",
@@ -417,7 +442,8 @@ def run_ours(args):
             "clocks": clocks,
             "e2e": {"value": e2e_v, "unit": "MC samples/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
             "gpu_launches": launches,
-            "sr_refinement": {"iterations": [r[0] for r in refine], "residual": [r[1] for r in refine]},
+            "sr_refinement": {"iterations": [r[0] for r in refine], "residual": [r[1] for r in refine],
+                              "cholesky_attempts": [r[2] for r in refine]},
             "plain_fp64": plain}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cb = cpu_baseline(w, problem)
@@ -430,6 +456,86 @@ def run_ours(args):
     return 0
 
 
+def run_sr_precision(args):
+    """Error table of the split-BF16 SR path at full size (10x10, 100 translations, 4096 walkers x 16 samples,
+    Nv = 10404): after W optimisation steps, two contexts in the same state sample identical chains; one builds
+    S in FP64, the other in split-BF16 on the tensor cores; both take the SR step (FP64 Cholesky solve, and
+    the split one refined on the exact S); then both sample and measure the energy at their new parameters.
+    Reported: the S entry error, the SR-direction and lambda errors, the energy-per-site difference, and the
+    phase times of both paths."""
+    import torch
+    from rbm_pp_b200 import capi
+    from rbm_pp_b200 import distributed as rdist
+    torch.cuda.set_device(0)
+    w = WORKLOADS["j1j2_10x10_trans"]
+    problem = make_problem(w)
+    inp = problem.inp
+    a = capi.Context(problem, n_walkers=w["walkers"], nsample_per_walker=w["ns"])
+    runner = rdist.SRRunner(a, problem, iseed0=12345, precision=capi.SR_FP64)
+    for _ in range(args.warmup):
+        runner.step()
+    b = capi.Context(problem, n_walkers=w["walkers"], nsample_per_walker=w["ns"])
+    b.copy_state_from(a)
+    res = {}
+    for c, prec, key in ((a, capi.SR_FP64, "fp64"), (b, capi.SR_SPLIT_BF16, "split")):
+        c.make_sample(False)
+        c.set_s_precision(prec)
+        m = c.measure(want_S=True)
+        res[key] = dict(m=m, x=c.samples()[0], sbuild_ms=c.stats()["sbuild_ms"])
+    assert np.array_equal(res["fp64"]["x"], res["split"]["x"]), "the two contexts sampled different chains"
+    m64, m16 = res["fp64"]["m"], res["split"]["m"]
+    norm = m64["norm"]
+    mv = m64["Ovec"] / norm
+    S64 = m64["S"] / norm - np.outer(mv, mv)
+    d = m16["S"] / norm - np.outer(mv, mv) - S64
+    smax = float(np.abs(S64).max())
+    dg = np.diag(S64)
+    sd = float(dg[dg > 0].mean())
+    table = {"S_max_abs_err_over_max_S": float(np.abs(d).max()) / smax,
+             "S_rms_err_over_max_S": float(np.sqrt(np.mean(d * d))) / smax,
+             "S_max_abs_err_over_mean_diag": float(np.abs(d).max()) / sd,
+             "S_diag_max_rel_err": float(np.abs(np.diag(d)).max() / np.abs(dg).max())}
+    del d, S64, m64["S"], m16["S"]
+    out = {}
+    for c, prec, key in ((a, capi.SR_FP64, "fp64"), (b, capi.SR_SPLIT_BF16, "split")):
+        sout, dx = c.sr_step(1000 + args.warmup, inp.delta_tau, inp.s_factor0, inp.s_cut, precision=prec,
+                             refine_steps=200)
+        st = c.stats()
+        out[key] = dict(dx=dx, lam=sout.lambda_, it=sout.refine_iterations, res=sout.refine_residual,
+                        attempts=st["cholesky_attempts"], sbuild_ms=res[key]["sbuild_ms"], solve_ms=st["solve_ms"],
+                        refine_ms=st["refine_ms"], precond_shift=sout.precond_shift)
+    dx64, dx16 = out["fp64"]["dx"], out["split"]["dx"]
+    table["dtheta_max_rel_err"] = float(np.abs(dx16 - dx64).max() / np.abs(dx64).max())
+    table["lambda_rel_err"] = abs(out["split"]["lam"] - out["fp64"]["lam"]) / abs(out["fp64"]["lam"])
+    pa, pb = a.get_params(), b.get_params()
+    table["params_max_rel_diff"] = float(max(np.abs(pa[i] - pb[i]).max() / max(np.abs(pa[i]).max(), 1e-300)
+                                             for i in range(3)))
+    e = {}
+    for c, key in ((a, "fp64"), (b, "split")):
+        c.make_sample(False)
+        me = c.measure_energy()
+        e[key] = me["Etot"] / me["norm"] / (w["L"] ** 2)
+    table["energy_per_site_fp64"] = e["fp64"]
+    table["energy_per_site_split"] = e["split"]
+    table["delta_energy_per_site"] = abs(e["split"] - e["fp64"])
+    table["next_chains_identical"] = bool(np.array_equal(a.samples()[0], b.samples()[0]))
+    sr = {k: {kk: vv for kk, vv in v.items() if kk != "dx"} for k, v in out.items()}
+    for k in sr:
+        sr[k]["sr_phase_ms"] = sr[k]["sbuild_ms"] + sr[k]["solve_ms"] + sr[k]["refine_ms"]
+    line = {"metric": "split-BF16 SR error table and phase times at 10x10 (Nv = 10404, 65536 samples)",
+            "value": table["delta_energy_per_site"], "unit": "|dE/site|", "n_gpus": 1, "steps": 1,
+            "warmup": args.warmup, "higher_is_better": False, "dtype": "f64 / split-bf16",
+            "data": "synthetic (seeded, reference file shapes)",
+            "config": {"workload": "sr_precision_10x10", "L": 10, "Nv": a.Nv, "samples": w["walkers"] * w["ns"],
+                       "shift": "mean(diag S) * max(1e-4, s_factor0) (SR_pdposv.f90:167-170)"},
+            "errors": table, "sr": sr,
+            "sr_phase_speedup_chosen_vs_plain": sr["fp64"]["sr_phase_ms"] / sr["split"]["sr_phase_ms"]}
+    print(json.dumps(line), flush=True)
+    a.close()
+    b.close()
+    return 0
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -437,7 +543,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--workload", default="j1j2_10x10_trans",
-                    choices=sorted(WORKLOADS) + ["batch_l12_18", "batch_l12_18_small"])
+                    choices=sorted(WORKLOADS) + ["batch_l12_18", "batch_l12_18_small", "sr_precision_10x10"])
     ap.add_argument("--precision", default="split", choices=["fp64", "split"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-plain", action="store_true", help="skip the extra all-FP64 comparison step")
@@ -448,6 +554,8 @@ def main():
         return run_batch(args)
     if args.workload.startswith("corr_"):
         return run_corr(args)
+    if args.workload == "sr_precision_10x10":
+        return run_sr_precision(args)
     return run_ours(args)
 
 

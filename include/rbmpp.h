@@ -98,9 +98,15 @@ int rbmpp_query(const rbmpp_ctx* ctx, int what, long long* value);
 
 /* Tables: W_map(N, 1, N_MP_Trans) (main.f90:94-122; also MP_Trans_Idx, parameter.f90:105-109),
  * para_mp_trans(N_MP_Trans) complex, Orbital_Idx(N,N) (parameter.f90:88-100),
- * Orbital_Sgn(N,N) or NULL (all +1; l_AP = .false.).  Replaces the module setup of main.f90:89-300. */
+ * Orbital_Sgn(N,N) or NULL (all +1; l_AP = .false.),
+ * subB(N) = 1 for sites of sublattice B, 0 otherwise (subB_or_not, define_sublattice interface_for_PP.f90:110-136)
+ * or NULL (derived: site i = i2 L + i1 + 1 is on B when i1 + i2 is odd),
+ * sp_weights(3, 2) = {SP_GL_Cos, SP_GL_Sin, para_spin_proj} of the two spin-projection points
+ * (InitSPWeight, spin_projection.f90:5-79) or NULL (beta = 0 and pi, para_spin_proj = (1, spin_parity)).
+ * The weights must make SP_GL_Cos * SP_GL_Sin vanish (relative 1e-12) at both points.
+ * Replaces the module setup of main.f90:89-300. */
 int rbmpp_set_tables(rbmpp_ctx* ctx, const int* W_map, const double* para_mp_trans, const int* Orbital_Idx,
-                     const int* Orbital_Sgn);
+                     const int* Orbital_Sgn, const int* subB, const double* sp_weights);
 
 /* Parameters: Wrirr(N, alphar), brirr(alphar), Slater(N_Slater), shift (module.f90 mod_RBM, mod_PP,
  * mod_main).  Wc/bc must be NULL (alphac = 0).  Also rebuilds Slater_Elm on the device
@@ -165,13 +171,49 @@ int rbmpp_iteration(rbmpp_ctx* ctx, int precision, double delta_tau, double s_fa
 
 /* Device-side statistics of the last calls, timed with CUDA events on the library's stream:
  * out[0] make_sample kernel ms, [1] estimator kernel ms, [2] gvec/Ovec GEMV ms, [3] S build ms,
- * [4] Cholesky factor + solve ms, [5] accepted moves in all sweeps of the last make_sample,
- * [6] proposals of the last make_sample, [7] last rbmpp_iteration ms.  n = number of entries wanted. */
+ * [4] Cholesky factor(s) + first solve ms, [5] accepted moves in all sweeps of the last make_sample,
+ * [6] proposals of the last make_sample, [7] last rbmpp_iteration ms, [8] refinement ms (conjugate
+ * gradients on the exact S and the final lambda products), [9] Cholesky attempts of the last SR step.
+ * n = number of entries wanted (at most 10). */
 int rbmpp_get_stats(const rbmpp_ctx* ctx, double* out, int n);
+
+/* Copies the whole sampling state of src into dst (same shape, same device, tables set on both): every
+ * walker's configuration, inverse blocks, amplitudes, random stream, Nfastup and stored samples, the
+ * parameters and shift, and the iteration bookkeeping of rbmpp_iteration.  dst then continues exactly as src
+ * would (no counterpart in the reference, whose state is the rank's memory; used to run two SR variants
+ * from one state). */
+int rbmpp_copy_state(rbmpp_ctx* dst, const rbmpp_ctx* src);
 
 /* Per-walker sampler state: Nfastup (adaptive recompute interval, make_sample.f90:120-127) and the
  * accepted moves of the last make_sample over all sweeps.  Either pointer may be NULL. */
 int rbmpp_get_walker_state(const rbmpp_ctx* ctx, int* nfastup, int* naccept_all);
+
+/* Per-walker diagnostics of the last make_sample (the events of make_sample.f90, recorded on the device).
+ * events(5, n_walkers) = {global spin flips tried (:135), flips accepted (:145-157), make_initial_x re-seeds
+ * of a continued chain (:61), Nfastup checkpoints (:74-128), trace records produced (possibly more than were
+ * kept)}.  trace(6, max_records, n_walkers), filled when rbmpp_set_trace enabled it, lists the chain's
+ * random decisions in draw order:
+ *   {0, i1, i2, ratio^2, u, accepted}  exchange proposal of sites i1, i2 (0-based), accepted = u < ratio^2
+ *                                      with ratio = (|psi'| + shift) / (|psi| + shift) (:160-220);
+ *   {1, i0, inverse drift, Pf drift, Nfastup before, Nfastup after}  checkpoint at sweep i0 (:74-128; the
+ *                                      inverse drift is measured on the Np x Np block inverse);
+ *   {2, 0, 0, ratio^2, u, accepted}    global spin flip (:135-158);
+ *   {3, 0, 0, 0, 0, 0}                 make_initial_x re-seed of a continued chain (:61).
+ * Records beyond max_records are dropped.  Either pointer may be NULL. */
+int rbmpp_get_walker_events(const rbmpp_ctx* ctx, int* events, double* trace);
+/* Enables (max_records > 0) or disables (0) the per-walker chain trace of later make_sample calls. */
+int rbmpp_set_trace(rbmpp_ctx* ctx, int max_records);
+/* Verification replay (no counterpart in the reference): decisions(2, max_checkpoints, n_walkers) =
+ * {Nfastup after, 1 if the extra draw of make_sample.f90:122 is taken} replace the drift test of the first
+ * max_checkpoints checkpoints of each walker in later make_sample calls (the draw of :116 still happens).
+ * It lets a chain follow another implementation's recompute schedule; 0 turns it off. */
+int rbmpp_set_replay(rbmpp_ctx* ctx, const int* decisions, int max_checkpoints);
+/* Verification hooks of the failure paths (no counterpart in the reference; off by default):
+ * what 1: walker 0 of the streaming sampler never issues its bulk load number `value` (1-based, 0 = off), so
+ *         the consumer's bounded wait on it runs out: make_sample returns RBMPP_E_TIMEOUT and the context
+ *         stays usable (the next make_sample rebuilds every walker's state);
+ * what 2: poll bound of the streaming sampler's pipeline waits (0 = the default, 2^22 polls). */
+int rbmpp_debug_hook(rbmpp_ctx* ctx, int what, int value);
 
 /* Adjoint O_k kernel: for n configurations x(N, n): psi(0:N_QP, n) complex, hpsi(n) complex
  * (sum_x' <x|H|x'> psi(x'), calc_local_energy_correlation), and O(Nv, n) = d psi(x) / d theta_k
@@ -202,9 +244,9 @@ int rbmpp_batch_make_sample(rbmpp_batch* b, int first_iteration, long long* nacc
  * x, psi, hpsi, O have the layouts of rbmpp_eval_configs but are DEVICE pointers on the context's
  * device, owned by the caller (psi, hpsi, O may be NULL).  Scratch comes from one fixed array of
  * about 2 MiB in the library's device image: at most 4096 configurations per call (more returns
- * RBMPP_E_ARG).  The first call on a device looks up that array's device address; make that first
- * call before any stream capture.  All calls share the array, so calls whose GPU work overlaps race:
- * issue them one at a time.  Returns after the results are complete on the device. */
+ * RBMPP_E_ARG).  Each call looks up that array's device address on the context's device.  All calls share
+ * the array, so calls whose GPU work overlaps race: issue them one at a time.  Returns after the results are
+ * complete on the device. */
 int rbmpp_eval_configs_noalloc(rbmpp_ctx* ctx, int n, const int* d_x, double* d_psi, double* d_hpsi, double* d_O);
 
 #ifdef __cplusplus

@@ -61,6 +61,8 @@ def lib():
         L.orc_get_nfastup.argtypes = [P, ip]
         L.orc_make_sample.argtypes = [P, C.c_int, ip, C.c_int]
         L.orc_get_samples.argtypes = [P, P, P, P]
+        L.orc_set_trace.argtypes = [P, C.c_int]
+        L.orc_get_events.argtypes = [P, P, P]
         L.orc_set_samples.argtypes = [P, ip]
         L.orc_measure.argtypes = [P, dp, dp, dp, P, P, P, C.c_int]
         L.orc_measure_energy.argtypes = [P, dp, C.c_int]
@@ -169,6 +171,19 @@ class Oracle:
         nacc = np.zeros(self.nranks, dtype=np.int32)
         self._chk(lib().orc_make_sample(self.h, 1 if first else 0, nacc, self.nthreads))
         return nacc
+
+    def set_trace(self, max_records: int):
+        self.trace_max = int(max_records)
+        lib().orc_set_trace(self.h, self.trace_max)
+
+    def events(self):
+        """Per rank {global flips tried, accepted, make_initial_x re-seeds, checkpoints, trace records} of the
+        last make_sample, and the chain trace (nranks, trace_max, 6) when one is kept (the library's layout)."""
+        ev = np.zeros(5 * self.nranks, dtype=np.int32)
+        m = getattr(self, "trace_max", 0)
+        tr = np.zeros(6 * m * self.nranks) if m > 0 else None
+        lib().orc_get_events(self.h, _ptr(ev), _ptr(tr))
+        return ev.reshape(self.nranks, 5), (tr.reshape(self.nranks, m, 6) if tr is not None else None)
 
     def samples(self):
         x = np.zeros(self.N * self.nsample * self.nranks, dtype=np.int32)

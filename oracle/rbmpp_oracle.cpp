@@ -104,6 +104,22 @@ struct Rank {
   MT rng;
   int nfastup;
   int naccept;
+  // diagnostics of the last make_sample: global flips tried / accepted, make_initial_x re-seeds,
+  // checkpoints, trace records; and the chain trace (6 doubles per record, the library's record layout)
+  int ev[5] = {0, 0, 0, 0, 0};
+  std::vector<double> trace;
+  void rec(int max, int type, double a, double b, double x, double u, double e) {
+    if (ev[4] < max) {
+      double* q = &trace[(size_t)ev[4] * 6];
+      q[0] = type;
+      q[1] = a;
+      q[2] = b;
+      q[3] = x;
+      q[4] = u;
+      q[5] = e;
+    }
+    ev[4]++;
+  }
   std::vector<int> x_sample;      // x_sample(N, Nsample)            module.f90:39
   std::vector<cplx> psi_sample;   // psi_x_sample(0:N_QP, Nsample)   module.f90:40
   std::vector<double> pf_sample;  // PfM_sample(N_QP, Nsample)       module.f90:41
@@ -124,6 +140,7 @@ struct Ctx {
   std::vector<double> SE;  // Slater_Elm(2N, 2N, N_QP)                module.f90:55
   std::vector<Rank> ranks;
   int rank0 = 0;  // global MPI rank of local rank 0 (a shard of the ranks)
+  int trace_max = 0;  // chain-trace records kept per rank
   int err;
   char msg[256];
 };
@@ -614,13 +631,18 @@ static int make_sample_rank(const Ctx& c, Rank& R, bool first) {
   std::vector<double> va(N), vb(N);
   std::vector<int> tidx(N);
   int e;
+  for (int k = 0; k < 5; k++) R.ev[k] = 0;
+  R.trace.assign((size_t)c.trace_max * 6, 0.0);
   if (first) {
     if ((e = make_initial_x(c, w, rng))) return e;
   } else {
     for (int i = 0; i < N; i++) w.x[i] = R.x_sample[(size_t)N * (c.nsample - 1) + i];
     if ((e = full_state(c, w, rng))) return e;
-    if (grnd(rng) < 0.05)
+    if (grnd(rng) < 0.05) {
+      R.ev[2]++;
+      R.rec(c.trace_max, 3, 0, 0, 0, 0, 0);
       if ((e = make_initial_x(c, w, rng))) return e;
+    }
   }
   const int nwarm = std::max(30, c.nsample / 100);
   int naccept = 0, nacc_tmp = 0;
@@ -651,6 +673,7 @@ static int make_sample_rank(const Ctx& c, Rank& R, bool first) {
         for (size_t k = 0; k < (size_t)N * N; k++) diff_inv = std::max(diff_inv, std::fabs(Mo[k] - Mn[k]) / r3);
       }
       nacc_tmp = 0;
+      const int nf0 = R.nfastup;
       (void)grnd(rng);  // make_sample.f90:116 (diagnostic print only)
       if (diff_inv > 1.0e-5 || diff_pf > 1.0e-5) {
         R.nfastup = std::max(1, (int)lround_pos((double)R.nfastup / 1.2));
@@ -658,9 +681,12 @@ static int make_sample_rank(const Ctx& c, Rank& R, bool first) {
       } else {
         R.nfastup = std::min(100, (int)lround_pos((double)R.nfastup * 1.1));
       }
+      R.ev[3]++;
+      R.rec(c.trace_max, 1, i0, diff_inv, diff_pf, nf0, R.nfastup);
     }
     for (int iu = 0; iu < c.nupdate; iu++) {
       if (grnd(rng) < 3.0e-4) {  // global spin flip, make_sample.f90:135-158
+        R.ev[0]++;
         for (int i = 0; i < N; i++) t.x[i] = -w.x[i];
         calc_theta(c, t.x.data(), t.th.data());
         if (x_to_ele(c, t.x.data(), t.idx.data(), t.cfg.data())) return ORC_E_CONFIG;
@@ -669,7 +695,10 @@ static int make_sample_rank(const Ctx& c, Rank& R, bool first) {
         if (sign_pp(c, t.idx.data(), t.sgn.data())) return ORC_E_SIGN;
         amplitude(c, t.th.data(), t.pf.data(), t.sgn.data(), t.psi_wo.data(), t.psi.data(), rng);
         double r1 = (std::abs(t.psi[0]) + c.shift) / (std::abs(w.psi[0]) + c.shift);
-        if (grnd(rng) < r1 * r1) {
+        const double u = grnd(rng);
+        R.rec(c.trace_max, 2, 0, 0, r1 * r1, u, u < r1 * r1);
+        if (u < r1 * r1) {
+          R.ev[1]++;
           (void)grnd(rng);  // make_sample.f90:146
           w.x = t.x;
           w.th = t.th;
@@ -700,7 +729,9 @@ static int make_sample_rank(const Ctx& c, Rank& R, bool first) {
       }
       amplitude(c, t.th.data(), t.pf.data(), t.sgn.data(), t.psi_wo.data(), t.psi.data(), rng);
       double r1 = (std::abs(t.psi[0]) + c.shift) / (std::abs(w.psi[0]) + c.shift);
-      if (grnd(rng) < r1 * r1) {  // make_sample.f90:203-220
+      const double u = grnd(rng);
+      R.rec(c.trace_max, 0, i1, i2, r1 * r1, u, u < r1 * r1);
+      if (u < r1 * r1) {  // make_sample.f90:203-220
         if (i0 > 0) naccept++;
         nacc_tmp++;
         w.x[i1] = -w.x[i1];
@@ -1078,6 +1109,25 @@ int orc_make_sample(void* h, int first, int* naccept, int nthreads) {
 }
 
 // x (N, Nsample, nranks) int; psi ((N_QP+1) complex, Nsample, nranks) as (re,im); pf (N_QP, Nsample, nranks)
+int orc_set_trace(void* h, int max_records) {
+  ((Ctx*)h)->trace_max = max_records < 0 ? 0 : max_records;
+  return 0;
+}
+
+// events (5, nranks) and, when a trace is kept, the trace (6, trace_max, nranks) of the last make_sample
+int orc_get_events(void* h, int* events, double* trace) {
+  Ctx& c = *(Ctx*)h;
+  for (int r = 0; r < c.nranks; r++) {
+    const Rank& R = c.ranks[r];
+    if (events)
+      for (int k = 0; k < 5; k++) events[5 * r + k] = R.ev[k];
+    if (trace && c.trace_max > 0)
+      for (size_t k = 0; k < (size_t)c.trace_max * 6; k++)
+        trace[(size_t)r * c.trace_max * 6 + k] = k < R.trace.size() ? R.trace[k] : 0.0;
+  }
+  return 0;
+}
+
 int orc_get_samples(void* h, int* x, double* psi, double* pf) {
   Ctx& c = *(Ctx*)h;
   for (int r = 0; r < c.nranks; r++) {

@@ -9,7 +9,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "librbmpp.so")
-SOURCES = ["capi.cu", "sampler.cu", "sampler_stream.cu", "estimator.cu", "correlation.cu", "linalg.cu", "gemm_bf16x3.cu"]
+SOURCES = ["capi.cu", "sampler.cu", "sampler_stream.cu", "estimator.cu", "correlation.cu", "linalg.cu", "sr_solve.cu", "gemm_bf16x3.cu"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
          "-Xcompiler", "-O2", "--expt-relaxed-constexpr"]
@@ -21,7 +21,19 @@ def _stale() -> bool:
     t = min(os.path.getmtime(LIB), os.path.getmtime(DRIVER), os.path.getmtime(POST))
     deps = [os.path.join(CSRC, f) for f in os.listdir(CSRC)] + [os.path.join(HERE, "..", "include", "rbmpp.h"),
                                                                 DRIVER_SRC, POST_SRC]
+    objdir = os.path.join(HERE, "_build")
+    # a source edited while an earlier build ran leaves its object older than the source
+    for s in SOURCES:
+        o = os.path.join(objdir, s.replace(".cu", ".o"))
+        if os.path.exists(o) and os.path.getmtime(o) < os.path.getmtime(os.path.join(CSRC, s)):
+            return True
     return any(os.path.getmtime(p) > t for p in deps if os.path.exists(p))
+
+
+def _headers_mtime() -> float:
+    hs = [os.path.join(CSRC, f) for f in os.listdir(CSRC) if f.endswith((".cuh", ".h"))]
+    hs.append(os.path.join(HERE, "..", "include", "rbmpp.h"))
+    return max(os.path.getmtime(h) for h in hs if os.path.exists(h))
 
 
 def build(force: bool = False, verbose: bool = False, extra: list[str] | None = None) -> str:
@@ -30,9 +42,13 @@ def build(force: bool = False, verbose: bool = False, extra: list[str] | None = 
     objdir = os.path.join(HERE, "_build")
     os.makedirs(objdir, exist_ok=True)
     objs, cmds = [], []
+    th = _headers_mtime()
     for src in SOURCES:
         obj = os.path.join(objdir, src.replace(".cu", ".o"))
-        cmds.append([NVCC, *FLAGS, *(extra or []), "-c", os.path.join(CSRC, src), "-o", obj])
+        sp = os.path.join(CSRC, src)
+        # recompile a source whose object is older than it or than any shared header
+        if force or extra or not os.path.exists(obj) or os.path.getmtime(obj) < max(os.path.getmtime(sp), th):
+            cmds.append([NVCC, *FLAGS, *(extra or []), "-c", sp, "-o", obj])
         objs.append(obj)
     # one nvcc per source, run side by side (each is single-threaded)
     with concurrent.futures.ThreadPoolExecutor(max_workers=max(1, min(len(cmds), os.cpu_count() or 1))) as ex:

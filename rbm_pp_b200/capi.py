@@ -22,7 +22,9 @@ EXPORTS = ["rbmpp_create", "rbmpp_destroy", "rbmpp_last_error", "rbmpp_query", "
            "rbmpp_iteration", "rbmpp_eval_configs", "rbmpp_get_stats", "rbmpp_exchange_measurement",
            "rbmpp_set_shift", "rbmpp_get_walker_state", "rbmpp_eval_configs_noalloc",
            "rbmpp_set_s_precision", "rbmpp_batch_create", "rbmpp_batch_destroy", "rbmpp_batch_last_error",
-           "rbmpp_batch_tune", "rbmpp_batch_make_sample", "rbmpp_measure_correlation"]
+           "rbmpp_batch_tune", "rbmpp_batch_make_sample", "rbmpp_measure_correlation",
+           "rbmpp_get_walker_events", "rbmpp_set_trace", "rbmpp_set_replay", "rbmpp_debug_hook",
+           "rbmpp_copy_state"]
 
 SR_FP64 = 0
 SR_SPLIT_BF16 = 1
@@ -69,7 +71,7 @@ def lib():
         L.rbmpp_last_error.restype = C.c_char_p
         L.rbmpp_last_error.argtypes = [P]
         L.rbmpp_query.argtypes = [P, C.c_int, C.POINTER(C.c_longlong)]
-        L.rbmpp_set_tables.argtypes = [P, P, P, P, P]
+        L.rbmpp_set_tables.argtypes = [P, P, P, P, P, P, P]
         L.rbmpp_set_params.argtypes = [P, P, P, P, P, P, C.c_double]
         L.rbmpp_get_params.argtypes = [P, P, P, P, P]
         L.rbmpp_seed_walkers.argtypes = [P, C.c_int]
@@ -87,6 +89,11 @@ def lib():
         L.rbmpp_exchange_measurement.argtypes = [P, C.c_int, P, P, P, P]
         L.rbmpp_set_shift.argtypes = [P, C.c_double]
         L.rbmpp_get_walker_state.argtypes = [P, P, P]
+        L.rbmpp_get_walker_events.argtypes = [P, P, P]
+        L.rbmpp_set_trace.argtypes = [P, C.c_int]
+        L.rbmpp_set_replay.argtypes = [P, P, C.c_int]
+        L.rbmpp_debug_hook.argtypes = [P, C.c_int, C.c_int]
+        L.rbmpp_copy_state.argtypes = [P, P]
         L.rbmpp_eval_configs_noalloc.argtypes = [P, C.c_int, P, P, P, P]
         L.rbmpp_set_s_precision.argtypes = [P, C.c_int]
         L.rbmpp_batch_create.argtypes = [P, C.c_int, C.POINTER(P)]
@@ -110,7 +117,8 @@ def _f(a, dtype):
 class Context:
     """One library context: ``n_walkers`` emulated MPI ranks on one GPU."""
 
-    def __init__(self, problem, n_walkers: int, nsample_per_walker: int, device: int = 0, walker_offset: int = 0):
+    def __init__(self, problem, n_walkers: int, nsample_per_walker: int, device: int = 0, walker_offset: int = 0,
+                 subB=None, sp_weights=None):
         self.p = problem
         inp = problem.inp
         self.N = inp.L * inp.L
@@ -132,7 +140,10 @@ class Context:
         para[1::2] = problem.sym.para_mp.imag
         self._w = _f(problem.sym.W_map, np.int32)
         self._o = _f(problem.orbital_idx, np.int32)
-        self._chk(lib().rbmpp_set_tables(self.h, _p(self._w), _p(para), _p(self._o), None))
+        self._sb = None if subB is None else np.ascontiguousarray(subB, dtype=np.int32)
+        self._spw = None if sp_weights is None else _f(sp_weights, np.float64)
+        self._chk(lib().rbmpp_set_tables(self.h, _p(self._w), _p(para), _p(self._o), None, _p(self._sb),
+                                         _p(self._spw)))
 
     def close(self):
         if getattr(self, "h", None):
@@ -241,6 +252,34 @@ class Context:
         self._chk(lib().rbmpp_get_walker_state(self.h, _p(out), None))
         return out
 
+    def set_trace(self, max_records: int):
+        self._chk(lib().rbmpp_set_trace(self.h, int(max_records)))
+        self.trace_max = int(max_records)
+
+    def set_replay(self, decisions):
+        """decisions: int array (n_walkers, max_checkpoints, 2) of {Nfastup after, extra draw}, or None."""
+        if decisions is None:
+            self._chk(lib().rbmpp_set_replay(self.h, None, 0))
+            return
+        d = np.ascontiguousarray(decisions, dtype=np.int32)
+        self._chk(lib().rbmpp_set_replay(self.h, _p(d), int(d.shape[1])))
+
+    def events(self):
+        """Per walker {global flips tried, accepted, make_initial_x re-seeds, checkpoints, trace records} of
+        the last make_sample, and the chain trace (n_walkers, max_records, 6) when one is enabled."""
+        ev = np.zeros(5 * self.nw, dtype=np.int32)
+        m = getattr(self, "trace_max", 0)
+        tr = np.zeros(6 * m * self.nw) if m > 0 else None
+        self._chk(lib().rbmpp_get_walker_events(self.h, _p(ev), _p(tr)))
+        return ev.reshape(self.nw, 5), (tr.reshape(self.nw, m, 6) if tr is not None else None)
+
+    def debug_hook(self, what: int, value: int):
+        self._chk(lib().rbmpp_debug_hook(self.h, int(what), int(value)))
+
+    def copy_state_from(self, other: "Context"):
+        """Continue from other's sampling state, parameters and iteration bookkeeping."""
+        self._chk(lib().rbmpp_copy_state(self.h, other.h))
+
     def set_s_precision(self, precision):
         self._chk(lib().rbmpp_set_s_precision(self.h, int(precision)))
 
@@ -253,10 +292,10 @@ class Context:
                                                    C.c_void_p(ov_ptr), _p(scal6)))
 
     def stats(self):
-        out = np.zeros(8)
-        self._chk(lib().rbmpp_get_stats(self.h, _p(out), 8))
+        out = np.zeros(10)
+        self._chk(lib().rbmpp_get_stats(self.h, _p(out), 10))
         keys = ["sampler_ms", "estimator_ms", "gemv_ms", "sbuild_ms", "solve_ms", "accepts_all", "proposals",
-                "iteration_ms"]
+                "iteration_ms", "refine_ms", "cholesky_attempts"]
         return dict(zip(keys, out.tolist()))
 
     def eval_configs(self, x, want_h=True, want_O=False):

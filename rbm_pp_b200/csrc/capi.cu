@@ -30,8 +30,16 @@ size_t rbmpp_estimator_smem(const DevDims&, int);
 cudaError_t rbmpp_launch_advance_rng(uint32_t*, const int*, int, int, int, cudaStream_t);
 cudaError_t rbmpp_syrk_ot_o(int, int, const double*, double*, cudaStream_t);
 cudaError_t rbmpp_symmetrize(int, double*, cudaStream_t);
-cudaError_t rbmpp_potrf_upper(int, double*, int*, cudaStream_t);
-cudaError_t rbmpp_potrs_upper(int, const double*, double*, cudaStream_t);
+cudaError_t rbmpp_potrf_upper(int, double*, double*, int*, cudaStream_t);
+cudaError_t rbmpp_potrs_upper(int, const double*, const double*, double*, double*, cudaStream_t);
+int rbmpp_chol_blocks(int);
+int rbmpp_chol_nb();
+int rbmpp_gram_parts();
+cudaError_t rbmpp_sr_apply(int, int, int, const double*, const double*, double, double, double, const double*,
+                           double*, double*, double*, double*, double*, double*, double*, cudaStream_t);
+cudaError_t rbmpp_pcg_start(int, const double*, const double*, double*, double*, cudaStream_t);
+cudaError_t rbmpp_pcg_dir(int, const double*, const double*, double*, double*, int, cudaStream_t);
+cudaError_t rbmpp_pcg_step(int, const double*, const double*, double*, double*, double*, cudaStream_t);
 cudaError_t rbmpp_trmv_upper(int, const double*, const double*, double*, cudaStream_t);
 cudaError_t rbmpp_gemv_ot(int, int, const double*, const double*, const double*, double*, double*, double*, int,
                           cudaStream_t);
@@ -132,6 +140,11 @@ struct rbmpp_ctx {
   double *d_tmp_ns = nullptr, *d_rv = nullptr;
   int *d_info = nullptr, *d_err = nullptr;
   double* d_Sb = nullptr;  // copy of the shifted split-precision S (preconditioner retries)
+  double* d_dinv = nullptr;  // inverted diagonal blocks of the Cholesky factor
+  double* d_pcg = nullptr;   // refinement vectors (10 x Nv)
+  double* d_gpart = nullptr; // per-block partial sums of the one-pass O^T (O y)
+  double* d_sc = nullptr;    // device scalars of the refinement
+  double* h_sc = nullptr;    // pinned host copy of them
   // correlation measurement: per-sample rows (2 Nchi + 1), w SdotS rows (4N), ones, Chi_vbs blocks, sums
   double *d_crow = nullptr, *d_csd = nullptr, *d_cones = nullptr, *d_cvbs = nullptr, *d_cpart = nullptr,
          *d_csum = nullptr;
@@ -148,7 +161,7 @@ struct rbmpp_ctx {
   double wf_av_list[10] = {0};
   size_t bytes = 0;
   cudaEvent_t ev[12] = {};
-  double stats[8] = {0};
+  double stats[10] = {0};
   int stream_stages = 0;  // > 0: TMA-streamed sampler with this many stages
   bool est_fits = true;   // the estimator's workspace fits in shared memory
   // S of the current measurement: built lazily in the precision the SR step asks for
@@ -245,6 +258,11 @@ int ensure_measure_buffers(rbmpp_ctx* c) {
   if ((r = dalloc(c, &c->d_info, 4))) return r;
   if ((r = dalloc(c, &c->d_err, 4))) return r;
   if ((r = dalloc(c, &c->d_rv, (size_t)2 * d.Nv))) return r;
+  if ((r = dalloc(c, &c->d_dinv, (size_t)rbmpp_chol_blocks(d.Nv) * rbmpp_chol_nb() * rbmpp_chol_nb()))) return r;
+  if ((r = dalloc(c, &c->d_pcg, (size_t)10 * d.Nv))) return r;
+  if ((r = dalloc(c, &c->d_gpart, (size_t)rbmpp_gram_parts() * d.Nv))) return r;
+  if ((r = dalloc(c, &c->d_sc, 8))) return r;
+  CK(cudaMallocHost(&c->h_sc, 8 * sizeof(double)));
   return 0;
 }
 
@@ -292,28 +310,16 @@ int build_S(rbmpp_ctx* c, int prec) {
   return 0;
 }
 
-// y = A x with A = D (S_raw / norm - ov ov^T) D + sigma I, D = diag(1 on the RBM block, scal on the
-// Pfaffian block): the conditioned S of SR_pdposv.f90:4-170 applied exactly in FP64 through O
-// (S_raw x = O^T (O x)), without forming S.
-int apply_S_exact(rbmpp_ctx* c, const std::vector<double>& x, const std::vector<double>& ov, double norm, double scal,
-                  double sigma, std::vector<double>& y) {
-  const int Nv = c->d.Nv, Nrbm = c->d.Nv_rbm;
-  std::vector<double> y1(Nv), y2(Nv);
-  double ovy = 0.0;
-  for (int k = 0; k < Nv; k++) {
-    y1[k] = k < Nrbm ? x[k] : x[k] * scal;
-    ovy += ov[k] * y1[k];
-  }
-  CK(cudaMemcpyAsync(c->d_rv, y1.data(), sizeof(double) * Nv, cudaMemcpyHostToDevice, c->st));
-  CK(rbmpp_gemv_o(c->ns_tot, Nv, c->d_O, c->d_rv, c->d_tmp_ns, c->st));
-  CK(rbmpp_gemv_ot(c->ns_tot, Nv, c->d_O, c->d_tmp_ns, nullptr, c->d_rv + Nv, nullptr, c->d_part, 64, c->st));
-  CK(cudaMemcpyAsync(y2.data(), c->d_rv + Nv, sizeof(double) * Nv, cudaMemcpyDeviceToHost, c->st));
-  CK(cudaStreamSynchronize(c->st));
-  y.assign(Nv, 0.0);
-  for (int k = 0; k < Nv; k++) {
-    const double v = y2[k] / norm - ov[k] * ovy;
-    y[k] = (k < Nrbm ? v : v * scal) + sigma * x[k];
-  }
+// y = A x with A = D (S_raw / norm - m m^T) D + sigma I, D = diag(1 on the RBM block, scal on the Pfaffian
+// block), m = Ovec / norm in the refinement vector VM: the conditioned S of SR_pdposv.f90:4-170 applied
+// exactly in FP64 through O (S_raw x = O^T (O x)) without forming S.  x, y: device vectors.
+enum { VG = 0, VX, VR, VZ, VP, VAP, VWS, VZZ, VTMP, VM };
+int apply_A(rbmpp_ctx* c, double norm, double scal, double sigma, const double* x, double* y) {
+  const DevDims& d = c->d;
+  double* v = c->d_pcg;
+  const size_t Nv = d.Nv;
+  CK(rbmpp_sr_apply(c->ns_tot, d.Nv, d.Nv_rbm, c->d_O, v + VM * Nv, norm, scal, sigma, x, y, v + VWS * Nv,
+                    v + VZZ * Nv, c->d_gpart, c->d_tmp_ns, c->d_part, c->d_sc, c->st));
   return 0;
 }
 
@@ -425,6 +431,8 @@ int rbmpp_create(const rbmpp_dims* dims, rbmpp_ctx** out) {
   if ((r = dalloc(c, &W.naccept, nw))) return r;
   if ((r = dalloc(c, &W.nacc_all, nw))) return r;
   if ((r = dalloc(c, &W.status, nw))) return r;
+  if ((r = dalloc(c, &W.events, nw * 5))) return r;
+  CK(cudaMemset(W.events, 0, sizeof(int) * nw * 5));
   if ((r = dalloc(c, &W.xs, nw * ns * N))) return r;
   if ((r = dalloc(c, &W.pfs, nw * ns * d.n_qp))) return r;
   if ((r = dalloc(c, &W.psis, nw * ns * (d.n_qp + 1) * 2))) return r;
@@ -467,12 +475,13 @@ int rbmpp_destroy(rbmpp_ctx* c) {
   if (!c) return 0;
   void* ptrs[] = {c->d_wmap, c->d_winv, c->d_orb, c->d_bonds, c->d_subB, c->d_para, c->d_Wr, c->d_br, c->d_slater,
                   c->d_XF, c->d_XFT, c->W.x, c->W.idx, c->W.cfg, c->W.th, c->W.sgn, c->W.pf, c->W.psi, c->W.Y,
-                  c->W.mt, c->W.nfastup, c->W.naccept, c->W.nacc_all, c->W.status, c->W.xs, c->W.pfs, c->W.psis, c->W.gj, c->d_O, c->d_psiS,
+                  c->W.mt, c->W.nfastup, c->W.naccept, c->W.nacc_all, c->W.status, c->W.xs, c->W.pfs, c->W.psis, c->W.gj, c->W.events, c->W.trace, (void*)c->W.replay, c->d_O, c->d_psiS,
                   c->d_eloc, c->d_a, c->d_b, c->d_tmp_ns, c->d_acc4, c->d_nap, c->d_estat, c->d_gvec, c->d_Ovec,
                   c->d_vec, c->d_S, c->d_part, c->d_info, c->d_err, c->d_rv, c->d_hi, c->d_lo, c->d_Sf, c->d_Sb,
-                  c->d_crow, c->d_csd, c->d_cones, c->d_cvbs, c->d_cpart, c->d_csum};
+                  c->d_crow, c->d_csd, c->d_cones, c->d_cvbs, c->d_cpart, c->d_csum, c->d_dinv, c->d_pcg, c->d_gpart, c->d_sc};
   for (void* p : ptrs)
     if (p) cudaFree(p);
+  if (c->h_sc) cudaFreeHost(c->h_sc);
   for (auto& e : c->ev)
     if (e) cudaEventDestroy(e);
   if (c->st) cudaStreamDestroy(c->st);
@@ -497,10 +506,43 @@ int rbmpp_query(const rbmpp_ctx* c, int what, long long* v) {
   return 0;
 }
 
-int rbmpp_set_tables(rbmpp_ctx* c, const int* W_map, const double* para, const int* orb_idx, const int* orb_sgn) {
+int rbmpp_set_tables(rbmpp_ctx* c, const int* W_map, const double* para, const int* orb_idx, const int* orb_sgn,
+                     const int* subB, const double* sp_weights) {
   if (!c || !W_map || !para || !orb_idx) return fail(c, RBMPP_E_ARG, "null table");
-  const DevDims& d = c->d;
+  DevDims& d = c->d;
   const int N = d.N;
+  if (sp_weights) {
+    // InitSPWeight's products (spin_projection.f90:36-41); the kernels carry the Pfaffian as det X of the
+    // up-down block, which needs the same-spin blocks -(F - F^T) cos sin of slater.f90:36-44 to vanish
+    double cc[2], cs[2], ss[2];
+    for (int sp = 0; sp < 2; sp++) {
+      const double co = sp_weights[3 * sp], si = sp_weights[3 * sp + 1], w = sp_weights[3 * sp + 2];
+      if (!std::isfinite(co) || !std::isfinite(si) || !std::isfinite(w))
+        return fail(c, RBMPP_E_ARG, "sp_weights: non-finite value at point %d", sp + 1);
+      cc[sp] = co * co;
+      cs[sp] = co * si;
+      ss[sp] = si * si;
+      if (!(std::fabs(cs[sp]) <= 1e-12 * std::max(cc[sp], ss[sp])))
+        return fail(c, RBMPP_E_ARG,
+                    "sp_weights: point %d has cos*sin = %g, so the same-spin blocks of Slater_Elm (slater.f90:36-44) "
+                    "do not vanish; only projections with beta in {0, pi} are supported",
+                    sp + 1, cs[sp]);
+    }
+    for (int sp = 0; sp < 2; sp++) {
+      d.sp_cc[sp] = cc[sp];
+      d.sp_cs[sp] = cs[sp];
+      d.sp_ss[sp] = ss[sp];
+      d.para_sp[sp] = sp_weights[3 * sp + 2];
+    }
+  }
+  if (subB) {
+    std::vector<unsigned char> sb(N);
+    for (int i = 0; i < N; i++) {
+      if (subB[i] != 0 && subB[i] != 1) return fail(c, RBMPP_E_ARG, "subB(%d) = %d is neither 0 nor 1", i + 1, subB[i]);
+      sb[i] = (unsigned char)subB[i];
+    }
+    CK(cudaMemcpy(c->d_subB, sb.data(), N, cudaMemcpyHostToDevice));
+  }
   std::vector<int> wmap((size_t)d.n_mp * N), winv((size_t)d.n_mp * N);
   for (int mp = 0; mp < d.n_mp; mp++) {
     std::vector<char> seen(N, 0);
@@ -876,7 +918,6 @@ int rbmpp_sr_step(rbmpp_ctx* c, const rbmpp_sr_in* in, rbmpp_sr_out* out, double
   }
   for (int k = 0; k < Nv; k++) g[k] = g[k] - 2.0 * Etot * ov[k];  // :4-6
   double* d_ov = c->d_vec;
-  double* d_x = c->d_vec + Nv;
   double* d_y = c->d_vec + 2 * Nv;
   double* d_diag = c->d_vec + 3 * Nv;
   CK(cudaMemcpyAsync(d_ov, ov.data(), sizeof(double) * Nv, cudaMemcpyHostToDevice, c->st));
@@ -988,10 +1029,11 @@ int rbmpp_sr_step(rbmpp_ctx* c, const rbmpp_sr_in* in, rbmpp_sr_out* out, double
     }
     CK(cudaMemcpyAsync(c->d_Sb, c->d_S, s_bytes, cudaMemcpyDeviceToDevice, c->st));
   }
-  int info = 0;
+  int info = 0, attempts = 0;
   double tau = 0.0;
   for (int attempt = 0;; attempt++) {
-    CK(rbmpp_potrf_upper(Nv, c->d_S, c->d_info, c->st));
+    attempts = attempt + 1;
+    CK(rbmpp_potrf_upper(Nv, c->d_S, c->d_dinv, c->d_info, c->st));
     CK(cudaMemcpyAsync(&info, c->d_info, sizeof(int), cudaMemcpyDeviceToHost, c->st));
     CK(cudaStreamSynchronize(c->st));
     if (info == 0 || in->precision != RBMPP_SR_SPLIT_BF16 || in->refine_steps <= 0 || attempt == 12) break;
@@ -1000,78 +1042,80 @@ int rbmpp_sr_step(rbmpp_ctx* c, const rbmpp_sr_in* in, rbmpp_sr_out* out, double
     CK(rbmpp_add_diag(Nv, c->d_S, tau, c->st));
   }
   out->precond_shift = tau;
-  CK(cudaMemcpyAsync(d_x, g.data(), sizeof(double) * Nv, cudaMemcpyHostToDevice, c->st));
+  double* v = c->d_pcg;
+  const size_t nv = (size_t)Nv;
+  double *d_g = v + VG * nv, *d_xv = v + VX * nv, *d_r = v + VR * nv, *d_z = v + VZ * nv, *d_p = v + VP * nv;
+  double *d_ap = v + VAP * nv, *d_tmp = v + VTMP * nv, *d_m = v + VM * nv;
+  CK(cudaMemcpyAsync(d_g, g.data(), sizeof(double) * Nv, cudaMemcpyHostToDevice, c->st));
+  CK(cudaMemcpyAsync(d_xv, g.data(), sizeof(double) * Nv, cudaMemcpyHostToDevice, c->st));
   CK(cudaStreamSynchronize(c->st));
   if (info != 0) return fail(c, RBMPP_E_CHOL, "info (pdposv): %d", info);
-  CK(rbmpp_potrs_upper(Nv, c->d_S, d_x, c->st));
+  CK(rbmpp_potrs_upper(Nv, c->d_S, c->d_dinv, d_xv, d_tmp, c->st));
   CK(cudaEventRecord(c->ev[8], c->st));
   std::vector<double> x(Nv), ux(Nv), xr(Nv, 0.0), xp(Nv, 0.0);
-  CK(cudaMemcpyAsync(x.data(), d_x, sizeof(double) * Nv, cudaMemcpyDeviceToHost, c->st));
-  CK(cudaStreamSynchronize(c->st));
   const double sigma = sdiag * s_factor;
   double lam2 = 0.0, lrr = 0.0, lpp = 0.0;
+  float refine_ms = 0.f;
   if (refine) {
-    // the split-precision solve refined against the exact FP64 S (applied through O): conjugate
-    // gradients on A x = g preconditioned by the Cholesky factor of the split-precision S, started
-    // from the split solve; stops at relative residual 1e-13 or after refine_steps iterations
-    auto precond = [&](const std::vector<double>& rr, std::vector<double>& zz) -> int {
-      CK(cudaMemcpyAsync(d_y, rr.data(), sizeof(double) * Nv, cudaMemcpyHostToDevice, c->st));
-      CK(rbmpp_potrs_upper(Nv, c->d_S, d_y, c->st));
-      zz.resize(Nv);
-      CK(cudaMemcpyAsync(zz.data(), d_y, sizeof(double) * Nv, cudaMemcpyDeviceToHost, c->st));
-      CK(cudaStreamSynchronize(c->st));
-      return 0;
-    };
-    auto dot = [&](const std::vector<double>& a, const std::vector<double>& b) {
-      double t = 0.0;
-      for (int k = 0; k < Nv; k++) t += a[k] * b[k];
-      return t;
-    };
-    const double gn = std::sqrt(dot(g, g));
-    std::vector<double> ax, res(Nv), zv, pv, ap;
-    int r = apply_S_exact(c, x, ov, norm, scal, sigma, ax);
+    // the split-precision solve refined against the exact FP64 S (applied through O in one pass per product):
+    // conjugate gradients on A x = g preconditioned by the Cholesky factor of the split-precision S, started
+    // from the split solve; stops at relative residual 1e-13 or after refine_steps iterations.  Every vector
+    // stays on the device; the host reads the residual norm once per iteration.
+    CK(cudaMemcpyAsync(d_m, ov.data(), sizeof(double) * Nv, cudaMemcpyHostToDevice, c->st));
+    int r = apply_A(c, norm, scal, sigma, d_xv, d_ap);
     if (r) return r;
-    for (int k = 0; k < Nv; k++) res[k] = g[k] - ax[k];
-    if ((r = precond(res, zv))) return r;
-    pv = zv;
-    double rz = dot(res, zv);
+    CK(rbmpp_pcg_start(Nv, d_g, d_ap, d_r, c->d_sc, c->st));
+    CK(cudaMemcpyAsync(d_z, d_r, sizeof(double) * Nv, cudaMemcpyDeviceToDevice, c->st));
+    CK(rbmpp_potrs_upper(Nv, c->d_S, c->d_dinv, d_z, d_tmp, c->st));
+    CK(rbmpp_pcg_dir(Nv, d_r, d_z, d_p, c->d_sc, 0, c->st));
+    CK(cudaMemcpyAsync(c->h_sc, c->d_sc, 8 * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    const double gg = c->h_sc[4];
+    double rr = c->h_sc[2];
     int it = 0;
-    for (; it < in->refine_steps && gn > 0.0 && std::sqrt(dot(res, res)) > 1e-13 * gn; it++) {
-      if ((r = apply_S_exact(c, pv, ov, norm, scal, sigma, ap))) return r;
-      const double pap = dot(pv, ap);
-      if (!(pap > 0.0)) break;
-      const double alpha = rz / pap;
-      for (int k = 0; k < Nv; k++) {
-        x[k] += alpha * pv[k];
-        res[k] -= alpha * ap[k];
-      }
-      if ((r = precond(res, zv))) return r;
-      const double rz1 = dot(res, zv), beta = rz1 / rz;
-      rz = rz1;
-      for (int k = 0; k < Nv; k++) pv[k] = zv[k] + beta * pv[k];
+    for (; it < in->refine_steps && gg > 0.0 && std::sqrt(rr) > 1e-13 * std::sqrt(gg); it++) {
+      if ((r = apply_A(c, norm, scal, sigma, d_p, d_ap))) return r;
+      CK(rbmpp_pcg_step(Nv, d_p, d_ap, d_xv, d_r, c->d_sc, c->st));
+      CK(cudaMemcpyAsync(d_z, d_r, sizeof(double) * Nv, cudaMemcpyDeviceToDevice, c->st));
+      CK(rbmpp_potrs_upper(Nv, c->d_S, c->d_dinv, d_z, d_tmp, c->st));
+      CK(rbmpp_pcg_dir(Nv, d_r, d_z, d_p, c->d_sc, 1, c->st));
+      CK(cudaMemcpyAsync(c->h_sc, c->d_sc, 8 * sizeof(double), cudaMemcpyDeviceToHost, c->st));
+      CK(cudaStreamSynchronize(c->st));
+      rr = c->h_sc[2];
+      if (!(c->h_sc[3] > 0.0)) break;  // p.Ap <= 0: the step was not taken
     }
     out->refine_iterations = it;
     // lambda^2 = x^T A x and its block split (:251-277) with the exact A
+    CK(cudaMemcpyAsync(x.data(), d_xv, sizeof(double) * Nv, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
     for (int k = 0; k < Nv; k++) (k < Nrbm ? xr[k] : xp[k]) = x[k];
-    std::vector<double> axr, axp;
-    r = apply_S_exact(c, xr, ov, norm, scal, sigma, axr);
-    if (!r) r = apply_S_exact(c, xp, ov, norm, scal, sigma, axp);
-    if (r) return r;
+    std::vector<double> axr(Nv), axp(Nv);
+    CK(cudaMemcpyAsync(d_p, xr.data(), sizeof(double) * Nv, cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpyAsync(d_z, xp.data(), sizeof(double) * Nv, cudaMemcpyHostToDevice, c->st));
+    if ((r = apply_A(c, norm, scal, sigma, d_p, d_ap))) return r;
+    if ((r = apply_A(c, norm, scal, sigma, d_z, d_r))) return r;
+    CK(cudaEventRecord(c->ev[11], c->st));
+    CK(cudaMemcpyAsync(axr.data(), d_ap, sizeof(double) * Nv, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaMemcpyAsync(axp.data(), d_r, sizeof(double) * Nv, cudaMemcpyDeviceToHost, c->st));
+    CK(cudaStreamSynchronize(c->st));
+    CK(cudaEventElapsedTime(&refine_ms, c->ev[8], c->ev[11]));
     for (int k = 0; k < Nv; k++) {
       lrr += xr[k] * axr[k];
       lpp += xp[k] * axp[k];
       lam2 += x[k] * (axr[k] + axp[k]);
     }
     // true residual of the final x
-    double rn = 0.0;
+    double rn = 0.0, gn = 0.0;
     for (int k = 0; k < Nv; k++) {
       const double t = g[k] - (axr[k] + axp[k]);
       rn += t * t;
+      gn += g[k] * g[k];
     }
-    out->refine_residual = gn > 0.0 ? std::sqrt(rn) / gn : 0.0;
+    out->refine_residual = gn > 0.0 ? std::sqrt(rn / gn) : 0.0;
   } else {
     // lambda = sqrt(x^T S x) = ||U x|| and its block split (:251-277)
-    CK(rbmpp_trmv_upper(Nv, c->d_S, d_x, d_y, c->st));
+    CK(cudaMemcpyAsync(x.data(), d_xv, sizeof(double) * Nv, cudaMemcpyDeviceToHost, c->st));
+    CK(rbmpp_trmv_upper(Nv, c->d_S, d_xv, d_y, c->st));
     CK(cudaMemcpyAsync(ux.data(), d_y, sizeof(double) * Nv, cudaMemcpyDeviceToHost, c->st));
     CK(cudaStreamSynchronize(c->st));
     for (int k = 0; k < Nv; k++) lam2 += ux[k] * ux[k];
@@ -1091,6 +1135,8 @@ int rbmpp_sr_step(rbmpp_ctx* c, const rbmpp_sr_in* in, rbmpp_sr_out* out, double
     float ms = 0.f;
     CK(cudaEventElapsedTime(&ms, c->ev[7], c->ev[8]));
     c->stats[4] = ms;
+    c->stats[8] = refine_ms;
+    c->stats[9] = attempts;
   }
   double lrp = lam2 - lrr - lpp;
   double lam = std::sqrt(lam2);
@@ -1244,6 +1290,111 @@ int rbmpp_iteration(rbmpp_ctx* c, int precision, double delta_tau, double s_fact
   return 0;
 }
 
+int rbmpp_set_trace(rbmpp_ctx* c, int max_records) {
+  if (!c || max_records < 0) return RBMPP_E_ARG;
+  if (c->W.trace) {
+    CK(cudaFree(c->W.trace));
+    c->W.trace = nullptr;
+  }
+  c->d.trace_max = 0;
+  if (max_records == 0) return 0;
+  const size_t n = (size_t)c->d.nw * max_records * 6;
+  int r = dalloc(c, &c->W.trace, n);
+  if (r) return r;
+  CK(cudaMemset(c->W.trace, 0, sizeof(double) * n));
+  c->d.trace_max = max_records;
+  return 0;
+}
+
+int rbmpp_set_replay(rbmpp_ctx* c, const int* decisions, int max_checkpoints) {
+  if (!c || max_checkpoints < 0 || (max_checkpoints > 0 && !decisions)) return RBMPP_E_ARG;
+  if (c->W.replay) {
+    CK(cudaFree((void*)c->W.replay));
+    c->W.replay = nullptr;
+  }
+  c->d.replay_max = 0;
+  if (max_checkpoints == 0) return 0;
+  const size_t n = (size_t)c->d.nw * max_checkpoints * 2;
+  for (size_t k = 0; k < n; k += 2)
+    if (decisions[k] < 1 || decisions[k] > 100 || (decisions[k + 1] != 0 && decisions[k + 1] != 1))
+      return fail(c, RBMPP_E_ARG, "replay decision %zu out of range (Nfastup %d, extra draw %d)", k / 2,
+                  decisions[k], decisions[k + 1]);
+  int* p = nullptr;
+  int r = dalloc(c, &p, n);
+  if (r) return r;
+  c->W.replay = p;
+  CK(cudaMemcpy(p, decisions, sizeof(int) * n, cudaMemcpyHostToDevice));
+  c->d.replay_max = max_checkpoints;
+  return 0;
+}
+
+int rbmpp_debug_hook(rbmpp_ctx* c, int what, int value) {
+  if (!c || value < 0) return RBMPP_E_ARG;
+  switch (what) {
+    case 1: c->d.skip_load = value; break;
+    case 2: c->d.wait_polls = value; break;
+    default: return fail(c, RBMPP_E_ARG, "unknown debug hook %d", what);
+  }
+  return 0;
+}
+
+int rbmpp_get_walker_events(const rbmpp_ctx* cc, int* events, double* trace) {
+  rbmpp_ctx* c = const_cast<rbmpp_ctx*>(cc);
+  if (!c) return RBMPP_E_ARG;
+  if (events) CK(cudaMemcpy(events, c->W.events, sizeof(int) * 5 * c->d.nw, cudaMemcpyDeviceToHost));
+  if (trace && c->W.trace)
+    CK(cudaMemcpy(trace, c->W.trace, sizeof(double) * 6 * c->d.trace_max * c->d.nw, cudaMemcpyDeviceToHost));
+  return 0;
+}
+
+int rbmpp_copy_state(rbmpp_ctx* dst, const rbmpp_ctx* src) {
+  if (!dst || !src || dst == src) return RBMPP_E_ARG;
+  rbmpp_ctx* c = dst;  // errors are reported on the destination context
+  const DevDims &a = dst->d, &b = src->d;
+  if (a.L != b.L || a.n_mp != b.n_mp || a.alphar != b.alphar || a.n_slater != b.n_slater || a.nw != b.nw ||
+      a.ns != b.ns || dst->dims.device != src->dims.device)
+    return fail(dst, RBMPP_E_ARG, "copy_state: the two contexts differ in shape or device");
+  if (!src->tables_set || !dst->tables_set) return fail(dst, RBMPP_E_STATE, "copy_state: tables must be set on both");
+  const size_t nw = a.nw, ns = a.ns, N = a.N;
+  const DevWalkers &S = src->W, &D = dst->W;
+  CK(cudaStreamSynchronize(src->st));
+  auto cp = [&](void* d, const void* s, size_t bytes) -> cudaError_t {
+    return cudaMemcpyAsync(d, s, bytes, cudaMemcpyDeviceToDevice, dst->st);
+  };
+  CK(cp(D.x, S.x, nw * N));
+  CK(cp(D.idx, S.idx, 2 * nw * N));
+  CK(cp(D.cfg, S.cfg, 2 * nw * N));
+  CK(cp(D.th, S.th, 8 * nw * std::max(1, a.Mr)));
+  CK(cp(D.sgn, S.sgn, nw * a.n_mp));
+  CK(cp(D.pf, S.pf, 8 * nw * a.n_qp));
+  CK(cp(D.psi, S.psi, 16 * nw * a.n_qp));
+  CK(cp(D.Y, S.Y, 8 * nw * a.n_qp * (size_t)a.Np * a.Np));
+  CK(cp(D.mt, S.mt, 4 * nw * 625));
+  CK(cp(D.nfastup, S.nfastup, 4 * nw));
+  CK(cp(D.naccept, S.naccept, 4 * nw));
+  CK(cp(D.nacc_all, S.nacc_all, 4 * nw));
+  CK(cp(D.xs, S.xs, nw * ns * N));
+  CK(cp(D.pfs, S.pfs, 8 * nw * ns * a.n_qp));
+  CK(cp(D.psis, S.psis, 16 * nw * ns * (a.n_qp + 1)));
+  CK(cp(D.events, S.events, 4 * 5 * nw));
+  CK(cudaStreamSynchronize(dst->st));
+  dst->Wr = src->Wr;
+  dst->br = src->br;
+  dst->slater = src->slater;
+  dst->shift = src->shift;
+  dst->params_set = src->params_set;
+  dst->seeded = src->seeded;
+  dst->sampled = src->sampled;
+  dst->measured = false;
+  dst->S_valid = false;
+  dst->naccept_total = src->naccept_total;
+  dst->iteration = src->iteration;
+  dst->s_factor0 = src->s_factor0;
+  dst->s_factor_init = src->s_factor_init;
+  std::memcpy(dst->wf_av_list, src->wf_av_list, sizeof(dst->wf_av_list));
+  return src->params_set ? upload_params(dst) : 0;
+}
+
 int rbmpp_get_walker_state(const rbmpp_ctx* cc, int* nfastup, int* nacc_all) {
   rbmpp_ctx* c = const_cast<rbmpp_ctx*>(cc);
   if (!c) return RBMPP_E_ARG;
@@ -1254,7 +1405,7 @@ int rbmpp_get_walker_state(const rbmpp_ctx* cc, int* nfastup, int* nacc_all) {
 
 int rbmpp_get_stats(const rbmpp_ctx* c, double* out, int n) {
   if (!c || !out || n < 0) return RBMPP_E_ARG;
-  for (int k = 0; k < n && k < 8; k++) out[k] = c->stats[k];
+  for (int k = 0; k < n && k < 10; k++) out[k] = c->stats[k];
   return 0;
 }
 
@@ -1571,10 +1722,6 @@ constexpr size_t kNoAllocBytes = kNoAllocBad + 256;
 
 static __device__ __align__(256) unsigned char g_eval_scratch[kNoAllocBytes];
 
-// Device address of g_eval_scratch on each device, looked up on the first call there.
-std::mutex g_noalloc_mu;
-void* g_noalloc_addr[64] = {};
-
 // Records n - i for the first configuration i whose status is non-zero (atomicMax keeps the smallest i).
 __global__ void first_bad_kernel(const int* status, int n, int* bad) {
   int i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -1582,20 +1729,14 @@ __global__ void first_bad_kernel(const int* status, int n, int* bad) {
 }
 
 int noalloc_run(rbmpp_ctx* c, int n, const int* d_x, double* d_psi, double* d_hpsi, double* d_O) {
-  const int dev = c->dims.device;
-  unsigned char* base = nullptr;
-  {
-    std::lock_guard<std::mutex> lock(g_noalloc_mu);
-    if (!g_noalloc_addr[dev]) {
-      void* p = nullptr;
-      cudaError_t e = cudaGetSymbolAddress(&p, g_eval_scratch);
-      if (e != cudaSuccess || !p)
-        return fail(c, RBMPP_E_CUDA, "cudaGetSymbolAddress(g_eval_scratch) on device %d: %s", dev,
-                    cudaGetErrorString(e));
-      g_noalloc_addr[dev] = p;
-    }
-    base = (unsigned char*)g_noalloc_addr[dev];
-  }
+  // the array's device address on the current device, looked up on every call (a cheap runtime query that
+  // stays right if the host code resets the device between calls)
+  void* p = nullptr;
+  cudaError_t e = cudaGetSymbolAddress(&p, g_eval_scratch);
+  if (e != cudaSuccess || !p)
+    return fail(c, RBMPP_E_CUDA, "cudaGetSymbolAddress(g_eval_scratch) on device %d: %s", c->dims.device,
+                cudaGetErrorString(e));
+  unsigned char* base = (unsigned char*)p;
   int8_t* x8 = (int8_t*)base;
   int* status = (int*)(base + kNoAllocStatus);
   int* bad = (int*)(base + kNoAllocBad);
@@ -1631,6 +1772,9 @@ extern "C" int rbmpp_eval_configs_noalloc(rbmpp_ctx* c, int n, const int* d_x, d
   if (c->dims.device < 0 || c->dims.device >= 64)
     return fail(c, RBMPP_E_ARG, "eval_configs_noalloc: device ordinal %d outside 0..63", c->dims.device);
   if (!c->params_set) return fail(c, RBMPP_E_STATE, "set_params must come first");
+  if (!c->est_fits)
+    return fail(c, RBMPP_E_ARG, "the estimator's workspace for N/2 = %d exceeds the shared memory of one block",
+                c->d.Np);
   if (n == 0) return 0;
   // the scratch address and every launch belong to the context's device: make it current for the call
   int prev = -1;

@@ -28,6 +28,11 @@ struct DevDims {
   int orb_injective;  // Orbital_Idx is injective within each spin block for one projection
   int pf_sign;        // (-1)^{Np(Np-1)/2}
   int gj_global;      // the direct sampler's Gauss-Jordan tile lives in DevWalkers::gj (too large for SMEM)
+  int trace_max;      // records per walker of DevWalkers::trace (0: no chain trace)
+  int replay_max;     // checkpoint decisions per walker in DevWalkers::replay (0: none)
+  int skip_load;      // verification hook: walker 0 of the streaming sampler never issues its load number
+                      //   skip_load (1-based), so the wait on it runs out (0: off)
+  int wait_polls;     // poll bound of the streaming sampler's pipeline waits (0: the default 2^22)
   double J1, J2, shift;
   double sp_cc[2], sp_cs[2], sp_ss[2], para_sp[2];
 };
@@ -66,6 +71,15 @@ struct DevWalkers {
   double* pfs;     // [w][s][n_qp]
   double* psis;    // [w][s][n_qp+1][2]
   double* gj;      // [w][Np][Np+1] Gauss-Jordan scratch when DevDims::gj_global, else null
+  int* events;     // [w][5] last make_sample: global flips tried, flips accepted, make_initial_x re-seeds,
+                   //        Nfastup checkpoints (make_sample.f90:135-158, :61, :74-128), trace records
+  double* trace;   // [w][trace_max][6] chain trace in draw order (null when trace_max = 0); records:
+                   //   {0, i1, i2, ratio^2, u, accepted}   exchange proposal (make_sample.f90:160-220)
+                   //   {1, i0, inverse drift, Pf drift, Nfastup before, after}   checkpoint (:74-128)
+                   //   {2, 0, 0, ratio^2, u, accepted}     global spin flip (:135-158)
+                   //   {3, 0, 0, 0, 0, 0}                  make_initial_x re-seed of a continued chain (:61)
+  const int* replay;  // [w][replay_max][2] verification replay of checkpoint decisions {Nfastup after, extra
+                      //   draw of :122}, used in place of the drift test for the first replay_max checkpoints
 };
 
 // One context of a batched launch (several lattices / couplings in one kernel)

@@ -1,7 +1,7 @@
 // linalg.cu -- FP64 dense kernels of the SR step: the S = O^T O build (the dgemm of
-// calc_phys_quantity.f90:240), the blocked Cholesky solve that replaces pdposv('U')
-// (SR_pdposv.f90:232), GEMVs over the O matrix, and the element-wise SR conditioning
-// (SR_pdposv.f90:1-170).  Matrices are column-major (Fortran layout), S is Nv x Nv.
+// calc_phys_quantity.f90:240) and the GEMM of the Cholesky's trailing update (sr_solve.cu holds the rest of
+// the solve that replaces pdposv('U'), SR_pdposv.f90:232), GEMVs over the O matrix, and the element-wise SR
+// conditioning (SR_pdposv.f90:1-170).  Matrices are column-major (Fortran layout), S is Nv x Nv.
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -103,117 +103,6 @@ __global__ void symmetrize_kernel(int n, double* S) {
     int i = bj * 32 + tx, j = bi * 32 + r;  // lower element (i, j) = upper (j, i)
     int ui = bi * 32 + r, uj = bj * 32 + tx;
     if (i < n && j < n && ui < uj) S[(long long)i + (long long)n * j] = tile[tx][r];
-  }
-}
-
-// ---- blocked Cholesky (upper: A = U^T U), panel width NB ----
-constexpr int NB = 64;
-
-// factor the NB x NB diagonal block at k0 in place (unblocked, one CTA)
-__global__ void potrf_diag_kernel(int n, double* A, long long lda, int k0, int* info) {
-  __shared__ double T[NB][NB + 1];
-  const int nb = min(NB, n - k0);
-  const int tid = threadIdx.x;
-  for (int e = tid; e < nb * nb; e += blockDim.x) {
-    int i = e % nb, j = e / nb;
-    T[i][j] = A[(long long)(k0 + i) + lda * (k0 + j)];
-  }
-  __syncthreads();
-  for (int k = 0; k < nb; k++) {
-    // T(k,k) = sqrt(T(k,k) - sum_{p<k} T(p,k)^2) already applied by the trailing updates
-    if (tid == 0) {
-      double d = T[k][k];
-      if (!(d > 0.0)) {
-        if (*info == 0) *info = k0 + k + 1;
-        d = 1.0;
-      }
-      T[k][k] = sqrt(d);
-    }
-    __syncthreads();
-    double dkk = T[k][k];
-    for (int j = k + 1 + tid; j < nb; j += blockDim.x) T[k][j] = T[k][j] / dkk;
-    __syncthreads();
-    for (int e = tid; e < (nb - k - 1) * (nb - k - 1); e += blockDim.x) {
-      int i = k + 1 + e % (nb - k - 1), j = k + 1 + e / (nb - k - 1);
-      if (i <= j) T[i][j] = T[i][j] - T[k][i] * T[k][j];
-    }
-    __syncthreads();
-  }
-  for (int e = tid; e < nb * nb; e += blockDim.x) {
-    int i = e % nb, j = e / nb;
-    if (i <= j) A[(long long)(k0 + i) + lda * (k0 + j)] = T[i][j];
-  }
-}
-
-// U(k0:k0+nb, j) = U_kk^{-T} A(k0:k0+nb, j) for j >= k0 + nb (one warp per column)
-__global__ void trsm_panel_kernel(int n, double* A, long long lda, int k0) {
-  __shared__ double U[NB][NB + 1];
-  const int nb = min(NB, n - k0);
-  for (int e = threadIdx.x; e < nb * nb; e += blockDim.x) {
-    int i = e % nb, j = e / nb;
-    U[i][j] = (i <= j) ? A[(long long)(k0 + i) + lda * (k0 + j)] : 0.0;
-  }
-  __syncthreads();
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
-  for (int j = k0 + nb + blockIdx.x * nwarps + warp; j < n; j += gridDim.x * nwarps) {
-    double* col = A + lda * j + k0;
-    // forward substitution: x_i = (b_i - sum_{p<i} U(p,i) x_p) / U(i,i); lanes hold x in chunks
-    double x0 = (lane < nb) ? col[lane] : 0.0;
-    double x1 = (lane + 32 < nb) ? col[lane + 32] : 0.0;
-    for (int i = 0; i < nb; i++) {
-      double xi_own = (i < 32) ? x0 : x1;
-      double xi = __shfl_sync(0xffffffffu, xi_own, i & 31) / U[i][i];
-      if (lane == (i & 31)) {
-        if (i < 32) x0 = xi;
-        else x1 = xi;
-      }
-      // subtract from later rows
-      if (lane > i && lane < nb) x0 -= U[i][lane] * xi;
-      if (lane + 32 > i && lane + 32 < nb) x1 -= U[i][lane + 32] * xi;
-    }
-    if (lane < nb) col[lane] = x0;
-    if (lane + 32 < nb) col[lane + 32] = x1;
-  }
-}
-
-// blocked triangular solves on one right-hand side b (n): forward U^T y = b, then back U x = y.
-// One CTA per diagonal block, then a GEMV update of the remaining rows.
-__global__ void trsv_diag_kernel(int n, const double* A, long long lda, double* b, int k0, int upper_t) {
-  __shared__ double x[NB];
-  const int nb = min(NB, n - k0);
-  if (threadIdx.x == 0) {
-    if (upper_t) {  // solve U_kk^T y = b_k (forward)
-      for (int i = 0; i < nb; i++) {
-        double s = b[k0 + i];
-        for (int p = 0; p < i; p++) s -= A[(long long)(k0 + p) + lda * (k0 + i)] * x[p];
-        x[i] = s / A[(long long)(k0 + i) + lda * (k0 + i)];
-      }
-    } else {  // solve U_kk x = y_k (backward)
-      for (int i = nb - 1; i >= 0; i--) {
-        double s = b[k0 + i];
-        for (int p = i + 1; p < nb; p++) s -= A[(long long)(k0 + i) + lda * (k0 + p)] * x[p];
-        x[i] = s / A[(long long)(k0 + i) + lda * (k0 + i)];
-      }
-    }
-    for (int i = 0; i < nb; i++) b[k0 + i] = x[i];
-  }
-}
-
-// forward: b(j) -= sum_{p in blk} U(p, j) x(p) for j >= k0+nb ; backward: b(i) -= sum_{p in blk} U(i, p) x(p) for i < k0
-__global__ void trsv_update_kernel(int n, const double* A, long long lda, double* b, int k0, int upper_t) {
-  const int nb = min(NB, n - k0);
-  if (upper_t) {
-    int j = k0 + nb + blockIdx.x * blockDim.x + threadIdx.x;
-    if (j >= n) return;
-    double s = 0.0;
-    for (int p = 0; p < nb; p++) s += A[(long long)(k0 + p) + lda * j] * b[k0 + p];
-    b[j] -= s;
-  } else {
-    int i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= k0) return;
-    double s = 0.0;
-    for (int p = 0; p < nb; p++) s += A[(long long)i + lda * (k0 + p)] * b[k0 + p];
-    b[i] -= s;
   }
 }
 
@@ -381,45 +270,15 @@ cudaError_t rbmpp_symmetrize(int n, double* S, cudaStream_t st) {
   return cudaGetLastError();
 }
 
-// In-place Cholesky of the upper triangle; *d_info = 0 or the failing column (1-based).
-cudaError_t rbmpp_potrf_upper(int n, double* A, int* d_info, cudaStream_t st) {
-  cudaMemsetAsync(d_info, 0, sizeof(int), st);
-  for (int k0 = 0; k0 < n; k0 += NB) {
-    rbmpp_note_launch();
-    potrf_diag_kernel<<<1, 256, 0, st>>>(n, A, n, k0, d_info);
-    int rest = n - (k0 + NB);
-    if (rest > 0) {
-      int blocks = min(1024, (rest + 7) / 8);
-      rbmpp_note_launch();
-      trsm_panel_kernel<<<blocks, 256, 0, st>>>(n, A, n, k0);
-      int nt = (rest + BM - 1) / BM;
-      rbmpp_note_launch();
-      gemm_atb_upper<true><<<nt * (nt + 1) / 2, 256, 0, st>>>(n, NB, A + k0, 1, n, -1.0, 1.0, A, n, k0 + NB);
-    }
-  }
-  return cudaGetLastError();
-}
-
-// b <- A^{-1} b with A = U^T U (upper factor in A)
-cudaError_t rbmpp_potrs_upper(int n, const double* A, double* b, cudaStream_t st) {
-  for (int k0 = 0; k0 < n; k0 += NB) {
-    rbmpp_note_launch();
-    trsv_diag_kernel<<<1, 32, 0, st>>>(n, A, n, b, k0, 1);
-    int rest = n - (k0 + NB);
-    if (rest > 0) {
-      rbmpp_note_launch();
-      trsv_update_kernel<<<(rest + 255) / 256, 256, 0, st>>>(n, A, n, b, k0, 1);
-    }
-  }
-  int last = ((n - 1) / NB) * NB;
-  for (int k0 = last; k0 >= 0; k0 -= NB) {
-    rbmpp_note_launch();
-    trsv_diag_kernel<<<1, 32, 0, st>>>(n, A, n, b, k0, 0);
-    if (k0 > 0) {
-      rbmpp_note_launch();
-      trsv_update_kernel<<<(k0 + 255) / 256, 256, 0, st>>>(n, A, n, b, k0, 0);
-    }
-  }
+// C(i, j) += alpha * sum_k A(k, i) A(k, j) on the upper triangle of rows and columns >= row0 (the trailing
+// update of the blocked Cholesky in sr_solve.cu; K = its panel width, A(k, i) contiguous in k)
+cudaError_t rbmpp_gemm_atb_upper_acc(int n, int K, const double* A, long long sk, long long si, double alpha,
+                                     double* C, long long ldc, int row0, cudaStream_t st) {
+  const int rest = n - row0;
+  if (rest <= 0) return cudaSuccess;
+  const int nt = (rest + BM - 1) / BM;
+  rbmpp_note_launch();
+  gemm_atb_upper<true><<<nt * (nt + 1) / 2, 256, 0, st>>>(n, K, A, sk, si, alpha, 1.0, C, ldc, row0);
   return cudaGetLastError();
 }
 

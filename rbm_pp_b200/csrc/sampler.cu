@@ -163,7 +163,10 @@ __device__ __forceinline__ void sampler_body(const DevDims& d, const DevTables& 
   const int N = d.N, Np = d.Np;
 
   for (int k = tid; k < 625; k += blockDim.x) s.mt[k] = W.mt[(size_t)w * 625 + k];
-  if (tid == 0) status(c) = 0;
+  if (tid == 0) {
+    status(c) = 0;
+    events_reset(s);
+  }
   __syncthreads();
   int nfastup = W.nfastup[w];
 
@@ -174,7 +177,11 @@ __device__ __forceinline__ void sampler_body(const DevDims& d, const DevTables& 
     __syncthreads();
     full_state(c);
     if (!status(c)) {
-      if (tid == 0) s.iflag[F_AUX] = grnd(s.mt) < 0.05;
+      if (tid == 0) {
+        s.iflag[F_AUX] = grnd(s.mt) < 0.05;  // make_sample.f90:61
+        s.iflag[F_EV_RESEED] += s.iflag[F_AUX];
+        if (s.iflag[F_AUX] && W.trace) trace_rec(c, 3, 0.0, 0.0, 0.0, 0.0, 0.0);
+      }
       __syncthreads();
       if (s.iflag[F_AUX]) make_initial_x(c);
     }
@@ -183,12 +190,15 @@ __device__ __forceinline__ void sampler_body(const DevDims& d, const DevTables& 
   int naccept = 0, nacc_tmp = 0, nacc_all = 0;
   for (int i0 = -d.nwarm; i0 <= d.ns && !status(c); i0++) {
     if (nacc_tmp > nfastup) {
-      checkpoint(c, nfastup);
+      checkpoint(c, nfastup, i0);
       if (status(c)) break;
       nacc_tmp = 0;
     }
     for (int iu = 0; iu < d.nupdate; iu++) {
-      if (tid == 0) s.iflag[F_FLIP] = grnd(s.mt) < 3.0e-4;
+      if (tid == 0) {
+        s.iflag[F_FLIP] = grnd(s.mt) < 3.0e-4;  // make_sample.f90:135
+        s.iflag[F_EV_FLIP] += s.iflag[F_FLIP];
+      }
       __syncthreads();
       if (s.iflag[F_FLIP]) {
         global_flip(c);
@@ -248,7 +258,9 @@ __device__ __forceinline__ void sampler_body(const DevDims& d, const DevTables& 
         s.dsc[D_PSIPI] = im;
         (void)grnd(s.mt);  // sub.f90:72
         double r1 = (hypot(re, im) + d.shift) / (hypot(s.dsc[D_PSI0R], s.dsc[D_PSI0I]) + d.shift);
-        s.iflag[F_ACCEPT] = grnd(s.mt) < r1 * r1;  // make_sample.f90:203-204
+        const double u = grnd(s.mt);
+        s.iflag[F_ACCEPT] = u < r1 * r1;  // make_sample.f90:203-204
+        if (W.trace) trace_rec(c, 0, (double)i1, (double)i2, r1 * r1, u, (double)s.iflag[F_ACCEPT]);
       }
       __syncthreads();
       if (s.iflag[F_ACCEPT]) {  // make_sample.f90:205-219
@@ -318,6 +330,7 @@ __device__ __forceinline__ void sampler_body(const DevDims& d, const DevTables& 
     W.naccept[w] = naccept;
     W.nacc_all[w] = nacc_all;
     W.status[w] = status(c);
+    events_store(c);
   }
 }
 

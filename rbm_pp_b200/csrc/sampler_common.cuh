@@ -201,9 +201,23 @@ __device__ __forceinline__ void make_initial_x(const SCtx& c) {
   __syncthreads();
 }
 
-// Nfastup checkpoint make_sample.f90:74-128
+// One record of the optional chain trace (thread 0 only; see DevWalkers::trace).
+__device__ __forceinline__ void trace_rec(const SCtx& c, int type, double a, double b, double x, double u, double e) {
+  const int k = c.s.iflag[F_EV_TRACE]++;
+  if (c.W.trace && k < c.d.trace_max) {
+    double* r = c.W.trace + ((size_t)c.w * c.d.trace_max + k) * 6;
+    r[0] = (double)type;
+    r[1] = a;
+    r[2] = b;
+    r[3] = x;
+    r[4] = u;
+    r[5] = e;
+  }
+}
+
+// Nfastup checkpoint make_sample.f90:74-128.  i0 (sweep) only labels the trace record.
 template <int KPL = 0, int NP = 0>
-__device__ __forceinline__ void checkpoint(const SCtx& c, int& nfastup) {
+__device__ __forceinline__ void checkpoint(const SCtx& c, int& nfastup, int i0) {
   const DevDims& d = c.d;
   const WS& s = c.s;
   for (int j = threadIdx.x; j < d.Mr; j += blockDim.x) s.thp[j] = s.th[j];
@@ -241,14 +255,22 @@ __device__ __forceinline__ void checkpoint(const SCtx& c, int& nfastup) {
     double dpf = -1.0;
     for (int qp = 0; qp < d.n_qp; qp++) dpf = fmax(dpf, fabs(s.pfp[qp] - s.pf[qp]) / r2);
     double dinv = s.dsc[D_DIFFINV];
+    const int nf0 = nfastup;
+    const int k = s.iflag[F_EV_CKPT]++;
     (void)grnd(s.mt);  // make_sample.f90:116
-    if (dinv > 1.0e-5 || dpf > 1.0e-5) {
+    if (c.W.replay && k < d.replay_max) {
+      // verification replay: the decision of this checkpoint is given (Nfastup after, extra draw)
+      const int* rp = c.W.replay + ((size_t)c.w * d.replay_max + k) * 2;
+      nfastup = rp[0];
+      if (rp[1]) (void)grnd(s.mt);
+    } else if (dinv > 1.0e-5 || dpf > 1.0e-5) {
       nfastup = max(1, (int)floor((double)nfastup / 1.2 + 0.5));
       if (dinv > 10.0 && dpf > 10.0) (void)grnd(s.mt);  // make_sample.f90:122
     } else {
       nfastup = min(100, (int)floor((double)nfastup * 1.1 + 0.5));
     }
     s.iflag[F_AUX] = nfastup;
+    if (c.W.trace) trace_rec(c, 1, (double)i0, dinv, dpf, (double)nf0, (double)nfastup);
   }
   __syncthreads();
   nfastup = s.iflag[F_AUX];
@@ -280,9 +302,12 @@ __device__ __forceinline__ void global_flip(const SCtx& c) {
   cta_amplitude(d, c.t, s, s.thp, s.pfp, s.sgnp, s.psip, D_PSIPR);
   if (threadIdx.x == 0) {
     double r1 = (hypot(s.dsc[D_PSIPR], s.dsc[D_PSIPI]) + d.shift) / (hypot(s.dsc[D_PSI0R], s.dsc[D_PSI0I]) + d.shift);
-    int acc = grnd(s.mt) < r1 * r1;
+    const double u = grnd(s.mt);
+    const int acc = u < r1 * r1;
+    if (c.W.trace) trace_rec(c, 2, 0.0, 0.0, r1 * r1, u, (double)acc);
     if (acc) (void)grnd(s.mt);  // make_sample.f90:146
     s.iflag[F_ACCEPT] = acc;
+    s.iflag[F_EV_FLIPACC] += acc;
   }
   __syncthreads();
   if (!s.iflag[F_ACCEPT]) return;
@@ -305,6 +330,21 @@ __device__ __forceinline__ void global_flip(const SCtx& c) {
   cta_scratch_all<KPL, NP>(c, s.idx, s.pf, true, false);  // Tmp_Inv_M of the accepted flipped state
 }
 
+
+// event counters of one make_sample: reset at its start (thread 0), stored with the walker state at its end
+__device__ __forceinline__ void events_reset(const WS& s) {
+  s.iflag[F_EV_FLIP] = s.iflag[F_EV_FLIPACC] = s.iflag[F_EV_RESEED] = s.iflag[F_EV_CKPT] = s.iflag[F_EV_TRACE] = 0;
+}
+__device__ __forceinline__ void events_store(const SCtx& c) {
+  if (c.W.events) {
+    int* e = c.W.events + (size_t)c.w * 5;
+    e[0] = c.s.iflag[F_EV_FLIP];
+    e[1] = c.s.iflag[F_EV_FLIPACC];
+    e[2] = c.s.iflag[F_EV_RESEED];
+    e[3] = c.s.iflag[F_EV_CKPT];
+    e[4] = c.s.iflag[F_EV_TRACE];
+  }
+}
 
 // make_spin_flip_candidate make_sample.f90:244-294 (thread 0): writes F_I1/F_I2 or sets ST_CANDIDATE
 __device__ __forceinline__ void candidate_search(const SCtx& c) {

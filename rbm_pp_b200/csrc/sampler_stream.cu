@@ -309,6 +309,13 @@ struct Pipe {
   int last_issued[16];  // per stage: last tile index loaded (thread 0 only), -1 if none
 };
 
+// Verification hook: walker 0 never issues load number skip_load (1-based over the launch), so the consumer's
+// bounded wait on it runs out and the CTA takes its timeout path.  The load is not recorded as issued.
+__device__ __forceinline__ bool skipped_load(const SCtx& c, uint32_t T) {
+  return c.d.skip_load > 0 && c.w == 0 && T + 1 == (uint32_t)c.d.skip_load;
+}
+__device__ __forceinline__ int wait_polls(const SCtx& c) { return c.d.wait_polls > 0 ? c.d.wait_polls : (1 << 22); }
+
 // producer (thread 0): first min(ST, n_qp) loads of a pass.  Every store of the previous pass has
 // completed: the consumer that issued it waited for it before the pass-ending barrier.
 __device__ __forceinline__ void pass_issue_first(const SCtx& c, const Stream& sm, Pipe& pp) {
@@ -318,6 +325,7 @@ __device__ __forceinline__ void pass_issue_first(const SCtx& c, const Stream& sm
   for (int t = 0; t < n0; t++) {
     uint32_t T = pp.T0 + t;
     int s = (int)(T % sm.ST);
+    if (skipped_load(c, T)) continue;
     mbar_arrive_expect_tx(&sm.full[s], sm.tile_bytes);
     bulk_load(sm.stage + (size_t)s * NN, c.Yw + (size_t)t * NN, sm.tile_bytes, &sm.full[s]);
     pp.last_issued[s] = (int)T;
@@ -331,8 +339,9 @@ __device__ __forceinline__ bool pass_produce(const SCtx& c, const Stream& sm, Pi
   for (int t = ST; t < n; t++) {
     uint32_t T = pp.T0 + t, Tp = T - ST;
     int s = (int)(T % ST);
-    if (!mbar_wait(&sm.empty[s], (Tp / ST) & 1u)) return false;
+    if (!mbar_wait(&sm.empty[s], (Tp / ST) & 1u, wait_polls(c))) return false;
     if (*abort_flag) return false;
+    if (skipped_load(c, T)) continue;
     mbar_arrive_expect_tx(&sm.full[s], sm.tile_bytes);
     bulk_load(sm.stage + (size_t)s * NN, c.Yw + (size_t)t * NN, sm.tile_bytes, &sm.full[s]);
     pp.last_issued[s] = (int)T;
@@ -428,7 +437,7 @@ __device__ __forceinline__ bool pass_consume(const SCtx& c, const Stream& sm, co
       if (tn < n) gather_regs<KPL, NP>(d, c.p, tn, s.idx, mk, gk);
     }
     __syncwarp();
-    bool bad = (*abort_flag != 0) || !mbar_wait(&sm.full[st], (T / sm.ST) & 1u);
+    bool bad = (*abort_flag != 0) || !mbar_wait(&sm.full[st], (T / sm.ST) & 1u, wait_polls(c));
     double* Y = sm.stage + (size_t)st * NN;
     if (pend) {
       if (update_half<KPL, NP>(d, Y, mk, ck, U0, V0, g, h, my_acc, other_acc, pS, pA, bad)) return false;
@@ -575,7 +584,10 @@ __global__ void __launch_bounds__(kWarps * 32, 1)
   int pass_id = 0;
 
   for (int k = tid; k < 625; k += blockDim.x) s.mt[k] = W.mt[(size_t)w * 625 + k];
-  if (tid == 0) status(c) = 0;
+  if (tid == 0) {
+    status(c) = 0;
+    events_reset(s);
+  }
   __syncthreads();
   int nfastup = W.nfastup[w];
 
@@ -586,7 +598,11 @@ __global__ void __launch_bounds__(kWarps * 32, 1)
     __syncthreads();
     full_state<KPL, NP>(c);
     if (!status(c)) {
-      if (tid == 0) s.iflag[F_AUX] = grnd(s.mt) < 0.05;
+      if (tid == 0) {
+        s.iflag[F_AUX] = grnd(s.mt) < 0.05;  // make_sample.f90:61
+        s.iflag[F_EV_RESEED] += s.iflag[F_AUX];
+        if (s.iflag[F_AUX] && W.trace) trace_rec(c, 3, 0.0, 0.0, 0.0, 0.0, 0.0);
+      }
       __syncthreads();
       if (s.iflag[F_AUX]) make_initial_x<KPL, NP>(c);
     }
@@ -601,12 +617,15 @@ __global__ void __launch_bounds__(kWarps * 32, 1)
       }
       drain(c);
       if (status(c)) break;
-      checkpoint<KPL, NP>(c, nfastup);
+      checkpoint<KPL, NP>(c, nfastup, i0);
       if (status(c)) break;
       nacc_tmp = 0;
     }
     for (int iu = 0; iu < d.nupdate; iu++) {
-      if (tid == 0) s.iflag[F_FLIP] = grnd(s.mt) < 3.0e-4;
+      if (tid == 0) {
+        s.iflag[F_FLIP] = grnd(s.mt) < 3.0e-4;  // make_sample.f90:135
+        s.iflag[F_EV_FLIP] += s.iflag[F_FLIP];
+      }
       __syncthreads();
       if (s.iflag[F_FLIP]) {
         drain(c);
@@ -631,7 +650,9 @@ __global__ void __launch_bounds__(kWarps * 32, 1)
         s.dsc[D_PSIPI] = im;
         (void)grnd(s.mt);  // sub.f90:72
         double r1 = (hypot(re, im) + d.shift) / (hypot(s.dsc[D_PSI0R], s.dsc[D_PSI0I]) + d.shift);
-        s.iflag[F_ACCEPT] = grnd(s.mt) < r1 * r1;  // make_sample.f90:203-204
+        const double u = grnd(s.mt);
+        s.iflag[F_ACCEPT] = u < r1 * r1;  // make_sample.f90:203-204
+        if (W.trace) trace_rec(c, 0, (double)i1, (double)i2, r1 * r1, u, (double)s.iflag[F_ACCEPT]);
       }
       __syncthreads();
       if (s.iflag[F_ACCEPT]) {  // make_sample.f90:205-219; the Y update is deferred to the next pass
@@ -704,6 +725,7 @@ __global__ void __launch_bounds__(kWarps * 32, 1)
     W.naccept[w] = naccept;
     W.nacc_all[w] = nacc_all;
     W.status[w] = status(c);
+    events_store(c);
   }
 }
 

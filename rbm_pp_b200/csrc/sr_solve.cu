@@ -1,0 +1,566 @@
+// sr_solve.cu -- the solve of the SR step on the device: the blocked Cholesky factorisation and the two
+// triangular solves that replace pdposv('U') (SR_pdposv.f90:200-249), the exact S applied matrix-free through
+// the per-sample derivatives O (S_raw x = O^T (O x), calc_phys_quantity.f90:240), and the vector steps of the
+// preconditioned conjugate-gradient refinement that uses both.  Matrices are column-major (Fortran layout).
+//
+// Cholesky (upper, A = U^T U, in place), panels of NB = 128 columns:
+//   potrf_block_kernel   one CTA factors the NB x NB diagonal block in shared memory (32-column sub-panels:
+//                        a warp factors each 32 x 32 diagonal piece in registers) and writes U_kk and its
+//                        inverse U_kk^{-1} (kept for the panel solve and for every later triangular solve);
+//   panel_kernel         U_kj = U_kk^{-T} A_kj, one warp per column j;
+//   gemm_atb_upper<true> (linalg.cu) the trailing update A_22 -= U_12^T U_12.
+// Triangular solves: one launch per block step; every CTA applies the inverted diagonal block to the block's
+// right-hand side (redundantly, from L2) and then updates its share of the rest of the vector.
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+void rbmpp_note_launch();  // capi.cu: counts kernel launches
+cudaError_t rbmpp_gemm_atb_upper_acc(int n, int K, const double* A, long long sk, long long si, double alpha,
+                                     double* C, long long ldc, int row0, cudaStream_t st);
+cudaError_t rbmpp_gemv_ot(int, int, const double*, const double*, const double*, double*, double*, double*, int,
+                          cudaStream_t);
+cudaError_t rbmpp_gemv_o(int, int, const double*, const double*, double*, cudaStream_t);
+
+namespace {
+
+constexpr int NB = 128;
+
+__device__ __forceinline__ double wsum(double v) {
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+  return v;
+}
+
+// ---------------------------------------------------------------------------------------------------
+// Diagonal block: Cholesky of the nb x nb block at (k0, k0) and the inverse of its factor.
+// T (shared, column-major, ld NB + 1) holds the block; warp 0 factors each 32 x 32 diagonal piece with the
+// piece's column c in lane c, then all warps solve the piece's row panel and update the trailing triangle.
+// ---------------------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(512, 1)
+    potrf_block_kernel(int n, double* __restrict__ A, long long lda, int k0, double* __restrict__ dinv,
+                       int* __restrict__ info) {
+  extern __shared__ double T[];  // [NB][NB + 1] column-major: T[i + (NB + 1) j]
+  constexpr int LD = NB + 1;
+  const int nb = min(NB, n - k0);
+  const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, nwarps = blockDim.x >> 5;
+  for (int e = tid; e < nb * nb; e += blockDim.x) {
+    const int i = e % nb, j = e / nb;
+    T[i + LD * j] = (i <= j) ? A[(long long)(k0 + i) + lda * (k0 + j)] : 0.0;
+  }
+  __syncthreads();
+  for (int p0 = 0; p0 < nb; p0 += 32) {
+    const int pw = min(32, nb - p0);
+    // (1) 32 x 32 piece in registers: col[r] = T(p0 + r, p0 + lane)
+    if (warp == 0) {
+      double col[32];
+#pragma unroll
+      for (int r = 0; r < 32; r++) col[r] = (r < pw && lane < pw) ? T[(p0 + r) + LD * (p0 + lane)] : 0.0;
+#pragma unroll
+      for (int k = 0; k < 32; k++) {
+        if (k < pw) {
+          double dkk = __shfl_sync(0xffffffffu, col[k], k);
+          if (!(dkk > 0.0)) {
+            if (lane == 0 && *info == 0) *info = k0 + p0 + k + 1;
+            dkk = 1.0;
+          }
+          const double ukk = sqrt(dkk);
+          // row k of U: U(k, c) = T(k, c) / U(k, k) for c > k (lane c), U(k, k) on lane k
+          double ukc = col[k] / ukk;
+          if (lane == k) ukc = ukk;
+          if (lane >= k) col[k] = ukc;
+          // rows r > k of columns c >= r: T(r, c) -= U(k, r) U(k, c)
+#pragma unroll
+          for (int r = k + 1; r < 32; r++) {
+            const double ukr = __shfl_sync(0xffffffffu, ukc, r);
+            if (lane > k && lane >= r) col[r] -= ukr * ukc;
+          }
+        }
+      }
+#pragma unroll
+      for (int r = 0; r < 32; r++)
+        if (r < pw && lane < pw && r <= lane) T[(p0 + r) + LD * (p0 + lane)] = col[r];
+    }
+    __syncthreads();
+    // (2) row panel: U(p0:p0+pw, c) = U_pp^{-T} T(p0:p0+pw, c) for c >= p0 + pw, one warp per column
+    for (int c = p0 + pw + warp; c < nb; c += nwarps) {
+      double x = (lane < pw) ? T[(p0 + lane) + LD * c] : 0.0;
+      for (int r = 0; r < pw; r++) {
+        const double xr = __shfl_sync(0xffffffffu, x, r) / T[(p0 + r) + LD * (p0 + r)];
+        if (lane == r) x = xr;
+        if (lane > r && lane < pw) x -= T[(p0 + r) + LD * (p0 + lane)] * xr;
+      }
+      if (lane < pw) T[(p0 + lane) + LD * c] = x;
+    }
+    __syncthreads();
+    // (3) trailing triangle: T(i, j) -= sum_r U(p0 + r, i) U(p0 + r, j) for p0 + pw <= i <= j
+    const int m = nb - (p0 + pw);
+    for (int e = tid; e < m * m; e += blockDim.x) {
+      const int i = p0 + pw + e % m, j = p0 + pw + e / m;
+      if (i <= j) {
+        double s = T[i + LD * j];
+        for (int r = 0; r < pw; r++) s -= T[(p0 + r) + LD * i] * T[(p0 + r) + LD * j];
+        T[i + LD * j] = s;
+      }
+    }
+    __syncthreads();
+  }
+  for (int e = tid; e < nb * nb; e += blockDim.x) {
+    const int i = e % nb, j = e / nb;
+    if (i <= j) A[(long long)(k0 + i) + lda * (k0 + j)] = T[i + LD * j];
+  }
+  // V = U_kk^{-1} (upper): column c solves U v = e_c by back substitution, one warp per column;
+  // lane holds rows lane + 32 q of the column
+  double* V = dinv;  // [NB][NB] column-major, ld NB
+  for (int c = warp; c < NB; c += nwarps) {
+    double v[NB / 32];
+#pragma unroll
+    for (int q = 0; q < NB / 32; q++) v[q] = 0.0;
+    if (c < nb) {
+      for (int i = c; i >= 0; i--) {
+        double s = 0.0;
+#pragma unroll
+        for (int q = 0; q < NB / 32; q++) {
+          const int j = lane + 32 * q;
+          if (j > i && j <= c) s += T[i + LD * j] * v[q];
+        }
+        s = wsum(s);
+        const double vi = ((i == c ? 1.0 : 0.0) - s) / T[i + LD * i];
+#pragma unroll
+        for (int q = 0; q < NB / 32; q++)
+          if (lane + 32 * q == i) v[q] = vi;
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < NB / 32; q++) V[(lane + 32 * q) + NB * c] = (c < nb && lane + 32 * q < nb) ? v[q] : 0.0;
+  }
+}
+
+// U(k0:k0+nb, j) = U_kk^{-T} A(k0:k0+nb, j) for j >= k0 + nb: out_p = sum_{q <= p} V(q, p) a_q.
+// One warp per column; V transposed in shared memory so the lanes read consecutive p.
+__global__ void __launch_bounds__(512) panel_kernel(int n, double* __restrict__ A, long long lda, int k0,
+                                                    const double* __restrict__ dinv) {
+  extern __shared__ double VT[];  // VT[p + NB q] = V(q, p)
+  const int nb = min(NB, n - k0);
+  for (int e = threadIdx.x; e < NB * NB; e += blockDim.x) {
+    const int q = e % NB, p = e / NB;
+    VT[p + NB * q] = dinv[e];  // dinv[q + NB p] = V(q, p)
+  }
+  __syncthreads();
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
+  for (int j = k0 + nb + blockIdx.x * nwarps + warp; j < n; j += gridDim.x * nwarps) {
+    double* col = A + lda * j + k0;
+    double a[NB / 32], out[NB / 32];
+#pragma unroll
+    for (int q = 0; q < NB / 32; q++) {
+      a[q] = (lane + 32 * q < nb) ? col[lane + 32 * q] : 0.0;
+      out[q] = 0.0;
+    }
+#pragma unroll
+    for (int t0 = 0; t0 < NB / 32; t0++) {
+      for (int ql = 0; ql < 32; ql++) {
+        const int qq = 32 * t0 + ql;
+        const double aq = __shfl_sync(0xffffffffu, a[t0], ql);
+#pragma unroll
+        for (int t = 0; t < NB / 32; t++) {
+          const int p = lane + 32 * t;
+          if (p >= qq && p < nb && qq < nb) out[t] = fma(VT[p + NB * qq], aq, out[t]);
+        }
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < NB / 32; q++)
+      if (lane + 32 * q < nb) col[lane + 32 * q] = out[q];
+  }
+}
+
+// ---------------------------------------------------------------------------------------------------
+// Triangular solves with the inverted diagonal blocks.  Forward U^T y = b: y_k = V_k^T b_k, then
+// b_j -= U(k-block, j) . y_k for j beyond the block (one warp per j, coalesced column reads).  Backward
+// U x = y: x_k = V_k y_k, then y_i -= U(i, k-block) . x_k for i < k0 (one thread per i, coalesced).
+// Every CTA forms y_k (or x_k) itself; the block's result goes to a separate vector so no CTA reads what
+// another one writes within the step.
+// ---------------------------------------------------------------------------------------------------
+__global__ void __launch_bounds__(256) trsv_fwd_step(int n, const double* __restrict__ A, long long lda, int k0,
+                                                     const double* __restrict__ V, double* __restrict__ b,
+                                                     double* __restrict__ y) {
+  __shared__ double sb[NB], sy[NB];
+  const int nb = min(NB, n - k0);
+  for (int p = threadIdx.x; p < nb; p += blockDim.x) sb[p] = b[k0 + p];
+  __syncthreads();
+  // sy[p] = sum_{q <= p} V(q, p) sb[q]: warp per p, lanes over q
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
+  for (int p = warp; p < nb; p += nwarps) {
+    double s = 0.0;
+    for (int q = lane; q <= p; q += 32) s = fma(V[q + NB * p], sb[q], s);
+    s = wsum(s);
+    if (lane == 0) sy[p] = s;
+  }
+  __syncthreads();
+  if (blockIdx.x == 0)
+    for (int p = threadIdx.x; p < nb; p += blockDim.x) y[k0 + p] = sy[p];
+  for (int j = k0 + nb + blockIdx.x * nwarps + warp; j < n; j += gridDim.x * nwarps) {
+    const double* col = A + lda * j + k0;
+    double s = 0.0;
+    for (int p = lane; p < nb; p += 32) s = fma(col[p], sy[p], s);
+    s = wsum(s);
+    if (lane == 0) b[j] -= s;
+  }
+}
+
+__global__ void __launch_bounds__(256) trsv_bwd_step(int n, const double* __restrict__ A, long long lda, int k0,
+                                                     const double* __restrict__ V, double* __restrict__ y,
+                                                     double* __restrict__ x) {
+  __shared__ double sb[NB], sx[NB];
+  const int nb = min(NB, n - k0);
+  for (int p = threadIdx.x; p < nb; p += blockDim.x) sb[p] = y[k0 + p];
+  __syncthreads();
+  // sx[p] = sum_{q >= p} V(p, q) sb[q]: thread per p (consecutive p read consecutive V entries)
+  for (int p = threadIdx.x; p < nb; p += blockDim.x) {
+    double s = 0.0;
+    for (int q = p; q < nb; q++) s = fma(V[p + NB * q], sb[q], s);
+    sx[p] = s;
+  }
+  __syncthreads();
+  if (blockIdx.x == 0)
+    for (int p = threadIdx.x; p < nb; p += blockDim.x) x[k0 + p] = sx[p];
+  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < k0; i += gridDim.x * blockDim.x) {
+    double s = 0.0;
+    for (int p = 0; p < nb; p++) s = fma(A[(long long)i + lda * (k0 + p)], sx[p], s);
+    y[i] -= s;
+  }
+}
+
+// ---------------------------------------------------------------------------------------------------
+// z = O^T (O y) in one pass over O (ns rows of nv FP64): each CTA keeps y and its partial z in shared memory
+// and takes groups of kRows rows; the second read of a group's rows (z += t_r O_r) hits L2.  zpart[block][k];
+// the partials are summed in block order afterwards, so the result does not depend on scheduling.
+// ---------------------------------------------------------------------------------------------------
+constexpr int kGramThreads = 512, kRows = 4;
+
+template <bool VEC>
+__global__ void __launch_bounds__(kGramThreads, 1)
+    gram_apply_kernel(int ns, int nv, const double* __restrict__ O, const double* __restrict__ y,
+                      double* __restrict__ zpart) {
+  extern __shared__ double sh[];
+  double* ys = sh;
+  double* zs = sh + nv;
+  double* red = zs + nv;  // [2][kRows][32]
+  const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+  constexpr int nwarps = kGramThreads / 32;
+  for (int k = tid; k < nv; k += kGramThreads) {
+    ys[k] = y[k];
+    zs[k] = 0.0;
+  }
+  __syncthreads();
+  const int ngroups = (ns + kRows - 1) / kRows;
+  int buf = 0;
+  for (int gi = blockIdx.x; gi < ngroups; gi += gridDim.x, buf ^= 1) {
+    const int s0 = gi * kRows, nr = min(kRows, ns - s0);
+    const double* Og = O + (size_t)s0 * nv;
+    double d[kRows];
+#pragma unroll
+    for (int r = 0; r < kRows; r++) d[r] = 0.0;
+    if (VEC) {
+      const int nh = nv >> 1;
+      for (int k2 = tid; k2 < nh; k2 += kGramThreads) {
+        const double2 yk = reinterpret_cast<const double2*>(ys)[k2];
+#pragma unroll
+        for (int r = 0; r < kRows; r++)
+          if (r < nr) {
+            const double2 o = reinterpret_cast<const double2*>(Og + (size_t)r * nv)[k2];
+            d[r] = fma(o.x, yk.x, d[r]);
+            d[r] = fma(o.y, yk.y, d[r]);
+          }
+      }
+    } else {
+      for (int k = tid; k < nv; k += kGramThreads) {
+        const double yk = ys[k];
+#pragma unroll
+        for (int r = 0; r < kRows; r++)
+          if (r < nr) d[r] = fma(Og[(size_t)r * nv + k], yk, d[r]);
+      }
+    }
+#pragma unroll
+    for (int r = 0; r < kRows; r++) {
+      const double v = wsum(d[r]);
+      if (lane == 0) red[(buf * kRows + r) * 32 + warp] = v;
+    }
+    __syncthreads();
+    double t[kRows];
+#pragma unroll
+    for (int r = 0; r < kRows; r++) {
+      double a = 0.0;
+      for (int w = 0; w < nwarps; w++) a += red[(buf * kRows + r) * 32 + w];
+      t[r] = a;
+    }
+    if (VEC) {
+      const int nh = nv >> 1;
+      for (int k2 = tid; k2 < nh; k2 += kGramThreads) {
+        double2 z = reinterpret_cast<double2*>(zs)[k2];
+#pragma unroll
+        for (int r = 0; r < kRows; r++)
+          if (r < nr) {
+            const double2 o = __ldcs(reinterpret_cast<const double2*>(Og + (size_t)r * nv) + k2);
+            z.x = fma(t[r], o.x, z.x);
+            z.y = fma(t[r], o.y, z.y);
+          }
+        reinterpret_cast<double2*>(zs)[k2] = z;
+      }
+    } else {
+      for (int k = tid; k < nv; k += kGramThreads) {
+        double z = zs[k];
+#pragma unroll
+        for (int r = 0; r < kRows; r++)
+          if (r < nr) z = fma(t[r], Og[(size_t)r * nv + k], z);
+        zs[k] = z;
+      }
+    }
+  }
+  __syncthreads();
+  for (int k = tid; k < nv; k += kGramThreads) zpart[(size_t)blockIdx.x * nv + k] = zs[k];
+}
+
+__global__ void sum_blocks(int nv, int nparts, const double* __restrict__ part, double* __restrict__ out) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= nv) return;
+  double a = 0.0;
+  for (int c = 0; c < nparts; c++) a += part[(size_t)c * nv + k];
+  out[k] = a;
+}
+
+// ---------------------------------------------------------------------------------------------------
+// Vector steps of the refinement (one CTA of 1024 threads over the nv-vectors; sums in a fixed order).
+// The conditioned matrix of SR_pdposv.f90:4-170 is A = D (S_raw / norm - m m^T) D + sigma I, with
+// D = diag(1 on the RBM block, scal on the Pfaffian block) and m = Ovec / norm.
+// ---------------------------------------------------------------------------------------------------
+enum { SC_MX = 0, SC_RZ = 1, SC_RR = 2, SC_PAP = 3, SC_GG = 4, SC_ALPHA = 5 };
+
+__device__ double block_sum(double v, double* red) {
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+  v = wsum(v);
+  __syncthreads();
+  if (lane == 0) red[warp] = v;
+  __syncthreads();
+  double a = 0.0;
+  for (int w = 0; w < nw; w++) a += red[w];
+  return a;
+}
+
+// xs = D x, sc[SC_MX] = m . xs
+__global__ void __launch_bounds__(1024) sr_pre_kernel(int nv, int nrbm, const double* __restrict__ x, double scal,
+                                                      const double* __restrict__ m, double* __restrict__ xs,
+                                                      double* __restrict__ sc) {
+  __shared__ double red[32];
+  double a = 0.0;
+  for (int k = threadIdx.x; k < nv; k += blockDim.x) {
+    const double v = k < nrbm ? x[k] : x[k] * scal;
+    xs[k] = v;
+    a = fma(m[k], v, a);
+  }
+  a = block_sum(a, red);
+  if (threadIdx.x == 0) sc[SC_MX] = a;
+}
+
+// y = D (z / norm - m sc[SC_MX]) + sigma x
+__global__ void sr_post_kernel(int nv, int nrbm, const double* __restrict__ z, const double* __restrict__ m,
+                               const double* __restrict__ sc, const double* __restrict__ x, double scal, double sigma,
+                               double norm, double* __restrict__ y) {
+  const int k = blockIdx.x * blockDim.x + threadIdx.x;
+  if (k >= nv) return;
+  const double v = z[k] / norm - m[k] * sc[SC_MX];
+  y[k] = (k < nrbm ? v : v * scal) + sigma * x[k];
+}
+
+// r = g - Ax; sc[SC_GG] = g.g, sc[SC_RR] = r.r
+__global__ void __launch_bounds__(1024) pcg_start_kernel(int nv, const double* __restrict__ g,
+                                                         const double* __restrict__ ax, double* __restrict__ r,
+                                                         double* __restrict__ sc) {
+  __shared__ double red[32];
+  double gg = 0.0, rr = 0.0;
+  for (int k = threadIdx.x; k < nv; k += blockDim.x) {
+    const double v = g[k] - ax[k];
+    r[k] = v;
+    gg = fma(g[k], g[k], gg);
+    rr = fma(v, v, rr);
+  }
+  gg = block_sum(gg, red);
+  rr = block_sum(rr, red);
+  if (threadIdx.x == 0) {
+    sc[SC_GG] = gg;
+    sc[SC_RR] = rr;
+  }
+}
+
+// mode 0: p = z, rz = r.z (first direction); mode 1: rz' = r.z, p = z + (rz' / rz) p
+__global__ void __launch_bounds__(1024) pcg_dir_kernel(int nv, const double* __restrict__ r,
+                                                       const double* __restrict__ z, double* __restrict__ p,
+                                                       double* __restrict__ sc, int mode) {
+  __shared__ double red[32];
+  double a = 0.0;
+  for (int k = threadIdx.x; k < nv; k += blockDim.x) a = fma(r[k], z[k], a);
+  a = block_sum(a, red);
+  const double beta = mode ? a / sc[SC_RZ] : 0.0;
+  for (int k = threadIdx.x; k < nv; k += blockDim.x) p[k] = mode ? fma(beta, p[k], z[k]) : z[k];
+  __syncthreads();
+  if (threadIdx.x == 0) sc[SC_RZ] = a;
+}
+
+// alpha = rz / (p.Ap) (0 when p.Ap <= 0); x += alpha p; r -= alpha Ap; sc[SC_RR] = r.r; sc[SC_PAP] = p.Ap
+__global__ void __launch_bounds__(1024) pcg_step_kernel(int nv, const double* __restrict__ p,
+                                                        const double* __restrict__ ap, double* __restrict__ x,
+                                                        double* __restrict__ r, double* __restrict__ sc) {
+  __shared__ double red[32];
+  double a = 0.0;
+  for (int k = threadIdx.x; k < nv; k += blockDim.x) a = fma(p[k], ap[k], a);
+  const double pap = block_sum(a, red);
+  const double alpha = pap > 0.0 ? sc[SC_RZ] / pap : 0.0;
+  double rr = 0.0;
+  for (int k = threadIdx.x; k < nv; k += blockDim.x) {
+    x[k] = fma(alpha, p[k], x[k]);
+    const double v = fma(-alpha, ap[k], r[k]);
+    r[k] = v;
+    rr = fma(v, v, rr);
+  }
+  rr = block_sum(rr, red);
+  if (threadIdx.x == 0) {
+    sc[SC_PAP] = pap;
+    sc[SC_ALPHA] = alpha;
+    sc[SC_RR] = rr;
+  }
+}
+
+int sm_count() {
+  static int n = 0;
+  if (!n) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev);
+    if (n <= 0) n = 148;
+  }
+  return n;
+}
+
+}  // namespace
+
+// ---------------------------------------------------------------------------------------------------
+// host entry points
+// ---------------------------------------------------------------------------------------------------
+int rbmpp_chol_blocks(int n) { return (n + NB - 1) / NB; }
+int rbmpp_chol_nb() { return NB; }
+
+// In-place Cholesky of the upper triangle of A (n x n, lda = n); dinv: rbmpp_chol_blocks(n) * NB * NB doubles
+// of inverted diagonal factor blocks; *d_info = 0 or the first failing column (1-based).
+cudaError_t rbmpp_potrf_upper(int n, double* A, double* dinv, int* d_info, cudaStream_t st) {
+  cudaError_t e = cudaMemsetAsync(d_info, 0, sizeof(int), st);
+  if (e) return e;
+  const size_t smem = (size_t)NB * (NB + 1) * sizeof(double);
+  if ((e = cudaFuncSetAttribute(potrf_block_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem))) return e;
+  const size_t psmem = (size_t)NB * NB * sizeof(double);
+  if ((e = cudaFuncSetAttribute(panel_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psmem))) return e;
+  const int nsm = sm_count();
+  for (int k0 = 0, kb = 0; k0 < n; k0 += NB, kb++) {
+    double* V = dinv + (size_t)kb * NB * NB;
+    rbmpp_note_launch();
+    potrf_block_kernel<<<1, 512, smem, st>>>(n, A, n, k0, V, d_info);
+    const int rest = n - (k0 + NB);
+    if (rest > 0) {
+      const int blocks = min(nsm, (rest + 15) / 16);
+      rbmpp_note_launch();
+      panel_kernel<<<blocks, 512, psmem, st>>>(n, A, n, k0, V);
+      if ((e = rbmpp_gemm_atb_upper_acc(n, NB, A + k0, 1, n, -1.0, A, n, k0 + NB, st))) return e;
+    }
+  }
+  return cudaGetLastError();
+}
+
+// b <- A^{-1} b with A = U^T U (upper factor in A, inverted diagonal blocks in dinv); tmp: n doubles
+cudaError_t rbmpp_potrs_upper(int n, const double* A, const double* dinv, double* b, double* tmp, cudaStream_t st) {
+  const int nsm = sm_count();
+  const int nblk = rbmpp_chol_blocks(n);
+  for (int kb = 0; kb < nblk; kb++) {  // U^T y = b: y in tmp, b consumed
+    const int k0 = kb * NB, rest = n - (k0 + NB);
+    const int blocks = rest > 0 ? min(nsm, (rest + 7) / 8) : 1;
+    rbmpp_note_launch();
+    trsv_fwd_step<<<blocks, 256, 0, st>>>(n, A, n, k0, dinv + (size_t)kb * NB * NB, b, tmp);
+  }
+  for (int kb = nblk - 1; kb >= 0; kb--) {  // U x = y: x in b, tmp consumed
+    const int k0 = kb * NB;
+    const int blocks = k0 > 0 ? min(nsm, (k0 + 255) / 256) : 1;
+    rbmpp_note_launch();
+    trsv_bwd_step<<<blocks, 256, 0, st>>>(n, A, n, k0, dinv + (size_t)kb * NB * NB, tmp, b);
+  }
+  return cudaGetLastError();
+}
+
+// Partial-sum buffer of rbmpp_gram_apply: rbmpp_gram_parts() * nv doubles.
+int rbmpp_gram_parts() { return sm_count(); }
+
+// Largest nv the one-pass kernel takes (its shared memory holds two nv-vectors).
+int rbmpp_gram_max_nv() {
+  int dev = 0, maxsm = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+  return (maxsm / (int)sizeof(double) - 2 * kRows * 32) / 2;
+}
+
+// z = O^T (O y): O is ns x nv (row per sample).  part: rbmpp_gram_parts() * nv doubles.  When two
+// nv-vectors do not fit one block's shared memory, two passes: tmp_ns = O y, then O^T tmp_ns through
+// part64 (64 * nv doubles).
+cudaError_t rbmpp_gram_apply(int ns, int nv, const double* O, const double* y, double* z, double* part,
+                             double* tmp_ns, double* part64, cudaStream_t st) {
+  cudaError_t e;
+  if (nv > rbmpp_gram_max_nv()) {
+    if ((e = rbmpp_gemv_o(ns, nv, O, y, tmp_ns, st))) return e;
+    return rbmpp_gemv_ot(ns, nv, O, tmp_ns, nullptr, z, nullptr, part64, 64, st);
+  }
+  const int nb = rbmpp_gram_parts();
+  const size_t smem = (size_t)(2 * nv + 2 * kRows * 32) * sizeof(double);
+  const bool vec = (nv % 2) == 0 && ((uintptr_t)O % 16) == 0;
+  if (vec) {
+    if ((e = cudaFuncSetAttribute(gram_apply_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)))
+      return e;
+    rbmpp_note_launch();
+    gram_apply_kernel<true><<<nb, kGramThreads, smem, st>>>(ns, nv, O, y, part);
+  } else {
+    if ((e = cudaFuncSetAttribute(gram_apply_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)))
+      return e;
+    rbmpp_note_launch();
+    gram_apply_kernel<false><<<nb, kGramThreads, smem, st>>>(ns, nv, O, y, part);
+  }
+  rbmpp_note_launch();
+  sum_blocks<<<(nv + 255) / 256, 256, 0, st>>>(nv, nb, part, z);
+  return cudaGetLastError();
+}
+
+// y = A x with A = D (S_raw / norm - m m^T) D + sigma I applied through O; ws, z: nv doubles each;
+// sc: device scalars
+cudaError_t rbmpp_sr_apply(int ns, int nv, int nrbm, const double* O, const double* m, double norm, double scal,
+                           double sigma, const double* x, double* y, double* ws, double* z, double* part,
+                           double* tmp_ns, double* part64, double* sc, cudaStream_t st) {
+  rbmpp_note_launch();
+  sr_pre_kernel<<<1, 1024, 0, st>>>(nv, nrbm, x, scal, m, ws, sc);
+  cudaError_t e = rbmpp_gram_apply(ns, nv, O, ws, z, part, tmp_ns, part64, st);
+  if (e) return e;
+  rbmpp_note_launch();
+  sr_post_kernel<<<(nv + 255) / 256, 256, 0, st>>>(nv, nrbm, z, m, sc, x, scal, sigma, norm, y);
+  return cudaGetLastError();
+}
+
+cudaError_t rbmpp_pcg_start(int nv, const double* g, const double* ax, double* r, double* sc, cudaStream_t st) {
+  rbmpp_note_launch();
+  pcg_start_kernel<<<1, 1024, 0, st>>>(nv, g, ax, r, sc);
+  return cudaGetLastError();
+}
+
+cudaError_t rbmpp_pcg_dir(int nv, const double* r, const double* z, double* p, double* sc, int mode, cudaStream_t st) {
+  rbmpp_note_launch();
+  pcg_dir_kernel<<<1, 1024, 0, st>>>(nv, r, z, p, sc, mode);
+  return cudaGetLastError();
+}
+
+cudaError_t rbmpp_pcg_step(int nv, const double* p, const double* ap, double* x, double* r, double* sc,
+                           cudaStream_t st) {
+  rbmpp_note_launch();
+  pcg_step_kernel<<<1, 1024, 0, st>>>(nv, p, ap, x, r, sc);
+  return cudaGetLastError();
+}

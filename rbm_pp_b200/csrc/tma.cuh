@@ -32,8 +32,8 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
 
 // Bounded wait: returns false after ~2^22 polls (each poll suspends for a hardware-chosen time), so a
 // broken pipeline ends with an error status instead of a hung GPU.
-__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
-  for (int it = 0; it < (1 << 22); it++)
+__device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity, int polls = (1 << 22)) {
+  for (int it = 0; it < polls; it++)
     if (mbar_try_wait(bar, parity)) return true;
   return false;
 }

@@ -44,6 +44,12 @@ struct WS {
 #define F_PIV 5
 #define F_SINGULAR 6
 #define F_AUX 7
+// per-walker event counters of one make_sample (written to DevWalkers::events)
+#define F_EV_FLIP 8
+#define F_EV_FLIPACC 9
+#define F_EV_RESEED 10
+#define F_EV_CKPT 11
+#define F_EV_TRACE 12
 // shared double slots
 #define D_DET 0
 #define D_PVAL 1

@@ -69,6 +69,16 @@ class SRRunner:
         self.book = Bookkeeping(inp, ctx.N)
         self._bufs = None
 
+    @classmethod
+    def attach(cls, ctx: "capi.Context", problem, precision=capi.SR_FP64):
+        """A one-GPU runner over a context whose state is already set (seeded, parameters loaded, possibly
+        copied from another context with Context.copy_state_from): it continues from that state."""
+        r = cls.__new__(cls)
+        r.ctx, r.p, r.world, r.rank, r.precision, r.iteration = ctx, problem, 1, 0, precision, 0
+        r.book = Bookkeeping(problem.inp, ctx.N)
+        r._bufs = None
+        return r
+
     def step(self):
         import torch
         inp = self.p.inp

@@ -360,7 +360,7 @@ int main(int argc, char** argv) {
   d.walker_offset = 0;
   Lib lib;
   lib.ck(rbmpp_create(&d, &lib.c), "rbmpp_create");
-  lib.ck(rbmpp_set_tables(lib.c, in.W_map.data(), in.para.data(), in.orbital_idx.data(), nullptr), "set_tables");
+  lib.ck(rbmpp_set_tables(lib.c, in.W_map.data(), in.para.data(), in.orbital_idx.data(), nullptr, nullptr, nullptr), "set_tables");
   lib.ck(rbmpp_seed_walkers(lib.c, (int)seed), "seed_walkers");
   // initialize_parameters (parameter.f90:21-41): rank 0 draws U(-0.05, 0.05); W.input overrides
   std::vector<double> u((size_t)in.alphar * (N + 1));

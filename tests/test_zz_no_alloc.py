@@ -58,3 +58,26 @@ def test_noalloc_matches_eval_configs_on_consecutive_calls():
         g.eval_configs_noalloc(MAX_CONFIGS + 1, d_x.data_ptr(), 0, 0, 0)
     assert ei.value.code == 1 and "scratch limit" in str(ei.value)
     g.close()
+
+
+def test_noalloc_refuses_what_eval_configs_refuses():
+    """A lattice whose estimator workspace does not fit one block's shared memory is refused with the
+    same code and message as the allocating entry point, before any device work."""
+    import torch
+
+    p = fm.synthetic_problem(18, translations=False, alphar=1, nsample=1, seed=3)
+    g = capi.Context(p, n_walkers=1, nsample_per_walker=1)
+    g.set_params(p.br, p.Wr, p.slater, 0.0)
+    x = _configs(g.N, 1, 1)
+    try:
+        g.eval_configs(x, want_h=True)
+    except capi.RbmppError as e:
+        want = e
+    else:
+        want = None
+    if want is not None:
+        d_x = torch.from_numpy(x.reshape(-1)).to(torch.device("cuda", 0))
+        with pytest.raises(capi.RbmppError) as ei:
+            g.eval_configs_noalloc(1, d_x.data_ptr(), 0, 0, 0)
+        assert ei.value.code == want.code and str(ei.value) == str(want)
+    g.close()
