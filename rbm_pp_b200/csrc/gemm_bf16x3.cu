@@ -202,15 +202,19 @@ __global__ void __launch_bounds__(128, 1)
   }
 }
 
-// H^T and L^T ([nv_pad][k_pad] BF16) from O (ns x nv FP64, row per sample); zero padding
-__global__ void split_transpose_kernel(int ns, int nv, const double* __restrict__ O, __nv_bfloat16* __restrict__ hiT,
+// H^T and L^T ([nv_pad][k_pad] BF16) from O (ns x nv FP64, row per sample), centred when b and m are given:
+// O'(s, k) = O(s, k) - b_s m_k; zero padding
+__global__ void split_transpose_kernel(int ns, int nv, const double* __restrict__ O, const double* __restrict__ b,
+                                       const double* __restrict__ m, __nv_bfloat16* __restrict__ hiT,
                                        __nv_bfloat16* __restrict__ loT, int k_pad) {
   __shared__ double tile[32][33];
   const int s0 = blockIdx.x * 32, k0 = blockIdx.y * 32;
   const int tx = threadIdx.x, ty = threadIdx.y;  // 32 x 8
   for (int r = ty; r < 32; r += 8) {
     const int s = s0 + r, k = k0 + tx;
-    tile[r][tx] = (s < ns && k < nv) ? O[(size_t)s * nv + k] : 0.0;
+    double o = (s < ns && k < nv) ? O[(size_t)s * nv + k] : 0.0;
+    if (b && s < ns && k < nv) o = fma(-b[s], m[k], o);
+    tile[r][tx] = o;
   }
   __syncthreads();
   for (int r = ty; r < 32; r += 8) {
@@ -282,11 +286,12 @@ void rbmpp_bf16x3_pads(int ns, int nv, int* k_pad, int* nv_pad) {
   *nv_pad = (nv + BN - 1) / BN * BN;
 }
 
-// Upper triangle and exact diagonal of S = O^T O (column-major nv x nv) in split-BF16 form.
+// Upper triangle of S = O'^T O' in split-BF16 form, with O' = O - b m^T when b and m are given (else O' = O),
+// and the exact FP64 diagonal of O^T O (uncentred).  Column-major nv x nv.
 // hi, lo: nv_pad * k_pad BF16 each (16-byte aligned); part: kDiagChunks * nv doubles; d_err: one int,
 // set to 1 by a device wait that ran out.  Returns 0, 1 (no tensor-map encoder) or a CUDA error + 100.
-int rbmpp_syrk_bf16x3(int ns, int nv, const double* O, void* hi, void* lo, int* d_err, double* S, double* part,
-                      cudaStream_t st) {
+int rbmpp_syrk_bf16x3(int ns, int nv, const double* O, const double* b, const double* m, void* hi, void* lo,
+                      int* d_err, double* S, double* part, cudaStream_t st) {
   int k_pad = 0, nv_pad = 0;
   rbmpp_bf16x3_pads(ns, nv, &k_pad, &nv_pad);
   CUtensorMap mh, ml;
@@ -295,7 +300,7 @@ int rbmpp_syrk_bf16x3(int ns, int nv, const double* O, void* hi, void* lo, int* 
   if (e) return 100 + (int)e;
   rbmpp_note_launch();
   split_transpose_kernel<<<dim3(k_pad / 32, nv_pad / 32), dim3(32, 8), 0, st>>>(
-      ns, nv, O, (__nv_bfloat16*)hi, (__nv_bfloat16*)lo, k_pad);
+      ns, nv, O, b, m, (__nv_bfloat16*)hi, (__nv_bfloat16*)lo, k_pad);
   if ((e = cudaGetLastError())) return 100 + (int)e;
   if ((e = cudaFuncSetAttribute(syrk_bf16x3_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)SMEM_BYTES)))
     return 100 + (int)e;

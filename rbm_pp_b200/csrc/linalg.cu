@@ -164,6 +164,15 @@ __global__ void sr_form_kernel(int n, double* S, double norm, const double* ov) 
   S[e] = S[e] / norm - ov[i] * ov[j];
 }
 
+// the same from a centred split S: S(i, j) = S_c(i, j) / norm off the diagonal (S_c = sum of centred
+// products, the m m^T term already inside), S(k, k) = S_raw(k, k) / norm - m_k^2 from the exact raw diagonal
+__global__ void sr_form_centred_kernel(int n, double* S, double norm, const double* ov) {
+  long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (e >= (long long)n * n) return;
+  int i = (int)(e % n), j = (int)(e / n);
+  S[e] = (i == j) ? S[e] / norm - ov[i] * ov[i] : S[e] / norm;
+}
+
 // PP-block scaling (SR_pdposv.f90:56-73): columns k2 > Nv_RBM, then rows k1 > Nv_RBM
 __global__ void sr_scale_kernel(int n, int nrbm, double* S, double f) {
   long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -314,6 +323,13 @@ cudaError_t rbmpp_sr_form(int n, double* S, double norm, const double* ov, cudaS
   long long tot = (long long)n * n;
   rbmpp_note_launch();
   sr_form_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(n, S, norm, ov);
+  return cudaGetLastError();
+}
+
+cudaError_t rbmpp_sr_form_centred(int n, double* S, double norm, const double* ov, cudaStream_t st) {
+  long long tot = (long long)n * n;
+  rbmpp_note_launch();
+  sr_form_centred_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(n, S, norm, ov);
   return cudaGetLastError();
 }
 

@@ -210,23 +210,43 @@ __global__ void __launch_bounds__(256) trsv_fwd_step(int n, const double* __rest
 __global__ void __launch_bounds__(256) trsv_bwd_step(int n, const double* __restrict__ A, long long lda, int k0,
                                                      const double* __restrict__ V, double* __restrict__ y,
                                                      double* __restrict__ x) {
-  __shared__ double sb[NB], sx[NB];
+  __shared__ double sb[NB], sx[NB], red[2][NB];
   const int nb = min(NB, n - k0);
   for (int p = threadIdx.x; p < nb; p += blockDim.x) sb[p] = y[k0 + p];
   __syncthreads();
-  // sx[p] = sum_{q >= p} V(p, q) sb[q]: thread per p (consecutive p read consecutive V entries)
-  for (int p = threadIdx.x; p < nb; p += blockDim.x) {
-    double s = 0.0;
-    for (int q = p; q < nb; q++) s = fma(V[p + NB * q], sb[q], s);
-    sx[p] = s;
+  // sx[p] = sum_{q >= p} V(p, q) sb[q]: two threads per p (alternate q), four independent partial sums each;
+  // consecutive p read consecutive V entries (blockDim = 2 NB)
+  {
+    const int p = threadIdx.x & (NB - 1), half = threadIdx.x / NB;
+    double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+    if (p < nb) {
+      int q = p + half;
+      for (; q + 6 < nb; q += 8) {
+        a0 = fma(V[p + NB * q], sb[q], a0);
+        a1 = fma(V[p + NB * (q + 2)], sb[q + 2], a1);
+        a2 = fma(V[p + NB * (q + 4)], sb[q + 4], a2);
+        a3 = fma(V[p + NB * (q + 6)], sb[q + 6], a3);
+      }
+      for (; q < nb; q += 2) a0 = fma(V[p + NB * q], sb[q], a0);
+    }
+    red[half][p] = (a0 + a1) + (a2 + a3);
   }
+  __syncthreads();
+  for (int p = threadIdx.x; p < nb; p += blockDim.x) sx[p] = red[0][p] + red[1][p];
   __syncthreads();
   if (blockIdx.x == 0)
     for (int p = threadIdx.x; p < nb; p += blockDim.x) x[k0 + p] = sx[p];
   for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < k0; i += gridDim.x * blockDim.x) {
-    double s = 0.0;
-    for (int p = 0; p < nb; p++) s = fma(A[(long long)i + lda * (k0 + p)], sx[p], s);
-    y[i] -= s;
+    double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
+    int p = 0;
+    for (; p + 3 < nb; p += 4) {
+      a0 = fma(A[(long long)i + lda * (k0 + p)], sx[p], a0);
+      a1 = fma(A[(long long)i + lda * (k0 + p + 1)], sx[p + 1], a1);
+      a2 = fma(A[(long long)i + lda * (k0 + p + 2)], sx[p + 2], a2);
+      a3 = fma(A[(long long)i + lda * (k0 + p + 3)], sx[p + 3], a3);
+    }
+    for (; p < nb; p++) a0 = fma(A[(long long)i + lda * (k0 + p)], sx[p], a0);
+    y[i] -= (a0 + a1) + (a2 + a3);
   }
 }
 

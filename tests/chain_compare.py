@@ -53,8 +53,9 @@ def first_divergence(ta, na, tb, nb):
 
 
 def ratio_gap(a, b):
-    """Relative difference of the two ratio^2 of an accept record pair."""
-    return abs(a[3] - b[3]) / max(abs(a[3]), abs(b[3]), 1e-300)
+    """Difference of the two acceptance probabilities min(1, ratio^2) of an accept record pair: the width of
+    the interval of u for which the two accept decisions would differ."""
+    return abs(min(1.0, a[3]) - min(1.0, b[3]))
 
 
 def compare_walkers(tr_o, ev_o, tr_g, ev_g):

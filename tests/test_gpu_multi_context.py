@@ -61,8 +61,9 @@ def test_two_shards_equal_one_context():
             assert abs(o.lambda_ - o1.lambda_) <= 1e-9 * abs(o1.lambda_)
             assert _rel(dx, dx1) < 1e-9
         for c in shards:
+            # the two summation orders of S differ by rounding, which the solve amplifies by cond(S)
             for a, b in zip(c.get_params()[:3], one.get_params()[:3]):
-                assert _rel(a, b) < 1e-10
+                assert _rel(a, b) < 1e-8
     for c in [one] + shards:
         c.close()
 
