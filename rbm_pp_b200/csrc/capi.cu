@@ -54,7 +54,8 @@ cudaError_t rbmpp_sample_scalars(int, const double*, int, const double*, double,
 void rbmpp_bf16x3_pads(int, int, int*, int*);
 int rbmpp_syrk_bf16x3(int, int, const double*, const double*, const double*, void*, void*, int*, double*, double*,
                       cudaStream_t);
-cudaError_t rbmpp_sr_form_centred(int, double*, double, const double*, cudaStream_t);
+cudaError_t rbmpp_scale_copy(int, const double*, double, double*, cudaStream_t);
+cudaError_t rbmpp_add_outer_offdiag(int, double*, const double*, double, cudaStream_t);
 int rbmpp_correlation_fits(const DevDims&, int);
 cudaError_t rbmpp_launch_correlation(const DevDims&, const DevTables&, const DevParams&, const int8_t*, int, double*,
                                      double*, double*, double*, int*, int*, cudaStream_t);
@@ -167,7 +168,7 @@ struct rbmpp_ctx {
   int stream_stages = 0;  // > 0: TMA-streamed sampler with this many stages
   bool est_fits = true;   // the estimator's workspace fits in shared memory
   // S of the current measurement: built lazily in the precision the SR step asks for
-  bool S_valid = false, S_reduced = false, S_centred = false;
+  bool S_valid = false, S_reduced = false;
   int S_prec = RBMPP_SR_FP64, meas_prec = RBMPP_SR_FP64;
 };
 
@@ -270,12 +271,12 @@ int ensure_measure_buffers(rbmpp_ctx* c) {
 
 // S_raw = sum over samples of O O^T (the dgemm of calc_phys_quantity.f90:240) for the current
 // measurement, in FP64 or as split-BF16 products on the tensor cores (exact FP64 diagonal).
-// centred (split-BF16 only): the products are of O' = O - b m^T with b the per-sample weights of Ovec and
-// m = Ovec / norm on the device in d_m, so the split products carry S itself rather than S_raw, whose
-// cancellation against m m^T would magnify their rounding; the diagonal stays the exact raw one.
-int build_S(rbmpp_ctx* c, int prec, bool centred = false, const double* d_m = nullptr) {
-  if (prec != RBMPP_SR_SPLIT_BF16) centred = false;
-  if (c->S_valid && c->S_prec == prec && c->S_centred == centred) return 0;
+// The split-BF16 form multiplies the centred derivatives O' = O - b m^T (b: the per-sample weights of Ovec,
+// m = Ovec / norm), whose products sum to S_raw - Ovec Ovec^T / norm, and adds Ovec Ovec^T / norm back in
+// FP64: the BF16 pieces then carry the fluctuations only, not the mean that S = S_raw / norm - m m^T cancels,
+// which would magnify their rounding.  The diagonal is the exact FP64 one of S_raw.
+int build_S(rbmpp_ctx* c, int prec) {
+  if (c->S_valid && c->S_prec == prec) return 0;
   if (c->S_reduced)
     return fail(c, RBMPP_E_STATE, "S was loaded by exchange_measurement in precision %d; cannot rebuild in %d",
                 c->S_prec, prec);
@@ -294,10 +295,14 @@ int build_S(rbmpp_ctx* c, int prec, bool centred = false, const double* d_m = nu
                          cudaGetErrorString(e));
       c->bytes += 2 * bytes;
     }
-    const int r = rbmpp_syrk_bf16x3(c->ns_tot, d.Nv, c->d_O, centred ? c->d_b : nullptr, centred ? d_m : nullptr,
-                                    c->d_hi, c->d_lo, c->d_err, c->d_S, c->d_part, c->st);
+    const double norm = c->meas_scal[2];
+    double* d_m = c->d_rv;  // m = Ovec / norm
+    CK(rbmpp_scale_copy(d.Nv, c->d_Ovec, 1.0 / norm, d_m, c->st));
+    const int r = rbmpp_syrk_bf16x3(c->ns_tot, d.Nv, c->d_O, c->d_b, d_m, c->d_hi, c->d_lo, c->d_err, c->d_S,
+                                    c->d_part, c->st);
     if (r == 1) return fail(c, RBMPP_E_CUDA, "cuTensorMapEncodeTiled unavailable from the driver");
     if (r) return fail(c, RBMPP_E_CUDA, "split-BF16 S build: %s", cudaGetErrorString((cudaError_t)(r - 100)));
+    CK(rbmpp_add_outer_offdiag(d.Nv, c->d_S, c->d_Ovec, 1.0 / norm, c->st));  // upper triangle only
     CK(rbmpp_symmetrize(d.Nv, c->d_S, c->st));
   } else {
     return fail(c, RBMPP_E_ARG, "unknown S precision %d", prec);
@@ -314,7 +319,6 @@ int build_S(rbmpp_ctx* c, int prec, bool centred = false, const double* d_m = nu
   c->stats[3] = ms;
   c->S_valid = true;
   c->S_prec = prec;
-  c->S_centred = centred;
   return 0;
 }
 
@@ -925,16 +929,11 @@ int rbmpp_sr_step(rbmpp_ctx* c, const rbmpp_sr_in* in, rbmpp_sr_out* out, double
   double* d_y = c->d_vec + 2 * Nv;
   double* d_diag = c->d_vec + 3 * Nv;
   CK(cudaMemcpyAsync(d_ov, ov.data(), sizeof(double) * Nv, cudaMemcpyHostToDevice, c->st));
-  // S_raw of this measurement (the dgemm of calc_phys_quantity.f90:240), the split form centred on m
-  const bool centred = in->precision == RBMPP_SR_SPLIT_BF16 && !c->S_reduced;
   {
-    int r = build_S(c, in->precision, centred, d_ov);
+    int r = build_S(c, in->precision);  // S_raw of this measurement (the dgemm of calc_phys_quantity.f90:240)
     if (r) return r;
   }
-  if (c->S_centred)
-    CK(rbmpp_sr_form_centred(Nv, c->d_S, norm, d_ov, c->st));  // :11-15 with the m m^T term inside S_c
-  else
-    CK(rbmpp_sr_form(Nv, c->d_S, norm, d_ov, c->st));  // :11-15
+  CK(rbmpp_sr_form(Nv, c->d_S, norm, d_ov, c->st));  // :11-15
   std::vector<double> dg(Nv);
   CK(rbmpp_get_diag(Nv, c->d_S, d_diag, c->st));
   CK(cudaMemcpyAsync(dg.data(), d_diag, sizeof(double) * Nv, cudaMemcpyDeviceToHost, c->st));
@@ -1233,7 +1232,6 @@ int rbmpp_exchange_measurement(rbmpp_ctx* c, int direction, double* d_S, double*
       CK(cudaMemcpyAsync(c->d_S, d_S, nS, cudaMemcpyDeviceToDevice, c->st));
       c->S_valid = true;
       c->S_reduced = true;
-      c->S_centred = false;
       c->S_prec = c->meas_prec;
     }
     if (d_g) CK(cudaMemcpyAsync(c->d_gvec, d_g, nV, cudaMemcpyDeviceToDevice, c->st));

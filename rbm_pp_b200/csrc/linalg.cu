@@ -164,13 +164,18 @@ __global__ void sr_form_kernel(int n, double* S, double norm, const double* ov) 
   S[e] = S[e] / norm - ov[i] * ov[j];
 }
 
-// the same from a centred split S: S(i, j) = S_c(i, j) / norm off the diagonal (S_c = sum of centred
-// products, the m m^T term already inside), S(k, k) = S_raw(k, k) / norm - m_k^2 from the exact raw diagonal
-__global__ void sr_form_centred_kernel(int n, double* S, double norm, const double* ov) {
+// y = f x
+__global__ void scale_copy_kernel(int n, const double* x, double f, double* y) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < n) y[i] = x[i] * f;
+}
+
+// S(i, j) += f v_i v_j on the strict upper triangle (column-major)
+__global__ void add_outer_offdiag_kernel(int n, double* S, const double* v, double f) {
   long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (e >= (long long)n * n) return;
   int i = (int)(e % n), j = (int)(e / n);
-  S[e] = (i == j) ? S[e] / norm - ov[i] * ov[i] : S[e] / norm;
+  if (i < j) S[e] = fma(f * v[i], v[j], S[e]);
 }
 
 // PP-block scaling (SR_pdposv.f90:56-73): columns k2 > Nv_RBM, then rows k1 > Nv_RBM
@@ -326,10 +331,16 @@ cudaError_t rbmpp_sr_form(int n, double* S, double norm, const double* ov, cudaS
   return cudaGetLastError();
 }
 
-cudaError_t rbmpp_sr_form_centred(int n, double* S, double norm, const double* ov, cudaStream_t st) {
+cudaError_t rbmpp_scale_copy(int n, const double* x, double f, double* y, cudaStream_t st) {
+  rbmpp_note_launch();
+  scale_copy_kernel<<<(n + 255) / 256, 256, 0, st>>>(n, x, f, y);
+  return cudaGetLastError();
+}
+
+cudaError_t rbmpp_add_outer_offdiag(int n, double* S, const double* v, double f, cudaStream_t st) {
   long long tot = (long long)n * n;
   rbmpp_note_launch();
-  sr_form_centred_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(n, S, norm, ov);
+  add_outer_offdiag_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(n, S, v, f);
   return cudaGetLastError();
 }
 

@@ -40,6 +40,7 @@ __global__ void __launch_bounds__(512, 1)
     potrf_block_kernel(int n, double* __restrict__ A, long long lda, int k0, double* __restrict__ dinv,
                        int* __restrict__ info) {
   extern __shared__ double T[];  // [NB][NB + 1] column-major: T[i + (NB + 1) j]
+  __shared__ double rdiag[NB];   // 1 / U(i, i)
   constexpr int LD = NB + 1;
   const int nb = min(NB, n - k0);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, nwarps = blockDim.x >> 5;
@@ -63,9 +64,10 @@ __global__ void __launch_bounds__(512, 1)
             if (lane == 0 && *info == 0) *info = k0 + p0 + k + 1;
             dkk = 1.0;
           }
-          const double ukk = sqrt(dkk);
+          const double ukk = sqrt(dkk), rk = 1.0 / ukk;
+          if (lane == 0) rdiag[p0 + k] = rk;
           // row k of U: U(k, c) = T(k, c) / U(k, k) for c > k (lane c), U(k, k) on lane k
-          double ukc = col[k] / ukk;
+          double ukc = col[k] * rk;
           if (lane == k) ukc = ukk;
           if (lane >= k) col[k] = ukc;
           // rows r > k of columns c >= r: T(r, c) -= U(k, r) U(k, c)
@@ -85,7 +87,7 @@ __global__ void __launch_bounds__(512, 1)
     for (int c = p0 + pw + warp; c < nb; c += nwarps) {
       double x = (lane < pw) ? T[(p0 + lane) + LD * c] : 0.0;
       for (int r = 0; r < pw; r++) {
-        const double xr = __shfl_sync(0xffffffffu, x, r) / T[(p0 + r) + LD * (p0 + r)];
+        const double xr = __shfl_sync(0xffffffffu, x, r) * rdiag[p0 + r];
         if (lane == r) x = xr;
         if (lane > r && lane < pw) x -= T[(p0 + r) + LD * (p0 + lane)] * xr;
       }
@@ -124,7 +126,7 @@ __global__ void __launch_bounds__(512, 1)
           if (j > i && j <= c) s += T[i + LD * j] * v[q];
         }
         s = wsum(s);
-        const double vi = ((i == c ? 1.0 : 0.0) - s) / T[i + LD * i];
+        const double vi = ((i == c ? 1.0 : 0.0) - s) * rdiag[i];
 #pragma unroll
         for (int q = 0; q < NB / 32; q++)
           if (lane + 32 * q == i) v[q] = vi;
@@ -198,12 +200,28 @@ __global__ void __launch_bounds__(256) trsv_fwd_step(int n, const double* __rest
   __syncthreads();
   if (blockIdx.x == 0)
     for (int p = threadIdx.x; p < nb; p += blockDim.x) y[k0 + p] = sy[p];
-  for (int j = k0 + nb + blockIdx.x * nwarps + warp; j < n; j += gridDim.x * nwarps) {
-    const double* col = A + lda * j + k0;
-    double s = 0.0;
-    for (int p = lane; p < nb; p += 32) s = fma(col[p], sy[p], s);
-    s = wsum(s);
-    if (lane == 0) b[j] -= s;
+  // b_j -= U(k-block, j) . y_k: four columns per warp at a time, all their loads issued before any sum
+  double yl[NB / 32];
+#pragma unroll
+  for (int q = 0; q < NB / 32; q++) yl[q] = (lane + 32 * q < nb) ? sy[lane + 32 * q] : 0.0;
+  const int j0 = k0 + nb, ncol = n - j0, stride = gridDim.x * nwarps;
+  for (int c0 = (blockIdx.x * nwarps + warp) * 4; c0 < ncol; c0 += stride * 4) {
+    double v[4][NB / 32];
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+      const double* col = A + lda * (j0 + c0 + u) + k0;
+#pragma unroll
+      for (int q = 0; q < NB / 32; q++)
+        v[u][q] = (c0 + u < ncol && lane + 32 * q < nb) ? col[lane + 32 * q] : 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < 4; u++) {
+      double s = 0.0;
+#pragma unroll
+      for (int q = 0; q < NB / 32; q++) s = fma(v[u][q], yl[q], s);
+      s = wsum(s);
+      if (lane == 0 && c0 + u < ncol) b[j0 + c0 + u] -= s;
+    }
   }
 }
 
@@ -236,17 +254,31 @@ __global__ void __launch_bounds__(256) trsv_bwd_step(int n, const double* __rest
   __syncthreads();
   if (blockIdx.x == 0)
     for (int p = threadIdx.x; p < nb; p += blockDim.x) x[k0 + p] = sx[p];
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < k0; i += gridDim.x * blockDim.x) {
-    double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
-    int p = 0;
-    for (; p + 3 < nb; p += 4) {
-      a0 = fma(A[(long long)i + lda * (k0 + p)], sx[p], a0);
-      a1 = fma(A[(long long)i + lda * (k0 + p + 1)], sx[p + 1], a1);
-      a2 = fma(A[(long long)i + lda * (k0 + p + 2)], sx[p + 2], a2);
-      a3 = fma(A[(long long)i + lda * (k0 + p + 3)], sx[p + 3], a3);
+  // y_i -= U(i, k-block) . x_k for i < k0: the block takes 32 rows, its 8 warps 16 columns each (each lane one
+  // row, coalesced across the warp), and the 8 partial sums of a row meet in shared memory
+  const int lane = threadIdx.x & 31, wg = threadIdx.x >> 5;
+  for (int i0 = blockIdx.x * 32; i0 < k0; i0 += gridDim.x * 32) {
+    const int i = i0 + lane;
+    double a[16];
+#pragma unroll
+    for (int t = 0; t < 16; t++) {
+      const int p = wg * 16 + t;
+      a[t] = (i < k0 && p < nb) ? A[(long long)i + lda * (k0 + p)] : 0.0;
     }
-    for (; p < nb; p++) a0 = fma(A[(long long)i + lda * (k0 + p)], sx[p], a0);
-    y[i] -= (a0 + a1) + (a2 + a3);
+    double s = 0.0;
+#pragma unroll
+    for (int t = 0; t < 16; t++) {
+      const int p = wg * 16 + t;
+      s = fma(a[t], p < nb ? sx[p] : 0.0, s);
+    }
+    red[wg & 1][lane + 32 * (wg >> 1)] = s;  // 8 groups -> red as [8][32]
+    __syncthreads();
+    if (wg == 0 && i < k0) {
+      double t8 = 0.0;
+      for (int g = 0; g < 8; g++) t8 += red[g & 1][lane + 32 * (g >> 1)];
+      y[i] -= t8;
+    }
+    __syncthreads();
   }
 }
 
@@ -499,13 +531,13 @@ cudaError_t rbmpp_potrs_upper(int n, const double* A, const double* dinv, double
   const int nblk = rbmpp_chol_blocks(n);
   for (int kb = 0; kb < nblk; kb++) {  // U^T y = b: y in tmp, b consumed
     const int k0 = kb * NB, rest = n - (k0 + NB);
-    const int blocks = rest > 0 ? min(nsm, (rest + 7) / 8) : 1;
+    const int blocks = rest > 0 ? min(2 * nsm, (rest + 31) / 32) : 1;
     rbmpp_note_launch();
     trsv_fwd_step<<<blocks, 256, 0, st>>>(n, A, n, k0, dinv + (size_t)kb * NB * NB, b, tmp);
   }
   for (int kb = nblk - 1; kb >= 0; kb--) {  // U x = y: x in b, tmp consumed
     const int k0 = kb * NB;
-    const int blocks = k0 > 0 ? min(nsm, (k0 + 255) / 256) : 1;
+    const int blocks = k0 > 0 ? min(2 * nsm, (k0 + 31) / 32) : 1;
     rbmpp_note_launch();
     trsv_bwd_step<<<blocks, 256, 0, st>>>(n, A, n, k0, dinv + (size_t)kb * NB * NB, tmp, b);
   }
