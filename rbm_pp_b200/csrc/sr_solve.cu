@@ -5,12 +5,13 @@
 //
 // Cholesky (upper, A = U^T U, in place), panels of NB = 128 columns:
 //   potrf_block_kernel   one CTA factors the NB x NB diagonal block in shared memory (32-column sub-panels:
-//                        a warp factors each 32 x 32 diagonal piece in registers) and writes U_kk and its
-//                        inverse U_kk^{-1} (kept for the panel solve and for every later triangular solve);
-//   panel_kernel         U_kj = U_kk^{-T} A_kj, one warp per column j;
+//                        a warp factors each 32 x 32 diagonal piece in registers) and keeps 1 / U(i, i);
+//   panel_kernel         U_kj = U_kk^{-T} A_kj by forward substitution, one warp per column j, U_kk in shared
+//                        memory;
 //   gemm_atb_upper<true> (linalg.cu) the trailing update A_22 -= U_12^T U_12.
-// Triangular solves: one launch per block step; every CTA applies the inverted diagonal block to the block's
-// right-hand side (redundantly, from L2) and then updates its share of the rest of the vector.
+// Triangular solves: one launch per block step; in every CTA one warp solves the diagonal block for the block's
+// right-hand side (redundantly, from L2) while the others wait, then all update their share of the rest of the
+// vector.
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -24,6 +25,7 @@ cudaError_t rbmpp_gemv_o(int, int, const double*, const double*, double*, cudaSt
 namespace {
 
 constexpr int NB = 128;
+constexpr int NQ = NB / 32;  // rows of a block column held by one lane
 
 __device__ __forceinline__ double wsum(double v) {
 #pragma unroll
@@ -32,12 +34,12 @@ __device__ __forceinline__ double wsum(double v) {
 }
 
 // ---------------------------------------------------------------------------------------------------
-// Diagonal block: Cholesky of the nb x nb block at (k0, k0) and the inverse of its factor.
+// Diagonal block: Cholesky of the nb x nb block at (k0, k0) and the reciprocals of its diagonal.
 // T (shared, column-major, ld NB + 1) holds the block; warp 0 factors each 32 x 32 diagonal piece with the
 // piece's column c in lane c, then all warps solve the piece's row panel and update the trailing triangle.
 // ---------------------------------------------------------------------------------------------------
 __global__ void __launch_bounds__(512, 1)
-    potrf_block_kernel(int n, double* __restrict__ A, long long lda, int k0, double* __restrict__ dinv,
+    potrf_block_kernel(int n, double* __restrict__ A, long long lda, int k0, double* __restrict__ rdiag_out,
                        int* __restrict__ info) {
   extern __shared__ double T[];  // [NB][NB + 1] column-major: T[i + (NB + 1) j]
   __shared__ double rdiag[NB];   // 1 / U(i, i)
@@ -110,115 +112,127 @@ __global__ void __launch_bounds__(512, 1)
     const int i = e % nb, j = e / nb;
     if (i <= j) A[(long long)(k0 + i) + lda * (k0 + j)] = T[i + LD * j];
   }
-  // V = U_kk^{-1} (upper): column c solves U v = e_c by back substitution, one warp per column;
-  // lane holds rows lane + 32 q of the column
-  double* V = dinv;  // [NB][NB] column-major, ld NB
-  for (int c = warp; c < NB; c += nwarps) {
-    double v[NB / 32];
-#pragma unroll
-    for (int q = 0; q < NB / 32; q++) v[q] = 0.0;
-    if (c < nb) {
-      for (int i = c; i >= 0; i--) {
-        double s = 0.0;
-#pragma unroll
-        for (int q = 0; q < NB / 32; q++) {
-          const int j = lane + 32 * q;
-          if (j > i && j <= c) s += T[i + LD * j] * v[q];
-        }
-        s = wsum(s);
-        const double vi = ((i == c ? 1.0 : 0.0) - s) * rdiag[i];
-#pragma unroll
-        for (int q = 0; q < NB / 32; q++)
-          if (lane + 32 * q == i) v[q] = vi;
-      }
-    }
-#pragma unroll
-    for (int q = 0; q < NB / 32; q++) V[(lane + 32 * q) + NB * c] = (c < nb && lane + 32 * q < nb) ? v[q] : 0.0;
-  }
+  for (int i = tid; i < nb; i += blockDim.x) rdiag_out[k0 + i] = rdiag[i];
 }
 
-// U(k0:k0+nb, j) = U_kk^{-T} A(k0:k0+nb, j) for j >= k0 + nb: out_p = sum_{q <= p} V(q, p) a_q.
-// One warp per column; V transposed in shared memory so the lanes read consecutive p.
+// U(k0:k0+nb, j) = U_kk^{-T} A(k0:k0+nb, j) for j >= k0 + nb by forward substitution: one warp per column,
+// lane holding rows lane + 32 q; U_kk (upper) and its reciprocal diagonal in shared memory.
 __global__ void __launch_bounds__(512) panel_kernel(int n, double* __restrict__ A, long long lda, int k0,
-                                                    const double* __restrict__ dinv) {
-  extern __shared__ double VT[];  // VT[p + NB q] = V(q, p)
+                                                    const double* __restrict__ rdiag) {
+  extern __shared__ double U[];  // [NB][NB + 1] column-major
+  __shared__ double rd[NB];
+  constexpr int LD = NB + 1;
   const int nb = min(NB, n - k0);
-  for (int e = threadIdx.x; e < NB * NB; e += blockDim.x) {
-    const int q = e % NB, p = e / NB;
-    VT[p + NB * q] = dinv[e];  // dinv[q + NB p] = V(q, p)
+  for (int e = threadIdx.x; e < nb * nb; e += blockDim.x) {
+    const int i = e % nb, j = e / nb;
+    U[i + LD * j] = (i <= j) ? A[(long long)(k0 + i) + lda * (k0 + j)] : 0.0;
   }
+  for (int i = threadIdx.x; i < nb; i += blockDim.x) rd[i] = rdiag[k0 + i];
   __syncthreads();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
   for (int j = k0 + nb + blockIdx.x * nwarps + warp; j < n; j += gridDim.x * nwarps) {
     double* col = A + lda * j + k0;
-    double a[NB / 32], out[NB / 32];
+    double x[NQ];
 #pragma unroll
-    for (int q = 0; q < NB / 32; q++) {
-      a[q] = (lane + 32 * q < nb) ? col[lane + 32 * q] : 0.0;
-      out[q] = 0.0;
-    }
+    for (int q = 0; q < NQ; q++) x[q] = (lane + 32 * q < nb) ? col[lane + 32 * q] : 0.0;
+    // x_r = (b_r - sum_{s < r} U(s, r) x_s) / U(r, r), applied column by column of U^T: after x_r,
+    // x_p -= U(r, p) x_r for p > r
 #pragma unroll
-    for (int t0 = 0; t0 < NB / 32; t0++) {
-      for (int ql = 0; ql < 32; ql++) {
-        const int qq = 32 * t0 + ql;
-        const double aq = __shfl_sync(0xffffffffu, a[t0], ql);
+    for (int qr = 0; qr < NQ; qr++) {
+      for (int rl = 0; rl < 32; rl++) {
+        const int r = 32 * qr + rl;
+        if (r >= nb) break;
+        const double xr = __shfl_sync(0xffffffffu, x[qr], rl) * rd[r];
+        if (lane == rl) x[qr] = xr;
 #pragma unroll
-        for (int t = 0; t < NB / 32; t++) {
-          const int p = lane + 32 * t;
-          if (p >= qq && p < nb && qq < nb) out[t] = fma(VT[p + NB * qq], aq, out[t]);
+        for (int q = qr; q < NQ; q++) {
+          const int p = lane + 32 * q;
+          if (p > r && p < nb) x[q] -= U[r + LD * p] * xr;
         }
       }
     }
 #pragma unroll
-    for (int q = 0; q < NB / 32; q++)
-      if (lane + 32 * q < nb) col[lane + 32 * q] = out[q];
+    for (int q = 0; q < NQ; q++)
+      if (lane + 32 * q < nb) col[lane + 32 * q] = x[q];
   }
 }
 
 // ---------------------------------------------------------------------------------------------------
-// Triangular solves with the inverted diagonal blocks.  Forward U^T y = b: y_k = V_k^T b_k, then
-// b_j -= U(k-block, j) . y_k for j beyond the block (one warp per j, coalesced column reads).  Backward
-// U x = y: x_k = V_k y_k, then y_i -= U(i, k-block) . x_k for i < k0 (one thread per i, coalesced).
-// Every CTA forms y_k (or x_k) itself; the block's result goes to a separate vector so no CTA reads what
-// another one writes within the step.
+// Triangular solves.  Forward U^T y = b: warp 0 solves the block, y_r = (b_r - U(0:r, r) . y) / U(r, r), with
+// the block's columns read coalesced from global memory; then b_j -= U(k-block, j) . y_k for j beyond the block
+// (four columns per warp at a time).  Backward U x = y: warp 0 solves the block column by column,
+// x_r = y_r / U(r, r), y_p -= U(p, r) x_r; then y_i -= U(i, k-block) . x_k for i < k0.  The block's result goes
+// to a separate vector, so no CTA reads what another one writes within the step.
 // ---------------------------------------------------------------------------------------------------
-__global__ void __launch_bounds__(256) trsv_fwd_step(int n, const double* __restrict__ A, long long lda, int k0,
-                                                     const double* __restrict__ V, double* __restrict__ b,
-                                                     double* __restrict__ y) {
-  __shared__ double sb[NB], sy[NB];
-  const int nb = min(NB, n - k0);
-  for (int p = threadIdx.x; p < nb; p += blockDim.x) sb[p] = b[k0 + p];
+// The diagonal block (column-major, ld NB) and its reciprocal diagonal, staged in shared memory by all threads
+__device__ __forceinline__ void stage_block(int nb, const double* __restrict__ A, long long lda, int k0,
+                                            const double* __restrict__ rdiag, double* Ts, double* rd) {
+  for (int e = threadIdx.x; e < nb * nb; e += blockDim.x) {
+    const int i = e % nb, j = e / nb;
+    Ts[i + NB * j] = A[(long long)(k0 + i) + lda * (k0 + j)];
+  }
+  for (int i = threadIdx.x; i < nb; i += blockDim.x) rd[i] = rdiag[k0 + i];
   __syncthreads();
-  // sy[p] = sum_{q <= p} V(q, p) sb[q]: warp per p, lanes over q
+}
+
+__global__ void __launch_bounds__(256) trsv_fwd_step(int n, const double* __restrict__ A, long long lda, int k0,
+                                                     const double* __restrict__ rdiag, double* __restrict__ b,
+                                                     double* __restrict__ y) {
+  extern __shared__ double Ts[];
+  __shared__ double sy[NB], rd[NB];
+  const int nb = min(NB, n - k0);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
-  for (int p = warp; p < nb; p += nwarps) {
-    double s = 0.0;
-    for (int q = lane; q <= p; q += 32) s = fma(V[q + NB * p], sb[q], s);
-    s = wsum(s);
-    if (lane == 0) sy[p] = s;
+  stage_block(nb, A, lda, k0, rdiag, Ts, rd);
+  if (warp == 0) {
+    double yl[NQ], bl[NQ];
+#pragma unroll
+    for (int q = 0; q < NQ; q++) {
+      yl[q] = 0.0;
+      bl[q] = (lane + 32 * q < nb) ? b[k0 + lane + 32 * q] : 0.0;
+    }
+    for (int r = 0; r < nb; r++) {
+      const double* col = Ts + NB * r;  // U(0:r, r)
+      double s = 0.0;
+#pragma unroll
+      for (int q = 0; q < NQ; q++) {
+        const int p = lane + 32 * q;
+        if (p < r) s = fma(col[p], yl[q], s);
+      }
+      s = wsum(s);
+      double br = 0.0;
+#pragma unroll
+      for (int q = 0; q < NQ; q++)
+        if ((r >> 5) == q) br = __shfl_sync(0xffffffffu, bl[q], r & 31);
+      const double yr = (br - s) * rd[r];
+#pragma unroll
+      for (int q = 0; q < NQ; q++)
+        if (lane + 32 * q == r) yl[q] = yr;
+    }
+#pragma unroll
+    for (int q = 0; q < NQ; q++)
+      if (lane + 32 * q < nb) sy[lane + 32 * q] = yl[q];
   }
   __syncthreads();
   if (blockIdx.x == 0)
     for (int p = threadIdx.x; p < nb; p += blockDim.x) y[k0 + p] = sy[p];
   // b_j -= U(k-block, j) . y_k: four columns per warp at a time, all their loads issued before any sum
-  double yl[NB / 32];
+  double yl[NQ];
 #pragma unroll
-  for (int q = 0; q < NB / 32; q++) yl[q] = (lane + 32 * q < nb) ? sy[lane + 32 * q] : 0.0;
+  for (int q = 0; q < NQ; q++) yl[q] = (lane + 32 * q < nb) ? sy[lane + 32 * q] : 0.0;
   const int j0 = k0 + nb, ncol = n - j0, stride = gridDim.x * nwarps;
   for (int c0 = (blockIdx.x * nwarps + warp) * 4; c0 < ncol; c0 += stride * 4) {
-    double v[4][NB / 32];
+    double v[4][NQ];
 #pragma unroll
     for (int u = 0; u < 4; u++) {
       const double* col = A + lda * (j0 + c0 + u) + k0;
 #pragma unroll
-      for (int q = 0; q < NB / 32; q++)
-        v[u][q] = (c0 + u < ncol && lane + 32 * q < nb) ? col[lane + 32 * q] : 0.0;
+      for (int q = 0; q < NQ; q++) v[u][q] = (c0 + u < ncol && lane + 32 * q < nb) ? col[lane + 32 * q] : 0.0;
     }
 #pragma unroll
     for (int u = 0; u < 4; u++) {
       double s = 0.0;
 #pragma unroll
-      for (int q = 0; q < NB / 32; q++) s = fma(v[u][q], yl[q], s);
+      for (int q = 0; q < NQ; q++) s = fma(v[u][q], yl[q], s);
       s = wsum(s);
       if (lane == 0 && c0 + u < ncol) b[j0 + c0 + u] -= s;
     }
@@ -226,37 +240,41 @@ __global__ void __launch_bounds__(256) trsv_fwd_step(int n, const double* __rest
 }
 
 __global__ void __launch_bounds__(256) trsv_bwd_step(int n, const double* __restrict__ A, long long lda, int k0,
-                                                     const double* __restrict__ V, double* __restrict__ y,
+                                                     const double* __restrict__ rdiag, double* __restrict__ y,
                                                      double* __restrict__ x) {
-  __shared__ double sb[NB], sx[NB], red[2][NB];
+  extern __shared__ double Ts[];
+  __shared__ double sx[NB], rd[NB], red[8][32];
   const int nb = min(NB, n - k0);
-  for (int p = threadIdx.x; p < nb; p += blockDim.x) sb[p] = y[k0 + p];
-  __syncthreads();
-  // sx[p] = sum_{q >= p} V(p, q) sb[q]: two threads per p (alternate q), four independent partial sums each;
-  // consecutive p read consecutive V entries (blockDim = 2 NB)
-  {
-    const int p = threadIdx.x & (NB - 1), half = threadIdx.x / NB;
-    double a0 = 0.0, a1 = 0.0, a2 = 0.0, a3 = 0.0;
-    if (p < nb) {
-      int q = p + half;
-      for (; q + 6 < nb; q += 8) {
-        a0 = fma(V[p + NB * q], sb[q], a0);
-        a1 = fma(V[p + NB * (q + 2)], sb[q + 2], a1);
-        a2 = fma(V[p + NB * (q + 4)], sb[q + 4], a2);
-        a3 = fma(V[p + NB * (q + 6)], sb[q + 6], a3);
+  const int lane = threadIdx.x & 31, wg = threadIdx.x >> 5;
+  stage_block(nb, A, lda, k0, rdiag, Ts, rd);
+  if (wg == 0) {
+    double yl[NQ];
+#pragma unroll
+    for (int q = 0; q < NQ; q++) yl[q] = (lane + 32 * q < nb) ? y[k0 + lane + 32 * q] : 0.0;
+#pragma unroll
+    for (int qr = NQ - 1; qr >= 0; qr--) {
+      for (int rl = 31; rl >= 0; rl--) {
+        const int r = 32 * qr + rl;
+        if (r >= nb) continue;
+        const double xr = __shfl_sync(0xffffffffu, yl[qr], rl) * rd[r];
+        if (lane == rl) yl[qr] = xr;
+        const double* col = Ts + NB * r;  // U(0:r, r)
+#pragma unroll
+        for (int q = 0; q <= qr; q++) {
+          const int p = lane + 32 * q;
+          if (p < r) yl[q] -= col[p] * xr;
+        }
       }
-      for (; q < nb; q += 2) a0 = fma(V[p + NB * q], sb[q], a0);
     }
-    red[half][p] = (a0 + a1) + (a2 + a3);
+#pragma unroll
+    for (int q = 0; q < NQ; q++)
+      if (lane + 32 * q < nb) sx[lane + 32 * q] = yl[q];
   }
-  __syncthreads();
-  for (int p = threadIdx.x; p < nb; p += blockDim.x) sx[p] = red[0][p] + red[1][p];
   __syncthreads();
   if (blockIdx.x == 0)
     for (int p = threadIdx.x; p < nb; p += blockDim.x) x[k0 + p] = sx[p];
   // y_i -= U(i, k-block) . x_k for i < k0: the block takes 32 rows, its 8 warps 16 columns each (each lane one
   // row, coalesced across the warp), and the 8 partial sums of a row meet in shared memory
-  const int lane = threadIdx.x & 31, wg = threadIdx.x >> 5;
   for (int i0 = blockIdx.x * 32; i0 < k0; i0 += gridDim.x * 32) {
     const int i = i0 + lane;
     double a[16];
@@ -271,11 +289,11 @@ __global__ void __launch_bounds__(256) trsv_bwd_step(int n, const double* __rest
       const int p = wg * 16 + t;
       s = fma(a[t], p < nb ? sx[p] : 0.0, s);
     }
-    red[wg & 1][lane + 32 * (wg >> 1)] = s;  // 8 groups -> red as [8][32]
+    red[wg][lane] = s;
     __syncthreads();
     if (wg == 0 && i < k0) {
       double t8 = 0.0;
-      for (int g = 0; g < 8; g++) t8 += red[g & 1][lane + 32 * (g >> 1)];
+      for (int g = 0; g < 8; g++) t8 += red[g][lane];
       y[i] -= t8;
     }
     __syncthreads();
@@ -497,49 +515,48 @@ int sm_count() {
 // ---------------------------------------------------------------------------------------------------
 // host entry points
 // ---------------------------------------------------------------------------------------------------
-int rbmpp_chol_blocks(int n) { return (n + NB - 1) / NB; }
-int rbmpp_chol_nb() { return NB; }
-
-// In-place Cholesky of the upper triangle of A (n x n, lda = n); dinv: rbmpp_chol_blocks(n) * NB * NB doubles
-// of inverted diagonal factor blocks; *d_info = 0 or the first failing column (1-based).
-cudaError_t rbmpp_potrf_upper(int n, double* A, double* dinv, int* d_info, cudaStream_t st) {
+// In-place Cholesky of the upper triangle of A (n x n, lda = n); rdiag: n doubles, 1 / U(i, i) on return;
+// *d_info = 0 or the first failing column (1-based).
+cudaError_t rbmpp_potrf_upper(int n, double* A, double* rdiag, int* d_info, cudaStream_t st) {
   cudaError_t e = cudaMemsetAsync(d_info, 0, sizeof(int), st);
   if (e) return e;
   const size_t smem = (size_t)NB * (NB + 1) * sizeof(double);
   if ((e = cudaFuncSetAttribute(potrf_block_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem))) return e;
-  const size_t psmem = (size_t)NB * NB * sizeof(double);
-  if ((e = cudaFuncSetAttribute(panel_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psmem))) return e;
+  if ((e = cudaFuncSetAttribute(panel_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem))) return e;
   const int nsm = sm_count();
-  for (int k0 = 0, kb = 0; k0 < n; k0 += NB, kb++) {
-    double* V = dinv + (size_t)kb * NB * NB;
+  for (int k0 = 0; k0 < n; k0 += NB) {
     rbmpp_note_launch();
-    potrf_block_kernel<<<1, 512, smem, st>>>(n, A, n, k0, V, d_info);
+    potrf_block_kernel<<<1, 512, smem, st>>>(n, A, n, k0, rdiag, d_info);
     const int rest = n - (k0 + NB);
     if (rest > 0) {
       const int blocks = min(nsm, (rest + 15) / 16);
       rbmpp_note_launch();
-      panel_kernel<<<blocks, 512, psmem, st>>>(n, A, n, k0, V);
+      panel_kernel<<<blocks, 512, smem, st>>>(n, A, n, k0, rdiag);
       if ((e = rbmpp_gemm_atb_upper_acc(n, NB, A + k0, 1, n, -1.0, A, n, k0 + NB, st))) return e;
     }
   }
   return cudaGetLastError();
 }
 
-// b <- A^{-1} b with A = U^T U (upper factor in A, inverted diagonal blocks in dinv); tmp: n doubles
-cudaError_t rbmpp_potrs_upper(int n, const double* A, const double* dinv, double* b, double* tmp, cudaStream_t st) {
+// b <- A^{-1} b with A = U^T U (upper factor in A, reciprocal diagonal in rdiag); tmp: n doubles
+cudaError_t rbmpp_potrs_upper(int n, const double* A, const double* rdiag, double* b, double* tmp, cudaStream_t st) {
   const int nsm = sm_count();
-  const int nblk = rbmpp_chol_blocks(n);
+  const int nblk = (n + NB - 1) / NB;
+  const size_t smem = (size_t)NB * NB * sizeof(double);
+  cudaError_t e;
+  if ((e = cudaFuncSetAttribute(trsv_fwd_step, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem))) return e;
+  if ((e = cudaFuncSetAttribute(trsv_bwd_step, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem))) return e;
   for (int kb = 0; kb < nblk; kb++) {  // U^T y = b: y in tmp, b consumed
     const int k0 = kb * NB, rest = n - (k0 + NB);
-    const int blocks = rest > 0 ? min(2 * nsm, (rest + 31) / 32) : 1;
+    const int blocks = rest > 0 ? min(nsm, (rest + 31) / 32) : 1;
     rbmpp_note_launch();
-    trsv_fwd_step<<<blocks, 256, 0, st>>>(n, A, n, k0, dinv + (size_t)kb * NB * NB, b, tmp);
+    trsv_fwd_step<<<blocks, 256, smem, st>>>(n, A, n, k0, rdiag, b, tmp);
   }
   for (int kb = nblk - 1; kb >= 0; kb--) {  // U x = y: x in b, tmp consumed
     const int k0 = kb * NB;
-    const int blocks = k0 > 0 ? min(2 * nsm, (k0 + 31) / 32) : 1;
+    const int blocks = k0 > 0 ? min(nsm, (k0 + 31) / 32) : 1;
     rbmpp_note_launch();
-    trsv_bwd_step<<<blocks, 256, 0, st>>>(n, A, n, k0, dinv + (size_t)kb * NB * NB, tmp, b);
+    trsv_bwd_step<<<blocks, 256, smem, st>>>(n, A, n, k0, rdiag, tmp, b);
   }
   return cudaGetLastError();
 }
