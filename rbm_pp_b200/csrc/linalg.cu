@@ -158,10 +158,12 @@ __global__ void gemv_o_kernel(int ns, int nv, const double* __restrict__ O, cons
 
 // S(i,j) = Sraw(i,j)/norm - Ovec(i) Ovec(j)   (SR_pdposv.f90:11-15), full matrix
 __global__ void sr_form_kernel(int n, double* S, double norm, const double* ov) {
-  long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (e >= (long long)n * n) return;
-  int i = (int)(e % n), j = (int)(e / n);
-  S[e] = S[e] / norm - ov[i] * ov[j];
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;  // 2-D grid: no 64-bit division
+  if (i >= n) return;
+  for (int j = blockIdx.y; j < n; j += gridDim.y) {
+    const long long e = (long long)j * n + i;
+    S[e] = S[e] / norm - ov[i] * ov[j];
+  }
 }
 
 // y = f x
@@ -172,21 +174,22 @@ __global__ void scale_copy_kernel(int n, const double* x, double f, double* y) {
 
 // S(i, j) += f v_i v_j on the strict upper triangle (column-major)
 __global__ void add_outer_offdiag_kernel(int n, double* S, const double* v, double f) {
-  long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (e >= (long long)n * n) return;
-  int i = (int)(e % n), j = (int)(e / n);
-  if (i < j) S[e] = fma(f * v[i], v[j], S[e]);
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  for (int j = blockIdx.y; j < n; j += gridDim.y)
+    if (i < j) S[(long long)j * n + i] = fma(f * v[i], v[j], S[(long long)j * n + i]);
 }
 
 // PP-block scaling (SR_pdposv.f90:56-73): columns k2 > Nv_RBM, then rows k1 > Nv_RBM
 __global__ void sr_scale_kernel(int n, int nrbm, double* S, double f) {
-  long long e = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (e >= (long long)n * n) return;
-  int i = (int)(e % n), j = (int)(e / n);
-  double v = S[e];
-  if (j >= nrbm) v = v * f;
-  if (i >= nrbm) v = v * f;
-  S[e] = v;
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  for (int j = blockIdx.y; j < n; j += gridDim.y) {
+    const long long e = (long long)j * n + i;
+    double v = S[e];
+    if (j >= nrbm) v = v * f;
+    if (i >= nrbm) v = v * f;
+    S[e] = v;
+  }
 }
 
 __global__ void get_diag_kernel(int n, const double* S, double* d) {
@@ -325,9 +328,8 @@ cudaError_t rbmpp_gemv_o(int ns, int nv, const double* O, const double* x, doubl
 }
 
 cudaError_t rbmpp_sr_form(int n, double* S, double norm, const double* ov, cudaStream_t st) {
-  long long tot = (long long)n * n;
   rbmpp_note_launch();
-  sr_form_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(n, S, norm, ov);
+  sr_form_kernel<<<dim3((n + 255) / 256, n < 65535 ? n : 65535), 256, 0, st>>>(n, S, norm, ov);
   return cudaGetLastError();
 }
 
@@ -338,16 +340,14 @@ cudaError_t rbmpp_scale_copy(int n, const double* x, double f, double* y, cudaSt
 }
 
 cudaError_t rbmpp_add_outer_offdiag(int n, double* S, const double* v, double f, cudaStream_t st) {
-  long long tot = (long long)n * n;
   rbmpp_note_launch();
-  add_outer_offdiag_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(n, S, v, f);
+  add_outer_offdiag_kernel<<<dim3((n + 255) / 256, n < 65535 ? n : 65535), 256, 0, st>>>(n, S, v, f);
   return cudaGetLastError();
 }
 
 cudaError_t rbmpp_sr_scale(int n, int nrbm, double* S, double f, cudaStream_t st) {
-  long long tot = (long long)n * n;
   rbmpp_note_launch();
-  sr_scale_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, st>>>(n, nrbm, S, f);
+  sr_scale_kernel<<<dim3((n + 255) / 256, n < 65535 ? n : 65535), 256, 0, st>>>(n, nrbm, S, f);
   return cudaGetLastError();
 }
 

@@ -164,12 +164,16 @@ __global__ void __launch_bounds__(512) panel_kernel(int n, double* __restrict__ 
 // x_r = y_r / U(r, r), y_p -= U(p, r) x_r; then y_i -= U(i, k-block) . x_k for i < k0.  The block's result goes
 // to a separate vector, so no CTA reads what another one writes within the step.
 // ---------------------------------------------------------------------------------------------------
-// The diagonal block (column-major, ld NB) and its reciprocal diagonal, staged in shared memory by all threads
+// The upper triangle of the diagonal block and its reciprocal diagonal, staged in shared memory by all
+// threads: Ts[i + TLD j] = U(i, j) (column-major), or Ts[j + TLD i] = U(i, j) when transposed (rows of U
+// contiguous); the odd leading dimension keeps both the staging writes and the solve's reads off bank conflicts.
+constexpr int TLD = NB + 1;
+template <bool TRANS>
 __device__ __forceinline__ void stage_block(int nb, const double* __restrict__ A, long long lda, int k0,
                                             const double* __restrict__ rdiag, double* Ts, double* rd) {
   for (int e = threadIdx.x; e < nb * nb; e += blockDim.x) {
     const int i = e % nb, j = e / nb;
-    Ts[i + NB * j] = A[(long long)(k0 + i) + lda * (k0 + j)];
+    if (i <= j) Ts[TRANS ? j + TLD * i : i + TLD * j] = A[(long long)(k0 + i) + lda * (k0 + j)];
   }
   for (int i = threadIdx.x; i < nb; i += blockDim.x) rd[i] = rdiag[k0 + i];
   __syncthreads();
@@ -182,35 +186,30 @@ __global__ void __launch_bounds__(256) trsv_fwd_step(int n, const double* __rest
   __shared__ double sy[NB], rd[NB];
   const int nb = min(NB, n - k0);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
-  stage_block(nb, A, lda, k0, rdiag, Ts, rd);
+  stage_block<true>(nb, A, lda, k0, rdiag, Ts, rd);
   if (warp == 0) {
-    double yl[NQ], bl[NQ];
+    // column by column of U^T: y_r = b_r / U(r, r), then b_p -= U(r, p) y_r for p > r (row r of U contiguous)
+    double bl[NQ];
 #pragma unroll
-    for (int q = 0; q < NQ; q++) {
-      yl[q] = 0.0;
-      bl[q] = (lane + 32 * q < nb) ? b[k0 + lane + 32 * q] : 0.0;
-    }
-    for (int r = 0; r < nb; r++) {
-      const double* col = Ts + NB * r;  // U(0:r, r)
-      double s = 0.0;
+    for (int q = 0; q < NQ; q++) bl[q] = (lane + 32 * q < nb) ? b[k0 + lane + 32 * q] : 0.0;
 #pragma unroll
-      for (int q = 0; q < NQ; q++) {
-        const int p = lane + 32 * q;
-        if (p < r) s = fma(col[p], yl[q], s);
+    for (int qr = 0; qr < NQ; qr++) {
+      for (int rl = 0; rl < 32; rl++) {
+        const int r = 32 * qr + rl;
+        if (r >= nb) break;
+        const double yr = __shfl_sync(0xffffffffu, bl[qr], rl) * rd[r];
+        if (lane == rl) bl[qr] = yr;
+        const double* row = Ts + TLD * r;  // U(r, p) at row[p]
+#pragma unroll
+        for (int q = qr; q < NQ; q++) {
+          const int p = lane + 32 * q;
+          if (p > r && p < nb) bl[q] -= row[p] * yr;
+        }
       }
-      s = wsum(s);
-      double br = 0.0;
-#pragma unroll
-      for (int q = 0; q < NQ; q++)
-        if ((r >> 5) == q) br = __shfl_sync(0xffffffffu, bl[q], r & 31);
-      const double yr = (br - s) * rd[r];
-#pragma unroll
-      for (int q = 0; q < NQ; q++)
-        if (lane + 32 * q == r) yl[q] = yr;
     }
 #pragma unroll
     for (int q = 0; q < NQ; q++)
-      if (lane + 32 * q < nb) sy[lane + 32 * q] = yl[q];
+      if (lane + 32 * q < nb) sy[lane + 32 * q] = bl[q];
   }
   __syncthreads();
   if (blockIdx.x == 0)
@@ -246,7 +245,7 @@ __global__ void __launch_bounds__(256) trsv_bwd_step(int n, const double* __rest
   __shared__ double sx[NB], rd[NB], red[8][32];
   const int nb = min(NB, n - k0);
   const int lane = threadIdx.x & 31, wg = threadIdx.x >> 5;
-  stage_block(nb, A, lda, k0, rdiag, Ts, rd);
+  stage_block<false>(nb, A, lda, k0, rdiag, Ts, rd);
   if (wg == 0) {
     double yl[NQ];
 #pragma unroll
@@ -258,7 +257,7 @@ __global__ void __launch_bounds__(256) trsv_bwd_step(int n, const double* __rest
         if (r >= nb) continue;
         const double xr = __shfl_sync(0xffffffffu, yl[qr], rl) * rd[r];
         if (lane == rl) yl[qr] = xr;
-        const double* col = Ts + NB * r;  // U(0:r, r)
+        const double* col = Ts + TLD * r;  // U(0:r, r)
 #pragma unroll
         for (int q = 0; q <= qr; q++) {
           const int p = lane + 32 * q;
@@ -542,7 +541,7 @@ cudaError_t rbmpp_potrf_upper(int n, double* A, double* rdiag, int* d_info, cuda
 cudaError_t rbmpp_potrs_upper(int n, const double* A, const double* rdiag, double* b, double* tmp, cudaStream_t st) {
   const int nsm = sm_count();
   const int nblk = (n + NB - 1) / NB;
-  const size_t smem = (size_t)NB * NB * sizeof(double);
+  const size_t smem = (size_t)NB * TLD * sizeof(double);
   cudaError_t e;
   if ((e = cudaFuncSetAttribute(trsv_fwd_step, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem))) return e;
   if ((e = cudaFuncSetAttribute(trsv_bwd_step, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem))) return e;
