@@ -33,6 +33,28 @@ __device__ __forceinline__ double wsum(double v) {
   return v;
 }
 
+// Copies the upper triangle (or all, FULL) of the nb x nb block at (k0, k0) of A into shared memory,
+// dst[i * si + j * sj] = A(k0 + i, k0 + j), with eight loads in flight per thread before their stores (a
+// store waits for its load, so a one-element loop would pay a full memory latency per element).
+template <bool FULL>
+__device__ __forceinline__ void load_block(int nb, const double* __restrict__ A, long long lda, int k0, double* dst,
+                                           int si, int sj) {
+  const int tot = nb * nb, step = blockDim.x;
+  for (int e0 = threadIdx.x; e0 < tot; e0 += 8 * step) {
+    double v[8];
+#pragma unroll
+    for (int u = 0; u < 8; u++) {
+      const int e = e0 + u * step, i = e % nb, j = e / nb;
+      v[u] = (e < tot && (FULL || i <= j)) ? A[(long long)(k0 + i) + lda * (k0 + j)] : 0.0;
+    }
+#pragma unroll
+    for (int u = 0; u < 8; u++) {
+      const int e = e0 + u * step, i = e % nb, j = e / nb;
+      if (e < tot && (FULL || i <= j)) dst[i * si + j * sj] = v[u];
+    }
+  }
+}
+
 // ---------------------------------------------------------------------------------------------------
 // Diagonal block: Cholesky of the nb x nb block at (k0, k0) and the reciprocals of its diagonal.
 // T (shared, column-major, ld NB + 1) holds the block; warp 0 factors each 32 x 32 diagonal piece with the
@@ -46,10 +68,9 @@ __global__ void __launch_bounds__(512, 1)
   constexpr int LD = NB + 1;
   const int nb = min(NB, n - k0);
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31, nwarps = blockDim.x >> 5;
-  for (int e = tid; e < nb * nb; e += blockDim.x) {
-    const int i = e % nb, j = e / nb;
-    T[i + LD * j] = (i <= j) ? A[(long long)(k0 + i) + lda * (k0 + j)] : 0.0;
-  }
+  for (int e = tid; e < NB * LD; e += blockDim.x) T[e] = 0.0;
+  __syncthreads();
+  load_block<false>(nb, A, lda, k0, T, 1, LD);
   __syncthreads();
   for (int p0 = 0; p0 < nb; p0 += 32) {
     const int pw = min(32, nb - p0);
@@ -123,10 +144,7 @@ __global__ void __launch_bounds__(512) panel_kernel(int n, double* __restrict__ 
   __shared__ double rd[NB];
   constexpr int LD = NB + 1;
   const int nb = min(NB, n - k0);
-  for (int e = threadIdx.x; e < nb * nb; e += blockDim.x) {
-    const int i = e % nb, j = e / nb;
-    U[i + LD * j] = (i <= j) ? A[(long long)(k0 + i) + lda * (k0 + j)] : 0.0;
-  }
+  load_block<false>(nb, A, lda, k0, U, 1, LD);
   for (int i = threadIdx.x; i < nb; i += blockDim.x) rd[i] = rdiag[k0 + i];
   __syncthreads();
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
@@ -171,10 +189,10 @@ constexpr int TLD = NB + 1;
 template <bool TRANS>
 __device__ __forceinline__ void stage_block(int nb, const double* __restrict__ A, long long lda, int k0,
                                             const double* __restrict__ rdiag, double* Ts, double* rd) {
-  for (int e = threadIdx.x; e < nb * nb; e += blockDim.x) {
-    const int i = e % nb, j = e / nb;
-    if (i <= j) Ts[TRANS ? j + TLD * i : i + TLD * j] = A[(long long)(k0 + i) + lda * (k0 + j)];
-  }
+  if (TRANS)
+    load_block<false>(nb, A, lda, k0, Ts, TLD, 1);
+  else
+    load_block<false>(nb, A, lda, k0, Ts, 1, TLD);
   for (int i = threadIdx.x; i < nb; i += blockDim.x) rd[i] = rdiag[k0 + i];
   __syncthreads();
 }
