@@ -33,6 +33,7 @@ cudaError_t rbmpp_symmetrize(int, double*, cudaStream_t);
 cudaError_t rbmpp_potrf_upper(int, double*, double*, int*, cudaStream_t);
 cudaError_t rbmpp_potrs_upper(int, const double*, const double*, double*, double*, cudaStream_t);
 int rbmpp_gram_parts();
+size_t rbmpp_chol_work(int);
 cudaError_t rbmpp_sr_apply(int, int, int, const double*, const double*, double, double, double, const double*,
                            double*, double*, double*, double*, double*, double*, double*, cudaStream_t);
 cudaError_t rbmpp_pcg_start(int, const double*, const double*, double*, double*, cudaStream_t);
@@ -141,7 +142,7 @@ struct rbmpp_ctx {
   double *d_tmp_ns = nullptr, *d_rv = nullptr;
   int *d_info = nullptr, *d_err = nullptr;
   double* d_Sb = nullptr;  // copy of the shifted split-precision S (preconditioner retries)
-  double* d_dinv = nullptr;  // 1 / U(i, i) of the Cholesky factor
+  double* d_dinv = nullptr;  // Cholesky workspace: 1 / U(i, i) and the inverted diagonal blocks
   double* d_pcg = nullptr;   // refinement vectors (10 x Nv)
   double* d_gpart = nullptr; // per-block partial sums of the one-pass O^T (O y)
   double* d_sc = nullptr;    // device scalars of the refinement
@@ -259,7 +260,7 @@ int ensure_measure_buffers(rbmpp_ctx* c) {
   if ((r = dalloc(c, &c->d_info, 4))) return r;
   if ((r = dalloc(c, &c->d_err, 4))) return r;
   if ((r = dalloc(c, &c->d_rv, (size_t)2 * d.Nv))) return r;
-  if ((r = dalloc(c, &c->d_dinv, (size_t)d.Nv))) return r;
+  if ((r = dalloc(c, &c->d_dinv, rbmpp_chol_work(d.Nv)))) return r;
   if ((r = dalloc(c, &c->d_pcg, (size_t)10 * d.Nv))) return r;
   if ((r = dalloc(c, &c->d_gpart, (size_t)rbmpp_gram_parts() * d.Nv))) return r;
   if ((r = dalloc(c, &c->d_sc, 8))) return r;

@@ -9,9 +9,9 @@
 //   panel_kernel         U_kj = U_kk^{-T} A_kj by forward substitution, one warp per column j, U_kk in shared
 //                        memory;
 //   gemm_atb_upper<true> (linalg.cu) the trailing update A_22 -= U_12^T U_12.
-// Triangular solves: one launch per block step; in every CTA one warp solves the diagonal block for the block's
-// right-hand side (redundantly, from L2) while the others wait, then all update their share of the rest of the
-// vector.
+//   invert_blocks_kernel all diagonal blocks inverted at once afterwards (one CTA per block).
+// Triangular solves: one launch per block step; every CTA applies the inverted diagonal block to the block's
+// right-hand side (redundantly, staged from L2) and then updates its share of the rest of the vector.
 #include <cuda_runtime.h>
 #include <stdint.h>
 
@@ -176,59 +176,92 @@ __global__ void __launch_bounds__(512) panel_kernel(int n, double* __restrict__ 
 }
 
 // ---------------------------------------------------------------------------------------------------
-// Triangular solves.  Forward U^T y = b: warp 0 solves the block, y_r = (b_r - U(0:r, r) . y) / U(r, r), with
-// the block's columns read coalesced from global memory; then b_j -= U(k-block, j) . y_k for j beyond the block
-// (four columns per warp at a time).  Backward U x = y: warp 0 solves the block column by column,
-// x_r = y_r / U(r, r), y_p -= U(p, r) x_r; then y_i -= U(i, k-block) . x_k for i < k0.  The block's result goes
-// to a separate vector, so no CTA reads what another one writes within the step.
+// Inverses of all diagonal factor blocks at once (one CTA per block, after the factorisation): V_k = U_kk^{-1}
+// (upper), column c by back substitution v_i = (delta_ic - sum_{i < j <= c} U(i, j) v_j) / U(i, i), one warp
+// per column, U_kk in shared memory.  dinv: [block][NB][NB] column-major.
 // ---------------------------------------------------------------------------------------------------
-// The upper triangle of the diagonal block and its reciprocal diagonal, staged in shared memory by all
-// threads: Ts[i + TLD j] = U(i, j) (column-major), or Ts[j + TLD i] = U(i, j) when transposed (rows of U
-// contiguous); the odd leading dimension keeps both the staging writes and the solve's reads off bank conflicts.
+__global__ void __launch_bounds__(512, 1) invert_blocks_kernel(int n, const double* __restrict__ A, long long lda,
+                                                               const double* __restrict__ rdiag,
+                                                               double* __restrict__ dinv) {
+  extern __shared__ double U[];  // [NB][NB + 1] column-major
+  constexpr int LD = NB + 1;
+  const int k0 = blockIdx.x * NB, nb = min(NB, n - k0);
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
+  load_block<false>(nb, A, lda, k0, U, 1, LD);
+  __syncthreads();
+  double* V = dinv + (size_t)blockIdx.x * NB * NB;
+  for (int c = warp; c < NB; c += nwarps) {
+    double v[NQ];
+#pragma unroll
+    for (int q = 0; q < NQ; q++) v[q] = 0.0;
+    if (c < nb) {
+      for (int i = c; i >= 0; i--) {
+        double s = 0.0;
+#pragma unroll
+        for (int q = 0; q < NQ; q++) {
+          const int j = lane + 32 * q;
+          if (j > i && j <= c) s = fma(U[i + LD * j], v[q], s);
+        }
+        s = wsum(s);
+        const double vi = ((i == c ? 1.0 : 0.0) - s) * rdiag[k0 + i];
+#pragma unroll
+        for (int q = 0; q < NQ; q++)
+          if (lane + 32 * q == i) v[q] = vi;
+      }
+    }
+#pragma unroll
+    for (int q = 0; q < NQ; q++) V[(lane + 32 * q) + NB * c] = (c < nb && lane + 32 * q < nb) ? v[q] : 0.0;
+  }
+}
+
+// ---------------------------------------------------------------------------------------------------
+// Triangular solves with the inverted diagonal blocks, one launch per block step.  Every CTA stages V_k in
+// shared memory and forms the block's result itself: forward U^T y = b, y_k = V_k^T b_k, then
+// b_j -= U(k-block, j) . y_k beyond the block (four columns per warp at a time); backward U x = y,
+// x_k = V_k y_k, then y_i -= U(i, k-block) . x_k for i < k0.  The block's result goes to a separate vector, so
+// no CTA reads what another one writes within the step.
+// ---------------------------------------------------------------------------------------------------
 constexpr int TLD = NB + 1;
-template <bool TRANS>
-__device__ __forceinline__ void stage_block(int nb, const double* __restrict__ A, long long lda, int k0,
-                                            const double* __restrict__ rdiag, double* Ts, double* rd) {
-  if (TRANS)
-    load_block<false>(nb, A, lda, k0, Ts, TLD, 1);
-  else
-    load_block<false>(nb, A, lda, k0, Ts, 1, TLD);
-  for (int i = threadIdx.x; i < nb; i += blockDim.x) rd[i] = rdiag[k0 + i];
+
+// Vs[i + TLD j] = V(i, j) and the block's right-hand side rhs[0 .. nb) in shared memory
+__device__ __forceinline__ void stage_v(int nb, const double* __restrict__ V, const double* __restrict__ rhs,
+                                        double* Vs, double* sb) {
+  const int tot = NB * NB, step = blockDim.x;
+  for (int e0 = threadIdx.x; e0 < tot; e0 += 8 * step) {
+    double v[8];
+#pragma unroll
+    for (int u = 0; u < 8; u++) v[u] = (e0 + u * step < tot) ? V[e0 + u * step] : 0.0;
+#pragma unroll
+    for (int u = 0; u < 8; u++) {
+      const int e = e0 + u * step;
+      if (e < tot) Vs[(e % NB) + TLD * (e / NB)] = v[u];
+    }
+  }
+  for (int p = threadIdx.x; p < nb; p += blockDim.x) sb[p] = rhs[p];
   __syncthreads();
 }
 
 __global__ void __launch_bounds__(256) trsv_fwd_step(int n, const double* __restrict__ A, long long lda, int k0,
-                                                     const double* __restrict__ rdiag, double* __restrict__ b,
+                                                     const double* __restrict__ V, double* __restrict__ b,
                                                      double* __restrict__ y) {
-  extern __shared__ double Ts[];
-  __shared__ double sy[NB], rd[NB];
+  extern __shared__ double Vs[];
+  __shared__ double sb[NB], sy[NB], red[2][NB];
   const int nb = min(NB, n - k0);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
-  stage_block<true>(nb, A, lda, k0, rdiag, Ts, rd);
-  if (warp == 0) {
-    // column by column of U^T: y_r = b_r / U(r, r), then b_p -= U(r, p) y_r for p > r (row r of U contiguous)
-    double bl[NQ];
-#pragma unroll
-    for (int q = 0; q < NQ; q++) bl[q] = (lane + 32 * q < nb) ? b[k0 + lane + 32 * q] : 0.0;
-#pragma unroll
-    for (int qr = 0; qr < NQ; qr++) {
-      for (int rl = 0; rl < 32; rl++) {
-        const int r = 32 * qr + rl;
-        if (r >= nb) break;
-        const double yr = __shfl_sync(0xffffffffu, bl[qr], rl) * rd[r];
-        if (lane == rl) bl[qr] = yr;
-        const double* row = Ts + TLD * r;  // U(r, p) at row[p]
-#pragma unroll
-        for (int q = qr; q < NQ; q++) {
-          const int p = lane + 32 * q;
-          if (p > r && p < nb) bl[q] -= row[p] * yr;
-        }
+  stage_v(nb, V, b + k0, Vs, sb);
+  // sy[p] = sum_{q <= p} V(q, p) sb[q]: two threads per p (alternate q), consecutive p on consecutive lanes
+  {
+    const int p = threadIdx.x & (NB - 1), half = threadIdx.x / NB;
+    double a0 = 0.0, a1 = 0.0;
+    if (p < nb)
+      for (int q = half; q <= p; q += 4) {
+        a0 = fma(Vs[q + TLD * p], sb[q], a0);
+        if (q + 2 <= p) a1 = fma(Vs[q + 2 + TLD * p], sb[q + 2], a1);
       }
-    }
-#pragma unroll
-    for (int q = 0; q < NQ; q++)
-      if (lane + 32 * q < nb) sy[lane + 32 * q] = bl[q];
+    red[half][p] = a0 + a1;
   }
+  __syncthreads();
+  for (int p = threadIdx.x; p < nb; p += blockDim.x) sy[p] = red[0][p] + red[1][p];
   __syncthreads();
   if (blockIdx.x == 0)
     for (int p = threadIdx.x; p < nb; p += blockDim.x) y[k0 + p] = sy[p];
@@ -257,36 +290,26 @@ __global__ void __launch_bounds__(256) trsv_fwd_step(int n, const double* __rest
 }
 
 __global__ void __launch_bounds__(256) trsv_bwd_step(int n, const double* __restrict__ A, long long lda, int k0,
-                                                     const double* __restrict__ rdiag, double* __restrict__ y,
+                                                     const double* __restrict__ V, double* __restrict__ y,
                                                      double* __restrict__ x) {
-  extern __shared__ double Ts[];
-  __shared__ double sx[NB], rd[NB], red[8][32];
+  extern __shared__ double Vs[];
+  __shared__ double sb[NB], sx[NB], hred[2][NB], red[8][32];
   const int nb = min(NB, n - k0);
   const int lane = threadIdx.x & 31, wg = threadIdx.x >> 5;
-  stage_block<false>(nb, A, lda, k0, rdiag, Ts, rd);
-  if (wg == 0) {
-    double yl[NQ];
-#pragma unroll
-    for (int q = 0; q < NQ; q++) yl[q] = (lane + 32 * q < nb) ? y[k0 + lane + 32 * q] : 0.0;
-#pragma unroll
-    for (int qr = NQ - 1; qr >= 0; qr--) {
-      for (int rl = 31; rl >= 0; rl--) {
-        const int r = 32 * qr + rl;
-        if (r >= nb) continue;
-        const double xr = __shfl_sync(0xffffffffu, yl[qr], rl) * rd[r];
-        if (lane == rl) yl[qr] = xr;
-        const double* col = Ts + TLD * r;  // U(0:r, r)
-#pragma unroll
-        for (int q = 0; q <= qr; q++) {
-          const int p = lane + 32 * q;
-          if (p < r) yl[q] -= col[p] * xr;
-        }
+  stage_v(nb, V, y + k0, Vs, sb);
+  // sx[p] = sum_{q >= p} V(p, q) sb[q]: two threads per p (alternate q), consecutive p on consecutive lanes
+  {
+    const int p = threadIdx.x & (NB - 1), half = threadIdx.x / NB;
+    double a0 = 0.0, a1 = 0.0;
+    if (p < nb)
+      for (int q = p + half; q < nb; q += 4) {
+        a0 = fma(Vs[p + TLD * q], sb[q], a0);
+        if (q + 2 < nb) a1 = fma(Vs[p + TLD * (q + 2)], sb[q + 2], a1);
       }
-    }
-#pragma unroll
-    for (int q = 0; q < NQ; q++)
-      if (lane + 32 * q < nb) sx[lane + 32 * q] = yl[q];
+    hred[half][p] = a0 + a1;
   }
+  __syncthreads();
+  for (int p = threadIdx.x; p < nb; p += blockDim.x) sx[p] = hred[0][p] + hred[1][p];
   __syncthreads();
   if (blockIdx.x == 0)
     for (int p = threadIdx.x; p < nb; p += blockDim.x) x[k0 + p] = sx[p];
@@ -532,9 +555,13 @@ int sm_count() {
 // ---------------------------------------------------------------------------------------------------
 // host entry points
 // ---------------------------------------------------------------------------------------------------
-// In-place Cholesky of the upper triangle of A (n x n, lda = n); rdiag: n doubles, 1 / U(i, i) on return;
-// *d_info = 0 or the first failing column (1-based).
-cudaError_t rbmpp_potrf_upper(int n, double* A, double* rdiag, int* d_info, cudaStream_t st) {
+// Workspace of the factorisation: n reciprocal diagonal entries, then the inverted diagonal blocks.
+size_t rbmpp_chol_work(int n) { return (size_t)n + (size_t)((n + NB - 1) / NB) * NB * NB; }
+
+// In-place Cholesky of the upper triangle of A (n x n, lda = n); work: rbmpp_chol_work(n) doubles, holding
+// 1 / U(i, i) and the inverted diagonal blocks on return; *d_info = 0 or the first failing column (1-based).
+cudaError_t rbmpp_potrf_upper(int n, double* A, double* work, int* d_info, cudaStream_t st) {
+  double* rdiag = work;
   cudaError_t e = cudaMemsetAsync(d_info, 0, sizeof(int), st);
   if (e) return e;
   const size_t smem = (size_t)NB * (NB + 1) * sizeof(double);
@@ -552,11 +579,16 @@ cudaError_t rbmpp_potrf_upper(int n, double* A, double* rdiag, int* d_info, cuda
       if ((e = rbmpp_gemm_atb_upper_acc(n, NB, A + k0, 1, n, -1.0, A, n, k0 + NB, st))) return e;
     }
   }
+  if ((e = cudaFuncSetAttribute(invert_blocks_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)))
+    return e;
+  rbmpp_note_launch();
+  invert_blocks_kernel<<<(n + NB - 1) / NB, 512, smem, st>>>(n, A, n, rdiag, work + n);
   return cudaGetLastError();
 }
 
-// b <- A^{-1} b with A = U^T U (upper factor in A, reciprocal diagonal in rdiag); tmp: n doubles
-cudaError_t rbmpp_potrs_upper(int n, const double* A, const double* rdiag, double* b, double* tmp, cudaStream_t st) {
+// b <- A^{-1} b with A = U^T U (upper factor in A, work as rbmpp_potrf_upper left it); tmp: n doubles
+cudaError_t rbmpp_potrs_upper(int n, const double* A, const double* work, double* b, double* tmp, cudaStream_t st) {
+  const double* dinv = work + n;
   const int nsm = sm_count();
   const int nblk = (n + NB - 1) / NB;
   const size_t smem = (size_t)NB * TLD * sizeof(double);
@@ -567,13 +599,13 @@ cudaError_t rbmpp_potrs_upper(int n, const double* A, const double* rdiag, doubl
     const int k0 = kb * NB, rest = n - (k0 + NB);
     const int blocks = rest > 0 ? min(nsm, (rest + 31) / 32) : 1;
     rbmpp_note_launch();
-    trsv_fwd_step<<<blocks, 256, smem, st>>>(n, A, n, k0, rdiag, b, tmp);
+    trsv_fwd_step<<<blocks, 256, smem, st>>>(n, A, n, k0, dinv + (size_t)kb * NB * NB, b, tmp);
   }
   for (int kb = nblk - 1; kb >= 0; kb--) {  // U x = y: x in b, tmp consumed
     const int k0 = kb * NB;
     const int blocks = k0 > 0 ? min(nsm, (k0 + 31) / 32) : 1;
     rbmpp_note_launch();
-    trsv_bwd_step<<<blocks, 256, smem, st>>>(n, A, n, k0, rdiag, tmp, b);
+    trsv_bwd_step<<<blocks, 256, smem, st>>>(n, A, n, k0, dinv + (size_t)kb * NB * NB, tmp, b);
   }
   return cudaGetLastError();
 }
