@@ -31,7 +31,7 @@ cudaError_t rbmpp_launch_advance_rng(uint32_t*, const int*, int, int, int, cudaS
 cudaError_t rbmpp_syrk_ot_o(int, int, const double*, double*, cudaStream_t);
 cudaError_t rbmpp_symmetrize(int, double*, cudaStream_t);
 cudaError_t rbmpp_potrf_upper(int, double*, double*, int*, cudaStream_t);
-cudaError_t rbmpp_potrs_upper(int, const double*, const double*, double*, double*, cudaStream_t);
+cudaError_t rbmpp_potrs_upper(int, const double*, const double*, double*, double*, unsigned*, cudaStream_t);
 int rbmpp_gram_parts();
 size_t rbmpp_chol_work(int);
 cudaError_t rbmpp_sr_apply(int, int, int, const double*, const double*, double, double, double, const double*,
@@ -146,6 +146,7 @@ struct rbmpp_ctx {
   double* d_pcg = nullptr;   // refinement vectors (10 x Nv)
   double* d_gpart = nullptr; // per-block partial sums of the one-pass O^T (O y)
   double* d_sc = nullptr;    // device scalars of the refinement
+  unsigned* d_bar = nullptr; // grid barrier of the one-launch triangular solves
   double* h_sc = nullptr;    // pinned host copy of them
   // correlation measurement: per-sample rows (2 Nchi + 1), w SdotS rows (4N), ones, Chi_vbs blocks, sums
   double *d_crow = nullptr, *d_csd = nullptr, *d_cones = nullptr, *d_cvbs = nullptr, *d_cpart = nullptr,
@@ -264,6 +265,7 @@ int ensure_measure_buffers(rbmpp_ctx* c) {
   if ((r = dalloc(c, &c->d_pcg, (size_t)10 * d.Nv))) return r;
   if ((r = dalloc(c, &c->d_gpart, (size_t)rbmpp_gram_parts() * d.Nv))) return r;
   if ((r = dalloc(c, &c->d_sc, 8))) return r;
+  if ((r = dalloc(c, &c->d_bar, 4))) return r;
   CK(cudaMallocHost(&c->h_sc, 8 * sizeof(double)));
   return 0;
 }
@@ -489,7 +491,7 @@ int rbmpp_destroy(rbmpp_ctx* c) {
                   c->W.mt, c->W.nfastup, c->W.naccept, c->W.nacc_all, c->W.status, c->W.xs, c->W.pfs, c->W.psis, c->W.gj, c->W.events, c->W.trace, (void*)c->W.replay, c->d_O, c->d_psiS,
                   c->d_eloc, c->d_a, c->d_b, c->d_tmp_ns, c->d_acc4, c->d_nap, c->d_estat, c->d_gvec, c->d_Ovec,
                   c->d_vec, c->d_S, c->d_part, c->d_info, c->d_err, c->d_rv, c->d_hi, c->d_lo, c->d_Sf, c->d_Sb,
-                  c->d_crow, c->d_csd, c->d_cones, c->d_cvbs, c->d_cpart, c->d_csum, c->d_dinv, c->d_pcg, c->d_gpart, c->d_sc};
+                  c->d_crow, c->d_csd, c->d_cones, c->d_cvbs, c->d_cpart, c->d_csum, c->d_dinv, c->d_pcg, c->d_gpart, c->d_sc, c->d_bar};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (c->h_sc) cudaFreeHost(c->h_sc);
@@ -1059,9 +1061,10 @@ int rbmpp_sr_step(rbmpp_ctx* c, const rbmpp_sr_in* in, rbmpp_sr_out* out, double
   double *d_ap = v + VAP * nv, *d_tmp = v + VTMP * nv, *d_m = v + VM * nv;
   CK(cudaMemcpyAsync(d_g, g.data(), sizeof(double) * Nv, cudaMemcpyHostToDevice, c->st));
   CK(cudaMemcpyAsync(d_xv, g.data(), sizeof(double) * Nv, cudaMemcpyHostToDevice, c->st));
+  CK(cudaMemsetAsync(c->d_bar, 0, 4 * sizeof(unsigned), c->st));
   CK(cudaStreamSynchronize(c->st));
   if (info != 0) return fail(c, RBMPP_E_CHOL, "info (pdposv): %d", info);
-  CK(rbmpp_potrs_upper(Nv, c->d_S, c->d_dinv, d_xv, d_tmp, c->st));
+  CK(rbmpp_potrs_upper(Nv, c->d_S, c->d_dinv, d_xv, d_tmp, c->d_bar, c->st));
   CK(cudaEventRecord(c->ev[8], c->st));
   std::vector<double> x(Nv), ux(Nv), xr(Nv, 0.0), xp(Nv, 0.0);
   const double sigma = sdiag * s_factor;
@@ -1077,7 +1080,7 @@ int rbmpp_sr_step(rbmpp_ctx* c, const rbmpp_sr_in* in, rbmpp_sr_out* out, double
     if (r) return r;
     CK(rbmpp_pcg_start(Nv, d_g, d_ap, d_r, c->d_sc, c->st));
     CK(cudaMemcpyAsync(d_z, d_r, sizeof(double) * Nv, cudaMemcpyDeviceToDevice, c->st));
-    CK(rbmpp_potrs_upper(Nv, c->d_S, c->d_dinv, d_z, d_tmp, c->st));
+    CK(rbmpp_potrs_upper(Nv, c->d_S, c->d_dinv, d_z, d_tmp, c->d_bar, c->st));
     CK(rbmpp_pcg_dir(Nv, d_r, d_z, d_p, c->d_sc, 0, c->st));
     CK(cudaMemcpyAsync(c->h_sc, c->d_sc, 8 * sizeof(double), cudaMemcpyDeviceToHost, c->st));
     CK(cudaStreamSynchronize(c->st));
@@ -1088,7 +1091,7 @@ int rbmpp_sr_step(rbmpp_ctx* c, const rbmpp_sr_in* in, rbmpp_sr_out* out, double
       if ((r = apply_A(c, norm, scal, sigma, d_p, d_ap))) return r;
       CK(rbmpp_pcg_step(Nv, d_p, d_ap, d_xv, d_r, c->d_sc, c->st));
       CK(cudaMemcpyAsync(d_z, d_r, sizeof(double) * Nv, cudaMemcpyDeviceToDevice, c->st));
-      CK(rbmpp_potrs_upper(Nv, c->d_S, c->d_dinv, d_z, d_tmp, c->st));
+      CK(rbmpp_potrs_upper(Nv, c->d_S, c->d_dinv, d_z, d_tmp, c->d_bar, c->st));
       CK(rbmpp_pcg_dir(Nv, d_r, d_z, d_p, c->d_sc, 1, c->st));
       CK(cudaMemcpyAsync(c->h_sc, c->d_sc, 8 * sizeof(double), cudaMemcpyDeviceToHost, c->st));
       CK(cudaStreamSynchronize(c->st));
@@ -1148,6 +1151,9 @@ int rbmpp_sr_step(rbmpp_ctx* c, const rbmpp_sr_in* in, rbmpp_sr_out* out, double
     c->stats[4] = ms;
     c->stats[8] = refine_ms;
     c->stats[9] = attempts;
+    unsigned bar[4];
+    CK(cudaMemcpy(bar, c->d_bar, sizeof(bar), cudaMemcpyDeviceToHost));
+    if (bar[2]) return fail(c, RBMPP_E_TIMEOUT, "triangular solve: a bounded grid-barrier wait ran out");
   }
   double lrp = lam2 - lrr - lpp;
   double lam = std::sqrt(lam2);

@@ -223,9 +223,17 @@ __global__ void __launch_bounds__(512, 1) invert_blocks_kernel(int n, const doub
 // ---------------------------------------------------------------------------------------------------
 constexpr int TLD = NB + 1;
 
+// Vectors another CTA may have written since this CTA last read them are loaded past L1 (__ldcg) when the
+// steps run inside one persistent launch.
+template <bool COH>
+__device__ __forceinline__ double ldv(const double* p) {
+  return COH ? __ldcg(p) : *p;
+}
+
 // Vs[i + TLD j] = V(i, j) and the block's right-hand side rhs[0 .. nb) in shared memory
-__device__ __forceinline__ void stage_v(int nb, const double* __restrict__ V, const double* __restrict__ rhs,
-                                        double* Vs, double* sb) {
+template <bool COH>
+__device__ __forceinline__ void stage_v(int nb, const double* __restrict__ V, const double* rhs, double* Vs,
+                                        double* sb) {
   const int tot = NB * NB, step = blockDim.x;
   for (int e0 = threadIdx.x; e0 < tot; e0 += 8 * step) {
     double v[8];
@@ -237,40 +245,45 @@ __device__ __forceinline__ void stage_v(int nb, const double* __restrict__ V, co
       if (e < tot) Vs[(e % NB) + TLD * (e / NB)] = v[u];
     }
   }
-  for (int p = threadIdx.x; p < nb; p += blockDim.x) sb[p] = rhs[p];
+  for (int p = threadIdx.x; p < nb; p += blockDim.x) sb[p] = ldv<COH>(rhs + p);
   __syncthreads();
 }
 
-__global__ void __launch_bounds__(256) trsv_fwd_step(int n, const double* __restrict__ A, long long lda, int k0,
-                                                     const double* __restrict__ V, double* __restrict__ b,
-                                                     double* __restrict__ y) {
-  extern __shared__ double Vs[];
-  __shared__ double sb[NB], sy[NB], red[2][NB];
+struct StepSmem {
+  double* Vs;  // [NB][TLD]
+  double *sb, *sy, *hred, *red8;  // [NB], [NB], [2][NB], [8][32]
+};
+
+// One forward block step by CTA bid of nbk: y_k = V_k^T b_k into y (CTA 0 stores it), b_j -= U(k-block, j) . y_k
+template <bool COH>
+__device__ __forceinline__ void fwd_step(int n, const double* __restrict__ A, long long lda, int k0,
+                                         const double* __restrict__ V, double* b, double* y, const StepSmem& sm,
+                                         int bid, int nbk) {
   const int nb = min(NB, n - k0);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
-  stage_v(nb, V, b + k0, Vs, sb);
+  stage_v<COH>(nb, V, b + k0, sm.Vs, sm.sb);
   // sy[p] = sum_{q <= p} V(q, p) sb[q]: two threads per p (alternate q), consecutive p on consecutive lanes
   {
     const int p = threadIdx.x & (NB - 1), half = threadIdx.x / NB;
     double a0 = 0.0, a1 = 0.0;
     if (p < nb)
       for (int q = half; q <= p; q += 4) {
-        a0 = fma(Vs[q + TLD * p], sb[q], a0);
-        if (q + 2 <= p) a1 = fma(Vs[q + 2 + TLD * p], sb[q + 2], a1);
+        a0 = fma(sm.Vs[q + TLD * p], sm.sb[q], a0);
+        if (q + 2 <= p) a1 = fma(sm.Vs[q + 2 + TLD * p], sm.sb[q + 2], a1);
       }
-    red[half][p] = a0 + a1;
+    sm.hred[half * NB + p] = a0 + a1;
   }
   __syncthreads();
-  for (int p = threadIdx.x; p < nb; p += blockDim.x) sy[p] = red[0][p] + red[1][p];
+  for (int p = threadIdx.x; p < nb; p += blockDim.x) sm.sy[p] = sm.hred[p] + sm.hred[NB + p];
   __syncthreads();
-  if (blockIdx.x == 0)
-    for (int p = threadIdx.x; p < nb; p += blockDim.x) y[k0 + p] = sy[p];
+  if (bid == 0)
+    for (int p = threadIdx.x; p < nb; p += blockDim.x) y[k0 + p] = sm.sy[p];
   // b_j -= U(k-block, j) . y_k: four columns per warp at a time, all their loads issued before any sum
   double yl[NQ];
 #pragma unroll
-  for (int q = 0; q < NQ; q++) yl[q] = (lane + 32 * q < nb) ? sy[lane + 32 * q] : 0.0;
-  const int j0 = k0 + nb, ncol = n - j0, stride = gridDim.x * nwarps;
-  for (int c0 = (blockIdx.x * nwarps + warp) * 4; c0 < ncol; c0 += stride * 4) {
+  for (int q = 0; q < NQ; q++) yl[q] = (lane + 32 * q < nb) ? sm.sy[lane + 32 * q] : 0.0;
+  const int j0 = k0 + nb, ncol = n - j0, stride = nbk * nwarps;
+  for (int c0 = (bid * nwarps + warp) * 4; c0 < ncol; c0 += stride * 4) {
     double v[4][NQ];
 #pragma unroll
     for (int u = 0; u < 4; u++) {
@@ -284,38 +297,39 @@ __global__ void __launch_bounds__(256) trsv_fwd_step(int n, const double* __rest
 #pragma unroll
       for (int q = 0; q < NQ; q++) s = fma(v[u][q], yl[q], s);
       s = wsum(s);
-      if (lane == 0 && c0 + u < ncol) b[j0 + c0 + u] -= s;
+      if (lane == 0 && c0 + u < ncol) b[j0 + c0 + u] = ldv<COH>(b + j0 + c0 + u) - s;
     }
   }
 }
 
-__global__ void __launch_bounds__(256) trsv_bwd_step(int n, const double* __restrict__ A, long long lda, int k0,
-                                                     const double* __restrict__ V, double* __restrict__ y,
-                                                     double* __restrict__ x) {
-  extern __shared__ double Vs[];
-  __shared__ double sb[NB], sx[NB], hred[2][NB], red[8][32];
+// One backward block step: x_k = V_k y_k into x (CTA 0 stores it), y_i -= U(i, k-block) . x_k for i < k0
+template <bool COH>
+__device__ __forceinline__ void bwd_step(int n, const double* __restrict__ A, long long lda, int k0,
+                                         const double* __restrict__ V, double* y, double* x, const StepSmem& sm,
+                                         int bid, int nbk) {
   const int nb = min(NB, n - k0);
   const int lane = threadIdx.x & 31, wg = threadIdx.x >> 5;
-  stage_v(nb, V, y + k0, Vs, sb);
+  stage_v<COH>(nb, V, y + k0, sm.Vs, sm.sb);
   // sx[p] = sum_{q >= p} V(p, q) sb[q]: two threads per p (alternate q), consecutive p on consecutive lanes
   {
     const int p = threadIdx.x & (NB - 1), half = threadIdx.x / NB;
     double a0 = 0.0, a1 = 0.0;
     if (p < nb)
       for (int q = p + half; q < nb; q += 4) {
-        a0 = fma(Vs[p + TLD * q], sb[q], a0);
-        if (q + 2 < nb) a1 = fma(Vs[p + TLD * (q + 2)], sb[q + 2], a1);
+        a0 = fma(sm.Vs[p + TLD * q], sm.sb[q], a0);
+        if (q + 2 < nb) a1 = fma(sm.Vs[p + TLD * (q + 2)], sm.sb[q + 2], a1);
       }
-    hred[half][p] = a0 + a1;
+    sm.hred[half * NB + p] = a0 + a1;
   }
   __syncthreads();
-  for (int p = threadIdx.x; p < nb; p += blockDim.x) sx[p] = hred[0][p] + hred[1][p];
+  double* sx = sm.sy;
+  for (int p = threadIdx.x; p < nb; p += blockDim.x) sx[p] = sm.hred[p] + sm.hred[NB + p];
   __syncthreads();
-  if (blockIdx.x == 0)
+  if (bid == 0)
     for (int p = threadIdx.x; p < nb; p += blockDim.x) x[k0 + p] = sx[p];
-  // y_i -= U(i, k-block) . x_k for i < k0: the block takes 32 rows, its 8 warps 16 columns each (each lane one
-  // row, coalesced across the warp), and the 8 partial sums of a row meet in shared memory
-  for (int i0 = blockIdx.x * 32; i0 < k0; i0 += gridDim.x * 32) {
+  // y_i -= U(i, k-block) . x_k for i < k0: 32 rows per CTA pass, its 8 warps 16 columns each (each lane one
+  // row, coalesced across the warp); the 8 partial sums of a row meet in shared memory
+  for (int i0 = bid * 32; i0 < k0; i0 += nbk * 32) {
     const int i = i0 + lane;
     double a[16];
 #pragma unroll
@@ -329,14 +343,73 @@ __global__ void __launch_bounds__(256) trsv_bwd_step(int n, const double* __rest
       const int p = wg * 16 + t;
       s = fma(a[t], p < nb ? sx[p] : 0.0, s);
     }
-    red[wg][lane] = s;
+    sm.red8[wg * 32 + lane] = s;
     __syncthreads();
     if (wg == 0 && i < k0) {
       double t8 = 0.0;
-      for (int g = 0; g < 8; g++) t8 += red[g][lane];
-      y[i] -= t8;
+      for (int g = 0; g < 8; g++) t8 += sm.red8[g * 32 + lane];
+      y[i] = ldv<COH>(y + i) - t8;
     }
     __syncthreads();
+  }
+}
+
+__global__ void __launch_bounds__(256) trsv_fwd_step(int n, const double* __restrict__ A, long long lda, int k0,
+                                                     const double* __restrict__ V, double* b, double* y) {
+  extern __shared__ double Vs[];
+  __shared__ double sb[NB], sy[NB], hred[2 * NB], red8[8 * 32];
+  fwd_step<false>(n, A, lda, k0, V, b, y, StepSmem{Vs, sb, sy, hred, red8}, blockIdx.x, gridDim.x);
+}
+
+__global__ void __launch_bounds__(256) trsv_bwd_step(int n, const double* __restrict__ A, long long lda, int k0,
+                                                     const double* __restrict__ V, double* y, double* x) {
+  extern __shared__ double Vs[];
+  __shared__ double sb[NB], sy[NB], hred[2 * NB], red8[8 * 32];
+  bwd_step<false>(n, A, lda, k0, V, y, x, StepSmem{Vs, sb, sy, hred, red8}, blockIdx.x, gridDim.x);
+}
+
+// Barrier of all CTAs of a cooperative launch: bar[0] arrival count, bar[1] generation, bar[2] set to 1 when a
+// wait ran out (bounded: the CTA then goes on, and the host reports the error).
+__device__ __forceinline__ void grid_sync(unsigned* bar, unsigned nblocks) {
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    volatile unsigned* gen = bar + 1;
+    const unsigned g = *gen;
+    __threadfence();
+    if (atomicAdd(bar, 1u) + 1u == nblocks) {
+      bar[0] = 0u;
+      __threadfence();
+      atomicAdd(bar + 1, 1u);
+    } else {
+      for (int it = 0; *gen == g; it++) {
+        if (it > (1 << 24)) {
+          atomicExch(bar + 2, 1u);
+          break;
+        }
+        __nanosleep(32);
+      }
+    }
+    __threadfence();
+  }
+  __syncthreads();
+}
+
+// Both triangular solves in one cooperative launch (all CTAs resident), a grid barrier between block steps:
+// U^T y = b (y in tmp, b consumed), then U x = y (x in b).
+__global__ void __launch_bounds__(256, 1) potrs_persistent_kernel(int n, const double* __restrict__ A,
+                                                                  const double* __restrict__ dinv, double* b,
+                                                                  double* tmp, unsigned* bar) {
+  extern __shared__ double Vs[];
+  __shared__ double sb[NB], sy[NB], hred[2 * NB], red8[8 * 32];
+  const StepSmem sm{Vs, sb, sy, hred, red8};
+  const int nblk = (n + NB - 1) / NB;
+  for (int kb = 0; kb < nblk; kb++) {
+    fwd_step<true>(n, A, n, kb * NB, dinv + (size_t)kb * NB * NB, b, tmp, sm, blockIdx.x, gridDim.x);
+    grid_sync(bar, gridDim.x);
+  }
+  for (int kb = nblk - 1; kb >= 0; kb--) {
+    bwd_step<true>(n, A, n, kb * NB, dinv + (size_t)kb * NB * NB, tmp, b, sm, blockIdx.x, gridDim.x);
+    if (kb > 0) grid_sync(bar, gridDim.x);
   }
 }
 
@@ -586,13 +659,39 @@ cudaError_t rbmpp_potrf_upper(int n, double* A, double* work, int* d_info, cudaS
   return cudaGetLastError();
 }
 
-// b <- A^{-1} b with A = U^T U (upper factor in A, work as rbmpp_potrf_upper left it); tmp: n doubles
-cudaError_t rbmpp_potrs_upper(int n, const double* A, const double* work, double* b, double* tmp, cudaStream_t st) {
+// b <- A^{-1} b with A = U^T U (upper factor in A, work as rbmpp_potrf_upper left it); tmp: n doubles.
+// bar: 4 unsigned of device memory for the persistent form (one cooperative launch); bar[2] becomes 1 if one of
+// its bounded barrier waits ran out.  Without bar, or where the cooperative launch is refused, one launch per
+// block step.
+cudaError_t rbmpp_potrs_upper(int n, const double* A, const double* work, double* b, double* tmp, unsigned* bar,
+                              cudaStream_t st) {
   const double* dinv = work + n;
   const int nsm = sm_count();
   const int nblk = (n + NB - 1) / NB;
   const size_t smem = (size_t)NB * TLD * sizeof(double);
   cudaError_t e;
+  if (bar) {
+    static int coop = -1;  // the device supports cooperative launches with this shape
+    if (coop < 0) {
+      int dev = 0, attr = 0, nb_sm = 0;
+      cudaGetDevice(&dev);
+      cudaDeviceGetAttribute(&attr, cudaDevAttrCooperativeLaunch, dev);
+      cudaFuncSetAttribute(potrs_persistent_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb_sm, potrs_persistent_kernel, 256, smem);
+      coop = (attr && nb_sm >= 1) ? 1 : 0;
+      cudaGetLastError();
+    }
+    if (coop) {
+      if ((e = cudaMemsetAsync(bar, 0, 2 * sizeof(unsigned), st))) return e;  // count, generation (bar[2] sticks)
+      int nn = n;
+      void* args[] = {&nn, (void*)&A, (void*)&dinv, &b, &tmp, &bar};
+      rbmpp_note_launch();
+      e = cudaLaunchCooperativeKernel((const void*)potrs_persistent_kernel, dim3(nsm), dim3(256), args, smem, st);
+      if (e == cudaSuccess) return cudaSuccess;
+      cudaGetLastError();
+      coop = 0;
+    }
+  }
   if ((e = cudaFuncSetAttribute(trsv_fwd_step, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem))) return e;
   if ((e = cudaFuncSetAttribute(trsv_bwd_step, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem))) return e;
   for (int kb = 0; kb < nblk; kb++) {  // U^T y = b: y in tmp, b consumed
