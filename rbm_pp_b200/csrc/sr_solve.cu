@@ -15,6 +15,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include "tma.cuh"
+
 void rbmpp_note_launch();  // capi.cu: counts kernel launches
 cudaError_t rbmpp_gemm_atb_upper_acc(int n, int K, const double* A, long long sk, long long si, double alpha,
                                      double* C, long long ldc, int row0, cudaStream_t st);
@@ -26,6 +28,13 @@ namespace {
 
 constexpr int NB = 128;
 constexpr int NQ = NB / 32;  // rows of a block column held by one lane
+// An inverted diagonal block is kept as two packed upper triangles (NB (NB + 1) / 2 doubles each, 16-byte
+// multiples): by rows, V(q, q..NB-1) from off_rows(q), for the forward solve (y_p = sum_{q <= p} V(q, p) b_q
+// reads consecutive p), and by columns, V(0..q, q) from off_cols(q), for the backward one
+// (x_p = sum_{q >= p} V(p, q) y_q reads consecutive p).
+constexpr int PK = NB * (NB + 1) / 2;
+__host__ __device__ __forceinline__ int off_rows(int q) { return q * NB - q * (q - 1) / 2; }
+__host__ __device__ __forceinline__ int off_cols(int q) { return q * (q + 1) / 2; }
 
 __device__ __forceinline__ double wsum(double v) {
 #pragma unroll
@@ -178,7 +187,7 @@ __global__ void __launch_bounds__(512) panel_kernel(int n, double* __restrict__ 
 // ---------------------------------------------------------------------------------------------------
 // Inverses of all diagonal factor blocks at once (one CTA per block, after the factorisation): V_k = U_kk^{-1}
 // (upper), column c by back substitution v_i = (delta_ic - sum_{i < j <= c} U(i, j) v_j) / U(i, i), one warp
-// per column, U_kk in shared memory.  dinv: [block][NB][NB] column-major.
+// per column, U_kk in shared memory.  dinv: nblk triangles packed by rows, then nblk packed by columns.
 // ---------------------------------------------------------------------------------------------------
 __global__ void __launch_bounds__(512, 1) invert_blocks_kernel(int n, const double* __restrict__ A, long long lda,
                                                                const double* __restrict__ rdiag,
@@ -189,7 +198,8 @@ __global__ void __launch_bounds__(512, 1) invert_blocks_kernel(int n, const doub
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
   load_block<false>(nb, A, lda, k0, U, 1, LD);
   __syncthreads();
-  double* V = dinv + (size_t)blockIdx.x * NB * NB;
+  double* VR = dinv + (size_t)blockIdx.x * PK;                          // packed by rows
+  double* VC = dinv + (size_t)(gridDim.x + blockIdx.x) * PK;             // packed by columns
   for (int c = warp; c < NB; c += nwarps) {
     double v[NQ];
 #pragma unroll
@@ -210,7 +220,14 @@ __global__ void __launch_bounds__(512, 1) invert_blocks_kernel(int n, const doub
       }
     }
 #pragma unroll
-    for (int q = 0; q < NQ; q++) V[(lane + 32 * q) + NB * c] = (c < nb && lane + 32 * q < nb) ? v[q] : 0.0;
+    for (int q = 0; q < NQ; q++) {
+      const int i = lane + 32 * q;  // V(i, c), i <= c
+      if (i <= c) {
+        const double vi = (c < nb && i < nb) ? v[q] : 0.0;
+        VR[off_rows(i) + (c - i)] = vi;
+        VC[off_cols(c) + i] = vi;
+      }
+    }
   }
 }
 
@@ -221,8 +238,6 @@ __global__ void __launch_bounds__(512, 1) invert_blocks_kernel(int n, const doub
 // x_k = V_k y_k, then y_i -= U(i, k-block) . x_k for i < k0.  The block's result goes to a separate vector, so
 // no CTA reads what another one writes within the step.
 // ---------------------------------------------------------------------------------------------------
-constexpr int TLD = NB + 1;
-
 // Vectors another CTA may have written since this CTA last read them are loaded past L1 (__ldcg) when the
 // steps run inside one persistent launch.
 template <bool COH>
@@ -230,46 +245,51 @@ __device__ __forceinline__ double ldv(const double* p) {
   return COH ? __ldcg(p) : *p;
 }
 
-// Vs[i + TLD j] = V(i, j) and the block's right-hand side rhs[0 .. nb) in shared memory
+// A packed triangle Vp (PK doubles) and the block's right-hand side rhs[0 .. nb) into shared memory
 template <bool COH>
-__device__ __forceinline__ void stage_v(int nb, const double* __restrict__ V, const double* rhs, double* Vs,
+__device__ __forceinline__ void stage_v(int nb, const double* __restrict__ Vp, const double* rhs, double* Vs,
                                         double* sb) {
-  const int tot = NB * NB, step = blockDim.x;
-  for (int e0 = threadIdx.x; e0 < tot; e0 += 8 * step) {
+  const int step = blockDim.x;
+  for (int e0 = threadIdx.x; e0 < PK; e0 += 8 * step) {
     double v[8];
 #pragma unroll
-    for (int u = 0; u < 8; u++) v[u] = (e0 + u * step < tot) ? V[e0 + u * step] : 0.0;
+    for (int u = 0; u < 8; u++) v[u] = (e0 + u * step < PK) ? Vp[e0 + u * step] : 0.0;
 #pragma unroll
-    for (int u = 0; u < 8; u++) {
-      const int e = e0 + u * step;
-      if (e < tot) Vs[(e % NB) + TLD * (e / NB)] = v[u];
-    }
+    for (int u = 0; u < 8; u++)
+      if (e0 + u * step < PK) Vs[e0 + u * step] = v[u];
   }
   for (int p = threadIdx.x; p < nb; p += blockDim.x) sb[p] = ldv<COH>(rhs + p);
   __syncthreads();
 }
 
 struct StepSmem {
-  double* Vs;  // [NB][TLD]
+  double* Vs;  // a packed triangle (PK)
   double *sb, *sy, *hred, *red8;  // [NB], [NB], [2][NB], [8][32]
 };
 
 // One forward block step by CTA bid of nbk: y_k = V_k^T b_k into y (CTA 0 stores it), b_j -= U(k-block, j) . y_k
+// V: the block's triangle packed by rows (staged here), or null when sm.Vs already holds it and only the
+// right-hand side is to be staged
 template <bool COH>
 __device__ __forceinline__ void fwd_step(int n, const double* __restrict__ A, long long lda, int k0,
                                          const double* __restrict__ V, double* b, double* y, const StepSmem& sm,
                                          int bid, int nbk) {
   const int nb = min(NB, n - k0);
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nwarps = blockDim.x >> 5;
-  stage_v<COH>(nb, V, b + k0, sm.Vs, sm.sb);
+  if (V) {
+    stage_v<COH>(nb, V, b + k0, sm.Vs, sm.sb);
+  } else {
+    for (int p = threadIdx.x; p < nb; p += blockDim.x) sm.sb[p] = ldv<COH>(b + k0 + p);
+    __syncthreads();
+  }
   // sy[p] = sum_{q <= p} V(q, p) sb[q]: two threads per p (alternate q), consecutive p on consecutive lanes
   {
     const int p = threadIdx.x & (NB - 1), half = threadIdx.x / NB;
     double a0 = 0.0, a1 = 0.0;
     if (p < nb)
       for (int q = half; q <= p; q += 4) {
-        a0 = fma(sm.Vs[q + TLD * p], sm.sb[q], a0);
-        if (q + 2 <= p) a1 = fma(sm.Vs[q + 2 + TLD * p], sm.sb[q + 2], a1);
+        a0 = fma(sm.Vs[off_rows(q) + p - q], sm.sb[q], a0);
+        if (q + 2 <= p) a1 = fma(sm.Vs[off_rows(q + 2) + p - q - 2], sm.sb[q + 2], a1);
       }
     sm.hred[half * NB + p] = a0 + a1;
   }
@@ -303,21 +323,27 @@ __device__ __forceinline__ void fwd_step(int n, const double* __restrict__ A, lo
 }
 
 // One backward block step: x_k = V_k y_k into x (CTA 0 stores it), y_i -= U(i, k-block) . x_k for i < k0
+// V: the block's triangle packed by columns (staged here), or null when sm.Vs already holds it
 template <bool COH>
 __device__ __forceinline__ void bwd_step(int n, const double* __restrict__ A, long long lda, int k0,
                                          const double* __restrict__ V, double* y, double* x, const StepSmem& sm,
                                          int bid, int nbk) {
   const int nb = min(NB, n - k0);
   const int lane = threadIdx.x & 31, wg = threadIdx.x >> 5;
-  stage_v<COH>(nb, V, y + k0, sm.Vs, sm.sb);
+  if (V) {
+    stage_v<COH>(nb, V, y + k0, sm.Vs, sm.sb);
+  } else {
+    for (int p = threadIdx.x; p < nb; p += blockDim.x) sm.sb[p] = ldv<COH>(y + k0 + p);
+    __syncthreads();
+  }
   // sx[p] = sum_{q >= p} V(p, q) sb[q]: two threads per p (alternate q), consecutive p on consecutive lanes
   {
     const int p = threadIdx.x & (NB - 1), half = threadIdx.x / NB;
     double a0 = 0.0, a1 = 0.0;
     if (p < nb)
       for (int q = p + half; q < nb; q += 4) {
-        a0 = fma(sm.Vs[p + TLD * q], sm.sb[q], a0);
-        if (q + 2 < nb) a1 = fma(sm.Vs[p + TLD * (q + 2)], sm.sb[q + 2], a1);
+        a0 = fma(sm.Vs[off_cols(q) + p], sm.sb[q], a0);
+        if (q + 2 < nb) a1 = fma(sm.Vs[off_cols(q + 2) + p], sm.sb[q + 2], a1);
       }
     sm.hred[half * NB + p] = a0 + a1;
   }
@@ -395,21 +421,48 @@ __device__ __forceinline__ void grid_sync(unsigned* bar, unsigned nblocks) {
 }
 
 // Both triangular solves in one cooperative launch (all CTAs resident), a grid barrier between block steps:
-// U^T y = b (y in tmp, b consumed), then U x = y (x in b).
+// U^T y = b (y in tmp, b consumed), then U x = y (x in b).  Step s uses triangle s of the sequence (forward
+// blocks 0..nblk-1 packed by rows, then backward blocks nblk-1..0 packed by columns); thread 0 copies the next
+// step's triangle into the other shared-memory buffer (one bulk copy) while the current step computes.
 __global__ void __launch_bounds__(256, 1) potrs_persistent_kernel(int n, const double* __restrict__ A,
                                                                   const double* __restrict__ dinv, double* b,
                                                                   double* tmp, unsigned* bar) {
-  extern __shared__ double Vs[];
+  extern __shared__ __align__(128) double Vbuf[];  // [2][PK]
   __shared__ double sb[NB], sy[NB], hred[2 * NB], red8[8 * 32];
-  const StepSmem sm{Vs, sb, sy, hred, red8};
-  const int nblk = (n + NB - 1) / NB;
-  for (int kb = 0; kb < nblk; kb++) {
-    fwd_step<true>(n, A, n, kb * NB, dinv + (size_t)kb * NB * NB, b, tmp, sm, blockIdx.x, gridDim.x);
-    grid_sync(bar, gridDim.x);
+  __shared__ __align__(8) uint64_t full[2];
+  const int nblk = (n + NB - 1) / NB, nsteps = 2 * nblk;
+  auto tri = [&](int st) -> const double* {
+    return st < nblk ? dinv + (size_t)st * PK : dinv + (size_t)(nblk + (2 * nblk - 1 - st)) * PK;
+  };
+  constexpr uint32_t kBytes = PK * sizeof(double);
+  if (threadIdx.x == 0) {
+    mbar_init(&full[0], 1);
+    mbar_init(&full[1], 1);
+    fence_mbar_init();
+    mbar_arrive_expect_tx(&full[0], kBytes);
+    bulk_load(Vbuf, tri(0), kBytes, &full[0]);
   }
-  for (int kb = nblk - 1; kb >= 0; kb--) {
-    bwd_step<true>(n, A, n, kb * NB, dinv + (size_t)kb * NB * NB, tmp, b, sm, blockIdx.x, gridDim.x);
-    if (kb > 0) grid_sync(bar, gridDim.x);
+  __syncthreads();
+  for (int st = 0; st < nsteps; st++) {
+    const int buf = st & 1;
+    if (threadIdx.x == 0 && st + 1 < nsteps) {
+      fence_proxy_async_smem();  // the other buffer's generic reads (step st - 1) come before its refill
+      mbar_arrive_expect_tx(&full[buf ^ 1], kBytes);
+      bulk_load(Vbuf + (buf ^ 1) * PK, tri(st + 1), kBytes, &full[buf ^ 1]);
+    }
+    if (!mbar_wait(&full[buf], (uint32_t)((st >> 1) & 1))) {
+      atomicExch(bar + 2, 1u);
+      // the copy may still land: wait for it (bounded) before its buffer is reused or the CTA exits
+      (void)mbar_wait(&full[buf], (uint32_t)((st >> 1) & 1));
+    }
+    const StepSmem sm{Vbuf + buf * PK, sb, sy, hred, red8};
+    if (st < nblk) {
+      fwd_step<true>(n, A, n, st * NB, nullptr, b, tmp, sm, blockIdx.x, gridDim.x);
+    } else {
+      const int kb = 2 * nblk - 1 - st;
+      bwd_step<true>(n, A, n, kb * NB, nullptr, tmp, b, sm, blockIdx.x, gridDim.x);
+    }
+    if (st + 1 < nsteps) grid_sync(bar, gridDim.x);
   }
 }
 
@@ -629,12 +682,12 @@ int sm_count() {
 // host entry points
 // ---------------------------------------------------------------------------------------------------
 // Workspace of the factorisation: n reciprocal diagonal entries, then the inverted diagonal blocks.
-size_t rbmpp_chol_work(int n) { return (size_t)n + (size_t)((n + NB - 1) / NB) * NB * NB; }
+size_t rbmpp_chol_work(int n) { return (size_t)2 * ((n + NB - 1) / NB) * PK + (size_t)n; }
 
 // In-place Cholesky of the upper triangle of A (n x n, lda = n); work: rbmpp_chol_work(n) doubles, holding
 // 1 / U(i, i) and the inverted diagonal blocks on return; *d_info = 0 or the first failing column (1-based).
 cudaError_t rbmpp_potrf_upper(int n, double* A, double* work, int* d_info, cudaStream_t st) {
-  double* rdiag = work;
+  double* rdiag = work + (size_t)2 * ((n + NB - 1) / NB) * PK;  // after the packed triangles (16-byte aligned)
   cudaError_t e = cudaMemsetAsync(d_info, 0, sizeof(int), st);
   if (e) return e;
   const size_t smem = (size_t)NB * (NB + 1) * sizeof(double);
@@ -655,7 +708,7 @@ cudaError_t rbmpp_potrf_upper(int n, double* A, double* work, int* d_info, cudaS
   if ((e = cudaFuncSetAttribute(invert_blocks_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)))
     return e;
   rbmpp_note_launch();
-  invert_blocks_kernel<<<(n + NB - 1) / NB, 512, smem, st>>>(n, A, n, rdiag, work + n);
+  invert_blocks_kernel<<<(n + NB - 1) / NB, 512, smem, st>>>(n, A, n, rdiag, work);
   return cudaGetLastError();
 }
 
@@ -665,10 +718,10 @@ cudaError_t rbmpp_potrf_upper(int n, double* A, double* work, int* d_info, cudaS
 // block step.
 cudaError_t rbmpp_potrs_upper(int n, const double* A, const double* work, double* b, double* tmp, unsigned* bar,
                               cudaStream_t st) {
-  const double* dinv = work + n;
+  const double* dinv = work;
   const int nsm = sm_count();
   const int nblk = (n + NB - 1) / NB;
-  const size_t smem = (size_t)NB * TLD * sizeof(double);
+  const size_t smem = (size_t)PK * sizeof(double), psmem = 2 * smem;
   cudaError_t e;
   if (bar) {
     static int coop = -1;  // the device supports cooperative launches with this shape
@@ -676,8 +729,8 @@ cudaError_t rbmpp_potrs_upper(int n, const double* A, const double* work, double
       int dev = 0, attr = 0, nb_sm = 0;
       cudaGetDevice(&dev);
       cudaDeviceGetAttribute(&attr, cudaDevAttrCooperativeLaunch, dev);
-      cudaFuncSetAttribute(potrs_persistent_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb_sm, potrs_persistent_kernel, 256, smem);
+      cudaFuncSetAttribute(potrs_persistent_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)psmem);
+      cudaOccupancyMaxActiveBlocksPerMultiprocessor(&nb_sm, potrs_persistent_kernel, 256, psmem);
       coop = (attr && nb_sm >= 1) ? 1 : 0;
       cudaGetLastError();
     }
@@ -686,7 +739,7 @@ cudaError_t rbmpp_potrs_upper(int n, const double* A, const double* work, double
       int nn = n;
       void* args[] = {&nn, (void*)&A, (void*)&dinv, &b, &tmp, &bar};
       rbmpp_note_launch();
-      e = cudaLaunchCooperativeKernel((const void*)potrs_persistent_kernel, dim3(nsm), dim3(256), args, smem, st);
+      e = cudaLaunchCooperativeKernel((const void*)potrs_persistent_kernel, dim3(nsm), dim3(256), args, psmem, st);
       if (e == cudaSuccess) return cudaSuccess;
       cudaGetLastError();
       coop = 0;
@@ -698,13 +751,13 @@ cudaError_t rbmpp_potrs_upper(int n, const double* A, const double* work, double
     const int k0 = kb * NB, rest = n - (k0 + NB);
     const int blocks = rest > 0 ? min(nsm, (rest + 31) / 32) : 1;
     rbmpp_note_launch();
-    trsv_fwd_step<<<blocks, 256, smem, st>>>(n, A, n, k0, dinv + (size_t)kb * NB * NB, b, tmp);
+    trsv_fwd_step<<<blocks, 256, smem, st>>>(n, A, n, k0, dinv + (size_t)kb * PK, b, tmp);
   }
   for (int kb = nblk - 1; kb >= 0; kb--) {  // U x = y: x in b, tmp consumed
     const int k0 = kb * NB;
     const int blocks = k0 > 0 ? min(nsm, (k0 + 31) / 32) : 1;
     rbmpp_note_launch();
-    trsv_bwd_step<<<blocks, 256, smem, st>>>(n, A, n, k0, dinv + (size_t)kb * NB * NB, tmp, b);
+    trsv_bwd_step<<<blocks, 256, smem, st>>>(n, A, n, k0, dinv + (size_t)(nblk + kb) * PK, tmp, b);
   }
   return cudaGetLastError();
 }
