@@ -40,7 +40,8 @@ enum {
   RBMPP_E_LAMBDA = 12,      /* lambda block split check (SR_pdposv.f90:308)                       */
   RBMPP_E_CUDA = 20,        /* CUDA runtime error                                                 */
   RBMPP_E_STATE = 21,       /* call out of order (e.g. measure before make_sample)                */
-  RBMPP_E_TIMEOUT = 22      /* a bounded device-side wait ran out (copy pipeline did not progress) */
+  RBMPP_E_TIMEOUT = 22,     /* a bounded device-side wait ran out (copy pipeline did not progress) */
+  RBMPP_E_COMM = 23         /* the host all-reduce of rbmpp_set_allreduce returned non-zero         */
 };
 
 /* Sizes (RBM.input, sym_info.txt, orbitalidx.def; main.f90:75-141). */
@@ -157,6 +158,22 @@ int rbmpp_measure_correlation(rbmpp_ctx* ctx, double* scal, double* chi_sp, doub
  *              host scal6 = {Etot, Etot2, norm, wf_av, naccept_total, n_samples};
  * direction 1: load reduced sums (same layout) back for rbmpp_sr_step. */
 int rbmpp_exchange_measurement(rbmpp_ctx* ctx, int direction, double* d_S, double* d_g, double* d_ov, double* scal6);
+
+/* Cross-rank sums done by the library itself, through a host-supplied all-reduce: fn(user, buf, n) must sum
+ * n doubles at the DEVICE address buf over all ranks, in place, and return 0 when the result is in buf (the
+ * library's stream is synchronised before the call and its next launch follows the return).  Every rank
+ * must get bit-identical sums (NCCL and MPI all-reduces do).  With it set:
+ *  - rbmpp_measure reduces {Etot, Etot2, norm, wf_av, naccept_total, n_samples}, gvec and Ovec in one call,
+ *    and rbmpp_measure_energy the scalars: the MPI_ALLREDUCE calls of main.f90:348-369;
+ *  - the S build reduces each rank's S (Nv x Nv): S_raw in FP64, or, in split-BF16, the centred product of the
+ *    rank's samples about the global mean plus the exact FP64 diagonal, before the global mean is added back;
+ *  - the split-BF16 refinement reduces O^T (O x) (Nv doubles) once per conjugate-gradient iteration, so it
+ *    runs on the exact S of all ranks' samples (SR_pdposv.f90:232 distributed as pdposv is);
+ *  - rbmpp_exchange_measurement is refused (the context reduces by itself).
+ * Every rank then takes identical SR steps (the parameter broadcast of main.f90:427-438 is not needed).
+ * fn = NULL switches it off. */
+typedef int (*rbmpp_allreduce_fn)(void* user, double* buf, long long n);
+int rbmpp_set_allreduce(rbmpp_ctx* ctx, rbmpp_allreduce_fn fn, void* user);
 
 /* SR block (SR_pdposv.f90:1-432 with the normalisation of main.f90:351-369) on the device-resident
  * measurement of the last rbmpp_measure; replaces pdposv.  Updates the parameters in place.

@@ -24,10 +24,29 @@ EXPORTS = ["rbmpp_create", "rbmpp_destroy", "rbmpp_last_error", "rbmpp_query", "
            "rbmpp_set_s_precision", "rbmpp_batch_create", "rbmpp_batch_destroy", "rbmpp_batch_last_error",
            "rbmpp_batch_tune", "rbmpp_batch_make_sample", "rbmpp_measure_correlation",
            "rbmpp_get_walker_events", "rbmpp_set_trace", "rbmpp_set_replay", "rbmpp_debug_hook",
-           "rbmpp_copy_state"]
+           "rbmpp_copy_state", "rbmpp_set_allreduce"]
 
 SR_FP64 = 0
 SR_SPLIT_BF16 = 1
+
+# int (*)(void* user, double* device_buffer, long long n): the host all-reduce of rbmpp_set_allreduce
+ALLREDUCE_FN = C.CFUNCTYPE(C.c_int, C.c_void_p, C.c_void_p, C.c_longlong)
+
+
+def allreduce_callback(fn, on_error=None):
+    """The C function pointer rbmpp_set_allreduce takes, around fn(pointer: int, n: int) -> None: returns 0,
+    or 1 after an exception (passed to on_error)."""
+
+    def _cb(user, ptr, n):
+        try:
+            fn(int(ptr), int(n))
+            return 0
+        except Exception as e:
+            if on_error is not None:
+                on_error(e)
+            return 1
+
+    return ALLREDUCE_FN(_cb)
 
 
 class Dims(C.Structure):
@@ -94,6 +113,7 @@ def lib():
         L.rbmpp_set_replay.argtypes = [P, P, C.c_int]
         L.rbmpp_debug_hook.argtypes = [P, C.c_int, C.c_int]
         L.rbmpp_copy_state.argtypes = [P, P]
+        L.rbmpp_set_allreduce.argtypes = [P, ALLREDUCE_FN, P]
         L.rbmpp_eval_configs_noalloc.argtypes = [P, C.c_int, P, P, P, P]
         L.rbmpp_set_s_precision.argtypes = [P, C.c_int]
         L.rbmpp_batch_create.argtypes = [P, C.c_int, C.POINTER(P)]
@@ -285,6 +305,21 @@ class Context:
 
     def set_shift(self, shift):
         self._chk(lib().rbmpp_set_shift(self.h, float(shift)))
+
+    def set_allreduce(self, fn):
+        """fn(device_pointer: int, n: int) -> None sums n float64 at the device address over all ranks in place
+        (None switches the library's own reductions off).  An exception in fn becomes RBMPP_E_COMM; the
+        exception itself is kept in self.allreduce_error."""
+        if fn is None:
+            self._allreduce = None
+            self._chk(lib().rbmpp_set_allreduce(self.h, ALLREDUCE_FN(), None))
+            return
+
+        def on_error(e):
+            self.allreduce_error = e
+
+        self._allreduce = allreduce_callback(fn, on_error)  # kept alive while the context uses it
+        self._chk(lib().rbmpp_set_allreduce(self.h, self._allreduce, None))
 
     def exchange_measurement(self, direction, S_ptr, g_ptr, ov_ptr, scal6):
         """Device pointers (ints) for S, gvec, Ovec; scal6 a float64 array of 6."""

@@ -34,8 +34,10 @@ cudaError_t rbmpp_potrf_upper(int, double*, double*, int*, cudaStream_t);
 cudaError_t rbmpp_potrs_upper(int, const double*, const double*, double*, double*, unsigned*, cudaStream_t);
 int rbmpp_gram_parts();
 size_t rbmpp_chol_work(int);
-cudaError_t rbmpp_sr_apply(int, int, int, const double*, const double*, double, double, double, const double*,
-                           double*, double*, double*, double*, double*, double*, double*, cudaStream_t);
+cudaError_t rbmpp_sr_apply_gram(int, int, int, const double*, const double*, double, const double*, double*, double*,
+                                double*, double*, double*, double*, cudaStream_t);
+cudaError_t rbmpp_sr_apply_finish(int, int, const double*, double, double, double, const double*, const double*,
+                                  const double*, double*, cudaStream_t);
 cudaError_t rbmpp_pcg_start(int, const double*, const double*, double*, double*, cudaStream_t);
 cudaError_t rbmpp_pcg_dir(int, const double*, const double*, double*, double*, int, cudaStream_t);
 cudaError_t rbmpp_pcg_step(int, const double*, const double*, double*, double*, double*, cudaStream_t);
@@ -167,6 +169,10 @@ struct rbmpp_ctx {
   double stats[10] = {0};
   int stream_stages = 0;  // > 0: TMA-streamed sampler with this many stages
   bool est_fits = true;   // the estimator's workspace fits in shared memory
+  // host-supplied cross-rank sum (rbmpp_set_allreduce) and its packed buffer: 6 scalars, gvec, Ovec
+  rbmpp_allreduce_fn red_fn = nullptr;
+  void* red_user = nullptr;
+  double* d_xch = nullptr;
   // S of the current measurement: built lazily in the precision the SR step asks for
   bool S_valid = false, S_reduced = false;
   int S_prec = RBMPP_SR_FP64, meas_prec = RBMPP_SR_FP64;
@@ -270,6 +276,40 @@ int ensure_measure_buffers(rbmpp_ctx* c) {
   return 0;
 }
 
+// The host all-reduce of rbmpp_set_allreduce on n doubles at device address p, with the stream drained first.
+int reduce_dev(rbmpp_ctx* c, double* p, long long n, const char* what) {
+  CK(cudaStreamSynchronize(c->st));
+  const int r = c->red_fn(c->red_user, p, n);
+  if (r) return fail(c, RBMPP_E_COMM, "host all-reduce of %s returned %d", what, r);
+  return 0;
+}
+
+// main.f90:348-369 across ranks: {Etot, Etot2, norm, wf_av, naccept_total, n_samples} and, when with_vectors,
+// gvec and Ovec, summed in one call of the host all-reduce.
+int reduce_measurement(rbmpp_ctx* c, bool with_vectors) {
+  const size_t nv = c->d.Nv;
+  int r;
+  if (!c->d_xch && (r = dalloc(c, &c->d_xch, 6 + 2 * nv))) return r;
+  double h6[6] = {c->meas_scal[0], c->meas_scal[1], c->meas_scal[2], c->meas_scal[3], (double)c->naccept_total,
+                  c->n_samples_total};
+  CK(cudaMemcpyAsync(c->d_xch, h6, sizeof(h6), cudaMemcpyHostToDevice, c->st));
+  if (with_vectors) {
+    CK(cudaMemcpyAsync(c->d_xch + 6, c->d_gvec, sizeof(double) * nv, cudaMemcpyDeviceToDevice, c->st));
+    CK(cudaMemcpyAsync(c->d_xch + 6 + nv, c->d_Ovec, sizeof(double) * nv, cudaMemcpyDeviceToDevice, c->st));
+  }
+  if ((r = reduce_dev(c, c->d_xch, with_vectors ? 6 + 2 * (long long)nv : 6, "the measurement"))) return r;
+  CK(cudaMemcpyAsync(h6, c->d_xch, sizeof(h6), cudaMemcpyDeviceToHost, c->st));
+  if (with_vectors) {
+    CK(cudaMemcpyAsync(c->d_gvec, c->d_xch + 6, sizeof(double) * nv, cudaMemcpyDeviceToDevice, c->st));
+    CK(cudaMemcpyAsync(c->d_Ovec, c->d_xch + 6 + nv, sizeof(double) * nv, cudaMemcpyDeviceToDevice, c->st));
+  }
+  CK(cudaStreamSynchronize(c->st));
+  for (int k = 0; k < 4; k++) c->meas_scal[k] = h6[k];
+  c->naccept_total = (long long)h6[4];
+  c->n_samples_total = h6[5];
+  return 0;
+}
+
 // S_raw = sum over samples of O O^T (the dgemm of calc_phys_quantity.f90:240) for the current
 // measurement, in FP64 or as split-BF16 products on the tensor cores (exact FP64 diagonal).
 // The split-BF16 form multiplies the centred derivatives O' = O - b m^T (b: the per-sample weights of Ovec,
@@ -283,8 +323,13 @@ int build_S(rbmpp_ctx* c, int prec) {
                 c->S_prec, prec);
   const DevDims& d = c->d;
   CK(cudaEventRecord(c->ev[5], c->st));
+  const long long nS = (long long)d.Nv * d.Nv;
   if (prec == RBMPP_SR_FP64) {
     CK(rbmpp_syrk_ot_o(d.Nv, c->ns_tot, c->d_O, c->d_S, c->st));
+    if (c->red_fn) {
+      const int r = reduce_dev(c, c->d_S, nS, "S");
+      if (r) return r;
+    }
   } else if (prec == RBMPP_SR_SPLIT_BF16) {
     if (!c->d_hi) {
       int kp = 0, np = 0;
@@ -303,6 +348,11 @@ int build_S(rbmpp_ctx* c, int prec) {
                                     c->d_part, c->st);
     if (r == 1) return fail(c, RBMPP_E_CUDA, "cuTensorMapEncodeTiled unavailable from the driver");
     if (r) return fail(c, RBMPP_E_CUDA, "split-BF16 S build: %s", cudaGetErrorString((cudaError_t)(r - 100)));
+    if (c->red_fn) {
+      // every rank's centred product about the global mean, and its exact diagonal, summed over the ranks
+      const int rr = reduce_dev(c, c->d_S, nS, "S");
+      if (rr) return rr;
+    }
     CK(rbmpp_add_outer_offdiag(d.Nv, c->d_S, c->d_Ovec, 1.0 / norm, c->st));  // upper triangle only
     CK(rbmpp_symmetrize(d.Nv, c->d_S, c->st));
   } else {
@@ -331,8 +381,13 @@ int apply_A(rbmpp_ctx* c, double norm, double scal, double sigma, const double* 
   const DevDims& d = c->d;
   double* v = c->d_pcg;
   const size_t Nv = d.Nv;
-  CK(rbmpp_sr_apply(c->ns_tot, d.Nv, d.Nv_rbm, c->d_O, v + VM * Nv, norm, scal, sigma, x, y, v + VWS * Nv,
-                    v + VZZ * Nv, c->d_gpart, c->d_tmp_ns, c->d_part, c->d_sc, c->st));
+  CK(rbmpp_sr_apply_gram(c->ns_tot, d.Nv, d.Nv_rbm, c->d_O, v + VM * Nv, scal, x, v + VWS * Nv, v + VZZ * Nv,
+                         c->d_gpart, c->d_tmp_ns, c->d_part, c->d_sc, c->st));
+  if (c->red_fn) {
+    const int r = reduce_dev(c, v + VZZ * Nv, d.Nv, "O^T O x");
+    if (r) return r;
+  }
+  CK(rbmpp_sr_apply_finish(d.Nv, d.Nv_rbm, v + VM * Nv, norm, scal, sigma, x, v + VZZ * Nv, c->d_sc, y, c->st));
   return 0;
 }
 
@@ -491,7 +546,7 @@ int rbmpp_destroy(rbmpp_ctx* c) {
                   c->W.mt, c->W.nfastup, c->W.naccept, c->W.nacc_all, c->W.status, c->W.xs, c->W.pfs, c->W.psis, c->W.gj, c->W.events, c->W.trace, (void*)c->W.replay, c->d_O, c->d_psiS,
                   c->d_eloc, c->d_a, c->d_b, c->d_tmp_ns, c->d_acc4, c->d_nap, c->d_estat, c->d_gvec, c->d_Ovec,
                   c->d_vec, c->d_S, c->d_part, c->d_info, c->d_err, c->d_rv, c->d_hi, c->d_lo, c->d_Sf, c->d_Sb,
-                  c->d_crow, c->d_csd, c->d_cones, c->d_cvbs, c->d_cpart, c->d_csum, c->d_dinv, c->d_pcg, c->d_gpart, c->d_sc, c->d_bar};
+                  c->d_crow, c->d_csd, c->d_cones, c->d_cvbs, c->d_cpart, c->d_csum, c->d_dinv, c->d_pcg, c->d_gpart, c->d_sc, c->d_bar, c->d_xch};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (c->h_sc) cudaFreeHost(c->h_sc);
@@ -758,6 +813,7 @@ int rbmpp_measure(rbmpp_ctx* c, double* scal, double* gvec, double* Ovec, double
     CK(cudaEventElapsedTime(&a1, c->ev[4], c->ev[11]));
     c->stats[2] = a1;
   }
+  if (c->red_fn && (r = reduce_measurement(c, true))) return r;
   // S itself is built when it is first needed (here if Smat is wanted, else by exchange or SR step)
   if (Smat && (r = build_S(c, c->meas_prec))) return r;
   if (scal) std::memcpy(scal, c->meas_scal, sizeof(double) * 4);
@@ -773,6 +829,7 @@ int rbmpp_measure_energy(rbmpp_ctx* c, double* scal) {
   if (!c->sampled) return fail(c, RBMPP_E_STATE, "measure before make_sample");
   int r = measure_common(c, false);
   if (r) return r;
+  if (c->red_fn && (r = reduce_measurement(c, false))) return r;
   if (scal) std::memcpy(scal, c->meas_scal, sizeof(double) * 4);
   return 0;
 }
@@ -905,10 +962,10 @@ int rbmpp_sr_step(rbmpp_ctx* c, const rbmpp_sr_in* in, rbmpp_sr_out* out, double
   const DevDims& d = c->d;
   const int Nv = d.Nv, Nrbm = d.Nv_rbm, N = d.N;
   const bool refine = in->precision == RBMPP_SR_SPLIT_BF16 && in->refine_steps > 0;
-  if (refine && c->n_samples_total != (double)c->ns_tot)
+  if (refine && c->n_samples_total != (double)c->ns_tot && !c->red_fn)
     return fail(c, RBMPP_E_ARG,
                 "split-BF16 refinement applies S through this context's samples only; with a measurement reduced "
-                "over several contexts use refine_steps = 0");
+                "over several contexts use refine_steps = 0 or rbmpp_set_allreduce");
   std::memset(out, 0, sizeof(*out));
   const double norm = c->meas_scal[2];
   const double ntot = c->n_samples_total;
@@ -1219,6 +1276,7 @@ int rbmpp_sr_step(rbmpp_ctx* c, const rbmpp_sr_in* in, rbmpp_sr_out* out, double
 int rbmpp_exchange_measurement(rbmpp_ctx* c, int direction, double* d_S, double* d_g, double* d_ov, double* scal6) {
   if (!c || !scal6) return RBMPP_E_ARG;
   if (!c->measured) return fail(c, RBMPP_E_STATE, "exchange_measurement before measure");
+  if (c->red_fn) return fail(c, RBMPP_E_STATE, "exchange_measurement with rbmpp_set_allreduce set: already reduced");
   const int Nv = c->d.Nv;
   const size_t nS = (size_t)Nv * Nv * sizeof(double), nV = (size_t)Nv * sizeof(double);
   if (direction == 0) {
@@ -1246,6 +1304,13 @@ int rbmpp_exchange_measurement(rbmpp_ctx* c, int direction, double* d_S, double*
     c->n_samples_total = scal6[5];
   }
   CK(cudaStreamSynchronize(c->st));
+  return 0;
+}
+
+int rbmpp_set_allreduce(rbmpp_ctx* c, rbmpp_allreduce_fn fn, void* user) {
+  if (!c) return RBMPP_E_ARG;
+  c->red_fn = fn;
+  c->red_user = fn ? user : nullptr;
   return 0;
 }
 

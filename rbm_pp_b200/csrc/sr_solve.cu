@@ -802,15 +802,20 @@ cudaError_t rbmpp_gram_apply(int ns, int nv, const double* O, const double* y, d
   return cudaGetLastError();
 }
 
-// y = A x with A = D (S_raw / norm - m m^T) D + sigma I applied through O; ws, z: nv doubles each;
-// sc: device scalars
-cudaError_t rbmpp_sr_apply(int ns, int nv, int nrbm, const double* O, const double* m, double norm, double scal,
-                           double sigma, const double* x, double* y, double* ws, double* z, double* part,
-                           double* tmp_ns, double* part64, double* sc, cudaStream_t st) {
+// y = A x with A = D (S_raw / norm - m m^T) D + sigma I applied through O, in two halves so that a cross-rank
+// sum of z = O^T (O D x) can come between them.  First half: ws = D x, sc[SC_MX] = m . ws, z = O^T (O ws);
+// ws, z: nv doubles each; sc: device scalars.
+cudaError_t rbmpp_sr_apply_gram(int ns, int nv, int nrbm, const double* O, const double* m, double scal,
+                                const double* x, double* ws, double* z, double* part, double* tmp_ns, double* part64,
+                                double* sc, cudaStream_t st) {
   rbmpp_note_launch();
   sr_pre_kernel<<<1, 1024, 0, st>>>(nv, nrbm, x, scal, m, ws, sc);
-  cudaError_t e = rbmpp_gram_apply(ns, nv, O, ws, z, part, tmp_ns, part64, st);
-  if (e) return e;
+  return rbmpp_gram_apply(ns, nv, O, ws, z, part, tmp_ns, part64, st);
+}
+
+// Second half: y = D (z / norm - m sc[SC_MX]) + sigma x.
+cudaError_t rbmpp_sr_apply_finish(int nv, int nrbm, const double* m, double norm, double scal, double sigma,
+                                  const double* x, const double* z, const double* sc, double* y, cudaStream_t st) {
   rbmpp_note_launch();
   sr_post_kernel<<<(nv + 255) / 256, 256, 0, st>>>(nv, nrbm, z, m, sc, x, scal, sigma, norm, y);
   return cudaGetLastError();

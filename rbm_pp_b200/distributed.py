@@ -1,13 +1,16 @@
 """SR iterations over one or several GPUs (one process per GPU, walkers sharded across ranks).
 
-Rank r holds global walkers r*nw .. r*nw+nw-1 (the reference's MPI ranks).  Each SR step runs
-make_sample and the estimators locally, then the one exchange of the reference -- the
-MPI_ALLREDUCE of Etot, Etot2, norm, wf_av, naccept, gvec, Ovec and the full S matrix
-(main.f90:348-369) -- as NCCL all-reduces over NVLink, then the identical SR solve on every rank
-(so the parameter broadcast of main.f90:427-438 is not needed), then the s_factor0 / shift
-bookkeeping of main.f90:439-453.
+Rank r holds global walkers r*nw .. r*nw+nw-1 (the reference's MPI ranks).  The library does the
+cross-rank sums itself through a host all-reduce handed to it once (rbmpp_set_allreduce): the
+MPI_ALLREDUCE of Etot, Etot2, norm, wf_av, naccept, gvec and Ovec (main.f90:348-369), the S matrix,
+and, on the split-BF16 path, one Nv-vector per conjugate-gradient iteration of the refinement on the
+exact S.  Here that all-reduce is NCCL over NVLink on the library's own device buffers.  Every rank
+then takes the identical SR step (so the parameter broadcast of main.f90:427-438 is not needed), and
+the s_factor0 / shift bookkeeping of main.f90:439-453.
 """
 from __future__ import annotations
+
+import ctypes as C
 
 import numpy as np
 
@@ -51,66 +54,83 @@ def reduce_measurement(parts):
     return scal, S, g, ov
 
 
+class _DeviceVector:
+    """n float64 at a raw device address, seen by torch without a copy (CUDA array interface v3, no stream:
+    the library has drained its stream before it hands the buffer out)."""
+
+    def __init__(self, ptr: int, n: int):
+        self.__cuda_array_interface__ = {"shape": (n,), "typestr": "<f8", "data": (ptr, False), "version": 3,
+                                         "strides": None}
+
+
+def allreduce_fn(group=None, where="cuda"):
+    """The host all-reduce for Context.set_allreduce: fn(ptr, n) sums n float64 at ptr over the ranks of
+    `group`, in place, and returns when the sum is there.
+      where="cuda": ptr is a device address; torch.distributed all-reduces it there (NCCL over NVLink);
+      where="host": ptr is a host address (the same call over gloo, for CPU tests of this adapter)."""
+    import torch
+    import torch.distributed as dist
+
+    def fn(ptr, n):
+        if where == "cuda":
+            t = torch.as_tensor(_DeviceVector(ptr, n), device="cuda")
+        else:
+            t = torch.from_numpy(np.ctypeslib.as_array((C.c_double * n).from_address(ptr)))
+        dist.all_reduce(t, op=dist.ReduceOp.SUM, group=group)
+        if where == "cuda":
+            torch.cuda.current_stream().synchronize()
+
+    return fn
+
+
+def broadcast_initial_params(br, Wr, group=None):
+    """The MPI_BCAST of rank 0's initial RBM parameters (parameter.f90:21-75): only rank 0 draws them."""
+    import torch
+    import torch.distributed as dist
+    dev = "cuda" if dist.get_backend(group) == "nccl" else "cpu"
+    t = torch.from_numpy(np.concatenate([np.ravel(br), np.ravel(Wr, order="F")])).to(dev)
+    dist.broadcast(t, src=0, group=group)
+    v = t.cpu().numpy()
+    nb = np.size(br)
+    return v[:nb].copy(), v[nb:].reshape(np.shape(Wr), order="F").copy()
+
+
 class SRRunner:
-    def __init__(self, ctx: "capi.Context", problem, iseed0: int, precision=capi.SR_FP64, world=1, rank=0):
+    """main.f90:311-455 on this rank's context: one rbmpp_iteration per step.  With world > 1 the context
+    sums over the ranks by itself (allreduce_fn on the process group)."""
+
+    def __init__(self, ctx: "capi.Context", problem, iseed0: int, precision=capi.SR_FP64, world=1, rank=0,
+                 group=None):
         self.ctx = ctx
         self.p = problem
         self.world = world
         self.rank = rank
         self.precision = precision
-        self.iteration = 0
         inp = problem.inp
         ctx.seed(iseed0)
         if rank == 0:
             br, Wr = capi.initial_params(ctx, problem)
         else:
-            br, Wr = problem.br, problem.Wr
+            br = np.zeros(inp.alphar) if problem.br is None else problem.br
+            Wr = np.zeros((ctx.N, inp.alphar)) if problem.Wr is None else problem.Wr
+        if world > 1:
+            br, Wr = broadcast_initial_params(br, Wr, group)
+            ctx.set_allreduce(allreduce_fn(group))
         ctx.set_params(br, Wr, problem.slater, 0.0)
         self.book = Bookkeeping(inp, ctx.N)
-        self._bufs = None
 
     @classmethod
     def attach(cls, ctx: "capi.Context", problem, precision=capi.SR_FP64):
         """A one-GPU runner over a context whose state is already set (seeded, parameters loaded, possibly
         copied from another context with Context.copy_state_from): it continues from that state."""
         r = cls.__new__(cls)
-        r.ctx, r.p, r.world, r.rank, r.precision, r.iteration = ctx, problem, 1, 0, precision, 0
+        r.ctx, r.p, r.world, r.rank, r.precision = ctx, problem, 1, 0, precision
         r.book = Bookkeeping(problem.inp, ctx.N)
-        r._bufs = None
         return r
 
     def step(self):
-        import torch
         inp = self.p.inp
-        if self.world == 1:
-            out = self.ctx.iteration(self.precision, inp.delta_tau, inp.s_factor_scale, inp.s_cut, inp.s_factor0)
-            rec = out.as_dict()
-            rec["device_ms"] = self.ctx.stats()["iteration_ms"]
-            return rec
-        self.iteration += 1
-        ev0 = torch.cuda.Event(enable_timing=True)
-        ev1 = torch.cuda.Event(enable_timing=True)
-        ev0.record()
-        self.ctx.make_sample(self.iteration == 1)
-        self.ctx.measure(want_S=False, want_vectors=False)
-        nv = self.ctx.Nv
-        if self._bufs is None:
-            self._bufs = (torch.empty((nv, nv), dtype=torch.float64, device="cuda"),
-                          torch.empty(nv, dtype=torch.float64, device="cuda"),
-                          torch.empty(nv, dtype=torch.float64, device="cuda"))
-        S, g, ov = self._bufs
-        scal = np.zeros(6)
-        torch.cuda.synchronize()
-        self.ctx.exchange_measurement(0, S.data_ptr(), g.data_ptr(), ov.data_ptr(), scal)
-        sc = torch.tensor(scal, dtype=torch.float64, device="cuda")
-        allreduce_measurement(S, g, ov, sc)
-        torch.cuda.synchronize()
-        scal = sc.cpu().numpy()
-        self.ctx.exchange_measurement(1, S.data_ptr(), g.data_ptr(), ov.data_ptr(), scal)
-        out, _ = self.ctx.sr_step(self.iteration, inp.delta_tau, self.book.s_factor0, inp.s_cut, self.precision)
-        self.ctx.set_shift(self.book.after_step(out.wf_av))
-        ev1.record()
-        torch.cuda.synchronize()
+        out = self.ctx.iteration(self.precision, inp.delta_tau, inp.s_factor_scale, inp.s_cut, inp.s_factor0)
         rec = out.as_dict()
-        rec["device_ms"] = ev0.elapsed_time(ev1)
+        rec["device_ms"] = self.ctx.stats()["iteration_ms"]
         return rec

@@ -1,10 +1,14 @@
-"""Walker sharding and the one cross-rank exchange of an SR step, run as 2 gloo ranks on the CPU.
+"""Walker sharding and the cross-rank sums of an SR step, run as 2 gloo ranks on the CPU.
 
 Each rank holds half of the walkers (global ranks offset..offset+nw-1, seeded by the rule of
-main.f90:224-234), measures them, sums the measurement over the ranks with the product's
-``allreduce_measurement`` (the MPI_ALLREDUCE calls of main.f90:348-369), and takes the SR step and
-the shift bookkeeping on the reduced sums.  The CPU oracle stands in for the per-GPU context.  The
-result must equal one process holding all walkers: the same parameters, energies and shift.
+main.f90:224-234), measures them, sums the measurement over the ranks (the MPI_ALLREDUCE calls of
+main.f90:348-369), and takes the SR step and the shift bookkeeping on the reduced sums.  The CPU oracle
+stands in for the per-GPU context; the sums go through the product's host all-reduce
+(``distributed.allreduce_fn`` behind the C function pointer ``capi.allreduce_callback`` builds for
+rbmpp_set_allreduce, called through that pointer on buffers packed as the library packs them:
+{Etot, Etot2, norm, wf_av, naccept, n_samples, gvec, Ovec}, then S).  Rank 0's random initial RBM
+parameters reach the other rank through ``distributed.broadcast_initial_params``.  The result must
+equal one process holding all walkers: the same parameters, energies and shift.
 """
 import datetime
 import multiprocessing as mp
@@ -37,18 +41,36 @@ def _rank_main(rank, world, port, q):
         import torch
         import torch.distributed as dist
 
+        import ctypes as C
+
         import pyoracle as po
-        from rbm_pp_b200.distributed import allreduce_measurement
+        from rbm_pp_b200 import capi
+        from rbm_pp_b200.distributed import allreduce_fn, broadcast_initial_params
         os.environ["MASTER_ADDR"] = "127.0.0.1"
         os.environ["MASTER_PORT"] = str(port)
         dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
         p = _problem()
         nw = NW_TOTAL // world
+        # rank 0's initial parameters, broadcast (rank 1 starts from zeros)
+        br0 = np.arange(3.0) + 1.0 if rank == 0 else np.zeros(3)
+        Wr0 = np.arange(12.0).reshape(4, 3) if rank == 0 else np.zeros((4, 3))
+        bb, wb = broadcast_initial_params(br0, Wr0)
+        assert np.array_equal(bb, np.arange(3.0) + 1.0) and np.array_equal(wb, np.arange(12.0).reshape(4, 3))
+        # the C function pointer the library would hold, called through that pointer
+        cb = capi.allreduce_callback(allreduce_fn(where="host"))
+        native = capi.ALLREDUCE_FN(C.cast(cb, C.c_void_p).value)
+
+        def call(buf):
+            rc = native(None, buf.ctypes.data, buf.size)
+            assert rc == 0, rc
 
         def reduce(scal6, S, g, ov):
-            t = [torch.from_numpy(np.ascontiguousarray(a, dtype=np.float64)) for a in (S, g, ov, scal6)]
-            allreduce_measurement(t[0], t[1], t[2], t[3])
-            return t[3].numpy(), t[0].numpy(), t[1].numpy(), t[2].numpy()
+            nv = g.size
+            packed = np.concatenate([np.asarray(scal6, dtype=np.float64), g, ov])
+            call(packed)
+            Sr = np.array(S, dtype=np.float64, order="F")
+            call(Sr.reshape(-1, order="F"))
+            return packed[:6].copy(), Sr, packed[6:6 + nv].copy(), packed[6 + nv:].copy()
 
         o = po.Oracle(p, nranks=nw, nsample_per_rank=NS, nthreads=2)
         loop = po.VMCLoop(o, p, iseed0=4242, offset=rank * nw, allreduce=reduce)

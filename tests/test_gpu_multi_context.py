@@ -1,8 +1,16 @@
-"""The product's multi-GPU path on one GPU: walkers sharded over two contexts, the one exchange of an SR step
-(rbmpp_exchange_measurement, the MPI_ALLREDUCE block of main.f90:348-369) done by summing the two contexts'
-device buffers, then the SR step on the reduced sums.  It must equal one context holding all walkers.
-Also: rbmpp_copy_state makes a second context continue exactly as the first.
+"""The product's multi-GPU path on one GPU: walkers sharded over two contexts.
+
+1. The exchange of an SR step through caller buffers (rbmpp_exchange_measurement, the MPI_ALLREDUCE block of
+   main.f90:348-369) done by summing the two contexts' device buffers, then the SR step on the reduced sums.
+2. The library's own cross-rank sums (rbmpp_set_allreduce), which the split-BF16 path needs: the measurement,
+   S, and O^T (O x) once per conjugate-gradient iteration.  The two ranks are two host threads, each driving
+   its context through rbmpp_iteration; the all-reduce copies each rank's buffer to the host, waits for the
+   other rank on a host barrier and writes back the sum taken in rank order.  No kernel waits on another.
+Both must equal one context holding all walkers.  Also: rbmpp_copy_state makes a second context continue
+exactly as the first.
 """
+import threading
+
 import numpy as np
 import pytest
 
@@ -87,3 +95,125 @@ def test_copy_state_continues_identically(precision):
         assert np.array_equal(np.asarray(x), np.asarray(y))
     a.close()
     b.close()
+
+
+class ThreadAllreduce:
+    """Ranks as threads of this process: rank r's fn(ptr, n) copies its device buffer to the host, waits for
+    every rank, and writes back the sum in rank order (the same bits on every rank, as NCCL gives)."""
+
+    def __init__(self, world):
+        self.world = world
+        self.parts = [None] * world
+        self.bar = threading.Barrier(world, timeout=120)
+        self.calls = [0] * world
+
+    def fn(self, rank):
+        import torch
+
+        def f(ptr, n):
+            t = torch.as_tensor(rdist._DeviceVector(ptr, n), device="cuda")
+            self.parts[rank] = t.cpu().numpy()
+            self.bar.wait()
+            s = self.parts[0].copy()
+            for r in range(1, self.world):
+                s += self.parts[r]
+            self.bar.wait()
+            t.copy_(torch.from_numpy(s))
+            torch.cuda.synchronize()
+            self.calls[rank] += 1
+
+        return f
+
+
+def _run_threads(ctxs, body):
+    out = [None] * len(ctxs)
+    errs = []
+
+    def run(r):
+        try:
+            out[r] = body(ctxs[r])
+        except Exception as e:  # noqa: BLE001 - reported below
+            errs.append((r, e))
+
+    th = [threading.Thread(target=run, args=(r,)) for r in range(len(ctxs))]
+    for t in th:
+        t.start()
+    for t in th:
+        t.join(timeout=600)
+    assert not errs, errs
+    return out
+
+
+@pytest.mark.parametrize("precision", [capi.SR_FP64, capi.SR_SPLIT_BF16])
+def test_library_allreduce_shards_equal_one_context(precision):
+    import torch
+
+    L, nw, ns, steps = 4, 8, 16, 3
+    p = fm.synthetic_problem(L, translations=True, alphar=1, nsample=2 * nw * ns, seed=63)
+    inp = p.inp
+    one = capi.Context(p, n_walkers=2 * nw, nsample_per_walker=ns)
+    shards = [capi.Context(p, n_walkers=nw, nsample_per_walker=ns, walker_offset=r * nw) for r in range(2)]
+    red = ThreadAllreduce(2)
+    for r, c in enumerate(shards):
+        c.set_allreduce(red.fn(r))
+    for c in [one] + shards:
+        c.set_params(p.br, p.Wr, p.slater, 0.0)
+        c.seed(4343)
+    torch.cuda.synchronize()
+
+    def body(c):
+        return [c.iteration(precision, inp.delta_tau, inp.s_factor_scale, inp.s_cut, inp.s_factor0).as_dict()
+                for _ in range(steps)]
+
+    want = body(one)
+    got = _run_threads(shards, body)
+    # the measurement, S, and per refinement iteration one O^T O x; lambda needs two more
+    assert red.calls[0] == red.calls[1] and red.calls[0] >= 2 * steps
+    for recs in got:
+        for a, b in zip(recs, want):
+            assert abs(a["Etot"] - b["Etot"]) <= 1e-12 * abs(b["Etot"])
+            assert abs(a["accept_ratio"] - b["accept_ratio"]) == 0.0
+            assert abs(a["lambda_"] - b["lambda_"]) <= 1e-8 * abs(b["lambda_"])
+            if precision == capi.SR_SPLIT_BF16:
+                assert a["refine_iterations"] > 0 and a["refine_residual"] < 1e-12
+    pw = one.get_params()
+    for c in shards:
+        for a, b in zip(c.get_params()[:3], pw[:3]):
+            assert _rel(a, b) < 1e-8
+        assert np.array_equal(c.get_params()[0], shards[0].get_params()[0])  # ranks bit-identical
+    for c in [one] + shards:
+        c.close()
+
+
+def test_failing_allreduce_is_reported():
+    """A host all-reduce that raises (a rank that has gone away) ends the call with RBMPP_E_COMM, and the
+    context is usable again once the all-reduce is removed."""
+    L, nw, ns = 4, 4, 8
+    p = fm.synthetic_problem(L, translations=True, alphar=1, nsample=nw * ns, seed=64)
+    inp = p.inp
+    g = capi.Context(p, n_walkers=nw, nsample_per_walker=ns)
+    g.set_params(p.br, p.Wr, p.slater, 0.0)
+    g.seed(11)
+
+    def gone(ptr, n):
+        raise ConnectionError("peer rank left")
+
+    g.make_sample(True)
+    m0 = g.measure(want_S=False)
+    # a world of one rank: the sum is the buffer itself, so the measurement is unchanged
+    g.set_allreduce(lambda ptr, n: None)
+    m1 = g.measure(want_S=False)
+    assert m1["Etot"] == m0["Etot"] and np.array_equal(m1["gvec"], m0["gvec"])
+    # the context reduces by itself: the caller-buffer exchange is refused
+    with pytest.raises(capi.RbmppError) as ei:
+        g.exchange_measurement(0, 0, 0, 0, np.zeros(6))
+    assert ei.value.code == 21, str(ei.value)
+    g.set_allreduce(gone)
+    with pytest.raises(capi.RbmppError) as ei:
+        g.measure(want_S=False)
+    assert ei.value.code == 23 and "all-reduce" in str(ei.value)
+    assert isinstance(g.allreduce_error, ConnectionError)
+    g.set_allreduce(None)
+    m = g.measure(want_S=False)
+    assert np.isfinite(m["Etot"])
+    g.close()
