@@ -397,8 +397,9 @@ int main(int argc, char** argv) {
     const double var = (o.Etot2 - o.Etot * o.Etot) / (o.Etot * o.Etot);
     std::printf("Iteration :%6d\n   Total Energy         :%20.10f\n   Energy Variance      :%20.10f\n"
                 "   Acceptance Ratio     :%20.10f\n   Stabilization Factor :%20.10f%20.10f\n"
-                "   wf_av, shift         :%20.5E%20.5E\n   Maximum change in W  :%20.10f%20.10f%8d\n",
-                it, o.Etot, var, o.accept_ratio, o.s_factor, in.s_cut, o.wf_av, shift_now,
+                "   wf_av, shift         :%s%s\n   Maximum change in W  :%20.10f%20.10f%8d\n",
+                it, o.Etot, var, o.accept_ratio, o.s_factor, in.s_cut, fort_e(o.wf_av, 20, 5).c_str(),
+                fort_e(shift_now, 20, 5).c_str(),
                 std::fmin(o.delW_max, 0.04), o.delW_max / 0.04, o.kmax);
     std::fprintf(fe, "%12d %25.16E %25.16E\n", it, o.Etot, var);
     if (it > in.Nstep - in.Nav) {  // :410-422
@@ -426,6 +427,7 @@ int main(int argc, char** argv) {
   // final energy (:486-575): warm up, then Nav measurements
   const size_t nchi = (size_t)N * (N + 1) / 2;
   std::vector<double> chi_sp, chi_vbs;
+  double shift_meas = shift_av;  // mod_main's shift during the measurements
   if (correlation) {  // Calc_Correlation/main.f90:498-527
     chi_sp.resize(2 * nchi);
     chi_vbs.resize(4 * nchi);
@@ -439,7 +441,8 @@ int main(int argc, char** argv) {
       wf += std::hypot(q[0], q[1]);
     }
     wf /= (double)ns * walkers;
-    lib.ck(rbmpp_set_shift(lib.c, wf * 1e-5), "set_shift");
+    shift_meas = wf * 1e-5;
+    lib.ck(rbmpp_set_shift(lib.c, shift_meas), "set_shift");
     std::printf("wf_av, shift =%15.5E%15.5E\n", wf, wf * 1e-5);
     for (int it = 0; it < 7; it++) lib.ck(rbmpp_make_sample(lib.c, 0, nullptr, nullptr), "make_sample");
   } else {
@@ -468,15 +471,22 @@ int main(int argc, char** argv) {
                      chi_vbs[i + 2 * nchi] / sc[2], chi_vbs[i + 3 * nchi] / sc[2]);
       std::fclose(f6);
       std::fclose(f7);
-      std::printf("   wf_sgn               :%20.10f\n", sc[4] / ((double)ns * walkers));
     } else {
       lib.ck(rbmpp_measure_energy(lib.c, sc), "measure_energy");
     }
     const double E = sc[0] / sc[2], E2 = sc[1] / sc[2];
-    const double acc = (double)nacc / ((double)ns * walkers) / (double)N;
+    const double nst = (double)ns * walkers;
+    const double acc = (double)nacc / nst / (double)N;
+    // main.f90:548-554; Calc_Correlation/main.f90:587-594 adds wf_sgn (abs, re, im; the real path has im = 0)
     std::printf("Iteration (Energy Measuement) :%6d\n   total energy         :%20.10f\n"
-                "   energy variance      :%20.10f\n   acceptance ratio     :%20.10f\n",
-                it, E, (E2 - E * E) / (E * E), acc);
+                "   energy variance      :%20.10f\n   acceptance ratio     :%20.10f\n"
+                "   wf_av, shift         :%s%s\n   norm                 :%20.10f\n",
+                it, E, (E2 - E * E) / (E * E), acc, fort_e(sc[3] / nst, 20, 5).c_str(),
+                fort_e(shift_meas, 20, 5).c_str(), sc[2] / nst);
+    if (correlation) {
+      const double sg = sc[4] / nst;
+      std::printf("   wf_sgn               :%20.10f%20.10f%20.10f\n", std::fabs(sg), sg, 0.0);
+    }
     std::fprintf(fa, "%12d %25.16E %25.16E\n", it, E, (E2 - E * E) / (E * E));
     e1.push_back(E);
     e2.push_back(E2 - E * E);

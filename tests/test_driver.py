@@ -120,6 +120,23 @@ def test_driver_correlation_files(tmp_path):
         assert np.allclose(sp[diag, 1], 1.0, rtol=1e-12) and np.allclose(sp[diag, 2], 1.0, rtol=1e-12)
         e = sum(J[t] * (sp[pair(a, b), 1] + 2.0 * sp[pair(a, b), 2]) for t, a, b in bonds)
         assert abs(e - fin[it - 1, 1]) <= 1e-9 * abs(fin[it - 1, 1]), (it, e, fin[it - 1, 1])
+    # the measurement block of Calc_Correlation/main.f90:587-594 on standard output, in its order and formats
+    lines = out.stdout.splitlines()
+    heads = [k for k, ln in enumerate(lines) if ln.startswith("Iteration (Energy Measuement) :")]
+    assert len(heads) == nav
+    for h in heads:
+        blk = lines[h:h + 7]
+        keys = ["   total energy         :", "   energy variance      :", "   acceptance ratio     :",
+                "   wf_av, shift         :", "   norm                 :", "   wf_sgn               :"]
+        for ln, key in zip(blk[1:], keys):
+            assert ln.startswith(key), (ln, key)
+        wf = blk[4][len(keys[3]):]
+        assert len(wf) == 40 and wf[:20].strip().startswith("0.") and "E" in wf[:20]  # 2E20.5
+        sg = blk[6][len(keys[5]):]
+        assert len(sg) == 60
+        a, re_, im = (float(sg[i:i + 20]) for i in (0, 20, 40))
+        assert a == abs(re_) and im == 0.0 and a <= 1.0
+        assert abs(float(blk[5][len(keys[4]):]) - 1.0) < 1.0  # norm / (Nsample Nmpi), weights <= 1
 
 
 def test_driver_writes_input_checks(tmp_path):
