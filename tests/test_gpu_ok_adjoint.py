@@ -14,10 +14,13 @@ amplitudes): Nv = 10404 parameters; 16384 configurations drawn uniformly from th
       of psi itself against O_k, on every configuration.  psi is exactly linear in each pair amplitude f_ij
       here (every f_ij fills one entry of each projection's X) and smooth in the RBM parameters, so these
       differences carry rounding only (and an h^2 term of about 1e-12 for the RBM parameters);
-      of ln psi against O_k / psi, on every configuration away from a node of psi.  Near a node the
-      log-derivative a = O_k / psi grows and the differences of ln|psi| err by about (h a)^2 / 3 relative
-      (exactly so for a linear dependence), which reaches 1e-3 on some of 16384 random configurations; the
-      entries with (h a)^2 / 3 > 1e-9 are counted and left to the first comparison;
+      of ln psi against O_k / psi, on the configurations where those differences resolve 1e-8.  They err in
+      two ways the first comparison does not: near a node of psi the log-derivative a = O_k / psi grows and
+      the differences of ln|psi| err by about (h a)^2 / 3 relative (exactly so for a linear dependence),
+      which reaches 1e-3 on some of 16384 random configurations; and where the projection sum psi =
+      sum_qp psi_qp cancels (c = sum |psi_qp| / |psi| large; its median is about 9 at 10x10) the rounding of
+      psi, about c * 1e-16 relative, divided by h reaches 1e-7.  Entries with (h a)^2 / 3 > 1e-9 or c > 10 are
+      counted and left to the first comparison;
   - the oracle's O_k (its full 2N Pfaffian form) on the first 16 configurations of the batch within 1e-10 of
     each configuration's largest derivative.
 A smaller 6x6 case without translations runs the generic (runtime block size) kernels the same way.
@@ -100,6 +103,8 @@ def test_ok_adjoint(L, trans, alphar, n, capsys):
     g.set_params(br, Wr, sl, 0.0)
     r0 = g.eval_configs(x, want_h=False, want_O=True)
     psi0 = r0["psi"][:, 0].real
+    canc = np.abs(r0["psi"][:, 1:]).sum(axis=1) / np.abs(psi0)  # cancellation of the projection sum
+    assert np.abs(r0["psi"][:, 1:].sum(axis=1).real - psi0).max() <= 1e-12 * np.abs(r0["psi"][:, 1:]).sum(axis=1).max()
     dlog = r0["O"] / psi0[:, None]
     del r0
     assert np.allclose(ad, w.numpy() @ dlog, rtol=1e-12, atol=1e-12 * np.abs(ad).max())
@@ -133,7 +138,7 @@ def test_ok_adjoint(L, trans, alphar, n, capsys):
         err_psi.append(float(np.abs((pp - pm) / (2 * H) - ok).max() / np.abs(ok).max()))
         fd = (np.log(np.abs(pp)) - np.log(np.abs(pm))) / (2 * H)
         a = np.abs(dlog[:, k])
-        off = (H * a) ** 2 / 3 <= 1e-9
+        off = ((H * a) ** 2 / 3 <= 1e-9) & (canc <= 10.0)
         near_node += int((~off).sum())
         err_log.append(float(np.abs(fd - dlog[:, k])[off].max() / a[off].max()))
         err_log_all.append(float(np.abs(fd - dlog[:, k]).max() / scales[k]))
@@ -141,9 +146,9 @@ def test_ok_adjoint(L, trans, alphar, n, capsys):
     with capsys.disabled():
         print(f"\nOK_FD L={L} n={n} parameters={len(ks)}: psi differences max {err_psi.max():.3e} "
               f"(median {np.median(err_psi):.3e}); ln psi differences off nodes max {err_log.max():.3e} "
-              f"(median {np.median(err_log):.3e}), {near_node} of {n * len(ks)} entries near a node, "
+              f"(median {np.median(err_log):.3e}), {near_node} of {n * len(ks)} entries near a node or cancelling, "
               f"all entries max {max(err_log_all):.3e}")
     assert err_psi.max() <= TOL_FD, (ks[err_psi.argmax()], err_psi.max())
     assert err_log.max() <= TOL_FD, (ks[err_log.argmax()], err_log.max())
-    assert near_node <= 0.01 * n * len(ks)
+    assert near_node <= 0.75 * n * len(ks)
     g.close()
