@@ -52,6 +52,7 @@ def lib():
         L.orc_nv.argtypes = [P]
         L.orc_set_tables.argtypes = [P, ip, dp, ip, P]
         L.orc_set_params.argtypes = [P, dp, dp, dp, C.c_double]
+        L.orc_set_sp_weights.argtypes = [P, dp]
         L.orc_get_params.argtypes = [P, dp, dp, dp, P]
         L.orc_get_slater_elements.argtypes = [P, dp]
         L.orc_seed.argtypes = [P, C.c_int]
@@ -97,7 +98,7 @@ class OracleError(RuntimeError):
 class Oracle:
     """One oracle context: nranks emulated MPI ranks (walkers), each with its own MT19937 stream."""
 
-    def __init__(self, problem, nranks: int, nsample_per_rank: int, nthreads: int = 1):
+    def __init__(self, problem, nranks: int, nsample_per_rank: int, nthreads: int = 1, sp_weights=None):
         self.p = problem
         inp = problem.inp
         self.L = inp.L
@@ -118,6 +119,8 @@ class Oracle:
         para[1::2] = problem.sym.para_mp.imag
         self._chk(L.orc_set_tables(self.h, fortran_array(problem.sym.W_map, np.int32), para,
                                    fortran_array(problem.orbital_idx, np.int32), None))
+        if sp_weights is not None:  # (3, 2): SP_GL_Cos, SP_GL_Sin, para_spin_proj per point
+            self._chk(L.orc_set_sp_weights(self.h, fortran_array(sp_weights, np.float64)))
 
     def __del__(self):
         if getattr(self, "h", None):
@@ -295,8 +298,9 @@ class VMCLoop:
     the shard of global ranks offset.. and ``allreduce`` (called with scal6, S, g, ov) sums the
     measurement over the shards, as the MPI_ALLREDUCE calls of main.f90:348-369 do."""
 
-    def __init__(self, orc: Oracle, problem, iseed0: int, offset: int = 0, allreduce=None):
+    def __init__(self, orc: Oracle, problem, iseed0: int, offset: int = 0, allreduce=None, shift_coef=0.001):
         self.o = orc
+        self.shift_coef = shift_coef  # main.f90:451 (0.003 in transverse_code/main.f90:451)
         self.p = problem
         inp = problem.inp
         self.s_factor0 = inp.s_factor0
@@ -351,7 +355,7 @@ class VMCLoop:
         for v in self.wf_av_list:
             wf = wf + v
         wf = wf / 10.0
-        self.shift = wf * 0.001 / float(o.N) / float(o.N)
+        self.shift = wf * self.shift_coef / float(o.N) / float(o.N)
         br, Wr, sl, _ = o.get_params()
         o.set_params(br, Wr, sl, self.shift)
         rec = dict(iteration=self.iteration, Etot=Etot, Etot2=Etot2, accept=accept_ratio, wf_av=wf_av,

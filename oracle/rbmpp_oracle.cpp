@@ -1038,6 +1038,23 @@ int orc_set_params(void* h, const double* Wr, const double* br, const double* sl
   return update_slater_elements(c);
 }
 
+// InitSPWeight with given weights w(3, 2) = {SP_GL_Cos, SP_GL_Sin, para_spin_proj} of the two points, as the
+// transverse code's spin_projection.f90:30-38 sets them (beta = -pi/2, pi/2, sqrt(2)-scaled); the
+// CosCos/CosSin/SinSin products follow spin_projection.f90:39-41.  Rebuilds Slater_Elm when parameters are set.
+int orc_set_sp_weights(void* h, const double* w) {
+  Ctx& c = *(Ctx*)h;
+  for (int s = 0; s < 2; s++) {
+    c.sp_cos[s] = w[3 * s];
+    c.sp_sin[s] = w[3 * s + 1];
+    c.para_sp[s] = w[3 * s + 2];
+    c.sp_cc[s] = c.sp_cos[s] * c.sp_cos[s];
+    c.sp_cs[s] = c.sp_cos[s] * c.sp_sin[s];
+    c.sp_ss[s] = c.sp_sin[s] * c.sp_sin[s];
+  }
+  if (!c.slater.empty() && !c.W_map.empty()) return update_slater_elements(c);
+  return 0;
+}
+
 int orc_get_params(void* h, double* Wr, double* br, double* slater, double* shift) {
   Ctx& c = *(Ctx*)h;
   if (Wr) std::memcpy(Wr, c.Wr.data(), sizeof(double) * c.Wr.size());

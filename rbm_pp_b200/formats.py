@@ -292,6 +292,25 @@ def read_W(path: str, N: int, alphar: int) -> tuple[np.ndarray, np.ndarray]:
     return br, Wr
 
 
+def spin_projection_weights(spin_parity: int = 1, transverse: bool = False) -> np.ndarray:
+    """InitSPWeight's values for the two Gauss-Legendre points as the (3, 2) array {SP_GL_Cos, SP_GL_Sin,
+    para_spin_proj} per point that rbmpp_set_tables takes.  The normal code sets beta = 0, pi
+    (spin_projection.f90:29-32, :37-38); the transverse code beta = -pi/2, pi/2 with sqrt(2)-scaled cosines and
+    sines (transverse_code/spin_projection.f90:30-31, :37-38).  para_spin_proj = (1, spin_parity)
+    (spin_projection.f90:55-62)."""
+    if transverse:
+        beta = np.array([-0.5 * np.pi, 0.5 * np.pi])
+        scale = np.sqrt(2.0)
+    else:
+        beta = np.array([0.0, np.pi])
+        scale = 1.0
+    w = np.zeros((3, 2))
+    w[0] = scale * np.cos(0.5 * beta)
+    w[1] = scale * np.sin(0.5 * beta)
+    w[2] = [1.0, 1.0 if spin_parity == 1 else -1.0]
+    return w
+
+
 @dataclass
 class Problem:
     """Everything the sampling/SR loop needs, in the reference's layouts."""

@@ -102,6 +102,54 @@ def test_local_energy_matches_exact_hamiltonian(translations):
     assert np.abs(hp - r["hpsi"]).max() <= 1e-10 * scale
 
 
+@pytest.mark.parametrize("spin_parity", [1, -1])
+def test_transverse_local_energy_matches_exact_hamiltonian(spin_parity):
+    """The transverse code's projection (beta = -pi/2, pi/2, transverse_code/spin_projection.f90:30-38): every
+    block of the Pfaffian matrix is non-zero, and (H psi)(x) from the fast-update local energy still equals the
+    ED Hamiltonian applied to the oracle's psi over the whole Sz = 0 sector."""
+    p = fm.synthetic_problem(4, translations=False, alphar=1, nsample=64, seed=13, spin_parity=spin_parity)
+    o = po.Oracle(p, nranks=1, nsample_per_rank=8, sp_weights=fm.spin_projection_weights(spin_parity, True))
+    o.set_params(p.br, p.Wr, p.slater, 0.0)
+    SE = o.slater_elements()
+    N = 16
+    assert np.abs(SE[:N, :N, 0]).max() > 0.01  # same-spin block present
+    basis = ed.sz0_basis(16)
+    r = o.eval_configs(basis, want_h=True)
+    H = ed.hamiltonian(4, 1.0, 0.5, basis)
+    hp = H @ r["psi"][:, 0]
+    assert np.abs(hp - r["hpsi"]).max() <= 1e-10 * np.abs(hp).max()
+
+
+def test_transverse_chain_and_ok():
+    """Transverse projection: stored Pf along a chain (skew rank-4 fast updates) against scratch, and O_k
+    against central differences of psi."""
+    p = fm.synthetic_problem(4, translations=True, alphar=1, nsample=16, seed=21)
+    w = fm.spin_projection_weights(1, True)
+    o = po.Oracle(p, nranks=2, nsample_per_rank=8, sp_weights=w)
+    o.set_params(p.br, p.Wr, p.slater, 0.0)
+    o.seed(78)
+    o.make_sample(True)
+    x, psi, pf = o.samples()
+    r = o.eval_configs(x.reshape(-1, 16), want_h=False)
+    # the fast-update products drift; the reference bounds that drift by 1e-5 between recomputes
+    assert np.allclose(np.abs(psi.reshape(-1, psi.shape[-1])[:, 0]), np.abs(r["psi"][:, 0]), rtol=1e-6)
+    xs = x.reshape(-1, 16)[:3]
+    base = o.eval_configs(xs, want_h=False, want_O=True)
+    theta0 = np.concatenate([p.br, p.Wr.reshape(-1, order="F"), p.slater])
+    rng = np.random.default_rng(3)
+    h = 1e-6
+    for k in list(rng.choice(o.Nv, 16, replace=False)) + [0, 5]:
+        def psi_at(delta):
+            t = theta0.copy()
+            t[k] += delta
+            o.set_params(t[:1], t[1:17].reshape((16, 1), order="F"), t[17:], 0.0)
+            return o.eval_configs(xs, want_h=False)["psi"][:, 0].real
+        fd = (psi_at(h) - psi_at(-h)) / (2 * h)
+        an = base["O"][:, k].real
+        assert np.all(np.abs(fd - an) <= 1e-6 * np.abs(base["psi"][:, 0]) + 1e-8 * np.abs(an)), (k, fd, an)
+    o.set_params(p.br, p.Wr, p.slater, 0.0)
+
+
 def test_ed_gauge_invariance_and_value():
     E_g = ed.ground_state_energy(4, 1.0, 0.5, gauge=True)
     E_u = ed.ground_state_energy(4, 1.0, 0.5, gauge=False)
