@@ -9,7 +9,7 @@ import sys
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "librbmpp.so")
-SOURCES = ["capi.cu", "sampler.cu", "sampler_stream.cu", "estimator.cu", "correlation.cu", "linalg.cu", "sr_solve.cu", "gemm_bf16x3.cu"]
+SOURCES = ["capi.cu", "sampler.cu", "sampler_stream.cu", "estimator.cu", "correlation.cu", "linalg.cu", "sr_solve.cu", "gemm_bf16x3.cu", "skew.cu"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC",
          "-Xcompiler", "-O2", "--expt-relaxed-constexpr"]

@@ -58,6 +58,13 @@ int rbmpp_syrk_bf16x3(int, int, const double*, const double*, const double*, voi
 cudaError_t rbmpp_scale_copy(int, const double*, double, double*, cudaStream_t);
 cudaError_t rbmpp_add_outer_offdiag(int, double*, const double*, double, cudaStream_t);
 int rbmpp_correlation_fits(const DevDims&, int);
+int rbmpp_skew_max_n();
+size_t rbmpp_skew_smem_shortfall(const DevDims&, int);
+cudaError_t rbmpp_build_se(const DevDims&, const int*, const int*, const double*, double*, cudaStream_t);
+cudaError_t rbmpp_launch_sampler_skew(const DevDims&, const DevTables&, const DevParams&, const DevWalkers&, int,
+                                      cudaStream_t);
+cudaError_t rbmpp_launch_estimator_skew(const DevDims&, const DevTables&, const DevParams&, const int8_t*, int,
+                                        double*, double*, double*, int*, int*, int, cudaStream_t);
 cudaError_t rbmpp_launch_correlation(const DevDims&, const DevTables&, const DevParams&, const int8_t*, int, double*,
                                      double*, double*, double*, int*, int*, cudaStream_t);
 cudaError_t rbmpp_fill(double*, long long, double, cudaStream_t);
@@ -169,6 +176,7 @@ struct rbmpp_ctx {
   double stats[10] = {0};
   int stream_stages = 0;  // > 0: TMA-streamed sampler with this many stages
   bool est_fits = true;   // the estimator's workspace fits in shared memory
+  double* d_SE = nullptr;  // Slater_Elm [qp][2N][2N] of the skew form (transverse projection)
   // host-supplied cross-rank sum (rbmpp_set_allreduce) and its packed buffer: 6 scalars, gvec, Ovec
   rbmpp_allreduce_fn red_fn = nullptr;
   void* red_user = nullptr;
@@ -221,6 +229,7 @@ DevParams params(const rbmpp_ctx* c) {
   p.br = c->d_br;
   p.XF = c->d_XF;
   p.XFT = c->d_XFT;
+  p.SE = c->d_SE;
   return p;
 }
 
@@ -234,12 +243,16 @@ int upload_params(rbmpp_ctx* c) {
     CK(cudaMemcpyAsync(c->d_br, c->br.data(), sizeof(double) * d.alphar, cudaMemcpyHostToDevice, c->st));
   }
   CK(cudaMemcpyAsync(c->d_slater, c->slater.data(), sizeof(double) * d.n_slater, cudaMemcpyHostToDevice, c->st));
-  long long tot = (long long)d.n_qp * d.N * d.N;
-  rbmpp_note_launch();
-  build_xf_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, c->st>>>(d.N, d.n_mp, c->d_wmap, c->d_orb, c->d_slater,
-                                                                      d.sp_cc[0], d.sp_ss[0], d.sp_cc[1], d.sp_ss[1],
-                                                                      c->d_XF, c->d_XFT);
-  CK(cudaGetLastError());
+  if (d.skew) {
+    CK(rbmpp_build_se(d, c->d_wmap, c->d_orb, c->d_slater, c->d_SE, c->st));
+  } else {
+    long long tot = (long long)d.n_qp * d.N * d.N;
+    rbmpp_note_launch();
+    build_xf_kernel<<<(unsigned)((tot + 255) / 256), 256, 0, c->st>>>(d.N, d.n_mp, c->d_wmap, c->d_orb, c->d_slater,
+                                                                        d.sp_cc[0], d.sp_ss[0], d.sp_cc[1],
+                                                                        d.sp_ss[1], c->d_XF, c->d_XFT);
+    CK(cudaGetLastError());
+  }
   c->d.shift = c->shift;
   CK(cudaStreamSynchronize(c->st));
   return 0;
@@ -546,7 +559,7 @@ int rbmpp_destroy(rbmpp_ctx* c) {
                   c->W.mt, c->W.nfastup, c->W.naccept, c->W.nacc_all, c->W.status, c->W.xs, c->W.pfs, c->W.psis, c->W.gj, c->W.events, c->W.trace, (void*)c->W.replay, c->d_O, c->d_psiS,
                   c->d_eloc, c->d_a, c->d_b, c->d_tmp_ns, c->d_acc4, c->d_nap, c->d_estat, c->d_gvec, c->d_Ovec,
                   c->d_vec, c->d_S, c->d_part, c->d_info, c->d_err, c->d_rv, c->d_hi, c->d_lo, c->d_Sf, c->d_Sb,
-                  c->d_crow, c->d_csd, c->d_cones, c->d_cvbs, c->d_cpart, c->d_csum, c->d_dinv, c->d_pcg, c->d_gpart, c->d_sc, c->d_bar, c->d_xch};
+                  c->d_crow, c->d_csd, c->d_cones, c->d_cvbs, c->d_cpart, c->d_csum, c->d_dinv, c->d_pcg, c->d_gpart, c->d_sc, c->d_bar, c->d_xch, c->d_SE};
   for (void* p : ptrs)
     if (p) cudaFree(p);
   if (c->h_sc) cudaFreeHost(c->h_sc);
@@ -580,9 +593,12 @@ int rbmpp_set_tables(rbmpp_ctx* c, const int* W_map, const double* para, const i
   DevDims& d = c->d;
   const int N = d.N;
   if (sp_weights) {
-    // InitSPWeight's products (spin_projection.f90:36-41); the kernels carry the Pfaffian as det X of the
-    // up-down block, which needs the same-spin blocks -(F - F^T) cos sin of slater.f90:36-44 to vanish
+    // InitSPWeight's products (spin_projection.f90:36-41).  When cos*sin vanishes at both points (beta in
+    // {0, pi}) the same-spin blocks -(F - F^T) cos sin of slater.f90:36-44 vanish and the kernels carry the
+    // Pfaffian as det X of the up-down block; otherwise (the transverse code's beta = -/+pi/2) they carry the
+    // full N x N skew form.
     double cc[2], cs[2], ss[2];
+    int skew = 0;
     for (int sp = 0; sp < 2; sp++) {
       const double co = sp_weights[3 * sp], si = sp_weights[3 * sp + 1], w = sp_weights[3 * sp + 2];
       if (!std::isfinite(co) || !std::isfinite(si) || !std::isfinite(w))
@@ -590,11 +606,30 @@ int rbmpp_set_tables(rbmpp_ctx* c, const int* W_map, const double* para, const i
       cc[sp] = co * co;
       cs[sp] = co * si;
       ss[sp] = si * si;
-      if (!(std::fabs(cs[sp]) <= 1e-12 * std::max(cc[sp], ss[sp])))
-        return fail(c, RBMPP_E_ARG,
-                    "sp_weights: point %d has cos*sin = %g, so the same-spin blocks of Slater_Elm (slater.f90:36-44) "
-                    "do not vanish; only projections with beta in {0, pi} are supported",
-                    sp + 1, cs[sp]);
+      if (!(std::fabs(cs[sp]) <= 1e-12 * std::max(cc[sp], ss[sp]))) skew = 1;
+    }
+    if (skew && d.N > rbmpp_skew_max_n())
+      return fail(c, RBMPP_E_ARG, "sp_weights: the skew form (same-spin blocks present) supports N <= %d, not %d",
+                  rbmpp_skew_max_n(), d.N);
+    if (skew) {
+      DevDims t = d;
+      t.skew = 1;
+      int maxsm = 0;
+      CK(cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, c->dims.device));
+      const size_t need = rbmpp_skew_smem_shortfall(t, maxsm);
+      if (need) return fail(c, RBMPP_E_ARG, "skew-form workspace %zu B exceeds %d B of shared memory", need, maxsm);
+    }
+    if (skew != d.skew) {
+      // the per-walker inverses change shape: Np x Np blocks or N x N skew matrices
+      const size_t nw = d.nw, np2 = (size_t)d.n_qp * (skew ? (size_t)d.N * d.N : (size_t)d.Np * d.Np);
+      CK(cudaFree(c->W.Y));
+      c->bytes -= sizeof(double) * nw * d.n_qp * (d.skew ? (size_t)d.N * d.N : (size_t)d.Np * d.Np);
+      c->W.Y = nullptr;
+      int r = dalloc(c, &c->W.Y, nw * np2);
+      if (r) return r;
+      if (skew && !c->d_SE && (r = dalloc(c, &c->d_SE, (size_t)d.n_qp * 4 * d.N * d.N))) return r;
+      d.skew = skew;
+      c->sampled = false;
     }
     for (int sp = 0; sp < 2; sp++) {
       d.sp_cc[sp] = cc[sp];
@@ -702,7 +737,9 @@ int rbmpp_make_sample(rbmpp_ctx* c, int first, int* naccept, long long* naccept_
   if (!first && !c->sampled) return fail(c, RBMPP_E_STATE, "make_sample(first=0) before any sample exists");
   c->d.shift = c->shift;
   CK(cudaEventRecord(c->ev[0], c->st));
-  if (c->stream_stages > 0)
+  if (c->d.skew)
+    CK(rbmpp_launch_sampler_skew(c->d, tables(c), params(c), c->W, first ? 1 : 0, c->st));
+  else if (c->stream_stages > 0)
     CK(rbmpp_launch_sampler_stream(c->d, tables(c), params(c), c->W, first ? 1 : 0, c->stream_stages, c->st));
   else
     CK(rbmpp_launch_sampler(c->d, tables(c), params(c), c->W, first ? 1 : 0, c->st));
@@ -769,7 +806,7 @@ int rbmpp_set_samples(rbmpp_ctx* c, const int* x) {
 
 static int measure_common(rbmpp_ctx* c, bool with_o) {
   const DevDims& d = c->d;
-  if (!c->est_fits)
+  if (!c->est_fits && !d.skew)
     return fail(c, RBMPP_E_ARG, "the estimator's workspace for N/2 = %d exceeds the shared memory of one block", d.Np);
   int r = ensure_measure_buffers(c);
   if (r) return r;
@@ -777,8 +814,12 @@ static int measure_common(rbmpp_ctx* c, bool with_o) {
   c->S_reduced = false;
   c->d.shift = c->shift;
   CK(cudaEventRecord(c->ev[2], c->st));
-  CK(rbmpp_launch_estimator(c->d, tables(c), params(c), c->W.xs, c->ns_tot, c->d_psiS, c->d_eloc,
-                            with_o ? c->d_O : nullptr, c->d_nap, c->d_estat, 1, c->st));
+  if (d.skew)
+    CK(rbmpp_launch_estimator_skew(c->d, tables(c), params(c), c->W.xs, c->ns_tot, c->d_psiS, c->d_eloc,
+                                   with_o ? c->d_O : nullptr, c->d_nap, c->d_estat, 1, c->st));
+  else
+    CK(rbmpp_launch_estimator(c->d, tables(c), params(c), c->W.xs, c->ns_tot, c->d_psiS, c->d_eloc,
+                              with_o ? c->d_O : nullptr, c->d_nap, c->d_estat, 1, c->st));
   CK(cudaEventRecord(c->ev[3], c->st));
   CK(cudaStreamSynchronize(c->st));
   {
@@ -840,6 +881,8 @@ int rbmpp_measure_energy(rbmpp_ctx* c, double* scal) {
 int rbmpp_measure_correlation(rbmpp_ctx* c, double* scal, double* chi_sp, double* chi_vbs) {
   if (!c) return RBMPP_E_ARG;
   if (!c->sampled) return fail(c, RBMPP_E_STATE, "measure before make_sample");
+  if (c->d.skew)
+    return fail(c, RBMPP_E_ARG, "correlation measurement: the Calc_Correlation program has no transverse projection");
   const DevDims& d = c->d;
   int dev = 0, maxsm = 0;
   CK(cudaGetDevice(&dev));
@@ -913,7 +956,7 @@ int rbmpp_eval_configs(rbmpp_ctx* c, int n, const int* x, double* psi, double* h
   if (!c || n < 0 || !x) return RBMPP_E_ARG;
   if (!c->params_set) return fail(c, RBMPP_E_STATE, "set_params must come first");
   if (n == 0) return 0;
-  if (!c->est_fits)
+  if (!c->est_fits && !c->d.skew)
     return fail(c, RBMPP_E_ARG, "the estimator's workspace for N/2 = %d exceeds the shared memory of one block",
                 c->d.Np);
   const DevDims& d = c->d;
@@ -935,7 +978,9 @@ int rbmpp_eval_configs(rbmpp_ctx* c, int n, const int* x, double* psi, double* h
     int_to_i8_kernel<<<(unsigned)((nx + 255) / 256), 256, 0, c->st>>>(dx, dx8, nx);
     e = cudaGetLastError();
   }
-  if (!e) e = rbmpp_launch_estimator(c->d, tables(c), params(c), dx8, n, dpsi, dh, dO, nullptr, dst, 0, c->st);
+  if (!e)
+    e = d.skew ? rbmpp_launch_estimator_skew(c->d, tables(c), params(c), dx8, n, dpsi, dh, dO, nullptr, dst, 0, c->st)
+               : rbmpp_launch_estimator(c->d, tables(c), params(c), dx8, n, dpsi, dh, dO, nullptr, dst, 0, c->st);
   if (!e) e = cudaStreamSynchronize(c->st);
   if (!e) rc = check_walker_status(c, dst, n, "eval_configs");
   if (!e && !rc && psi) e = cudaMemcpy(psi, dpsi, sizeof(double) * (size_t)n * (d.n_qp + 1) * 2, cudaMemcpyDeviceToHost);
@@ -1362,7 +1407,8 @@ int rbmpp_iteration(rbmpp_ctx* c, int precision, double delta_tau, double s_fact
   double wf = 0.0;
   for (int k = 0; k < 10; k++) wf = wf + c->wf_av_list[k];
   wf = wf / 10.0;
-  c->shift = wf * 0.001 / (double)c->d.N / (double)c->d.N;
+  // main.f90:451; transverse_code/main.f90:451 uses 0.003
+  c->shift = wf * (c->d.skew ? 0.003 : 0.001) / (double)c->d.N / (double)c->d.N;
   c->d.shift = c->shift;
   CK(cudaEventRecord(c->ev[10], c->st));
   CK(cudaEventSynchronize(c->ev[10]));
@@ -1434,7 +1480,7 @@ int rbmpp_copy_state(rbmpp_ctx* dst, const rbmpp_ctx* src) {
   rbmpp_ctx* c = dst;  // errors are reported on the destination context
   const DevDims &a = dst->d, &b = src->d;
   if (a.L != b.L || a.n_mp != b.n_mp || a.alphar != b.alphar || a.n_slater != b.n_slater || a.nw != b.nw ||
-      a.ns != b.ns || dst->dims.device != src->dims.device)
+      a.ns != b.ns || a.skew != b.skew || dst->dims.device != src->dims.device)
     return fail(dst, RBMPP_E_ARG, "copy_state: the two contexts differ in shape or device");
   if (!src->tables_set || !dst->tables_set) return fail(dst, RBMPP_E_STATE, "copy_state: tables must be set on both");
   const size_t nw = a.nw, ns = a.ns, N = a.N;
@@ -1450,7 +1496,7 @@ int rbmpp_copy_state(rbmpp_ctx* dst, const rbmpp_ctx* src) {
   CK(cp(D.sgn, S.sgn, nw * a.n_mp));
   CK(cp(D.pf, S.pf, 8 * nw * a.n_qp));
   CK(cp(D.psi, S.psi, 16 * nw * a.n_qp));
-  CK(cp(D.Y, S.Y, 8 * nw * a.n_qp * (size_t)a.Np * a.Np));
+  CK(cp(D.Y, S.Y, 8 * nw * a.n_qp * (a.skew ? (size_t)N * N : (size_t)a.Np * a.Np)));
   CK(cp(D.mt, S.mt, 4 * nw * 625));
   CK(cp(D.nfastup, S.nfastup, 4 * nw));
   CK(cp(D.naccept, S.naccept, 4 * nw));
@@ -1602,6 +1648,7 @@ int rbmpp_batch_create(rbmpp_ctx* const* ctxs, int n, rbmpp_batch** out) {
     rbmpp_ctx* c = ctxs[k];
     if (!c) return bfail(b, RBMPP_E_ARG, "context %d is null", k);
     if (!c->tables_set || !c->params_set) return bfail(b, RBMPP_E_STATE, "context %d: tables and params first", k);
+    if (c->d.skew) return bfail(b, RBMPP_E_ARG, "context %d: the batched sampler carries the block form only", k);
     if (dev < 0) dev = c->dims.device;
     if (c->dims.device != dev) return bfail(b, RBMPP_E_ARG, "contexts on different devices");
     b->ctx.push_back(c);
@@ -1854,6 +1901,7 @@ extern "C" int rbmpp_eval_configs_noalloc(rbmpp_ctx* c, int n, const int* d_x, d
   if (c->dims.device < 0 || c->dims.device >= 64)
     return fail(c, RBMPP_E_ARG, "eval_configs_noalloc: device ordinal %d outside 0..63", c->dims.device);
   if (!c->params_set) return fail(c, RBMPP_E_STATE, "set_params must come first");
+  if (c->d.skew) return fail(c, RBMPP_E_ARG, "eval_configs_noalloc carries the block form only; use eval_configs");
   if (!c->est_fits)
     return fail(c, RBMPP_E_ARG, "the estimator's workspace for N/2 = %d exceeds the shared memory of one block",
                 c->d.Np);

@@ -33,6 +33,9 @@ struct DevDims {
   int skip_load;      // verification hook: walker 0 of the streaming sampler never issues its load number
                       //   skip_load (1-based), so the wait on it runs out (0: off)
   int wait_polls;     // poll bound of the streaming sampler's pipeline waits (0: the default 2^22)
+  int skew;           // the same-spin blocks of Slater_Elm do not vanish (transverse spin projection): the
+                      //   Pfaffian matrix is carried in its full N x N skew form (skew.cu), DevWalkers::Y holds
+                      //   [w][qp][N][N] and DevParams::SE the Slater elements
   double J1, J2, shift;
   double sp_cc[2], sp_cs[2], sp_ss[2], para_sp[2];
 };
@@ -51,6 +54,7 @@ struct DevParams {
   const double* br;   // [f]
   const double* XF;   // [qp][N][N]
   const double* XFT;  // [qp][N][N]
+  const double* SE;   // [qp][2N][2N] Slater_Elm(r, r') row-major (skew form only)
 };
 
 struct DevWalkers {
@@ -96,6 +100,7 @@ struct BatchInst {
 #define ST_THETA 4
 #define ST_CANDIDATE 5
 #define ST_INITX 6
+#define ST_SKEW 7
 #define ST_SINGULAR 8
 
 // ------------------------------------------------------------------------------------------------

@@ -147,8 +147,17 @@ __device__ __forceinline__ void cta_scratch_all(const SCtx& c, const int* idx, d
   __syncthreads();
 }
 
+// The from-scratch Pfaffians and inverses of every projection (calculate_MAll) as a policy of the walker
+// routines below: the block form's, or the full skew form's (skew.cu).
+template <int KPL, int NP>
+struct BlockScratch {
+  static __device__ __forceinline__ void run(const SCtx& c, const int* idx, double* pf_out, bool write_y, bool diff) {
+    cta_scratch_all<KPL, NP>(c, idx, pf_out, write_y, diff);
+  }
+};
+
 // calc_theta, x_to_Ele_Idx, calculate_MAll, sign_PP, calc_amplitude (make_sample.f90:54-60 / :345-350)
-template <int KPL = 0, int NP = 0>
+template <int KPL = 0, int NP = 0, class F = BlockScratch<KPL, NP>>
 __device__ __forceinline__ void full_state(const SCtx& c) {
   const WS& s = c.s;
   cta_calc_theta(c.d, c.t, c.p, s.x, s.th);
@@ -158,7 +167,7 @@ __device__ __forceinline__ void full_state(const SCtx& c) {
   }
   __syncthreads();
   if (status(c)) return;
-  cta_scratch_all<KPL, NP>(c, s.idx, s.pf, true, false);
+  F::run(c, s.idx, s.pf, true, false);
   if (status(c)) return;
   cta_sign_pp(c.d, c.t, s, s.idx, s.sgn);
   __syncthreads();
@@ -171,7 +180,7 @@ __device__ __forceinline__ void full_state(const SCtx& c) {
 }
 
 // make_initial_x make_sample.f90:298-362
-template <int KPL = 0, int NP = 0>
+template <int KPL = 0, int NP = 0, class F = BlockScratch<KPL, NP>>
 __device__ __forceinline__ void make_initial_x(const SCtx& c) {
   const WS& s = c.s;
   for (int it1 = 0; it1 < 1000000; it1++) {
@@ -193,7 +202,7 @@ __device__ __forceinline__ void make_initial_x(const SCtx& c) {
     }
     __syncthreads();
     if (status(c)) return;
-    full_state<KPL, NP>(c);
+    full_state<KPL, NP, F>(c);
     if (status(c)) return;
     if (hypot(s.dsc[D_PSI0R], s.dsc[D_PSI0I]) > 1e-300) return;
   }
@@ -216,7 +225,7 @@ __device__ __forceinline__ void trace_rec(const SCtx& c, int type, double a, dou
 }
 
 // Nfastup checkpoint make_sample.f90:74-128.  i0 (sweep) only labels the trace record.
-template <int KPL = 0, int NP = 0>
+template <int KPL = 0, int NP = 0, class F = BlockScratch<KPL, NP>>
 __device__ __forceinline__ void checkpoint(const SCtx& c, int& nfastup, int i0) {
   const DevDims& d = c.d;
   const WS& s = c.s;
@@ -245,7 +254,7 @@ __device__ __forceinline__ void checkpoint(const SCtx& c, int& nfastup, int i0) 
   // old Pf kept in pfp for the drift measure
   for (int qp = threadIdx.x; qp < d.n_qp; qp += blockDim.x) s.pfp[qp] = s.pf[qp];
   __syncthreads();
-  cta_scratch_all<KPL, NP>(c, s.idx, s.pf, true, true);
+  F::run(c, s.idx, s.pf, true, true);
   if (status(c)) return;
   cta_amplitude(d, c.t, s, s.th, s.pf, s.sgn, s.psi, D_PSI0R);
   if (threadIdx.x == 0) {
@@ -277,7 +286,7 @@ __device__ __forceinline__ void checkpoint(const SCtx& c, int& nfastup, int i0) 
 }
 
 // Global spin flip make_sample.f90:135-158 (RNG check already drawn by the caller).
-template <int KPL = 0, int NP = 0>
+template <int KPL = 0, int NP = 0, class F = BlockScratch<KPL, NP>>
 __device__ __forceinline__ void global_flip(const SCtx& c) {
   const DevDims& d = c.d;
   const WS& s = c.s;
@@ -290,7 +299,7 @@ __device__ __forceinline__ void global_flip(const SCtx& c) {
   }
   __syncthreads();
   if (status(c)) return;
-  cta_scratch_all<KPL, NP>(c, s.idx2, s.pfp, false, false);  // Pf of the flipped configuration
+  F::run(c, s.idx2, s.pfp, false, false);  // Pf of the flipped configuration
   if (status(c)) return;
   cta_sign_pp(d, c.t, s, s.idx2, s.sgnp);
   __syncthreads();
@@ -327,7 +336,7 @@ __device__ __forceinline__ void global_flip(const SCtx& c) {
     s.dsc[D_PSI0I] = s.dsc[D_PSIPI];
   }
   __syncthreads();
-  cta_scratch_all<KPL, NP>(c, s.idx, s.pf, true, false);  // Tmp_Inv_M of the accepted flipped state
+  F::run(c, s.idx, s.pf, true, false);  // Tmp_Inv_M of the accepted flipped state
 }
 
 

@@ -2,8 +2,8 @@
 kernels, and a bounded device wait that runs out returns RBMPP_E_TIMEOUT with the context still usable.
 
 No test here faults, traps or hangs a GPU.  Bad inputs are made on the host (a non-permutation W_map, an
-out-of-range orbital index, a sublattice flag of 2, transverse spin-projection weights, a stored sample
-outside the Sz = 0 sector).  The timeout is made by a verification hook: walker 0 never issues one bulk
+out-of-range orbital index, a sublattice flag of 2, non-finite spin-projection weights, a transverse
+projection beyond the skew form's size, a stored sample outside the Sz = 0 sector).  The timeout is made by a verification hook: walker 0 never issues one bulk
 load, so the wait on it runs out after a short poll bound.
 """
 import numpy as np
@@ -53,11 +53,11 @@ def test_bad_tables_are_refused():
     sb = np.zeros(16, dtype=np.int32)
     sb[7] = 2
     _refused(p, "neither 0 nor 1", subB=sb)
-    # the transverse code's weights (transverse_code/spin_projection.f90:30-38): cos*sin = -/+ 1
-    r2 = np.sqrt(2.0)
-    spw = np.array([[r2 * np.cos(-np.pi / 4), r2 * np.sin(-np.pi / 4), 1.0],
-                    [r2 * np.cos(np.pi / 4), r2 * np.sin(np.pi / 4), 1.0]]).T
-    _refused(_problem(), "same-spin blocks", sp_weights=spw)
+    spw = fm.spin_projection_weights(1, transverse=True)
+    spw[1, 0] = np.nan
+    _refused(_problem(), "non-finite value", sp_weights=spw)
+    # the skew form (transverse projection) takes N <= 128
+    _refused(_problem(L=12), "supports N <= 128", sp_weights=fm.spin_projection_weights(1, transverse=True))
     p = _problem()
     p.sym.para_mp = p.sym.para_mp.astype(np.complex128) + 0.5j
     _refused(p, "complex para_mp_trans")
