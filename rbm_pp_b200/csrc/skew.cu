@@ -140,6 +140,38 @@ __device__ double warp_pfaffian(double* T, int n, bool& singular) {
   return pf;
 }
 
+// G = (B^-1 - B^-T) / 2 in place (matrix.f90:96-105) from warp_gj's inverse, whose column j sits at perm[j].
+// The symmetric part of the computed inverse is rounding noise, which the exchange-ratio formula would amplify
+// by the conditioning of B; the skew part alone gives ratios to about 1e-13.
+template <int KPL>
+__device__ void warp_unpermute_skew(double* T, int n, const int* perm) {
+  const int ld = n + 1, lane = threadIdx.x & 31;
+  for (int i = 0; i < n; i++) {
+    double v[KPL];
+#pragma unroll
+    for (int m = 0; m < KPL; m++) {
+      const int j = lane + 32 * m;
+      v[m] = j < n ? T[i * ld + perm[j]] : 0.0;
+    }
+    __syncwarp();
+#pragma unroll
+    for (int m = 0; m < KPL; m++) {
+      const int j = lane + 32 * m;
+      if (j < n) T[i * ld + j] = v[m];
+    }
+    __syncwarp();
+  }
+  for (int i = 0; i < n; i++) {
+    for (int j = i + 1 + lane; j < n; j += 32) {
+      const double g = 0.5 * (T[i * ld + j] - T[j * ld + i]);
+      T[i * ld + j] = g;
+      T[j * ld + i] = -g;
+    }
+    if (lane == 0) T[i * ld + i] = 0.0;
+    __syncwarp();
+  }
+}
+
 // calculate_MAll for the skew form (policy of the walker routines of sampler_common.cuh): one warp per
 // projection on its own shared-memory tile; writes G (when write_y) and pf_out; with diff, the drift measure
 // of make_sample.f90:106-113 against the stored G.
@@ -712,6 +744,7 @@ __global__ void __launch_bounds__(kSkThreads, 1)
       if (!sing) {
         warp_gather_skew(T, d, p, qp, s.idx);
         (void)warp_gj<KPL, 0, 4>(T, N, src, sing);
+        if (!sing) warp_unpermute_skew<KPL>(T, N, src);
       }
       if (sing) bad = 1;
       const cplx cw = psi_wo_pf(d, t, s.rbm[qp], s.sgn[mp], qp);
@@ -720,7 +753,7 @@ __global__ void __launch_bounds__(kSkThreads, 1)
         s.psi[2 * qp] = cw.re * pfq;
         s.psi[2 * qp + 1] = cw.im * pfq;
       }
-      // exchange ratio of every antiparallel bond against G = B^{-1} (the tile, columns through src)
+      // exchange ratio of every antiparallel bond against G = B^{-1} (the tile, skew-symmetrised)
       for (int b = 0; b < nap && !sing; b++) {
         const int i1 = e.ap[2 * b], i2 = e.ap[2 * b + 1];
         const int ea = s.cfg[i1], eb = s.cfg[i2];  // electron ea moves to i2, eb to i1
@@ -729,25 +762,25 @@ __global__ void __launch_bounds__(kSkThreads, 1)
         const double* SEb = se_row(d, p, qp, rb);
         warp_gather_xy(d, SEa, SEb, s.idx, ea, eb, xh, yh);
         const double ya = -SEa[rb];
-        // (G y^)_i for this lane's rows, G(i, j) = T(i, src[j])
+        // (G y^)_i for this lane's rows
         double xgy = 0.0;
         for (int i = lane; i < N; i += 32) {
           const double* Tr = T + i * ld;
           double acc = 0.0;
-          for (int j = 0; j < N; j++) acc = fma(Tr[src[j]], yh[j], acc);
+          for (int j = 0; j < N; j++) acc = fma(Tr[j], yh[j], acc);
           gy[i] = acc;
           xgy = fma(xh[i], acc, xgy);
         }
         double gxa = 0.0, gxb = 0.0;
         for (int j = lane; j < N; j += 32) {
-          gxa = fma(T[ea * ld + src[j]], xh[j], gxa);
-          gxb = fma(T[eb * ld + src[j]], xh[j], gxb);
+          gxa = fma(T[ea * ld + j], xh[j], gxa);
+          gxb = fma(T[eb * ld + j], xh[j], gxb);
         }
         xgy = warp_sum(xgy);
         gxa = warp_sum(gxa);
         gxb = warp_sum(gxb);
         __syncwarp();
-        const double gab = T[ea * ld + src[eb]];
+        const double gab = T[ea * ld + eb];
         if (lane == 0) Rw[b] = -gab * (ya + xgy) + gxa * gy[eb] - gxb * gy[ea];
         __syncwarp();
       }
@@ -780,7 +813,6 @@ __global__ void __launch_bounds__(kSkThreads, 1)
       for (int w = 0; w < e.nqw && q0 + w < d.n_qp; w++) {
         const int qp = q0 + w, mp = qp >> 1, sp = qp & 1;
         const double* Tw = e.tiles + (size_t)w * N * ld;
-        const int* srcw = e.perm + (size_t)w * N;
         const int* wm = t.wmap + (size_t)mp * N;
         const cplx cw = psi_wo_pf(d, t, s.rbm[qp], s.sgn[mp], qp);
         const double pw = e.pfw[qp] * cw.re;
@@ -791,7 +823,7 @@ __global__ void __launch_bounds__(kSkThreads, 1)
           while (j * (j - 1) / 2 > pr) j--;
           while ((j + 1) * j / 2 <= pr) j++;
           const int i = pr - j * (j - 1) / 2;
-          const double gji = Tw[j * ld + srcw[i]];
+          const double gji = Tw[j * ld + i];
           const int ti = wm[s.idx[i]], tj = wm[s.idx[j]];
           double c1, c2;
           skew_coef(d, sp, i >= Np, j >= Np, c1, c2);
