@@ -104,7 +104,12 @@ int rbmpp_query(const rbmpp_ctx* ctx, int what, long long* value);
  * or NULL (derived: site i = i2 L + i1 + 1 is on B when i1 + i2 is odd),
  * sp_weights(3, 2) = {SP_GL_Cos, SP_GL_Sin, para_spin_proj} of the two spin-projection points
  * (InitSPWeight, spin_projection.f90:5-79) or NULL (beta = 0 and pi, para_spin_proj = (1, spin_parity)).
- * The weights must make SP_GL_Cos * SP_GL_Sin vanish (relative 1e-12) at both points.
+ * Where SP_GL_Cos * SP_GL_Sin vanishes (relative 1e-12) at both points, the Pfaffian matrix is block
+ * off-diagonal and the library carries its Np x Np up-down block; otherwise (the transverse code's
+ * beta = -pi/2, pi/2 with sqrt(2)-scaled weights, transverse_code/spin_projection.f90:30-38) it carries the full
+ * N x N skew matrix (N <= 128), and rbmpp_iteration uses the transverse shift schedule
+ * (transverse_code/main.f90:451).  The skew form has no batched sampler, no correlation measurement and no
+ * allocation-free evaluation.
  * Replaces the module setup of main.f90:89-300. */
 int rbmpp_set_tables(rbmpp_ctx* ctx, const int* W_map, const double* para_mp_trans, const int* Orbital_Idx,
                      const int* Orbital_Sgn, const int* subB, const double* sp_weights);

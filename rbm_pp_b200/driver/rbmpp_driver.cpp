@@ -19,8 +19,12 @@
 // of its samples, 7 more make_samples, then Nav rounds of make_sample + rbmpp_measure_correlation, each
 // writing Chi_sp / norm to fort.<60000+it> and Chi_vbs / norm to fort.<70000+it> in the reference's formats.
 //
+// With --transverse it runs the transverse code instead (transverse_code/main.f90): spin projection at
+// beta = -pi/2, pi/2 with sqrt(2)-scaled weights (transverse_code/spin_projection.f90:30-38) and the shift
+// schedule of transverse_code/main.f90:451; the library then carries the full skew Pfaffian matrix.
+//
 // Usage: rbmpp_driver [--dir D] [--walkers W] [--seed S] [--precision fp64|split] [--device G]
-//                     [--nstep N] [--correlation] [--check-inputs]
+//                     [--nstep N] [--correlation | --transverse] [--check-inputs]
 // --check-inputs parses and validates the inputs, prints a summary and exits without touching a GPU.
 #include <chrono>
 #include <cmath>
@@ -298,7 +302,7 @@ int main(int argc, char** argv) {
   std::string dir = ".", prec = "fp64";
   int walkers = 1, device = 0, nstep_override = -1;
   long long seed = -1;
-  bool check_only = false, correlation = false;
+  bool check_only = false, correlation = false, transverse = false;
   for (int i = 1; i < argc; i++) {
     std::string a = argv[i];
     auto next = [&]() -> std::string {
@@ -313,8 +317,10 @@ int main(int argc, char** argv) {
     else if (a == "--nstep") nstep_override = std::atoi(next().c_str());
     else if (a == "--check-inputs") check_only = true;
     else if (a == "--correlation") correlation = true;
+    else if (a == "--transverse") transverse = true;
     else die("unknown argument " + a);
   }
+  if (correlation && transverse) die("--correlation and --transverse: the Calc_Correlation program has no transverse form");
   Inputs in;
   read_rbm_input(dir, in);
   if (in.alphac != 0) die("alphac > 0 (complex RBM) is not supported by this library");
@@ -360,7 +366,22 @@ int main(int argc, char** argv) {
   d.walker_offset = 0;
   Lib lib;
   lib.ck(rbmpp_create(&d, &lib.c), "rbmpp_create");
-  lib.ck(rbmpp_set_tables(lib.c, in.W_map.data(), in.para.data(), in.orbital_idx.data(), nullptr, nullptr, nullptr), "set_tables");
+  // InitSPWeight: SP_GL_Cos, SP_GL_Sin, para_spin_proj per point (spin_projection.f90:25-63; transverse:
+  // transverse_code/spin_projection.f90:30-38)
+  std::vector<double> spw(6);
+  {
+    const double pi = std::acos(-1.0);
+    const double beta[2] = {transverse ? -0.5 * pi : 0.0, transverse ? 0.5 * pi : pi};
+    const double scale = transverse ? std::sqrt(2.0) : 1.0;
+    for (int sp = 0; sp < 2; sp++) {
+      spw[3 * sp] = scale * std::cos(0.5 * beta[sp]);
+      spw[3 * sp + 1] = scale * std::sin(0.5 * beta[sp]);
+      spw[3 * sp + 2] = (sp == 0 || in.spin_parity == 1) ? 1.0 : -1.0;
+    }
+  }
+  lib.ck(rbmpp_set_tables(lib.c, in.W_map.data(), in.para.data(), in.orbital_idx.data(), nullptr, nullptr,
+                          spw.data()),
+         "set_tables");
   lib.ck(rbmpp_seed_walkers(lib.c, (int)seed), "seed_walkers");
   // initialize_parameters (parameter.f90:21-41): rank 0 draws U(-0.05, 0.05); W.input overrides
   std::vector<double> u((size_t)in.alphar * (N + 1));

@@ -168,3 +168,24 @@ def test_driver_writes_input_checks(tmp_path):
     f = np.array([float(v) for v in vals])
     assert np.allclose(f, q.slater, rtol=1e-14, atol=0)
     assert abs(np.abs(f).mean() - 0.25) < 1e-12
+
+
+@pytest.mark.gpu
+def test_driver_transverse_matches_oracle(tmp_path):
+    """--transverse: the transverse code's main program (transverse_code/main.f90) over the library's skew form;
+    its energies per iteration follow the oracle's loop with the transverse weights and shift schedule.  No RBM
+    units: with this projection the bias has no fluctuation (O_b / psi = tanh b), which the reference's S-diagonal
+    check stops on."""
+    import pyoracle as po
+    nw, ns, nstep, seed = 8, 8, 3, 4343
+    p = fm.synthetic_problem(4, translations=False, alphar=0, nsample=nw * ns, seed=18, Nstep=nstep, Nav=1)
+    fm.write_problem(str(tmp_path), p)
+    out = subprocess.run([_driver(), "--dir", str(tmp_path), "--walkers", str(nw), "--seed", str(seed),
+                          "--transverse"], capture_output=True, text=True, timeout=600)
+    assert out.returncode == 0, out.stderr + out.stdout
+    got = np.loadtxt(os.path.join(tmp_path, "Energy_vs_Iteration.txt"))
+    o = po.Oracle(p, nranks=nw, nsample_per_rank=ns, nthreads=4, sp_weights=fm.spin_projection_weights(1, True))
+    loop = po.VMCLoop(o, p, iseed0=seed, shift_coef=0.003)
+    for it in range(1, nstep + 1):
+        rec = loop.iteration_step()
+        assert abs(got[it - 1, 1] - rec["Etot"]) <= 1e-9 * abs(rec["Etot"]), (it, got[it - 1, 1], rec["Etot"])
