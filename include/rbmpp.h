@@ -239,7 +239,9 @@ int rbmpp_debug_hook(rbmpp_ctx* ctx, int what, int value);
 
 /* Adjoint O_k kernel: for n configurations x(N, n): psi(0:N_QP, n) complex, hpsi(n) complex
  * (sum_x' <x|H|x'> psi(x'), calc_local_energy_correlation), and O(Nv, n) = d psi(x) / d theta_k
- * (Ovec_loc_x before reweighting, calc_phys_quantity.f90:115-220).  Any output may be NULL. */
+ * (Ovec_loc_x before reweighting, calc_phys_quantity.f90:115-220).  With complex para_mp_trans, O is complex and
+ * comes as O(Nv, 2, n): real part, then imaginary part, per configuration (the Ovec_Store columns of
+ * calc_phys_quantity.f90:227-228).  Any output may be NULL. */
 int rbmpp_eval_configs(rbmpp_ctx* ctx, int n, const int* x, double* psi, double* hpsi, double* O);
 
 /* Batched sampling: one persistent launch over the walkers of several contexts on one device (different

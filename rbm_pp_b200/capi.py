@@ -164,6 +164,8 @@ class Context:
         self._spw = None if sp_weights is None else _f(sp_weights, np.float64)
         self._chk(lib().rbmpp_set_tables(self.h, _p(self._w), _p(para), _p(self._o), None, _p(self._sb),
                                          _p(self._spw)))
+        # complex para_mp_trans: psi, H psi and O_k are complex (O comes as a real and an imaginary row)
+        self.complex_weights = bool(np.any(para[1::2] != 0.0))
 
     def close(self):
         if getattr(self, "h", None):
@@ -338,13 +340,15 @@ class Context:
         n = x.shape[0]
         psi = np.zeros(2 * (self.n_qp + 1) * n)
         hp = np.zeros(2 * n) if want_h else None
-        O = np.zeros(self.Nv * n) if want_O else None
+        rows = 2 if self.complex_weights else 1
+        O = np.zeros(self.Nv * n * rows) if want_O else None
         self._chk(lib().rbmpp_eval_configs(self.h, n, _p(x.reshape(-1)), _p(psi), _p(hp), _p(O)))
         out = dict(psi=psi.view(np.complex128).reshape(n, self.n_qp + 1))
         if hp is not None:
             out["hpsi"] = hp.view(np.complex128)
         if O is not None:
-            out["O"] = O.reshape(n, self.Nv)
+            O = O.reshape(n, rows, self.Nv)
+            out["O"] = O[:, 0] + 1j * O[:, 1] if rows == 2 else O[:, 0]
         return out
 
     def eval_configs_noalloc(self, n: int, d_x: int, d_psi: int, d_hpsi: int, d_O: int):

@@ -50,7 +50,7 @@ cudaError_t rbmpp_sr_scale(int, int, double*, double, cudaStream_t);
 cudaError_t rbmpp_get_diag(int, const double*, double*, cudaStream_t);
 cudaError_t rbmpp_add_diag(int, double*, double, cudaStream_t);
 cudaError_t rbmpp_rowcol_absmax(int, const double*, const int*, int, double*, cudaStream_t);
-cudaError_t rbmpp_sample_scalars(int, const double*, int, const double*, double, double*, double*, double*,
+cudaError_t rbmpp_sample_scalars(int, const double*, int, const double*, double, double*, double*, double*, int,
                                  cudaStream_t);
 void rbmpp_bf16x3_pads(int, int, int*, int*);
 int rbmpp_syrk_bf16x3(int, int, const double*, const double*, const double*, void*, void*, int*, double*, double*,
@@ -145,6 +145,7 @@ struct rbmpp_ctx {
   DevWalkers W{};
   // measurement
   int ns_tot = 0;
+  int nrows = 0;  // rows of O: ns_tot, or 2 ns_tot with complex projection weights
   double *d_O = nullptr, *d_psiS = nullptr, *d_eloc = nullptr, *d_a = nullptr, *d_b = nullptr, *d_acc4 = nullptr;
   int *d_nap = nullptr, *d_estat = nullptr;
   double *d_gvec = nullptr, *d_Ovec = nullptr, *d_S = nullptr, *d_part = nullptr, *d_vec = nullptr;
@@ -262,13 +263,14 @@ int ensure_measure_buffers(rbmpp_ctx* c) {
   if (c->d_O) return 0;
   const DevDims& d = c->d;
   c->ns_tot = d.nw * d.ns;
+  c->nrows = c->ns_tot * (d.cplx ? 2 : 1);
   int r;
-  if ((r = dalloc(c, &c->d_O, (size_t)c->ns_tot * d.Nv))) return r;
+  if ((r = dalloc(c, &c->d_O, (size_t)c->nrows * d.Nv))) return r;
   if ((r = dalloc(c, &c->d_psiS, (size_t)c->ns_tot * (d.n_qp + 1) * 2))) return r;
   if ((r = dalloc(c, &c->d_eloc, (size_t)c->ns_tot * 2))) return r;
-  if ((r = dalloc(c, &c->d_a, (size_t)c->ns_tot))) return r;
-  if ((r = dalloc(c, &c->d_b, (size_t)c->ns_tot))) return r;
-  if ((r = dalloc(c, &c->d_tmp_ns, (size_t)c->ns_tot))) return r;
+  if ((r = dalloc(c, &c->d_a, (size_t)c->nrows))) return r;
+  if ((r = dalloc(c, &c->d_b, (size_t)c->nrows))) return r;
+  if ((r = dalloc(c, &c->d_tmp_ns, (size_t)c->nrows))) return r;
   if ((r = dalloc(c, &c->d_acc4, 4))) return r;
   if ((r = dalloc(c, &c->d_nap, (size_t)c->ns_tot))) return r;
   if ((r = dalloc(c, &c->d_estat, (size_t)c->ns_tot))) return r;
@@ -338,7 +340,7 @@ int build_S(rbmpp_ctx* c, int prec) {
   CK(cudaEventRecord(c->ev[5], c->st));
   const long long nS = (long long)d.Nv * d.Nv;
   if (prec == RBMPP_SR_FP64) {
-    CK(rbmpp_syrk_ot_o(d.Nv, c->ns_tot, c->d_O, c->d_S, c->st));
+    CK(rbmpp_syrk_ot_o(d.Nv, c->nrows, c->d_O, c->d_S, c->st));
     if (c->red_fn) {
       const int r = reduce_dev(c, c->d_S, nS, "S");
       if (r) return r;
@@ -346,7 +348,7 @@ int build_S(rbmpp_ctx* c, int prec) {
   } else if (prec == RBMPP_SR_SPLIT_BF16) {
     if (!c->d_hi) {
       int kp = 0, np = 0;
-      rbmpp_bf16x3_pads(c->ns_tot, d.Nv, &kp, &np);
+      rbmpp_bf16x3_pads(c->nrows, d.Nv, &kp, &np);
       const size_t bytes = (size_t)kp * np * 2;
       cudaError_t e = cudaMalloc(&c->d_hi, bytes);
       if (!e) e = cudaMalloc(&c->d_lo, bytes);
@@ -357,7 +359,7 @@ int build_S(rbmpp_ctx* c, int prec) {
     const double norm = c->meas_scal[2];
     double* d_m = c->d_rv;  // m = Ovec / norm
     CK(rbmpp_scale_copy(d.Nv, c->d_Ovec, 1.0 / norm, d_m, c->st));
-    const int r = rbmpp_syrk_bf16x3(c->ns_tot, d.Nv, c->d_O, c->d_b, d_m, c->d_hi, c->d_lo, c->d_err, c->d_S,
+    const int r = rbmpp_syrk_bf16x3(c->nrows, d.Nv, c->d_O, c->d_b, d_m, c->d_hi, c->d_lo, c->d_err, c->d_S,
                                     c->d_part, c->st);
     if (r == 1) return fail(c, RBMPP_E_CUDA, "cuTensorMapEncodeTiled unavailable from the driver");
     if (r) return fail(c, RBMPP_E_CUDA, "split-BF16 S build: %s", cudaGetErrorString((cudaError_t)(r - 100)));
@@ -394,7 +396,7 @@ int apply_A(rbmpp_ctx* c, double norm, double scal, double sigma, const double* 
   const DevDims& d = c->d;
   double* v = c->d_pcg;
   const size_t Nv = d.Nv;
-  CK(rbmpp_sr_apply_gram(c->ns_tot, d.Nv, d.Nv_rbm, c->d_O, v + VM * Nv, scal, x, v + VWS * Nv, v + VZZ * Nv,
+  CK(rbmpp_sr_apply_gram(c->nrows, d.Nv, d.Nv_rbm, c->d_O, v + VM * Nv, scal, x, v + VWS * Nv, v + VZZ * Nv,
                          c->d_gpart, c->d_tmp_ns, c->d_part, c->d_sc, c->st));
   if (c->red_fn) {
     const int r = reduce_dev(c, v + VZZ * Nv, d.Nv, "O^T O x");
@@ -658,9 +660,14 @@ int rbmpp_set_tables(rbmpp_ctx* c, const int* W_map, const double* para, const i
       winv[(size_t)mp * N + (v - 1)] = i;
     }
   }
+  int cplx = 0;
   for (int mp = 0; mp < d.n_mp; mp++)
-    if (para[2 * mp + 1] != 0.0)
-      return fail(c, RBMPP_E_ARG, "complex para_mp_trans is not supported (real projection weights only)");
+    if (para[2 * mp + 1] != 0.0) cplx = 1;
+  if (cplx && d.skew)
+    return fail(c, RBMPP_E_ARG, "complex para_mp_trans with the transverse (skew-form) projection is not supported");
+  if (cplx != d.cplx && c->d_O)
+    return fail(c, RBMPP_E_STATE, "complex para_mp_trans changed after measurement buffers were sized");
+  d.cplx = cplx;
   c->orb_host.assign((size_t)N * N, 0);
   std::vector<int> cnt(d.n_slater, 0);
   for (int p = 0; p < N; p++)
@@ -830,7 +837,7 @@ static int measure_common(rbmpp_ctx* c, bool with_o) {
   r = check_walker_status(c, c->d_estat, c->ns_tot, "calc_phys_quantity");
   if (r) return r;
   CK(rbmpp_sample_scalars(c->ns_tot, c->d_psiS, (d.n_qp + 1) * 2, c->d_eloc, c->shift, c->d_a, c->d_b, c->d_acc4,
-                          c->st));
+                          d.cplx, c->st));
   CK(cudaMemcpyAsync(c->meas_scal, c->d_acc4, sizeof(double) * 4, cudaMemcpyDeviceToHost, c->st));
   c->n_samples_total = (double)d.nw * (double)d.ns;
   // the amplitude draws of the measurement advance each walker's stream
@@ -846,7 +853,7 @@ int rbmpp_measure(rbmpp_ctx* c, double* scal, double* gvec, double* Ovec, double
   int r = measure_common(c, true);
   if (r) return r;
   CK(cudaEventRecord(c->ev[4], c->st));
-  CK(rbmpp_gemv_ot(c->ns_tot, d.Nv, c->d_O, c->d_a, c->d_b, c->d_gvec, c->d_Ovec, c->d_part, 64, c->st));
+  CK(rbmpp_gemv_ot(c->nrows, d.Nv, c->d_O, c->d_a, c->d_b, c->d_gvec, c->d_Ovec, c->d_part, 64, c->st));
   CK(cudaEventRecord(c->ev[11], c->st));
   CK(cudaStreamSynchronize(c->st));
   {
@@ -883,6 +890,8 @@ int rbmpp_measure_correlation(rbmpp_ctx* c, double* scal, double* chi_sp, double
   if (!c->sampled) return fail(c, RBMPP_E_STATE, "measure before make_sample");
   if (c->d.skew)
     return fail(c, RBMPP_E_ARG, "correlation measurement: the Calc_Correlation program has no transverse projection");
+  if (c->d.cplx)
+    return fail(c, RBMPP_E_ARG, "correlation measurement with complex para_mp_trans is not supported");
   const DevDims& d = c->d;
   int dev = 0, maxsm = 0;
   CK(cudaGetDevice(&dev));
@@ -918,7 +927,7 @@ int rbmpp_measure_correlation(rbmpp_ctx* c, double* scal, double* chi_sp, double
   r = check_walker_status(c, c->d_estat, c->ns_tot, "calc_phys_quantity_after_opt (correlation)");
   if (r) return r;
   CK(rbmpp_sample_scalars(c->ns_tot, c->d_psiS, (d.n_qp + 1) * 2, c->d_eloc, c->shift, c->d_a, c->d_b, c->d_acc4,
-                          c->st));
+                          0, c->st));
   CK(rbmpp_gemv_ot(c->ns_tot, (int)lr, c->d_crow, c->d_cones, nullptr, c->d_csum, nullptr, c->d_cpart, nparts, c->st));
   for (int t = 0; t < 4; t++)
     CK(rbmpp_gemm_atb_upper(d.N, c->ns_tot, c->d_csd + (size_t)t * d.N, 4LL * d.N, 1, c->d_cvbs + (size_t)t * d.N * d.N,
@@ -970,7 +979,8 @@ int rbmpp_eval_configs(rbmpp_ctx* c, int n, const int* x, double* psi, double* h
   if (!e) e = cudaMalloc(&dx8, nx);
   if (!e) e = cudaMalloc(&dpsi, sizeof(double) * (size_t)n * (d.n_qp + 1) * 2);
   if (!e) e = cudaMalloc(&dh, sizeof(double) * 2 * (size_t)n);
-  if (!e && O) e = cudaMalloc(&dO, sizeof(double) * (size_t)n * d.Nv);
+  const size_t orows = (size_t)n * (d.cplx ? 2 : 1);  // complex weights: real and imaginary row per configuration
+  if (!e && O) e = cudaMalloc(&dO, sizeof(double) * orows * d.Nv);
   if (!e) e = cudaMalloc(&dst, sizeof(int) * n);
   if (!e) e = cudaMemcpyAsync(dx, x, sizeof(int) * nx, cudaMemcpyHostToDevice, c->st);
   if (!e) {
@@ -985,7 +995,7 @@ int rbmpp_eval_configs(rbmpp_ctx* c, int n, const int* x, double* psi, double* h
   if (!e) rc = check_walker_status(c, dst, n, "eval_configs");
   if (!e && !rc && psi) e = cudaMemcpy(psi, dpsi, sizeof(double) * (size_t)n * (d.n_qp + 1) * 2, cudaMemcpyDeviceToHost);
   if (!e && !rc && hpsi) e = cudaMemcpy(hpsi, dh, sizeof(double) * 2 * (size_t)n, cudaMemcpyDeviceToHost);
-  if (!e && !rc && O) e = cudaMemcpy(O, dO, sizeof(double) * (size_t)n * d.Nv, cudaMemcpyDeviceToHost);
+  if (!e && !rc && O) e = cudaMemcpy(O, dO, sizeof(double) * orows * d.Nv, cudaMemcpyDeviceToHost);
   cudaFree(dx);
   cudaFree(dx8);
   cudaFree(dpsi);
@@ -1901,7 +1911,9 @@ extern "C" int rbmpp_eval_configs_noalloc(rbmpp_ctx* c, int n, const int* d_x, d
   if (c->dims.device < 0 || c->dims.device >= 64)
     return fail(c, RBMPP_E_ARG, "eval_configs_noalloc: device ordinal %d outside 0..63", c->dims.device);
   if (!c->params_set) return fail(c, RBMPP_E_STATE, "set_params must come first");
-  if (c->d.skew) return fail(c, RBMPP_E_ARG, "eval_configs_noalloc carries the block form only; use eval_configs");
+  if (c->d.skew || c->d.cplx)
+    return fail(c, RBMPP_E_ARG, "eval_configs_noalloc takes real projection weights and the block form only; use "
+                                "eval_configs");
   if (!c->est_fits)
     return fail(c, RBMPP_E_ARG, "the estimator's workspace for N/2 = %d exceeds the shared memory of one block",
                 c->d.Np);

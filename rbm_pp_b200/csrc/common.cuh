@@ -33,6 +33,8 @@ struct DevDims {
   int skip_load;      // verification hook: walker 0 of the streaming sampler never issues its load number
                       //   skip_load (1-based), so the wait on it runs out (0: off)
   int wait_polls;     // poll bound of the streaming sampler's pipeline waits (0: the default 2^22)
+  int cplx;           // complex para_mp_trans: psi, H psi and O_k are complex; O keeps two rows per
+                      //   configuration (real, imaginary parts: the Ovec_Store columns of calc_phys_quantity.f90:227-228)
   int skew;           // the same-spin blocks of Slater_Elm do not vanish (transverse spin projection): the
                       //   Pfaffian matrix is carried in its full N x N skew form (skew.cu), DevWalkers::Y holds
                       //   [w][qp][N][N] and DevParams::SE the Slater elements

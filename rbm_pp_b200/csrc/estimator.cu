@@ -112,11 +112,13 @@ __global__ void __launch_bounds__(kEstThreads, 1)
   const int N = d.N, Np = NP > 0 ? NP : d.Np, ld = Np + 1, NB = 4 * N;
   const int cfgi = blockIdx.x;
   if (cfgi >= n) return;
-  double* Orow = O ? O + (size_t)cfgi * d.Nv : nullptr;
+  // complex projection weights: a real row and an imaginary row per configuration
+  double* Orow = O ? O + (size_t)cfgi * d.Nv * (d.cplx ? 2 : 1) : nullptr;
+  double* OrowI = (Orow && d.cplx) ? Orow + d.Nv : nullptr;
 
   for (int i = tid; i < N; i += blockDim.x) s.x[i] = (int)xs[(size_t)cfgi * N + i];
   if (Orow)
-    for (int k = tid; k < d.Nv; k += blockDim.x) Orow[k] = 0.0;
+    for (int k = tid; k < d.Nv * (d.cplx ? 2 : 1); k += blockDim.x) Orow[k] = 0.0;
   if (tid == 0) s.iflag[F_STATUS] = 0;
   __syncthreads();
   if (tid == 0) {
@@ -178,7 +180,7 @@ __global__ void __launch_bounds__(kEstThreads, 1)
     jc[q] = j < Np ? j : Np - 1;  // in-tile index for every lane
   }
   bool bad = false;
-  double hacc = 0.0;  // this lane's share of sum_b 2 J sgn psi(x'_b)
+  double hacc = 0.0, hacci = 0.0;  // this lane's share of sum_b 2 J sgn psi(x'_b) (real, imaginary part)
   // rounds of nqw projections: warp w < nqw handles qp = round*nqw + w
   for (int q0 = 0; q0 < d.n_qp; q0 += e.nqw) {
     const int qp = q0 + warp;
@@ -322,12 +324,38 @@ __global__ void __launch_bounds__(kEstThreads, 1)
           const int sg = -s.sgn[mp] * (t.subB[i1] ? -1 : 1) * (t.subB[i2] ? -1 : 1);
           const cplx cbw = psi_wo_pf(d, t, ch, sg, qp);
           hacc = hacc + e.apc[b] * (cbw.re * (Rw[b] * pfq));
+          hacci = hacci + e.apc[b] * (cbw.im * (Rw[b] * pfq));
         }
       }
       __syncwarp();
     }
     __syncthreads();
-    // d Pf / d f_k scatter of this round's projections, in projection order (slater.f90:140-167)
+    // d Pf / d f_k scatter of this round's projections, in projection order (slater.f90:140-167); with complex
+    // weights the imaginary row takes the same scatter with the imaginary part of psi_x_wo_pf
+    if (OrowI) {
+      for (int w = 0; w < e.nqw && q0 + w < d.n_qp; w++) {
+        const int qp = q0 + w, mp = qp >> 1, sp = qp & 1;
+        const double* Tw = e.tiles + (size_t)w * Np * ld;
+        const int* srcw = e.perm + (size_t)w * Np;
+        const int* wm = t.wmap + (size_t)mp * N;
+        const double pfq = e.pfw[qp];
+        const cplx cw = psi_wo_pf(d, t, s.rbm[qp], s.sgn[mp], qp);
+        const double cc = pfq * d.sp_cc[sp] * cw.im, ss = pfq * d.sp_ss[sp] * cw.im;
+        for (int pr = tid; pr < Np * Np; pr += blockDim.x) {
+          const int j = pr / Np, i = pr - j * Np;
+          const double y = Tw[j * ld + srcw[i]];
+          const int tu = wm[s.idx[i]], td = wm[s.idx[Np + j]];
+          if (d.orb_injective) {
+            if (cc != 0.0) OrowI[off_pp + t.orb[(size_t)tu * N + td]] += y * cc;
+            if (ss != 0.0) OrowI[off_pp + t.orb[(size_t)td * N + tu]] += y * ss;
+          } else {
+            if (cc != 0.0) atomicAdd(OrowI + off_pp + t.orb[(size_t)tu * N + td], y * cc);
+            if (ss != 0.0) atomicAdd(OrowI + off_pp + t.orb[(size_t)td * N + tu], y * ss);
+          }
+        }
+        __syncthreads();
+      }
+    }
     if (Orow) {
       for (int w = 0; w < e.nqw && q0 + w < d.n_qp; w++) {
         const int qp = q0 + w, mp = qp >> 1, sp = qp & 1;
@@ -382,7 +410,11 @@ __global__ void __launch_bounds__(kEstThreads, 1)
   }
   if (lane == 0 && bad) s.iflag[F_STATUS] = ST_SINGULAR;
   hacc = warp_sum(hacc);
-  if (lane == 0) s.red[warp] = hacc;
+  hacci = warp_sum(hacci);
+  if (lane == 0) {
+    s.red[warp] = hacc;
+    s.red[32 + warp] = hacci;
+  }
   __syncthreads();
   if (s.iflag[F_STATUS]) {
     if (tid == 0 && out_status) out_status[cfgi] = s.iflag[F_STATUS];
@@ -398,7 +430,10 @@ __global__ void __launch_bounds__(kEstThreads, 1)
     s.dsc[D_PSI0R] = re;
     s.dsc[D_PSI0I] = im;
     double hr = e.diag[0] * re, hi = e.diag[0] * im;
-    for (int w = 0; w < kEstWarps; w++) hr += s.red[w];
+    for (int w = 0; w < kEstWarps; w++) {
+      hr += s.red[w];
+      hi += s.red[32 + w];
+    }
     s.dsc[D_PSIPR] = hr;
     s.dsc[D_PSIPI] = hi;
     if (out_nap) out_nap[cfgi] = nap;
@@ -407,24 +442,36 @@ __global__ void __launch_bounds__(kEstThreads, 1)
   __syncthreads();
   const double w = reweight ? 1.0 / (hypot(s.dsc[D_PSI0R], s.dsc[D_PSI0I]) + d.shift) : 1.0;
   if (Orow) {
-    // RBM part, real branch (calc_phys_quantity.f90:165-201); psi_qp real for real para_mp_trans
+    // RBM part, real branch (calc_phys_quantity.f90:165-201): tanh(theta) psi_qp, whose imaginary part comes from
+    // complex para_mp_trans
     for (int k = tid; k < d.alphar * (N + 1); k += blockDim.x) {
-      double acc = 0.0;
+      double acc = 0.0, acci = 0.0;
       if (k < d.alphar) {
         const int f = k;
-        for (int qp = 0; qp < d.n_qp; qp++) acc = acc + tanh(s.th[qp * d.alphar + f]) * s.psi[2 * qp];
+        for (int qp = 0; qp < d.n_qp; qp++) {
+          const double th = tanh(s.th[qp * d.alphar + f]);
+          acc = acc + th * s.psi[2 * qp];
+          acci = acci + th * s.psi[2 * qp + 1];
+        }
       } else {
         const int f = (k - d.alphar) / N, iw = (k - d.alphar) - f * N;
         for (int mp = 0; mp < d.n_mp; mp++) {
           const double xi = (double)s.x[t.winv[(size_t)mp * N + iw]];
           const int q0 = 2 * mp, q1 = 2 * mp + 1;
-          acc = acc + tanh(s.th[q0 * d.alphar + f]) * s.psi[2 * q0] * xi;
-          acc = acc - tanh(s.th[q1 * d.alphar + f]) * s.psi[2 * q1] * xi;
+          const double t0 = tanh(s.th[q0 * d.alphar + f]), t1 = tanh(s.th[q1 * d.alphar + f]);
+          acc = acc + t0 * s.psi[2 * q0] * xi;
+          acc = acc - t1 * s.psi[2 * q1] * xi;
+          acci = acci + t0 * s.psi[2 * q0 + 1] * xi;
+          acci = acci - t1 * s.psi[2 * q1 + 1] * xi;
         }
       }
       Orow[k] = acc * w;
+      if (OrowI) OrowI[k] = acci * w;
     }
-    for (int k = off_pp + tid; k < d.Nv; k += blockDim.x) Orow[k] = Orow[k] * w;
+    for (int k = off_pp + tid; k < d.Nv; k += blockDim.x) {
+      Orow[k] = Orow[k] * w;
+      if (OrowI) OrowI[k] = OrowI[k] * w;
+    }
   }
   if (tid == 0) {
     if (out_psi) {

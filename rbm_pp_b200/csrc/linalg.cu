@@ -224,8 +224,11 @@ __global__ void rowcol_absmax_kernel(int n, const double* S, const int* list, in
 
 // per-sample scalars of calc_phys_quantity.f90:102-109 and coefficient vectors of the gvec/Ovec GEMV:
 // a_s = 2 Re(Eloc_s) (gvec, :229), b_s = w_s Re(psi_s) (Ovec, :230), with real O rows.
+// Per-sample sums of calc_phys_quantity.f90:102-109 and the coefficients of gvec and Ovec per row of O:
+// gvec += 2 Re(conj(E) O), Ovec += w Re(conj(psi) O).  With complex rows (cplx) sample s owns rows 2s (real part)
+// and 2s + 1 (imaginary part) of O, so the coefficients are (2 Re E, 2 Im E) and (w Re psi, w Im psi).
 __global__ void sample_scalars_kernel(int ns, const double* psi, int psi_stride, const double* eloc, double shift,
-                                      double* a, double* b, double* acc4) {
+                                      double* a, double* b, double* acc4, int cplx) {
   __shared__ double r[4][256];
   double e1 = 0, e2 = 0, nn = 0, wf = 0;
   for (int s = threadIdx.x; s < ns; s += blockDim.x) {
@@ -237,8 +240,15 @@ __global__ void sample_scalars_kernel(int ns, const double* psi, int psi_stride,
     e2 += er * er + ei * ei;
     nn += (ap * w) * (ap * w);
     wf += ap;
-    a[s] = 2.0 * er;
-    b[s] = w * pr;
+    if (cplx) {
+      a[2 * s] = 2.0 * er;
+      a[2 * s + 1] = 2.0 * ei;
+      b[2 * s] = w * pr;
+      b[2 * s + 1] = w * pi;
+    } else {
+      a[s] = 2.0 * er;
+      b[s] = w * pr;
+    }
   }
   r[0][threadIdx.x] = e1;
   r[1][threadIdx.x] = e2;
@@ -371,8 +381,8 @@ cudaError_t rbmpp_rowcol_absmax(int n, const double* S, const int* list, int nli
 }
 
 cudaError_t rbmpp_sample_scalars(int ns, const double* psi, int psi_stride, const double* eloc, double shift,
-                                 double* a, double* b, double* acc4, cudaStream_t st) {
+                                 double* a, double* b, double* acc4, int cplx, cudaStream_t st) {
   rbmpp_note_launch();
-  sample_scalars_kernel<<<1, 256, 0, st>>>(ns, psi, psi_stride, eloc, shift, a, b, acc4);
+  sample_scalars_kernel<<<1, 256, 0, st>>>(ns, psi, psi_stride, eloc, shift, a, b, acc4, cplx);
   return cudaGetLastError();
 }
