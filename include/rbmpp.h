@@ -115,11 +115,16 @@ int rbmpp_set_tables(rbmpp_ctx* ctx, const int* W_map, const double* para_mp_tra
                      const int* Orbital_Sgn, const int* subB, const double* sp_weights);
 
 /* Parameters: Wrirr(N, alphar), brirr(alphar), Slater(N_Slater), shift (module.f90 mod_RBM, mod_PP,
- * mod_main).  Wc/bc must be NULL (alphac = 0).  Also rebuilds Slater_Elm on the device
- * (update_slater_elements, slater.f90:7-64). */
+ * mod_main); Wcirr(N, alphac), bcirr(alphac) complex as (re, im) pairs or NULL (kept).  Also rebuilds
+ * Slater_Elm on the device (update_slater_elements, slater.f90:7-64). */
 int rbmpp_set_params(rbmpp_ctx* ctx, const double* Wr, const double* br, const double* Wc, const double* bc,
                      const double* Slater, double shift);
 int rbmpp_get_params(rbmpp_ctx* ctx, double* Wr, double* br, double* Slater, double* shift);
+/* Complex RBM parameters Wcirr(N, alphac), bcirr(alphac) (complex, as (re, im) pairs) after SR steps; set them with
+ * rbmpp_set_params' Wc and bc.  Complex units (RBM.f90 thetac; sub.f90:37-41 multiplies psi_x_wo_pf by
+ * 0.5^alphac prod cosh(thetac)) make psi complex: O then has two rows per sample as with complex para_mp_trans, and
+ * the parameters are ordered as main.f90:136 and SR_pdposv.f90:385-413 order them (complex pairs first). */
+int rbmpp_get_params_c(rbmpp_ctx* ctx, double* Wc, double* bc);
 /* Sets mod_main's shift alone (main.f90:451), keeping the other parameters. */
 int rbmpp_set_shift(rbmpp_ctx* ctx, double shift);
 /* Precision of S builds that happen before rbmpp_sr_step names one: rbmpp_measure with Smat != NULL and

@@ -53,6 +53,8 @@ def lib():
         L.orc_set_tables.argtypes = [P, ip, dp, ip, P]
         L.orc_set_params.argtypes = [P, dp, dp, dp, C.c_double]
         L.orc_set_sp_weights.argtypes = [P, dp]
+        L.orc_set_params_c.argtypes = [P, dp, dp]
+        L.orc_get_params_c.argtypes = [P, dp, dp]
         L.orc_get_params.argtypes = [P, dp, dp, dp, P]
         L.orc_get_slater_elements.argtypes = [P, dp]
         L.orc_seed.argtypes = [P, C.c_int]
@@ -109,8 +111,9 @@ class Oracle:
         self.nsample = nsample_per_rank
         self.nthreads = nthreads
         L = lib()
-        self.h = L.orc_create(inp.L, self.n_mp, 0, inp.alphar, problem.n_slater, nsample_per_rank, nranks,
-                              inp.spin_parity, inp.J1, inp.J2)
+        self.alphac = getattr(inp, "alphac", 0)
+        self.h = L.orc_create(inp.L, self.n_mp, self.alphac, inp.alphar, problem.n_slater, nsample_per_rank,
+                              nranks, inp.spin_parity, inp.J1, inp.J2)
         if not self.h:
             raise OracleError("orc_create failed")
         self.Nv = L.orc_nv(self.h)
@@ -134,6 +137,19 @@ class Oracle:
     def set_params(self, br, Wr, slater, shift=0.0):
         self._chk(lib().orc_set_params(self.h, fortran_array(Wr, np.float64), np.ascontiguousarray(br, np.float64),
                                        np.ascontiguousarray(slater, np.float64), float(shift)))
+
+    def set_params_c(self, bc, Wc):
+        """Complex units: bc (alphac), Wc (N, alphac) complex."""
+        Wcp = fortran_array(np.asarray(Wc, np.complex128), np.complex128).view(np.float64)
+        bcp = np.ascontiguousarray(bc, np.complex128).view(np.float64)
+        self._chk(lib().orc_set_params_c(self.h, np.ascontiguousarray(Wcp), np.ascontiguousarray(bcp)))
+
+    def get_params_c(self):
+        ac = self.alphac
+        Wc = np.zeros(2 * self.N * ac)
+        bc = np.zeros(2 * ac)
+        lib().orc_get_params_c(self.h, Wc, bc)
+        return bc.view(np.complex128), Wc.view(np.complex128).reshape((self.N, ac), order="F")
 
     def get_params(self):
         inp = self.p.inp
@@ -313,10 +329,26 @@ class VMCLoop:
         # (when present) then overrides.
         if offset != 0 and problem.Wr is None:
             raise OracleError("a shard without global rank 0 needs W.input (rank 0's random init is broadcast)")
-        u = orc.rank_grnd(0, inp.alphar * (self.o.N + 1)) if offset == 0 else np.zeros(inp.alphar * (self.o.N + 1))
+        ac = orc.alphac
+        nd = 2 * ac * (self.o.N + 1) + inp.alphar * (self.o.N + 1)
+        u = orc.rank_grnd(0, nd) if offset == 0 else np.zeros(nd)
+        k = 0
+        bc = np.zeros(ac, np.complex128)
+        Wc = np.zeros((self.o.N, ac), np.complex128)
+        for f in range(ac):  # complex units first (parameter.f90:22-31)
+            bc[f] = 0.1 * (u[k] - 0.5) + 0.1j * (u[k + 1] - 0.5)
+            k += 2
+            if inp.spin_parity == -1:
+                bc[f] *= 10.0
+            for iw in range(self.o.N):
+                Wc[iw, f] = 0.1 * (u[k] - 0.5) + 0.1j * (u[k + 1] - 0.5)
+                k += 2
+        if getattr(problem, "Wc", None) is not None:
+            bc, Wc = problem.bc, problem.Wc
+        if ac:
+            orc.set_params_c(bc, Wc)
         br = np.zeros(inp.alphar)
         Wr = np.zeros((self.o.N, inp.alphar))
-        k = 0
         for f in range(inp.alphar):
             br[f] = 0.1 * (u[k] - 0.5)
             k += 1

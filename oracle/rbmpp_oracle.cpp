@@ -127,7 +127,7 @@ struct Rank {
 };
 
 struct Ctx {
-  int L, N, Npair, n_mp, alphac, alphar, n_slater, n_qp, Mr, Nv, Nv_rbm, nsample, nranks, nupdate;
+  int L, N, Npair, n_mp, alphac, alphar, n_slater, n_qp, Mr, Mc, Nv, Nv_rbm, nsample, nranks, nupdate;
   int spin_parity;
   double J1, J2;
   std::vector<int> W_map;  // W_map(N, n_mp), 0-based values          module.f90:34
@@ -136,6 +136,7 @@ struct Ctx {
   std::vector<char> subB;
   double sp_cos[2], sp_sin[2], sp_cc[2], sp_cs[2], sp_ss[2], para_sp[2];
   std::vector<double> Wr, br, slater;  // Wrirr(N,alphar), brirr(alphar), Slater(N_Slater)
+  std::vector<cplx> Wc, bc;            // Wcirr(N,alphac), bcirr(alphac)
   double shift;
   std::vector<double> SE;  // Slater_Elm(2N, 2N, N_QP)                module.f90:55
   std::vector<Rank> ranks;
@@ -212,11 +213,29 @@ static int update_slater_elements(Ctx& c) {
 }
 
 // ------------------------------------------------------------------------------------------------
-// RBM theta: calc_theta RBM.f90:31-91 (real branch), update_theta RBM.f90:95-148.
-// theta index j = mp*2*alphar + (s==+1 ? 0 : alphar) + f
+// RBM theta: calc_theta RBM.f90:31-91, update_theta RBM.f90:95-148.
+// th holds thetar (Mr reals, index j = mp*2*alphar + (s==+1 ? 0 : alphar) + f) followed by thetac
+// (Mc complex as (re, im) pairs, the same index pattern with alphac).
 // ------------------------------------------------------------------------------------------------
+static int n_theta(const Ctx& c) { return c.Mr + 2 * c.Mc; }
+static cplx thc(const Ctx& c, const double* th, int j) { return cplx(th[c.Mr + 2 * j], th[c.Mr + 2 * j + 1]); }
+
 static void calc_theta(const Ctx& c, const int* x, double* th) {
   const int N = c.N;
+  for (int mp = 0; mp < c.n_mp; mp++) {
+    int j = mp * 2 * c.alphac;
+    for (int s = 1; s >= -1; s -= 2)
+      for (int f = 0; f < c.alphac; f++) {
+        cplx t = c.bc[f];
+        for (int i = 0; i < N; i++) {
+          int iw = c.W_map[i + N * mp];
+          t = t + c.Wc[iw + N * f] * (double)x[i] * (double)s;
+        }
+        th[c.Mr + 2 * j] = t.real();
+        th[c.Mr + 2 * j + 1] = t.imag();
+        j++;
+      }
+  }
   for (int mp = 0; mp < c.n_mp; mp++) {
     int j = mp * 2 * c.alphar;
     for (int s = 1; s >= -1; s -= 2)
@@ -233,6 +252,19 @@ static void calc_theta(const Ctx& c, const int* x, double* th) {
 
 static void update_theta(const Ctx& c, const int* x, int i1, int i2, double* th) {
   const int N = c.N;
+  for (int mp = 0; mp < c.n_mp; mp++) {
+    int j = mp * 2 * c.alphac;
+    int iw1 = c.W_map[i1 + N * mp], iw2 = c.W_map[i2 + N * mp];
+    for (int s = 1; s >= -1; s -= 2)
+      for (int f = 0; f < c.alphac; f++) {
+        cplx t = thc(c, th, j);
+        t = t - 2.0 * c.Wc[iw1 + N * f] * (double)x[i1] * (double)s;
+        t = t - 2.0 * c.Wc[iw2 + N * f] * (double)x[i2] * (double)s;
+        th[c.Mr + 2 * j] = t.real();
+        th[c.Mr + 2 * j + 1] = t.imag();
+        j++;
+      }
+  }
   for (int mp = 0; mp < c.n_mp; mp++) {
     int j = mp * 2 * c.alphar;
     int iw1 = c.W_map[i1 + N * mp], iw2 = c.W_map[i2 + N * mp];
@@ -303,7 +335,7 @@ static int sign_pp(const Ctx& c, const int* idx, int* sgn) {
 }
 
 // ------------------------------------------------------------------------------------------------
-// Amplitude: calc_amplitude_RBM_PP sub.f90:4-89 (Ncopy = 1, alphac = 0 branch). qp = 2*mp + sp.
+// Amplitude: calc_amplitude_RBM_PP sub.f90:4-89 (Ncopy = 1). qp = 2*mp + sp.
 // Consumes exactly one grnd() per call (sub.f90:72); the self-check it guards only prints.
 // psi has n_qp+1 entries: psi[0] = total, psi[1+qp] = per projection.
 // ------------------------------------------------------------------------------------------------
@@ -311,7 +343,11 @@ static void amplitude(const Ctx& c, const double* th, const double* pf, const in
                       cplx* psi, MT& rng) {
   for (int qp = 0; qp < c.n_qp; qp++) {
     int mp = qp / 2, sp = qp % 2;
-    cplx c1 = 1.0;  // 0.5d0**alphac with alphac = 0
+    cplx c1 = std::pow(0.5, c.alphac);  // sub.f90:37-41
+    for (int f = 0; f < c.alphac; f++) {
+      const cplx t = thc(c, th, qp * c.alphac + f);
+      c1 = c1 * cplx(std::cosh(t.real()) * std::cos(t.imag()), std::sinh(t.real()) * std::sin(t.imag()));
+    }
     double r1 = 1.0;
     for (int f = 0; f < c.alphar; f++) r1 = r1 * std::cosh(th[qp * c.alphar + f]);
     c1 = c1 * r1;
@@ -551,7 +587,7 @@ struct WState {
     idx.assign(c.N, 0);
     cfg.assign(c.N, 0);
     sgn.assign(c.n_mp, 1);
-    th.assign(c.Mr, 0.0);
+    th.assign(n_theta(c), 0.0);
     pf.assign(c.n_qp, 0.0);
     inv.assign((size_t)c.N * c.N * c.n_qp, 0.0);
     psi.assign(c.n_qp + 1, 0.0);
@@ -653,6 +689,8 @@ static int make_sample_rank(const Ctx& c, Rank& R, bool first) {
       calc_theta(c, w.x.data(), w.th.data());
       if (check_ele(c, w.x.data(), w.idx.data(), w.cfg.data())) return ORC_E_CONFIG;
       if (sign_pp(c, w.idx.data(), w.sgn.data())) return ORC_E_SIGN;
+      for (int j = 0; j < c.Mc; j++)  // make_sample.f90:84-86
+        if (std::abs(thc(c, w.th.data(), j) - thc(c, th_old.data(), j)) > 1.0e-5) return ORC_E_THETA;
       for (int j = 0; j < c.Mr; j++)
         if (std::fabs(w.th[j] - th_old[j]) > 1.0e-5) return ORC_E_THETA;
       for (int mp = 0; mp < c.n_mp; mp++)
@@ -788,7 +826,7 @@ static int bond_map(const Ctx& c, int i0, int i1) {  // i0 in 1..4, i1 0-based -
 static cplx local_energy(const Ctx& c, const int* x, cplx psi0, const double* th, const int* idx, const int* cfg,
                          const int* sgn, const double* pf, const double* inv, MT& rng) {
   const int N = c.N;
-  std::vector<double> thp(c.Mr), tpf(c.n_qp), va(N), vb(N);
+  std::vector<double> thp(n_theta(c)), tpf(c.n_qp), va(N), vb(N);
   std::vector<int> tidx(N), tsgn(c.n_mp);
   std::vector<cplx> psip(c.n_qp + 1), psipw(c.n_qp);
   cplx E = 0.0;
@@ -798,7 +836,7 @@ static cplx local_energy(const Ctx& c, const int* x, cplx psi0, const double* th
       int i2 = bond_map(c, i0, i1);
       E = E + J * (double)x[i1] * (double)x[i2] * psi0;
       if (x[i1] != x[i2]) {
-        for (int j = 0; j < c.Mr; j++) thp[j] = th[j];
+        for (int j = 0; j < n_theta(c); j++) thp[j] = th[j];
         update_theta(c, x, i1, i2, thp.data());
         int i3 = cfg[i1], i4 = cfg[i2];
         for (int i = 0; i < N; i++) tidx[i] = idx[i];
@@ -860,7 +898,7 @@ static void deriv_pfaffian(const Ctx& c, const int* idx, const double* pf, const
 static int eval_config(const Ctx& c, const int* x, MT& rng, cplx* psi_out, cplx* hpsi, cplx* Oraw,
                        std::vector<double>* pf_out = nullptr) {
   const int N = c.N;
-  std::vector<double> th(c.Mr), pf(c.n_qp), inv((size_t)N * N * c.n_qp), deriv((size_t)c.n_slater * c.n_qp);
+  std::vector<double> th(n_theta(c)), pf(c.n_qp), inv((size_t)N * N * c.n_qp), deriv((size_t)c.n_slater * c.n_qp);
   std::vector<int> idx(N), cfg(N), sgn(c.n_mp);
   std::vector<cplx> psi(c.n_qp + 1), psiw(c.n_qp);
   calc_theta(c, x, th.data());
@@ -875,9 +913,40 @@ static int eval_config(const Ctx& c, const int* x, MT& rng, cplx* psi_out, cplx*
   if (hpsi) *hpsi = local_energy(c, x, psi[0], th.data(), idx.data(), cfg.data(), sgn.data(), pf.data(), inv.data(), rng);
   if (Oraw) {
     for (int k = 0; k < c.Nv; k++) Oraw[k] = 0.0;
-    // real RBM branch, calc_phys_quantity.f90:165-201 (alphac = 0 so offsets start at 0)
+    // complex RBM branch, calc_phys_quantity.f90:115-160: (re, im) parameter pairs, the imaginary partner
+    // derivative being i times the real one; tanh(t) of a complex t as (tanh a + i tan b) / (1 + i tanh a tan b)
+    auto ctanh = [](cplx t) {
+      return cplx(std::tanh(t.real()), std::tan(t.imag())) / cplx(1.0, std::tanh(t.real()) * std::tan(t.imag()));
+    };
+    const cplx ci(0.0, 1.0);
+    for (int f = 0; f < c.alphac; f++) {
+      int k1 = 2 * f, itmp = 0;
+      for (int mp = 0; mp < c.n_mp; mp++)
+        for (int s = 1; s >= -1; s -= 2) {
+          int j = itmp * c.alphac + f;
+          itmp++;
+          Oraw[k1] = Oraw[k1] + ctanh(thc(c, th.data(), j)) * psi[itmp];
+        }
+      Oraw[k1 + 1] = Oraw[k1] * ci;
+    }
+    for (int f = 0; f < c.alphac; f++) {
+      int off = 2 * c.alphac + f * N * 2, itmp = 0;
+      for (int mp = 0; mp < c.n_mp; mp++)
+        for (int s = 1; s >= -1; s -= 2) {
+          int j = itmp * c.alphac + f;
+          itmp++;
+          cplx c1 = ctanh(thc(c, th.data(), j)) * psi[itmp];
+          for (int i = 0; i < N; i++) {
+            int k1 = off + 2 * c.W_map[i + N * mp];
+            Oraw[k1] = Oraw[k1] + c1 * (double)x[i] * (double)s;
+            if (mp == c.n_mp - 1) Oraw[k1 + 1] = Oraw[k1] * ci;
+          }
+        }
+    }
+    // real RBM branch, calc_phys_quantity.f90:165-201
+    const int offr = 2 * c.alphac * (N + 1);
     for (int f = 0; f < c.alphar; f++) {
-      int k1 = f, itmp = 0;
+      int k1 = offr + f, itmp = 0;
       for (int mp = 0; mp < c.n_mp; mp++)
         for (int s = 1; s >= -1; s -= 2) {
           int j = itmp * c.alphar + f;
@@ -886,7 +955,7 @@ static int eval_config(const Ctx& c, const int* x, MT& rng, cplx* psi_out, cplx*
         }
     }
     for (int f = 0; f < c.alphar; f++) {
-      int off = c.alphar + f * N, itmp = 0;
+      int off = offr + c.alphar + f * N, itmp = 0;
       for (int mp = 0; mp < c.n_mp; mp++)
         for (int s = 1; s >= -1; s -= 2) {
           int j = itmp * c.alphar + f;
@@ -899,7 +968,7 @@ static int eval_config(const Ctx& c, const int* x, MT& rng, cplx* psi_out, cplx*
         }
     }
     deriv_pfaffian(c, idx.data(), pf.data(), inv.data(), deriv.data());
-    int off = c.alphar * (N + 1);
+    int off = offr + c.alphar * (N + 1);
     for (int o = 0; o < c.n_slater; o++) {
       cplx acc = Oraw[off + o];
       for (int qp = 0; qp < c.n_qp; qp++) acc = acc + deriv[o + (size_t)c.n_slater * qp] * psiw[qp];
@@ -957,7 +1026,7 @@ struct orc_sr_out {
 
 void* orc_create(int L, int n_mp, int alphac, int alphar, int n_slater, int nsample_per_rank, int nranks,
                  int spin_parity, double J1, double J2) {
-  if (L < 2 || n_mp < 1 || alphac != 0 || alphar < 0 || n_slater < 1 || nsample_per_rank < 1 || nranks < 1)
+  if (L < 2 || n_mp < 1 || alphac < 0 || alphar < 0 || n_slater < 1 || nsample_per_rank < 1 || nranks < 1)
     return nullptr;
   Ctx* c = new Ctx();
   c->L = L;
@@ -973,6 +1042,7 @@ void* orc_create(int L, int n_mp, int alphac, int alphar, int n_slater, int nsam
   c->n_slater = n_slater;
   c->n_qp = 2 * n_mp;
   c->Mr = alphar * n_mp * 2;                                   // main.f90:135
+  c->Mc = alphac * n_mp * 2;                                   // main.f90:134
   c->Nv = alphac * 2 * (c->N + 1) + alphar * (c->N + 1) + n_slater;  // main.f90:136
   c->Nv_rbm = c->Nv - n_slater;
   c->nsample = nsample_per_rank;
@@ -998,6 +1068,8 @@ void* orc_create(int L, int n_mp, int alphac, int alphar, int n_slater, int nsam
   }
   c->Wr.assign((size_t)c->N * alphar, 0.0);
   c->br.assign(alphar, 0.0);
+  c->Wc.assign((size_t)c->N * alphac, 0.0);
+  c->bc.assign(alphac, 0.0);
   c->slater.assign(n_slater, 0.0);
   return c;
 }
@@ -1052,6 +1124,27 @@ int orc_set_sp_weights(void* h, const double* w) {
     c.sp_ss[s] = c.sp_sin[s] * c.sp_sin[s];
   }
   if (!c.slater.empty() && !c.W_map.empty()) return update_slater_elements(c);
+  return 0;
+}
+
+// Complex RBM parameters Wcirr(N, alphac), bcirr(alphac) as (re, im) pairs (module.f90 mod_RBM).
+int orc_set_params_c(void* h, const double* Wc, const double* bc) {
+  Ctx& c = *(Ctx*)h;
+  for (size_t k = 0; k < c.Wc.size(); k++) c.Wc[k] = cplx(Wc[2 * k], Wc[2 * k + 1]);
+  for (size_t k = 0; k < c.bc.size(); k++) c.bc[k] = cplx(bc[2 * k], bc[2 * k + 1]);
+  return 0;
+}
+
+int orc_get_params_c(void* h, double* Wc, double* bc) {
+  Ctx& c = *(Ctx*)h;
+  for (size_t k = 0; k < c.Wc.size(); k++) {
+    Wc[2 * k] = c.Wc[k].real();
+    Wc[2 * k + 1] = c.Wc[k].imag();
+  }
+  for (size_t k = 0; k < c.bc.size(); k++) {
+    bc[2 * k] = c.bc[k].real();
+    bc[2 * k + 1] = c.bc[k].imag();
+  }
   return 0;
 }
 
@@ -1307,7 +1400,7 @@ struct ExchangeBuf {
   std::vector<int> tidx, tsgn;
   std::vector<cplx> psip, psipw;
   explicit ExchangeBuf(const Ctx& c)
-      : thp(c.Mr), tpf(c.n_qp), va(c.N), vb(c.N), tidx(c.N), tsgn(c.n_mp), psip(c.n_qp + 1), psipw(c.n_qp) {}
+      : thp(n_theta(c)), tpf(c.n_qp), va(c.N), vb(c.N), tidx(c.N), tsgn(c.n_mp), psip(c.n_qp + 1), psipw(c.n_qp) {}
 };
 
 // psi(x') for the exchange of the antiparallel spins on sites i1, i2 (0-based), as in
@@ -1315,7 +1408,7 @@ struct ExchangeBuf {
 static cplx exchange_psi(const Ctx& c, const int* x, const double* th, const int* idx, const int* cfg,
                          const int* sgn, const double* pf, const double* inv, MT& rng, int i1, int i2, ExchangeBuf& b) {
   const int N = c.N;
-  for (int j = 0; j < c.Mr; j++) b.thp[j] = th[j];
+  for (int j = 0; j < n_theta(c); j++) b.thp[j] = th[j];
   update_theta(c, x, i1, i2, b.thp.data());
   const int i3 = cfg[i1], i4 = cfg[i2];
   for (int i = 0; i < N; i++) b.tidx[i] = idx[i];
@@ -1337,7 +1430,7 @@ static cplx exchange_psi(const Ctx& c, const int* x, const double* th, const int
 // Chi_loc_x(2, Nchi).
 static int corr_sample(const Ctx& c, const int* x, MT& rng, cplx& psi0, cplx& eloc, cplx* sdots, cplx* chi) {
   const int N = c.N;
-  std::vector<double> th(c.Mr), pf(c.n_qp), inv((size_t)N * N * c.n_qp);
+  std::vector<double> th(n_theta(c)), pf(c.n_qp), inv((size_t)N * N * c.n_qp);
   std::vector<int> idx(N), cfg(N), sgn(c.n_mp);
   std::vector<cplx> psi(c.n_qp + 1), psiw(c.n_qp);
   ExchangeBuf b(c);
@@ -1589,9 +1682,19 @@ int orc_sr_step(void* h, const orc_sr_in* in, const double* mat_tmp, double norm
     }
     if (std::fabs(x[k]) > 1e-12) knz++;
   }
-  // gamma_save(:,Nsave) = current parameters (main.f90:263-294 ordering: b, W(iw,f), f_ij)
+  // gamma_save(:,Nsave) = current parameters (main.f90:263-294 ordering: complex b and W(iw,f) as (re, im)
+  // pairs, then real b, W(iw,f), then f_ij)
   std::vector<double> gam(Nv);
   int k1 = 0;
+  for (int f = 0; f < c.alphac; f++) {
+    gam[k1++] = c.bc[f].real();
+    gam[k1++] = c.bc[f].imag();
+  }
+  for (int f = 0; f < c.alphac; f++)
+    for (int iw = 0; iw < N; iw++) {
+      gam[k1++] = c.Wc[iw + (size_t)N * f].real();
+      gam[k1++] = c.Wc[iw + (size_t)N * f].imag();
+    }
   for (int f = 0; f < c.alphar; f++) gam[k1++] = c.br[f];
   for (int f = 0; f < c.alphar; f++)
     for (int iw = 0; iw < N; iw++) gam[k1++] = c.Wr[iw + (size_t)N * f];
@@ -1601,12 +1704,15 @@ int orc_sr_step(void* h, const orc_sr_in* in, const double* mat_tmp, double norm
     if (delW > max_change) gam[k] = gam[k] - in->delta_tau * x[k] * (max_change / delW);
     else gam[k] = gam[k] - in->delta_tau * x[k];
   }
-  int off = c.alphar * (N + 1);  // :356-366
+  int off = 2 * c.alphac * (N + 1) + c.alphar * (N + 1);  // :356-366
   double r1 = 0.0;
   for (int k = off; k < Nv; k++) r1 = r1 + std::fabs(gam[k]);
   r1 = r1 / (double)c.n_slater;
   for (int k = off; k < Nv; k++) gam[k] = gam[k] * 0.25 / r1;
   k1 = 0;  // :385-413 (parameter averaging is a no-op for Nsave = 1)
+  for (int f = 0; f < c.alphac; f++, k1 += 2) c.bc[f] = cplx(gam[k1], gam[k1 + 1]);
+  for (int f = 0; f < c.alphac; f++)
+    for (int iw = 0; iw < N; iw++, k1 += 2) c.Wc[iw + (size_t)N * f] = cplx(gam[k1], gam[k1 + 1]);
   for (int f = 0; f < c.alphar; f++) c.br[f] = gam[k1++];
   for (int f = 0; f < c.alphar; f++)
     for (int iw = 0; iw < N; iw++) c.Wr[iw + (size_t)N * f] = gam[k1++];

@@ -24,7 +24,7 @@ EXPORTS = ["rbmpp_create", "rbmpp_destroy", "rbmpp_last_error", "rbmpp_query", "
            "rbmpp_set_s_precision", "rbmpp_batch_create", "rbmpp_batch_destroy", "rbmpp_batch_last_error",
            "rbmpp_batch_tune", "rbmpp_batch_make_sample", "rbmpp_measure_correlation",
            "rbmpp_get_walker_events", "rbmpp_set_trace", "rbmpp_set_replay", "rbmpp_debug_hook",
-           "rbmpp_copy_state", "rbmpp_set_allreduce"]
+           "rbmpp_copy_state", "rbmpp_set_allreduce", "rbmpp_get_params_c"]
 
 SR_FP64 = 0
 SR_SPLIT_BF16 = 1
@@ -93,6 +93,7 @@ def lib():
         L.rbmpp_set_tables.argtypes = [P, P, P, P, P, P, P]
         L.rbmpp_set_params.argtypes = [P, P, P, P, P, P, C.c_double]
         L.rbmpp_get_params.argtypes = [P, P, P, P, P]
+        L.rbmpp_get_params_c.argtypes = [P, P, P]
         L.rbmpp_seed_walkers.argtypes = [P, C.c_int]
         L.rbmpp_rank0_grnd.argtypes = [P, C.c_int, P]
         L.rbmpp_make_sample.argtypes = [P, C.c_int, P, P]
@@ -146,8 +147,9 @@ class Context:
         self.n_qp = 2 * self.n_mp
         self.nw = n_walkers
         self.ns = nsample_per_walker
-        d = Dims(inp.L, self.n_mp, 0, inp.alphar, problem.n_slater, nsample_per_walker, n_walkers, inp.spin_parity,
-                 inp.J1, inp.J2, device, walker_offset)
+        self.alphac = getattr(inp, "alphac", 0)
+        d = Dims(inp.L, self.n_mp, self.alphac, inp.alphar, problem.n_slater, nsample_per_walker, n_walkers,
+                 inp.spin_parity, inp.J1, inp.J2, device, walker_offset)
         h = C.c_void_p()
         rc = lib().rbmpp_create(C.byref(d), C.byref(h))
         self.h = h
@@ -190,11 +192,22 @@ class Context:
         lib().rbmpp_query(self.h, 5, C.byref(v))
         return v.value
 
-    def set_params(self, br, Wr, slater, shift=0.0):
+    def set_params(self, br, Wr, slater, shift=0.0, bc=None, Wc=None):
+        """Real units (br, Wr(N, alphar)), f_ij, shift and, with complex units, bc (alphac) and Wc (N, alphac)
+        complex (None keeps the current ones)."""
         Wr = _f(Wr, np.float64)
         br = np.ascontiguousarray(br, np.float64)
         sl = np.ascontiguousarray(slater, np.float64)
-        self._chk(lib().rbmpp_set_params(self.h, _p(Wr), _p(br), None, None, _p(sl), float(shift)))
+        Wcp = None if Wc is None else _f(np.asarray(Wc, np.complex128), np.complex128).view(np.float64)
+        bcp = None if bc is None else np.ascontiguousarray(bc, np.complex128).view(np.float64)
+        self._chk(lib().rbmpp_set_params(self.h, _p(Wr), _p(br), _p(Wcp), _p(bcp), _p(sl), float(shift)))
+
+    def get_params_c(self):
+        """(bc, Wc(N, alphac)) complex."""
+        Wc = np.zeros(self.N * max(self.alphac, 1), np.complex128)
+        bc = np.zeros(max(self.alphac, 1), np.complex128)
+        self._chk(lib().rbmpp_get_params_c(self.h, _p(Wc.view(np.float64)), _p(bc.view(np.float64))))
+        return bc[:self.alphac], Wc[:self.N * self.alphac].reshape((self.N, self.alphac), order="F")
 
     def get_params(self):
         a = self.p.inp.alphar
@@ -391,6 +404,43 @@ class Batch:
 
     def __del__(self):
         self.close()
+
+
+def initial_params_c(ctx: Context, problem):
+    """initialize_parameters (parameter.f90:21-41) with complex units: rank 0 draws, in this order, for every
+    complex unit f the pair (re, im) of bcirr(f) and then of each Wcirr(iw, f), all U(-0.05, 0.05) (bcirr x10 for
+    spin_parity = -1), then the real units as initial_params does.  Returns (bc, Wc, br, Wr); W.input (the
+    problem's br, Wr and, when present, bc, Wc) overrides the draws."""
+    inp = problem.inp
+    N = inp.L * inp.L
+    ac = getattr(inp, "alphac", 0)
+    u = ctx.rank0_grnd(2 * ac * (N + 1) + inp.alphar * (N + 1))
+    k = 0
+    bc = np.zeros(ac, np.complex128)
+    Wc = np.zeros((N, ac), np.complex128)
+    for f in range(ac):
+        bc[f] = 0.1 * (u[k] - 0.5) + 0.1j * (u[k + 1] - 0.5)
+        k += 2
+        if inp.spin_parity == -1:
+            bc[f] *= 10.0
+        for iw in range(N):
+            Wc[iw, f] = 0.1 * (u[k] - 0.5) + 0.1j * (u[k + 1] - 0.5)
+            k += 2
+    br = np.zeros(inp.alphar)
+    Wr = np.zeros((N, inp.alphar))
+    for f in range(inp.alphar):
+        br[f] = 0.1 * (u[k] - 0.5)
+        k += 1
+        if inp.spin_parity == -1:
+            br[f] *= 10.0
+        for iw in range(N):
+            Wr[iw, f] = 0.1 * (u[k] - 0.5)
+            k += 1
+    if problem.Wr is not None:
+        br, Wr = problem.br, problem.Wr
+    if getattr(problem, "Wc", None) is not None:
+        bc, Wc = problem.bc, problem.Wc
+    return bc, Wc, br, Wr
 
 
 def initial_params(ctx: Context, problem):

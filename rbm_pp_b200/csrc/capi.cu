@@ -136,12 +136,14 @@ struct rbmpp_ctx {
   // host copies of the tables and parameters (Fortran layouts)
   std::vector<int> orb_host;     // Orbital_Idx 0-based [p][q] row-major (p*N+q)
   std::vector<double> Wr, br, slater;
+  std::vector<double> Wc, bc;  // Wcirr(N, alphac), bcirr(alphac) as (re, im) pairs
   double shift = 0.0;
   bool tables_set = false, params_set = false, seeded = false, sampled = false, measured = false;
   // device tables / params
   int *d_wmap = nullptr, *d_winv = nullptr, *d_orb = nullptr, *d_bonds = nullptr;
   unsigned char* d_subB = nullptr;
   double *d_para = nullptr, *d_Wr = nullptr, *d_br = nullptr, *d_slater = nullptr, *d_XF = nullptr, *d_XFT = nullptr;
+  double *d_Wc = nullptr, *d_bc = nullptr;
   DevWalkers W{};
   // measurement
   int ns_tot = 0;
@@ -228,6 +230,8 @@ DevParams params(const rbmpp_ctx* c) {
   DevParams p;
   p.Wr = c->d_Wr;
   p.br = c->d_br;
+  p.Wc = c->d_Wc;
+  p.bc = c->d_bc;
   p.XF = c->d_XF;
   p.XFT = c->d_XFT;
   p.SE = c->d_SE;
@@ -244,6 +248,10 @@ int upload_params(rbmpp_ctx* c) {
     CK(cudaMemcpyAsync(c->d_br, c->br.data(), sizeof(double) * d.alphar, cudaMemcpyHostToDevice, c->st));
   }
   CK(cudaMemcpyAsync(c->d_slater, c->slater.data(), sizeof(double) * d.n_slater, cudaMemcpyHostToDevice, c->st));
+  if (d.alphac > 0) {  // Wcirr(iw, f) pairs in column-major order = the device's [f][N][2]
+    CK(cudaMemcpyAsync(c->d_Wc, c->Wc.data(), sizeof(double) * c->Wc.size(), cudaMemcpyHostToDevice, c->st));
+    CK(cudaMemcpyAsync(c->d_bc, c->bc.data(), sizeof(double) * c->bc.size(), cudaMemcpyHostToDevice, c->st));
+  }
   if (d.skew) {
     CK(rbmpp_build_se(d, c->d_wmap, c->d_orb, c->d_slater, c->d_SE, c->st));
   } else {
@@ -431,11 +439,8 @@ int rbmpp_create(const rbmpp_dims* dims, rbmpp_ctx** out) {
     *out = c;
     return r;
   }
-  if (dims->alphac != 0) {
-    *out = c;
-    return fail(c, RBMPP_E_ARG, "alphac > 0 (complex RBM branch) is not supported");
-  }
-  if (dims->n_mp_trans < 1 || dims->alphar < 0 || dims->n_slater < 1 || dims->nsample < 1 || dims->n_walkers < 1) {
+  if (dims->n_mp_trans < 1 || dims->alphar < 0 || dims->alphac < 0 || dims->n_slater < 1 || dims->nsample < 1 ||
+      dims->n_walkers < 1) {
     *out = c;
     return fail(c, RBMPP_E_ARG, "bad dimensions");
   }
@@ -450,8 +455,11 @@ int rbmpp_create(const rbmpp_dims* dims, rbmpp_ctx** out) {
   d.n_qp = 2 * d.n_mp;
   d.alphar = dims->alphar;
   d.Mr = dims->alphar * d.n_mp * 2;
+  d.alphac = dims->alphac;
+  d.Mc = dims->alphac * d.n_mp * 2;  // main.f90:134
+  d.cplx = d.alphac > 0;             // complex units make psi complex
   d.n_slater = dims->n_slater;
-  d.Nv = dims->alphar * (d.N + 1) + d.n_slater;
+  d.Nv = 2 * dims->alphac * (d.N + 1) + dims->alphar * (d.N + 1) + d.n_slater;  // main.f90:136
   d.Nv_rbm = d.Nv - d.n_slater;
   d.nw = dims->n_walkers;
   d.ns = dims->nsample;
@@ -486,6 +494,7 @@ int rbmpp_create(const rbmpp_dims* dims, rbmpp_ctx** out) {
   c->est_fits = (long long)rbmpp_estimator_smem(d, 256) <= maxsm;
   c->stream_stages = rbmpp_stream_stages(d, maxsm);
   if (getenv("RBMPP_SAMPLER") && std::string(getenv("RBMPP_SAMPLER")) == "direct") c->stream_stages = 0;
+  if (d.alphac) c->stream_stages = 0;  // the streaming sampler carries real units only
   int r;
   const int N = d.N;
   if ((r = dalloc(c, &c->d_wmap, (size_t)d.n_mp * N))) return r;
@@ -496,6 +505,8 @@ int rbmpp_create(const rbmpp_dims* dims, rbmpp_ctx** out) {
   if ((r = dalloc(c, &c->d_para, (size_t)2 * d.n_mp))) return r;
   if ((r = dalloc(c, &c->d_Wr, (size_t)std::max(1, d.alphar) * N))) return r;
   if ((r = dalloc(c, &c->d_br, (size_t)std::max(1, d.alphar)))) return r;
+  if ((r = dalloc(c, &c->d_Wc, (size_t)2 * std::max(1, d.alphac) * N))) return r;
+  if ((r = dalloc(c, &c->d_bc, (size_t)2 * std::max(1, d.alphac)))) return r;
   if ((r = dalloc(c, &c->d_slater, (size_t)d.n_slater))) return r;
   if ((r = dalloc(c, &c->d_XF, (size_t)d.n_qp * N * N))) return r;
   if ((r = dalloc(c, &c->d_XFT, (size_t)d.n_qp * N * N))) return r;
@@ -550,6 +561,8 @@ int rbmpp_create(const rbmpp_dims* dims, rbmpp_ctx** out) {
   CK(cudaMemcpy(c->d_bonds, bonds.data(), sizeof(int) * 8 * N, cudaMemcpyHostToDevice));
   c->Wr.assign((size_t)N * d.alphar, 0.0);
   c->br.assign(d.alphar, 0.0);
+  c->Wc.assign((size_t)2 * N * d.alphac, 0.0);
+  c->bc.assign((size_t)2 * d.alphac, 0.0);
   c->slater.assign(d.n_slater, 0.0);
   return 0;
 }
@@ -557,6 +570,7 @@ int rbmpp_create(const rbmpp_dims* dims, rbmpp_ctx** out) {
 int rbmpp_destroy(rbmpp_ctx* c) {
   if (!c) return 0;
   void* ptrs[] = {c->d_wmap, c->d_winv, c->d_orb, c->d_bonds, c->d_subB, c->d_para, c->d_Wr, c->d_br, c->d_slater,
+                  c->d_Wc, c->d_bc,
                   c->d_XF, c->d_XFT, c->W.x, c->W.idx, c->W.cfg, c->W.th, c->W.sgn, c->W.pf, c->W.psi, c->W.Y,
                   c->W.mt, c->W.nfastup, c->W.naccept, c->W.nacc_all, c->W.status, c->W.xs, c->W.pfs, c->W.psis, c->W.gj, c->W.events, c->W.trace, (void*)c->W.replay, c->d_O, c->d_psiS,
                   c->d_eloc, c->d_a, c->d_b, c->d_tmp_ns, c->d_acc4, c->d_nap, c->d_estat, c->d_gvec, c->d_Ovec,
@@ -660,11 +674,12 @@ int rbmpp_set_tables(rbmpp_ctx* c, const int* W_map, const double* para, const i
       winv[(size_t)mp * N + (v - 1)] = i;
     }
   }
-  int cplx = 0;
+  int cplx = d.alphac > 0;
   for (int mp = 0; mp < d.n_mp; mp++)
     if (para[2 * mp + 1] != 0.0) cplx = 1;
   if (cplx && d.skew)
-    return fail(c, RBMPP_E_ARG, "complex para_mp_trans with the transverse (skew-form) projection is not supported");
+    return fail(c, RBMPP_E_ARG, "complex para_mp_trans or complex RBM units with the transverse (skew-form) projection "
+                                "are not supported");
   if (cplx != d.cplx && c->d_O)
     return fail(c, RBMPP_E_STATE, "complex para_mp_trans changed after measurement buffers were sized");
   d.cplx = cplx;
@@ -694,8 +709,10 @@ int rbmpp_set_tables(rbmpp_ctx* c, const int* W_map, const double* para, const i
 int rbmpp_set_params(rbmpp_ctx* c, const double* Wr, const double* br, const double* Wc, const double* bc,
                      const double* slater, double shift) {
   if (!c) return RBMPP_E_ARG;
-  if (Wc || bc) return fail(c, RBMPP_E_ARG, "complex RBM parameters given but alphac = 0");
+  if ((Wc || bc) && c->d.alphac == 0) return fail(c, RBMPP_E_ARG, "complex RBM parameters given but alphac = 0");
   if (!c->tables_set) return fail(c, RBMPP_E_STATE, "rbmpp_set_tables must come first");
+  if (Wc) std::memcpy(c->Wc.data(), Wc, sizeof(double) * c->Wc.size());
+  if (bc) std::memcpy(c->bc.data(), bc, sizeof(double) * c->bc.size());
   if (Wr) std::memcpy(c->Wr.data(), Wr, sizeof(double) * c->Wr.size());
   if (br) std::memcpy(c->br.data(), br, sizeof(double) * c->br.size());
   if (slater) std::memcpy(c->slater.data(), slater, sizeof(double) * c->slater.size());
@@ -710,6 +727,13 @@ int rbmpp_get_params(rbmpp_ctx* c, double* Wr, double* br, double* slater, doubl
   if (br) std::memcpy(br, c->br.data(), sizeof(double) * c->br.size());
   if (slater) std::memcpy(slater, c->slater.data(), sizeof(double) * c->slater.size());
   if (shift) *shift = c->shift;
+  return 0;
+}
+
+int rbmpp_get_params_c(rbmpp_ctx* c, double* Wc, double* bc) {
+  if (!c) return RBMPP_E_ARG;
+  if (Wc) std::memcpy(Wc, c->Wc.data(), sizeof(double) * c->Wc.size());
+  if (bc) std::memcpy(bc, c->bc.data(), sizeof(double) * c->bc.size());
   return 0;
 }
 
@@ -1288,8 +1312,11 @@ int rbmpp_sr_step(rbmpp_ctx* c, const rbmpp_sr_in* in, rbmpp_sr_out* out, double
     }
     if (std::fabs(x[k]) > 1e-12) knz++;
   }
+  // gamma: complex units as (re, im) pairs (bcirr, then Wcirr(iw, f)), real units, f_ij (SR_pdposv.f90:385-413)
   std::vector<double> gam(Nv);
   int k1 = 0;
+  for (size_t q = 0; q < c->bc.size(); q++) gam[k1++] = c->bc[q];
+  for (size_t q = 0; q < c->Wc.size(); q++) gam[k1++] = c->Wc[q];
   for (int f = 0; f < d.alphar; f++) gam[k1++] = c->br[f];
   for (int f = 0; f < d.alphar; f++)
     for (int iw = 0; iw < N; iw++) gam[k1++] = c->Wr[iw + (size_t)N * f];
@@ -1299,12 +1326,14 @@ int rbmpp_sr_step(rbmpp_ctx* c, const rbmpp_sr_in* in, rbmpp_sr_out* out, double
     if (delW > max_change) gam[k] = gam[k] - in->delta_tau * x[k] * (max_change / delW);
     else gam[k] = gam[k] - in->delta_tau * x[k];
   }
-  const int off = d.alphar * (N + 1);  // :356-366
+  const int off = 2 * d.alphac * (N + 1) + d.alphar * (N + 1);  // :356-366
   double r1 = 0.0;
   for (int k = off; k < Nv; k++) r1 = r1 + std::fabs(gam[k]);
   r1 = r1 / (double)d.n_slater;
   for (int k = off; k < Nv; k++) gam[k] = gam[k] * 0.25 / r1;
   k1 = 0;  // :385-413
+  for (size_t q = 0; q < c->bc.size(); q++) c->bc[q] = gam[k1++];
+  for (size_t q = 0; q < c->Wc.size(); q++) c->Wc[q] = gam[k1++];
   for (int f = 0; f < d.alphar; f++) c->br[f] = gam[k1++];
   for (int f = 0; f < d.alphar; f++)
     for (int iw = 0; iw < N; iw++) c->Wr[iw + (size_t)N * f] = gam[k1++];
@@ -1490,7 +1519,7 @@ int rbmpp_copy_state(rbmpp_ctx* dst, const rbmpp_ctx* src) {
   rbmpp_ctx* c = dst;  // errors are reported on the destination context
   const DevDims &a = dst->d, &b = src->d;
   if (a.L != b.L || a.n_mp != b.n_mp || a.alphar != b.alphar || a.n_slater != b.n_slater || a.nw != b.nw ||
-      a.ns != b.ns || a.skew != b.skew || dst->dims.device != src->dims.device)
+      a.ns != b.ns || a.skew != b.skew || a.alphac != b.alphac || dst->dims.device != src->dims.device)
     return fail(dst, RBMPP_E_ARG, "copy_state: the two contexts differ in shape or device");
   if (!src->tables_set || !dst->tables_set) return fail(dst, RBMPP_E_STATE, "copy_state: tables must be set on both");
   const size_t nw = a.nw, ns = a.ns, N = a.N;
@@ -1518,6 +1547,8 @@ int rbmpp_copy_state(rbmpp_ctx* dst, const rbmpp_ctx* src) {
   CK(cudaStreamSynchronize(dst->st));
   dst->Wr = src->Wr;
   dst->br = src->br;
+  dst->Wc = src->Wc;
+  dst->bc = src->bc;
   dst->slater = src->slater;
   dst->shift = src->shift;
   dst->params_set = src->params_set;
@@ -1659,6 +1690,7 @@ int rbmpp_batch_create(rbmpp_ctx* const* ctxs, int n, rbmpp_batch** out) {
     if (!c) return bfail(b, RBMPP_E_ARG, "context %d is null", k);
     if (!c->tables_set || !c->params_set) return bfail(b, RBMPP_E_STATE, "context %d: tables and params first", k);
     if (c->d.skew) return bfail(b, RBMPP_E_ARG, "context %d: the batched sampler carries the block form only", k);
+    if (c->d.alphac) return bfail(b, RBMPP_E_ARG, "context %d: the batched sampler carries real RBM units only", k);
     if (dev < 0) dev = c->dims.device;
     if (c->dims.device != dev) return bfail(b, RBMPP_E_ARG, "contexts on different devices");
     b->ctx.push_back(c);

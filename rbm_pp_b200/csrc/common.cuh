@@ -24,6 +24,8 @@ void rbmpp_note_launch();
 
 struct DevDims {
   int L, N, Np, n_mp, n_qp, alphar, Mr, n_slater, Nv, Nv_rbm;
+  int alphac, Mc;     // complex RBM units (RBM.f90 thetac): Mc = 2 alphac n_mp complex angles, kept after the
+                      //   Mr real ones in every theta array as (re, im) pairs
   int nw, ns, nupdate, nwarm;
   int orb_injective;  // Orbital_Idx is injective within each spin block for one projection
   int pf_sign;        // (-1)^{Np(Np-1)/2}
@@ -54,6 +56,8 @@ struct DevTables {
 struct DevParams {
   const double* Wr;   // [f][N]   Wrirr(iw, f)
   const double* br;   // [f]
+  const double* Wc;   // [f][N][2] Wcirr(iw, f) as (re, im)
+  const double* bc;   // [f][2]
   const double* XF;   // [qp][N][N]
   const double* XFT;  // [qp][N][N]
   const double* SE;   // [qp][2N][2N] Slater_Elm(r, r') row-major (skew form only)

@@ -55,7 +55,7 @@ __host__ __device__ __forceinline__ size_t est_layout(const DevDims& d, int nqw,
   t.idx = (int*)take(N * 4);
   t.cfg = (int*)take(N * 4);
   t.x2 = t.idx2 = t.cfg2 = nullptr;
-  t.th = (double*)take((size_t)d.Mr * 8);
+  t.th = (double*)take((size_t)(d.Mr + 2 * d.Mc) * 8);
   t.thp = nullptr;
   t.sgn = (int*)take(d.n_mp * 4);
   t.sgnp = nullptr;
@@ -65,6 +65,7 @@ __host__ __device__ __forceinline__ size_t est_layout(const DevDims& d, int nqw,
   t.psi = (double*)take((size_t)d.n_qp * 16);
   t.psip = nullptr;
   t.rbm = (double*)take((size_t)d.n_qp * 8);
+  t.rbmc = d.alphac ? (double*)take((size_t)d.n_qp * 16) : nullptr;
   t.colbuf = t.rowbuf = nullptr;
   t.perm = nullptr;
   t.wA = t.wS = nullptr;
@@ -163,13 +164,13 @@ __global__ void __launch_bounds__(kEstThreads, 1)
   if (tid == 0)
     for (int mp = 1; mp < d.n_mp; mp++)
       if (s.pb[mp] != s.pb[0]) s.iflag[F_STATUS] = ST_SIGN;
-  cta_rbm_factors(d, s.th, s.rbm);
+  cta_rbm_factors(d, s.th, s.rbm, s.rbmc);
   __syncthreads();
   if (s.iflag[F_STATUS]) {
     if (tid == 0 && out_status) out_status[cfgi] = s.iflag[F_STATUS];
     return;
   }
-  const int off_pp = d.alphar * (N + 1);
+  const int off_r = 2 * d.alphac * (N + 1), off_pp = off_r + d.alphar * (N + 1);  // calc_phys_quantity.f90:205
   double* Rw = e.Rb + (size_t)warp * NB;
   int* src = e.perm + (size_t)warp * Np;
   double* vp = e.vp + (size_t)warp * Np;
@@ -194,7 +195,7 @@ __global__ void __launch_bounds__(kEstThreads, 1)
       const double det = warp_gj<KPL, NP, (KPL <= 2 ? 16 : (KPL <= 4 ? 8 : 4))>(T, Np, src, sing);
       if (sing) bad = true;
       const double pfq = (double)d.pf_sign * det;
-      const cplx cw = psi_wo_pf(d, t, s.rbm[qp], s.sgn[mp], qp);
+      const cplx cw = psi_wo_pf_s(d, t, s, s.sgn[mp], qp);
       if (lane == 0) {
         e.pfw[qp] = pfq;
         s.psi[2 * qp] = cw.re * pfq;
@@ -322,7 +323,18 @@ __global__ void __launch_bounds__(kEstThreads, 1)
             ch = ch * cosh(th);
           }
           const int sg = -s.sgn[mp] * (t.subB[i1] ? -1 : 1) * (t.subB[i2] ? -1 : 1);
-          const cplx cbw = psi_wo_pf(d, t, ch, sg, qp);
+          cplx cbw = psi_wo_pf(d, t, ch, sg, qp);
+          if (d.alphac) {  // complex units: 0.5^alphac prod cosh(thetac') of the exchanged configuration
+            cplx cf = {1.0, 0.0};
+            for (int f = 0; f < d.alphac; f++) {
+              const int j = d.Mr + 2 * (qp * d.alphac + f);
+              const double* Wf = p.Wc + (size_t)f * N * 2;
+              const double ar = s.th[j] - 2.0 * Wf[2 * iw1] * x1 * s_sign - 2.0 * Wf[2 * iw2] * x2 * s_sign;
+              const double ai = s.th[j + 1] - 2.0 * Wf[2 * iw1 + 1] * x1 * s_sign - 2.0 * Wf[2 * iw2 + 1] * x2 * s_sign;
+              cf = cscale(cmul(cf, ccosh_(ar, ai)), 0.5);
+            }
+            cbw = cmul(cbw, cf);
+          }
           hacc = hacc + e.apc[b] * (cbw.re * (Rw[b] * pfq));
           hacci = hacci + e.apc[b] * (cbw.im * (Rw[b] * pfq));
         }
@@ -339,7 +351,7 @@ __global__ void __launch_bounds__(kEstThreads, 1)
         const int* srcw = e.perm + (size_t)w * Np;
         const int* wm = t.wmap + (size_t)mp * N;
         const double pfq = e.pfw[qp];
-        const cplx cw = psi_wo_pf(d, t, s.rbm[qp], s.sgn[mp], qp);
+        const cplx cw = psi_wo_pf_s(d, t, s, s.sgn[mp], qp);
         const double cc = pfq * d.sp_cc[sp] * cw.im, ss = pfq * d.sp_ss[sp] * cw.im;
         for (int pr = tid; pr < Np * Np; pr += blockDim.x) {
           const int j = pr / Np, i = pr - j * Np;
@@ -363,7 +375,7 @@ __global__ void __launch_bounds__(kEstThreads, 1)
         const int* srcw = e.perm + (size_t)w * Np;
         const int* wm = t.wmap + (size_t)mp * N;
         const double pfq = e.pfw[qp];
-        const cplx cw = psi_wo_pf(d, t, s.rbm[qp], s.sgn[mp], qp);
+        const cplx cw = psi_wo_pf_s(d, t, s, s.sgn[mp], qp);
         const double cc = pfq * d.sp_cc[sp] * cw.re, ss = pfq * d.sp_ss[sp] * cw.re;
         const int npr = Np * Np;
         if (d.orb_injective) {
@@ -465,8 +477,39 @@ __global__ void __launch_bounds__(kEstThreads, 1)
           acci = acci - t1 * s.psi[2 * q1 + 1] * xi;
         }
       }
-      Orow[k] = acc * w;
-      if (OrowI) OrowI[k] = acci * w;
+      Orow[off_r + k] = acc * w;
+      if (OrowI) OrowI[off_r + k] = acci * w;
+    }
+    // complex RBM part (calc_phys_quantity.f90:115-160): parameter pairs (re, im) with d psi / d Im = i d psi / d Re;
+    // tanh of a complex angle as (tanh a + i tan b) / (1 + i tanh a tan b)
+    for (int k = tid; k < d.alphac * (N + 1); k += blockDim.x) {
+      cplx v = {0.0, 0.0};
+      auto ctanh = [&](int qp, int f) {
+        const int j = d.Mr + 2 * (qp * d.alphac + f);
+        const double ta = tanh(s.th[j]), tb = tan(s.th[j + 1]);
+        const cplx num = {ta, tb}, den = {1.0, ta * tb};
+        const double dd = den.re * den.re + den.im * den.im;
+        return cplx{(num.re * den.re + num.im * den.im) / dd, (num.im * den.re - num.re * den.im) / dd};
+      };
+      int pos;
+      if (k < d.alphac) {
+        const int f = k;
+        for (int qp = 0; qp < d.n_qp; qp++) v = cadd(v, cmul(ctanh(qp, f), cplx{s.psi[2 * qp], s.psi[2 * qp + 1]}));
+        pos = 2 * f;
+      } else {
+        const int f = (k - d.alphac) / N, iw = (k - d.alphac) - f * N;
+        for (int mp = 0; mp < d.n_mp; mp++) {
+          const double xi = (double)s.x[t.winv[(size_t)mp * N + iw]];
+          const int qa = 2 * mp, qb = 2 * mp + 1;
+          v = cadd(v, cscale(cmul(ctanh(qa, f), cplx{s.psi[2 * qa], s.psi[2 * qa + 1]}), xi));
+          v = cadd(v, cscale(cmul(ctanh(qb, f), cplx{s.psi[2 * qb], s.psi[2 * qb + 1]}), -xi));
+        }
+        pos = 2 * d.alphac + f * 2 * N + 2 * iw;
+      }
+      Orow[pos] = v.re * w;        // d psi / d Re
+      OrowI[pos] = v.im * w;
+      Orow[pos + 1] = -v.im * w;   // d psi / d Im = i d psi / d Re
+      OrowI[pos + 1] = v.re * w;
     }
     for (int k = off_pp + tid; k < d.Nv; k += blockDim.x) {
       Orow[k] = Orow[k] * w;

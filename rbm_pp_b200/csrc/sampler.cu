@@ -226,7 +226,7 @@ __device__ __forceinline__ void sampler_body(const DevDims& d, const DevTables& 
       const int flipsign = (t.subB[i1] ? -1 : 1) * (t.subB[i2] ? -1 : 1);
       for (int mp = tid; mp < d.n_mp; mp += blockDim.x) s.sgnp[mp] = -s.sgn[mp] * flipsign;
       __syncthreads();
-      cta_rbm_factors(d, s.thp, s.rbm);
+      cta_rbm_factors(d, s.thp, s.rbm, s.rbmc);
       __syncthreads();
       double* u = s.wu + (size_t)warp * Np;
       double* v = s.wv + (size_t)warp * Np;
@@ -236,7 +236,7 @@ __device__ __forceinline__ void sampler_body(const DevDims& d, const DevTables& 
         if (lane == 0) {
           double pfn = R * s.pf[qp];
           s.pfp[qp] = pfn;
-          cplx cw = psi_wo_pf(d, t, s.rbm[qp], s.sgnp[qp >> 1], qp);
+          cplx cw = psi_wo_pf_s(d, t, s, s.sgnp[qp >> 1], qp);
           s.psip[2 * qp] = cw.re * pfn;
           s.psip[2 * qp + 1] = cw.im * pfn;
           pre += cw.re * pfn;
@@ -277,7 +277,7 @@ __device__ __forceinline__ void sampler_body(const DevDims& d, const DevTables& 
           warp_update<KPL>(d, c.Yw + (size_t)qp * Np * Np, ua, db, cc, u, v, s.wA + (size_t)warp * Np,
                            s.wS + (size_t)warp * Np);
         }
-        for (int j = tid; j < d.Mr; j += blockDim.x) s.th[j] = s.thp[j];
+        for (int j = tid; j < d.Mr + 2 * d.Mc; j += blockDim.x) s.th[j] = s.thp[j];
         for (int mp = tid; mp < d.n_mp; mp += blockDim.x) s.sgn[mp] = s.sgnp[mp];
         for (int qp = tid; qp < d.n_qp; qp += blockDim.x) {
           s.pf[qp] = s.pfp[qp];

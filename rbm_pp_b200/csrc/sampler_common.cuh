@@ -229,7 +229,7 @@ template <int KPL = 0, int NP = 0, class F = BlockScratch<KPL, NP>>
 __device__ __forceinline__ void checkpoint(const SCtx& c, int& nfastup, int i0) {
   const DevDims& d = c.d;
   const WS& s = c.s;
-  for (int j = threadIdx.x; j < d.Mr; j += blockDim.x) s.thp[j] = s.th[j];
+  for (int j = threadIdx.x; j < d.Mr + 2 * d.Mc; j += blockDim.x) s.thp[j] = s.th[j];
   for (int mp = threadIdx.x; mp < d.n_mp; mp += blockDim.x) s.sgnp[mp] = s.sgn[mp];
   __syncthreads();
   cta_calc_theta(d, c.t, c.p, s.x, s.th);
@@ -249,6 +249,9 @@ __device__ __forceinline__ void checkpoint(const SCtx& c, int& nfastup, int i0) 
   }
   for (int j = threadIdx.x; j < d.Mr; j += blockDim.x)
     if (fabs(s.th[j] - s.thp[j]) > 1.0e-5) status(c) = ST_THETA;
+  for (int j = threadIdx.x; j < d.Mc; j += blockDim.x)  // make_sample.f90:84-86
+    if (hypot(s.th[d.Mr + 2 * j] - s.thp[d.Mr + 2 * j], s.th[d.Mr + 2 * j + 1] - s.thp[d.Mr + 2 * j + 1]) > 1.0e-5)
+      status(c) = ST_THETA;
   __syncthreads();
   if (status(c)) return;
   // old Pf kept in pfp for the drift measure
@@ -325,7 +328,7 @@ __device__ __forceinline__ void global_flip(const SCtx& c) {
     s.idx[i] = s.idx2[i];
     s.cfg[i] = s.cfg2[i];
   }
-  for (int j = threadIdx.x; j < d.Mr; j += blockDim.x) s.th[j] = s.thp[j];
+  for (int j = threadIdx.x; j < d.Mr + 2 * d.Mc; j += blockDim.x) s.th[j] = s.thp[j];
   for (int mp = threadIdx.x; mp < d.n_mp; mp += blockDim.x) s.sgn[mp] = s.sgnp[mp];
   for (int qp = threadIdx.x; qp < d.n_qp; qp += blockDim.x) {
     s.psi[2 * qp] = s.psip[2 * qp];

@@ -22,6 +22,7 @@ struct WS {
   double* psi;   // [n_qp][2]
   double* psip;  // [n_qp][2]
   double* rbm;   // [n_qp] cosh products
+  double* rbmc;  // [n_qp][2] complex factor 0.5^alphac prod cosh(thetac) (null without complex units)
   double* tile;  // [Np][Np+1]
   double* colbuf;  // [Np]
   double* rowbuf;  // [Np]
@@ -81,8 +82,8 @@ __host__ __device__ __forceinline__ size_t ws_layout(const DevDims& d, int nwarp
   t.x2 = (int*)take(N * 4);
   t.idx2 = (int*)take(N * 4);
   t.cfg2 = (int*)take(N * 4);
-  t.th = (double*)take(d.Mr * 8);
-  t.thp = (double*)take(d.Mr * 8);
+  t.th = (double*)take((size_t)(d.Mr + 2 * d.Mc) * 8);
+  t.thp = (double*)take((size_t)(d.Mr + 2 * d.Mc) * 8);
   t.sgn = (int*)take(d.n_mp * 4);
   t.sgnp = (int*)take(d.n_mp * 4);
   t.pb = (int*)take(d.n_mp * 4);
@@ -91,6 +92,7 @@ __host__ __device__ __forceinline__ size_t ws_layout(const DevDims& d, int nwarp
   t.psi = (double*)take(d.n_qp * 16);
   t.psip = (double*)take(d.n_qp * 16);
   t.rbm = (double*)take(d.n_qp * 8);
+  t.rbmc = d.alphac ? (double*)take((size_t)d.n_qp * 16) : nullptr;
   t.tile = (own_tile && !d.gj_global) ? (double*)take((size_t)Np * (Np + 1) * 8) : nullptr;
   t.colbuf = (double*)take(Np * 8);
   t.rowbuf = (double*)take(Np * 8);
@@ -106,7 +108,8 @@ __host__ __device__ __forceinline__ size_t ws_layout(const DevDims& d, int nwarp
   return off;
 }
 
-// calc_theta RBM.f90:31-91 (real branch): th[j], j = mp*2*alphar + (s==+1 ? 0 : alphar) + f
+// calc_theta RBM.f90:31-91: th[j], j = mp*2*alphar + (s==+1 ? 0 : alphar) + f, then thetac as (re, im) pairs
+// at th[Mr + 2 j'] with the same index pattern over alphac
 __device__ __forceinline__ void cta_calc_theta(const DevDims& d, const DevTables& t, const DevParams& p, const int* x,
                                       double* th) {
   const int A2 = 2 * d.alphar;
@@ -120,9 +123,25 @@ __device__ __forceinline__ void cta_calc_theta(const DevDims& d, const DevTables
     for (int i = 0; i < d.N; i++) acc = acc + Wf[wm[i]] * (double)x[i] * s;
     th[j] = acc;
   }
+  const int C2 = 2 * d.alphac;
+  for (int j = threadIdx.x; j < d.Mc; j += blockDim.x) {
+    int mp = j / C2, rem = j - mp * C2;
+    double s = rem < d.alphac ? 1.0 : -1.0;
+    int f = rem < d.alphac ? rem : rem - d.alphac;
+    const int* wm = t.wmap + (size_t)mp * d.N;
+    const double* Wf = p.Wc + (size_t)f * d.N * 2;
+    double ar = p.bc[2 * f], ai = p.bc[2 * f + 1];
+    for (int i = 0; i < d.N; i++) {
+      const double xs = (double)x[i] * s;
+      ar = ar + Wf[2 * wm[i]] * xs;
+      ai = ai + Wf[2 * wm[i] + 1] * xs;
+    }
+    th[d.Mr + 2 * j] = ar;
+    th[d.Mr + 2 * j + 1] = ai;
+  }
 }
 
-// update_theta RBM.f90:95-148 (x is the spin configuration BEFORE the exchange)
+// update_theta RBM.f90:95-148 (x is the spin configuration BEFORE the exchange), real and complex angles
 __device__ __forceinline__ void cta_update_theta(const DevDims& d, const DevTables& t, const DevParams& p, const int* x, int i1,
                                         int i2, const double* th, double* thp) {
   const int A2 = 2 * d.alphar;
@@ -137,6 +156,21 @@ __device__ __forceinline__ void cta_update_theta(const DevDims& d, const DevTabl
     v = v - 2.0 * Wf[iw1] * x1 * s;
     v = v - 2.0 * Wf[iw2] * x2 * s;
     thp[j] = v;
+  }
+  const int C2 = 2 * d.alphac;
+  for (int j = threadIdx.x; j < d.Mc; j += blockDim.x) {
+    int mp = j / C2, rem = j - mp * C2;
+    double s = rem < d.alphac ? 1.0 : -1.0;
+    int f = rem < d.alphac ? rem : rem - d.alphac;
+    const double* Wf = p.Wc + (size_t)f * d.N * 2;
+    int iw1 = t.wmap[(size_t)mp * d.N + i1], iw2 = t.wmap[(size_t)mp * d.N + i2];
+    double vr = th[d.Mr + 2 * j], vi = th[d.Mr + 2 * j + 1];
+    vr = vr - 2.0 * Wf[2 * iw1] * x1 * s;
+    vi = vi - 2.0 * Wf[2 * iw1 + 1] * x1 * s;
+    vr = vr - 2.0 * Wf[2 * iw2] * x2 * s;
+    vi = vi - 2.0 * Wf[2 * iw2 + 1] * x2 * s;
+    thp[d.Mr + 2 * j] = vr;
+    thp[d.Mr + 2 * j + 1] = vi;
   }
 }
 
@@ -297,12 +331,31 @@ __device__ __forceinline__ void cta_gauss_jordan(const DevDims& d, const WS& s) 
   __syncthreads();
 }
 
-// RBM cosh products per projection for theta vector th (sub.f90:42-46)
-__device__ __forceinline__ void cta_rbm_factors(const DevDims& d, const double* th, double* rbm) {
+// cosh of a complex angle as sub.f90:40 writes it: (cosh a cos b, sinh a sin b)
+__device__ __forceinline__ cplx ccosh_(double a, double b) { return {cosh(a) * cos(b), sinh(a) * sin(b)}; }
+
+// 0.5^alphac prod_f cosh(thetac(qp, f)) (sub.f90:37-41) for the complex angles stored after the Mr real ones
+__device__ __forceinline__ cplx complex_factor(const DevDims& d, const double* th, int qp) {
+  cplx c = {1.0, 0.0};
+  for (int f = 0; f < d.alphac; f++) {
+    const int j = d.Mr + 2 * (qp * d.alphac + f);
+    c = cscale(cmul(c, ccosh_(th[j], th[j + 1])), 0.5);
+  }
+  return c;
+}
+
+// RBM cosh products per projection for theta vector th (sub.f90:37-46): the real product into rbm and, with
+// complex units, the complex factor into rbmc
+__device__ __forceinline__ void cta_rbm_factors(const DevDims& d, const double* th, double* rbm, double* rbmc = nullptr) {
   for (int qp = threadIdx.x; qp < d.n_qp; qp += blockDim.x) {
     double r = 1.0;
     for (int f = 0; f < d.alphar; f++) r = r * cosh(th[qp * d.alphar + f]);
     rbm[qp] = r;
+    if (d.alphac && rbmc) {
+      const cplx c = complex_factor(d, th, qp);
+      rbmc[2 * qp] = c.re;
+      rbmc[2 * qp + 1] = c.im;
+    }
   }
 }
 
@@ -315,13 +368,20 @@ __device__ __forceinline__ cplx psi_wo_pf(const DevDims& d, const DevTables& t, 
   return cscale(c, d.para_sp[sp]);
 }
 
+// psi_wo_pf with the complex factor of the workspace's current angles (rbmc) when there are complex units
+__device__ __forceinline__ cplx psi_wo_pf_s(const DevDims& d, const DevTables& t, const WS& s, int sgn_mp, int qp) {
+  cplx c = psi_wo_pf(d, t, s.rbm[qp], sgn_mp, qp);
+  if (d.alphac) c = cmul(c, cplx{s.rbmc[2 * qp], s.rbmc[2 * qp + 1]});
+  return c;
+}
+
 // calc_amplitude_RBM_PP sub.f90:4-89 for the current (th, pf, sgn): psi[qp], D_PSI0; one draw.
 __device__ __forceinline__ void cta_amplitude(const DevDims& d, const DevTables& t, const WS& s, const double* th,
                                      const double* pf, const int* sgn, double* psi, int psi0_slot) {
-  cta_rbm_factors(d, th, s.rbm);
+  cta_rbm_factors(d, th, s.rbm, s.rbmc);
   __syncthreads();
   for (int qp = threadIdx.x; qp < d.n_qp; qp += blockDim.x) {
-    cplx c = psi_wo_pf(d, t, s.rbm[qp], sgn[qp >> 1], qp);
+    cplx c = psi_wo_pf_s(d, t, s, sgn[qp >> 1], qp);
     psi[2 * qp] = c.re * pf[qp];
     psi[2 * qp + 1] = c.im * pf[qp];
   }

@@ -25,11 +25,11 @@ def test_library_exports_all_symbols():
 
 
 def test_unsupported_dimensions_are_refused_without_a_gpu():
-    """rbmpp_create checks the sizes before touching a device: the complex RBM (alphac > 0), an odd site
-    count and a lattice beyond the supported size come back as RBMPP_E_ARG with a message."""
+    """rbmpp_create checks the sizes before touching a device: a negative unit count, an odd site count and a
+    lattice beyond the supported size come back as RBMPP_E_ARG with a message."""
     build.build()
     lib = capi.lib()
-    cases = [(dict(L=4, alphac=1), "alphac > 0"), (dict(L=5), "unsupported L"), (dict(L=24), "unsupported L")]
+    cases = [(dict(L=4, alphac=-1), "bad dimensions"), (dict(L=5), "unsupported L"), (dict(L=24), "unsupported L")]
     for kw, msg in cases:
         d = capi.Dims(kw.get("L", 4), 1, kw.get("alphac", 0), 1, 16, 1, 1, 1, 1.0, 0.5, 0, 0)
         h = ctypes.c_void_p()

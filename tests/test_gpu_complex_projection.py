@@ -1,4 +1,5 @@
-"""Complex momentum-projection weights para_mp_trans (sym_info.txt; psi = sum_qp para_mp_trans(mp) ...,
+"""Complex amplitudes on the device against the oracle: complex momentum-projection weights para_mp_trans
+(sym_info.txt; psi = sum_qp para_mp_trans(mp) ...,
 sub.f90:47-50) on the device against the oracle.  psi, H psi and O_k become complex; O keeps a real and an
 imaginary row per sample, the Ovec_Store columns of calc_phys_quantity.f90:227-228, so S = sum over both rows and
 gvec, Ovec take the real parts of 2 conj(E) O and conj(psi) O (:225-226).
@@ -6,7 +7,9 @@ gvec, Ovec take the real parts of 2 conj(E) O and conj(psi) O (:225-226).
 - amplitudes, local energies and O_k of given configurations within 1e-10;
 - the summed measurement (scalars 1e-10; gvec, Ovec, S 1e-9 of the largest entry);
 - Markov chains decision by decision: exact or parting at a documented tie;
-- three SR iterations in lock step with the oracle, FP64 and split-BF16 with refinement.
+- three SR iterations in lock step with the oracle, FP64 and split-BF16 with refinement;
+and complex RBM units (alpha_c > 0: RBM.f90 thetac, 0.5^alpha_c prod cosh(thetac) in sub.f90:37-41, the (re, im)
+parameter pairs of calc_phys_quantity.f90:115-160 and SR_pdposv.f90:385-413) the same way.
 """
 import numpy as np
 import pytest
@@ -127,5 +130,85 @@ def test_sr_lockstep_complex(precision):
         bro, Wro, slo, sho = o.get_params()
         brg, Wrg, slg, shg = g.get_params()
         assert _rel(slg, slo) < 1e-8 and _rel(Wrg, Wro) < 1e-8
+        assert abs(shg - sho) <= 1e-9 * abs(sho) + 1e-300
+    g.close()
+
+
+# ---- complex RBM units (alpha_c > 0: RBM.f90 thetac, sub.f90:37-41, calc_phys_quantity.f90:115-160) ----
+
+def _units_pair(L, trans, alphac, alphar, nw, ns, seed, **kw):
+    p = fm.synthetic_problem(L, translations=trans, alphar=alphar, nsample=nw * ns, seed=seed, **kw)
+    p.inp.alphac = alphac
+    rng = np.random.default_rng(seed + 1)
+    N = L * L
+    p.bc = 0.05 * (rng.normal(size=alphac) + 1j * rng.normal(size=alphac))
+    p.Wc = 0.05 * (rng.normal(size=(N, alphac)) + 1j * rng.normal(size=(N, alphac)))
+    o = po.Oracle(p, nranks=nw, nsample_per_rank=ns, nthreads=8)
+    g = capi.Context(p, n_walkers=nw, nsample_per_walker=ns)
+    assert g.complex_weights
+    o.set_params_c(p.bc, p.Wc)
+    o.set_params(p.br, p.Wr, p.slater, 0.0)
+    g.set_params(p.br, p.Wr, p.slater, 0.0, bc=p.bc, Wc=p.Wc)
+    return p, o, g
+
+
+@pytest.mark.parametrize("L,trans,alphac,alphar,kw", [(4, False, 1, 1, dict()), (4, True, 2, 1, dict()),
+                                                      (6, True, 1, 0, dict(spin_parity=-1))])
+def test_eval_configs_complex_units(L, trans, alphac, alphar, kw):
+    p, o, g = _units_pair(L, trans, alphac, alphar, 1, 8, seed=100 + L, **kw)
+    x = _configs(L * L, 24, seed=L + 7)
+    ro = o.eval_configs(x, want_h=True, want_O=True)
+    rg = g.eval_configs(x, want_h=True, want_O=True)
+    assert _rel(rg["psi"], ro["psi"]) < RTOL
+    hscale = max(np.abs(ro["hpsi"]).max(), np.abs(ro["psi"][:, 0]).max())
+    oscale = np.abs(ro["O"]).max()
+    for j in range(x.shape[0]):
+        assert abs(rg["hpsi"][j] - ro["hpsi"][j]) <= RTOL * max(abs(ro["hpsi"][j]), abs(ro["psi"][j, 0]),
+                                                                 1e-3 * hscale), j
+        assert np.abs(rg["O"][j] - ro["O"][j]).max() <= RTOL * max(np.abs(ro["O"][j]).max(), 1e-3 * oscale), j
+    g.close()
+
+
+def test_chains_complex_units(capsys):
+    L, nw, ns = 4, 8, 8
+    p, o, g = _units_pair(L, True, 1, 1, nw, ns, seed=111)
+    for c in (o, g):
+        c.set_trace(8192)
+        c.seed(4040)
+    kinds = {}
+    for first in (True, False):
+        o.make_sample(first)
+        g.make_sample(first)
+        eo, to = o.events()
+        eg, tg = g.events()
+        for r in cc.compare_walkers(to, eo, tg, eg):
+            assert r["kind"] not in ("type", "draw", "length"), r
+            if r["kind"] == "checkpoint":
+                assert r["straddle"], r
+            kinds[r["kind"]] = kinds.get(r["kind"], 0) + 1
+    with capsys.disabled():
+        print(f"\nCOMPLEX_UNITS_CHAINS {kinds}")
+    assert kinds.get("exact", 0) >= nw
+    g.close()
+
+
+@pytest.mark.parametrize("precision", [capi.SR_FP64, capi.SR_SPLIT_BF16])
+def test_sr_lockstep_complex_units(precision):
+    L, nw, ns = 4, 8, 16
+    p, o, g = _units_pair(L, False, 1, 1, nw, ns, seed=12345)
+    loop = po.VMCLoop(o, p, iseed0=12345)
+    g.seed(12345)
+    bc, Wc, br, Wr = capi.initial_params_c(g, p)
+    g.set_params(br, Wr, p.slater, 0.0, bc=bc, Wc=Wc)
+    for it in range(1, 4):
+        rec = loop.iteration_step()
+        sg = g.iteration(precision, p.inp.delta_tau, p.inp.s_factor_scale, p.inp.s_cut, p.inp.s_factor0)
+        assert np.array_equal(o.samples()[0], g.samples()[0]), it
+        assert abs(sg.Etot - rec["Etot"]) <= 1e-9 * abs(rec["Etot"])
+        bro, Wro, slo, sho = o.get_params()
+        brg, Wrg, slg, shg = g.get_params()
+        bco, Wco = o.get_params_c()
+        bcg, Wcg = g.get_params_c()
+        assert _rel(slg, slo) < 1e-8 and _rel(Wrg, Wro) < 1e-8 and _rel(Wcg, Wco) < 1e-8 and _rel(bcg, bco) < 1e-8
         assert abs(shg - sho) <= 1e-9 * abs(sho) + 1e-300
     g.close()

@@ -243,3 +243,53 @@ def test_formats_round_trip(tmp_path):
     assert np.allclose(q.slater, p.slater, rtol=1e-14)
     assert np.allclose(q.Wr, p.Wr, atol=1e-15) and np.allclose(q.br, p.br, atol=1e-15)
     assert abs(np.abs(q.slater).mean() - 0.25) < 1e-12
+
+
+def _complex_problem(L, trans, alphar, seed):
+    p = fm.synthetic_problem(L, translations=trans, alphar=alphar, nsample=16, seed=seed)
+    p.inp.alphac = 1
+    rng = np.random.default_rng(seed + 1)
+    N = L * L
+    p.bc = 0.05 * (rng.normal(size=1) + 1j * rng.normal(size=1))
+    p.Wc = 0.05 * (rng.normal(size=(N, 1)) + 1j * rng.normal(size=(N, 1)))
+    return p
+
+
+def test_complex_units_local_energy_and_ok():
+    """Complex RBM units (alpha_c = 1, RBM.f90 thetac; sub.f90:37-41): H psi from the fast-update local energy
+    equals the ED Hamiltonian applied to psi over the Sz = 0 sector, and O_k equals central differences of psi for
+    the complex parameters' real and imaginary parts (the pairs of calc_phys_quantity.f90:115-160)."""
+    p = _complex_problem(4, False, 1, 31)
+    o = po.Oracle(p, nranks=1, nsample_per_rank=8)
+    o.set_params_c(p.bc, p.Wc)
+    o.set_params(p.br, p.Wr, p.slater, 0.0)
+    basis = ed.sz0_basis(16)
+    r = o.eval_configs(basis, want_h=True)
+    assert np.abs(r["psi"][:, 0].imag).max() > 1e-3 * np.abs(r["psi"][:, 0]).max()
+    H = ed.hamiltonian(4, 1.0, 0.5, basis)
+    hp = H @ r["psi"][:, 0]
+    assert np.abs(hp - r["hpsi"]).max() <= 1e-10 * np.abs(hp).max()
+    xs = basis[::997][:4]
+    base = o.eval_configs(xs, want_h=False, want_O=True)
+    h = 1e-6
+    # parameter order: bc (re, im), Wc(iw) (re, im), br, Wr, f
+    for k in [0, 1, 2, 3, 2 + 2 * 7, 2 + 2 * 7 + 1, 34, 35 + 4]:
+        def psi_at(delta):
+            bc, Wc, br, Wr = p.bc.copy(), p.Wc.copy(), p.br.copy(), p.Wr.copy()
+            if k < 2:
+                bc[0] += delta * (1.0 if k == 0 else 1j)
+            elif k < 34:
+                iw, part = divmod(k - 2, 2)
+                Wc[iw, 0] += delta * (1.0 if part == 0 else 1j)
+            elif k == 34:
+                br[0] += delta
+            else:
+                Wr[k - 35, 0] += delta
+            o.set_params_c(bc, Wc)
+            o.set_params(br, Wr, p.slater, 0.0)
+            return o.eval_configs(xs, want_h=False)["psi"][:, 0]
+        fd = (psi_at(h) - psi_at(-h)) / (2 * h)
+        an = base["O"][:, k]
+        assert np.all(np.abs(fd - an) <= 1e-7 * np.abs(base["psi"][:, 0]) + 1e-8 * np.abs(an)), (k, fd, an)
+    o.set_params_c(p.bc, p.Wc)
+    o.set_params(p.br, p.Wr, p.slater, 0.0)
