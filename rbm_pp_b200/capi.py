@@ -166,8 +166,9 @@ class Context:
         self._spw = None if sp_weights is None else _f(sp_weights, np.float64)
         self._chk(lib().rbmpp_set_tables(self.h, _p(self._w), _p(para), _p(self._o), None, _p(self._sb),
                                          _p(self._spw)))
-        # complex para_mp_trans: psi, H psi and O_k are complex (O comes as a real and an imaginary row)
-        self.complex_weights = bool(np.any(para[1::2] != 0.0))
+        # complex para_mp_trans or complex units: psi, H psi and O_k are complex (O comes as a real and an
+        # imaginary row)
+        self.complex_weights = bool(np.any(para[1::2] != 0.0)) or self.alphac > 0
 
     def close(self):
         if getattr(self, "h", None):

@@ -60,7 +60,7 @@ def test_bad_tables_are_refused():
     _refused(_problem(L=12), "supports N <= 128", sp_weights=fm.spin_projection_weights(1, transverse=True))
     p = _problem()
     p.sym.para_mp = p.sym.para_mp.astype(np.complex128) + 0.5j
-    _refused(p, "complex para_mp_trans with the transverse", sp_weights=fm.spin_projection_weights(1, True))
+    _refused(p, "with the transverse (skew-form) projection", sp_weights=fm.spin_projection_weights(1, True))
 
 
 def test_explicit_tables_equal_defaults():
