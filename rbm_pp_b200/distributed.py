@@ -66,19 +66,26 @@ class _DeviceVector:
 def allreduce_fn(group=None, where="cuda"):
     """The host all-reduce for Context.set_allreduce: fn(ptr, n) sums n float64 at ptr over the ranks of
     `group`, in place, and returns when the sum is there.
-      where="cuda": ptr is a device address; torch.distributed all-reduces it there (NCCL over NVLink);
+      where="cuda": ptr is a device address; with NCCL torch.distributed all-reduces it in place over NVLink,
+                    with gloo a host copy is reduced and copied back;
       where="host": ptr is a host address (the same call over gloo, for CPU tests of this adapter)."""
     import torch
     import torch.distributed as dist
+    nccl = dist.get_backend(group) == "nccl"
 
     def fn(ptr, n):
         if where == "cuda":
             t = torch.as_tensor(_DeviceVector(ptr, n), device="cuda")
+            if nccl:
+                dist.all_reduce(t, op=dist.ReduceOp.SUM, group=group)
+            else:
+                h = t.cpu()
+                dist.all_reduce(h, op=dist.ReduceOp.SUM, group=group)
+                t.copy_(h)
+            torch.cuda.current_stream().synchronize()
         else:
             t = torch.from_numpy(np.ctypeslib.as_array((C.c_double * n).from_address(ptr)))
-        dist.all_reduce(t, op=dist.ReduceOp.SUM, group=group)
-        if where == "cuda":
-            torch.cuda.current_stream().synchronize()
+            dist.all_reduce(t, op=dist.ReduceOp.SUM, group=group)
 
     return fn
 
@@ -108,15 +115,25 @@ class SRRunner:
         self.precision = precision
         inp = problem.inp
         ctx.seed(iseed0)
+        ac = getattr(ctx, "alphac", 0)
         if rank == 0:
-            br, Wr = capi.initial_params(ctx, problem)
+            bc, Wc, br, Wr = capi.initial_params_c(ctx, problem)
         else:
+            bc, Wc = np.zeros(ac, np.complex128), np.zeros((ctx.N, ac), np.complex128)
             br = np.zeros(inp.alphar) if problem.br is None else problem.br
             Wr = np.zeros((ctx.N, inp.alphar)) if problem.Wr is None else problem.Wr
         if world > 1:
             br, Wr = broadcast_initial_params(br, Wr, group)
+            if ac:
+                bcf, Wcf = broadcast_initial_params(np.asarray(bc, np.complex128).view(np.float64),
+                                                    np.asarray(Wc, np.complex128).reshape(-1, order="F")
+                                                    .view(np.float64), group)
+                bc, Wc = bcf.view(np.complex128), Wcf.view(np.complex128).reshape((ctx.N, ac), order="F")
             ctx.set_allreduce(allreduce_fn(group))
-        ctx.set_params(br, Wr, problem.slater, 0.0)
+        if ac:
+            ctx.set_params(br, Wr, problem.slater, 0.0, bc=bc, Wc=Wc)
+        else:
+            ctx.set_params(br, Wr, problem.slater, 0.0)
         self.book = Bookkeeping(inp, ctx.N)
 
     @classmethod
