@@ -27,6 +27,7 @@ cudaError_t rbmpp_launch_sampler_stream(const DevDims&, const DevTables&, const 
 cudaError_t rbmpp_launch_estimator(const DevDims&, const DevTables&, const DevParams&, const int8_t*, int, double*,
                                    double*, double*, int*, int*, int, cudaStream_t);
 size_t rbmpp_estimator_smem(const DevDims&, int);
+size_t rbmpp_estimator_smem_any(const DevDims&, int);
 cudaError_t rbmpp_launch_advance_rng(uint32_t*, const int*, int, int, int, cudaStream_t);
 cudaError_t rbmpp_syrk_ot_o(int, int, const double*, double*, cudaStream_t);
 cudaError_t rbmpp_symmetrize(int, double*, cudaStream_t);
@@ -178,7 +179,8 @@ struct rbmpp_ctx {
   cudaEvent_t ev[12] = {};
   double stats[10] = {0};
   int stream_stages = 0;  // > 0: TMA-streamed sampler with this many stages
-  bool est_fits = true;   // the estimator's workspace fits in shared memory
+  bool est_fits = true;   // the estimator's workspace fits in shared memory (tiles there or in global scratch)
+  bool est_smem_tiles = true;  // ... with its tiles in shared memory
   double* d_SE = nullptr;  // Slater_Elm [qp][2N][2N] of the skew form (transverse projection)
   // host-supplied cross-rank sum (rbmpp_set_allreduce) and its packed buffer: 6 scalars, gvec, Ovec
   rbmpp_allreduce_fn red_fn = nullptr;
@@ -491,7 +493,8 @@ int rbmpp_create(const rbmpp_dims* dims, rbmpp_ctx** out) {
   if ((long long)rbmpp_sampler_smem(d, 256) > maxsm)
     return fail(c, RBMPP_E_ARG, "sampler workspace %zu B exceeds %d B of shared memory", rbmpp_sampler_smem(d, 256),
                 maxsm);
-  c->est_fits = (long long)rbmpp_estimator_smem(d, 256) <= maxsm;
+  c->est_fits = (long long)rbmpp_estimator_smem_any(d, maxsm) <= maxsm;
+  c->est_smem_tiles = (long long)rbmpp_estimator_smem(d, 256) <= maxsm;
   c->stream_stages = rbmpp_stream_stages(d, maxsm);
   if (getenv("RBMPP_SAMPLER") && std::string(getenv("RBMPP_SAMPLER")) == "direct") c->stream_stages = 0;
   if (d.alphac) c->stream_stages = 0;  // the streaming sampler carries real units only
@@ -1946,7 +1949,7 @@ extern "C" int rbmpp_eval_configs_noalloc(rbmpp_ctx* c, int n, const int* d_x, d
   if (c->d.skew || c->d.cplx)
     return fail(c, RBMPP_E_ARG, "eval_configs_noalloc takes real projection weights and the block form only; use "
                                 "eval_configs");
-  if (!c->est_fits)
+  if (!c->est_smem_tiles)  // larger blocks need a global scratch buffer, which this entry point may not allocate
     return fail(c, RBMPP_E_ARG, "the estimator's workspace for N/2 = %d exceeds the shared memory of one block",
                 c->d.Np);
   if (n == 0) return 0;

@@ -41,7 +41,10 @@ struct Est {
   int nqw;
 };
 
-__host__ __device__ __forceinline__ size_t est_layout(const DevDims& d, int nqw, char* base, WS* w, Est* e) {
+// Shared-memory layout of one estimator block.  With gtiles the nqw Gauss-Jordan tiles live in global memory (a
+// per-block slice of a scratch buffer, for block sizes whose tiles do not fit one block's shared memory).
+__host__ __device__ __forceinline__ size_t est_layout(const DevDims& d, int nqw, char* base, WS* w, Est* e,
+                                                      bool gtiles = false) {
   size_t off = 0;
   auto take = [&](size_t bytes) -> char* {
     char* p = base ? base + off : nullptr;
@@ -86,13 +89,18 @@ __host__ __device__ __forceinline__ size_t est_layout(const DevDims& d, int nqw,
   x.nap = (int*)take(16);
   x.diag = (double*)take(16);
   const size_t tile = (size_t)Np * (Np + 1) * 8;
-  size_t tiles_bytes = (size_t)nqw * tile;
-  const size_t signbuf = (size_t)kEstWarps * N * 4;  // sign_PP scratch reuses the tile area
-  if (tiles_bytes < signbuf) tiles_bytes = signbuf;
-  x.tiles = (double*)take(tiles_bytes);
+  const size_t signbuf = (size_t)kEstWarps * N * 4;
+  if (gtiles) {
+    x.tiles = nullptr;  // set per block from the scratch buffer
+    t.wu = (double*)take(signbuf);  // per-warp N-int buffers of cta_sign_pp
+  } else {
+    size_t tiles_bytes = (size_t)nqw * tile;
+    if (tiles_bytes < signbuf) tiles_bytes = signbuf;  // sign_PP scratch reuses the tile area
+    x.tiles = (double*)take(tiles_bytes);
+    t.wu = x.tiles;  // per-warp N-int buffers of cta_sign_pp (used before the projection loop)
+  }
   x.nqw = nqw;
   t.tile = x.tiles;
-  t.wu = x.tiles;  // per-warp N-int buffers of cta_sign_pp (used before the projection loop)
   t.wv = nullptr;
   if (w) *w = t;
   if (e) *e = x;
@@ -100,19 +108,12 @@ __host__ __device__ __forceinline__ size_t est_layout(const DevDims& d, int nqw,
 }
 
 template <int KPL, int NP>
-__global__ void __launch_bounds__(kEstThreads, 1)
-    estimator_kernel(const __grid_constant__ DevDims d, const __grid_constant__ DevTables t,
-                     const __grid_constant__ DevParams p, const int8_t* xs, int n, double* out_psi, double* out_hpsi,
-                     double* O, int* out_nap, int* out_status, int reweight, int nqw) {
-  extern __shared__ __align__(16) char smem[];
-  __shared__ WS s;
-  __shared__ Est e;
-  if (threadIdx.x == 0) est_layout(d, nqw, smem, &s, &e);
-  __syncthreads();
+__device__ __forceinline__ void estimator_config(const DevDims& d, const DevTables& t, const DevParams& p,
+                                                 const int8_t* xs, int n, double* out_psi, double* out_hpsi,
+                                                 double* O, int* out_nap, int* out_status, int reweight, const WS& s,
+                                                 const Est& e, int cfgi) {
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int N = d.N, Np = NP > 0 ? NP : d.Np, ld = Np + 1, NB = 4 * N;
-  const int cfgi = blockIdx.x;
-  if (cfgi >= n) return;
   // complex projection weights: a real row and an imaginary row per configuration
   double* Orow = O ? O + (size_t)cfgi * d.Nv * (d.cplx ? 2 : 1) : nullptr;
   double* OrowI = (Orow && d.cplx) ? Orow + d.Nv : nullptr;
@@ -533,6 +534,30 @@ __global__ void __launch_bounds__(kEstThreads, 1)
   }
 }
 
+template <int KPL, int NP>
+__global__ void __launch_bounds__(kEstThreads, 1)
+    estimator_kernel(const __grid_constant__ DevDims d, const __grid_constant__ DevTables t,
+                     const __grid_constant__ DevParams p, const int8_t* xs, int n, double* out_psi, double* out_hpsi,
+                     double* O, int* out_nap, int* out_status, int reweight, int nqw, double* gtiles) {
+  extern __shared__ __align__(16) char smem[];
+  __shared__ WS s;
+  __shared__ Est e;
+  const int Np = NP > 0 ? NP : d.Np, ld = Np + 1;
+  if (threadIdx.x == 0) {
+    est_layout(d, nqw, smem, &s, &e, gtiles != nullptr);
+    if (gtiles) {
+      e.tiles = gtiles + (size_t)blockIdx.x * nqw * Np * ld;
+      s.tile = e.tiles;
+    }
+  }
+  __syncthreads();
+  // one configuration per block, or (global tiles) the configurations blockIdx.x, blockIdx.x + gridDim.x, ...
+  for (int cfgi = blockIdx.x; cfgi < n; cfgi += gridDim.x) {
+    __syncthreads();
+    estimator_config<KPL, NP>(d, t, p, xs, n, out_psi, out_hpsi, O, out_nap, out_status, reweight, s, e, cfgi);
+  }
+}
+
 // Advances every walker's MT19937 by its measurement draws: one per amplitude call, i.e.
 // 1 + n_antiparallel per stored sample (sub.f90:72 called from calc_phys_quantity.f90:95,369).
 __global__ void advance_rng_kernel(uint32_t* mt, const int* nap, int ns, int nw, int extra) {
@@ -555,9 +580,17 @@ int est_tile_warps(const DevDims& d, int max_smem) {
 
 }  // namespace
 
+// Shared memory of the estimator with its tiles in shared memory (one tile at least); larger than the opt-in
+// limit for N/2 beyond about 120, where the tiles move to a global scratch buffer.
 size_t rbmpp_estimator_smem(const DevDims& d, int threads) {
   (void)threads;
   return est_layout(d, 1, nullptr, nullptr, nullptr);
+}
+
+// Shared memory of the estimator in the mode its launch will use (global tiles when the shared ones do not fit).
+size_t rbmpp_estimator_smem_any(const DevDims& d, int max_smem) {
+  if (est_tile_warps(d, max_smem) >= 1) return est_layout(d, 1, nullptr, nullptr, nullptr);
+  return est_layout(d, kEstWarps, nullptr, nullptr, nullptr, true);
 }
 
 cudaError_t rbmpp_launch_estimator(const DevDims& d, const DevTables& t, const DevParams& p, const int8_t* xs, int n,
@@ -567,19 +600,38 @@ cudaError_t rbmpp_launch_estimator(const DevDims& d, const DevTables& t, const D
   int dev = 0, maxsm = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-  const int nqw = est_tile_warps(d, maxsm);
-  if (nqw < 1) return cudaErrorInvalidValue;
-  size_t smem = est_layout(d, nqw, nullptr, nullptr, nullptr);
+  int nqw = est_tile_warps(d, maxsm);
+  size_t smem = 0;
+  double* gtiles = nullptr;
+  int grid = n;
+  if (nqw >= 1) {
+    smem = est_layout(d, nqw, nullptr, nullptr, nullptr);
+  } else {
+    // tiles beyond one block's shared memory (N/2 beyond about 120): one block per SM loops over the
+    // configurations with its tiles in a stream-ordered scratch slice of global memory
+    nqw = kEstWarps;
+    smem = est_layout(d, nqw, nullptr, nullptr, nullptr, true);
+    if ((long long)smem > maxsm) return cudaErrorInvalidValue;
+    int nsm = 0;
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    grid = n < nsm ? n : nsm;
+    const size_t bytes = (size_t)grid * nqw * d.Np * (d.Np + 1) * sizeof(double);
+    cudaError_t e = cudaMallocAsync((void**)&gtiles, bytes, st);
+    if (e != cudaSuccess) return e;
+  }
   int kpl = (d.Np + 31) / 32;
+  cudaError_t rc = cudaErrorInvalidValue;
 #define LAUNCH(K, NPC)                                                                                     \
   do {                                                                                                     \
-    cudaError_t e = cudaFuncSetAttribute(estimator_kernel<K, NPC>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
-                                         (int)smem);                                                       \
-    if (e != cudaSuccess) return e;                                                                        \
-    rbmpp_note_launch();                                                                                   \
-    estimator_kernel<K, NPC><<<n, kEstThreads, smem, st>>>(d, t, p, xs, n, out_psi, out_hpsi, O, out_nap,   \
-                                                           out_status, reweight, nqw);                      \
-    return cudaGetLastError();                                                                             \
+    rc = cudaFuncSetAttribute(estimator_kernel<K, NPC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem); \
+    if (rc == cudaSuccess) {                                                                               \
+      rbmpp_note_launch();                                                                                 \
+      estimator_kernel<K, NPC><<<grid, kEstThreads, smem, st>>>(d, t, p, xs, n, out_psi, out_hpsi, O, out_nap, \
+                                                                out_status, reweight, nqw, gtiles);         \
+      rc = cudaGetLastError();                                                                             \
+    }                                                                                                      \
+    if (gtiles) cudaFreeAsync(gtiles, st);                                                                 \
+    return rc;                                                                                             \
   } while (0)
   switch (d.Np) {  // block sizes of the even-L lattices with a compile-time specialisation
     case 8: LAUNCH(1, 8);
@@ -593,7 +645,8 @@ cudaError_t rbmpp_launch_estimator(const DevDims& d, const DevTables& t, const D
   if (kpl <= 4) LAUNCH(4, 0);
   if (kpl <= 8) LAUNCH(8, 0);
 #undef LAUNCH
-  return cudaErrorInvalidValue;
+  if (gtiles) cudaFreeAsync(gtiles, st);
+  return rc;
 }
 
 cudaError_t rbmpp_launch_advance_rng(uint32_t* mt, const int* nap, int ns, int nw, int extra, cudaStream_t st) {

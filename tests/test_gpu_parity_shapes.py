@@ -113,3 +113,15 @@ def test_edge_cases(L, trans, alphar, kw):
     _eval_match(o, g, _configs(L * L, 12, seed=L))
     _measure_match(o, g, _configs(L * L, nw * ns, seed=L + 1), want_S=True)
     g.close()
+
+
+@pytest.mark.parametrize("L", [16, 18])
+def test_estimator_large_blocks(L):
+    """N/2 = 128 and 162: the estimator's Gauss-Jordan tiles no longer fit one block's shared memory and move to
+    a global scratch slice per block, one block per SM looping over the configurations.  Amplitudes, local
+    energies and O_k against the oracle at 1e-10; the summed measurement of stored samples too."""
+    nw, ns = 2, 2
+    p, o, g = _pair(L, False, 2, nw, ns, seed=130 + L)
+    _eval_match(o, g, _configs(L * L, 6, seed=L))
+    _measure_match(o, g, _configs(L * L, nw * ns, seed=L + 1))
+    g.close()
