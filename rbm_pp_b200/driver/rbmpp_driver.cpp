@@ -87,6 +87,7 @@ struct Inputs {
   std::vector<double> slater;    // N_Slater
   bool have_W = false;
   std::vector<double> Wr, br;    // (N, alphar) column-major, alphar
+  std::vector<double> Wc, bc;    // complex units as (re, im) pairs: (N, alphac) column-major, alphac
 };
 
 std::vector<std::string> tk(const std::vector<std::string>& L, size_t i, const std::string& file) {
@@ -185,7 +186,7 @@ void read_zqp(const std::string& dir, Inputs& in) {  // parameter.f90:114-141
   for (double& v : in.slater) v = v * 0.25 / r3;  // slater_abs_av, module.f90:66
 }
 
-void read_W(const std::string& dir, Inputs& in) {  // parameter.f90:42-75 (real RBM)
+void read_W(const std::string& dir, Inputs& in) {  // parameter.f90:42-75: complex units, then real ones
   const std::string fn = dir + "/W.input";
   std::ifstream probe(fn);
   if (!probe) return;
@@ -193,7 +194,23 @@ void read_W(const std::string& dir, Inputs& in) {  // parameter.f90:42-75 (real 
   const int N = in.N;
   in.Wr.assign((size_t)N * in.alphar, 0.0);
   in.br.assign(in.alphar, 0.0);
+  in.Wc.assign((size_t)2 * N * in.alphac, 0.0);
+  in.bc.assign((size_t)2 * in.alphac, 0.0);
   size_t pos = 1;
+  for (int f = 0; f < in.alphac; f++) {
+    auto u = tk(L, pos++, fn);  // "# bias f re im"
+    if (u.size() < 5 || std::atoi(u[2].c_str()) != f + 1) die("i1/=f (W.input)");
+    in.bc[2 * f] = fnum(u[3]);
+    in.bc[2 * f + 1] = fnum(u[4]);
+    for (int iw = 0; iw < N; iw++) {
+      auto v = tk(L, pos++, fn);
+      if (v.size() < 4 || std::atoi(v[0].c_str()) != f + 1 || std::atoi(v[1].c_str()) != iw + 1)
+        die("index mismatch (W.input)");
+      in.Wc[2 * (iw + (size_t)N * f)] = fnum(v[2]);
+      in.Wc[2 * (iw + (size_t)N * f) + 1] = fnum(v[3]);
+    }
+    pos++;
+  }
   for (int f = 0; f < in.alphar; f++) {
     auto u = tk(L, pos++, fn);  // "# bias f b 0"
     if (u.size() < 5 || std::atoi(u[2].c_str()) != f + 1) die("i1/=f (W.input)");
@@ -211,10 +228,18 @@ void read_W(const std::string& dir, Inputs& in) {  // parameter.f90:42-75 (real 
   in.have_W = true;
 }
 
-void write_W(const std::string& path, int N, int alphar, const std::vector<double>& br, const std::vector<double>& Wr) {
+void write_W(const std::string& path, int N, int alphar, const std::vector<double>& br, const std::vector<double>& Wr,
+             int alphac = 0, const std::vector<double>& bc = {}, const std::vector<double>& Wc = {}) {
   FILE* f = std::fopen(path.c_str(), "w");  // parameter.f90:159-175, 248-262
   if (!f) die("cannot write " + path);
   std::fprintf(f, "# index for independent neurons (f), index for interaction (iw), irreducible interaction Wirr(iw,f)\n");
+  for (int fi = 0; fi < alphac; fi++) {
+    std::fprintf(f, "# bias%6d%22.15f%22.15f\n", fi + 1, bc[2 * fi], bc[2 * fi + 1]);
+    for (int iw = 0; iw < N; iw++)
+      std::fprintf(f, "%6d%6d%22.15f%22.15f\n", fi + 1, iw + 1, Wc[2 * (iw + (size_t)N * fi)],
+                   Wc[2 * (iw + (size_t)N * fi) + 1]);
+    std::fprintf(f, "\n");
+  }
   for (int fi = 0; fi < alphar; fi++) {
     std::fprintf(f, "# bias%6d%22.15f%22.15f\n", fi + 1, br[fi], 0.0);
     for (int iw = 0; iw < N; iw++) std::fprintf(f, "%6d%6d%22.15f%22.15f\n", fi + 1, iw + 1, Wr[iw + (size_t)N * fi], 0.0);
@@ -323,7 +348,6 @@ int main(int argc, char** argv) {
   if (correlation && transverse) die("--correlation and --transverse: the Calc_Correlation program has no transverse form");
   Inputs in;
   read_rbm_input(dir, in);
-  if (in.alphac != 0) die("alphac > 0 (complex RBM) is not supported by this library");
   read_sym_info(dir, in);
   read_orbital_idx(dir, in);
   read_zqp(dir, in);
@@ -354,7 +378,7 @@ int main(int argc, char** argv) {
   std::memset(&d, 0, sizeof(d));
   d.L = in.L;
   d.n_mp_trans = in.n_mp;
-  d.alphac = 0;
+  d.alphac = in.alphac;
   d.alphar = in.alphar;
   d.n_slater = in.n_slater;
   d.nsample = ns;
@@ -383,11 +407,24 @@ int main(int argc, char** argv) {
                           spw.data()),
          "set_tables");
   lib.ck(rbmpp_seed_walkers(lib.c, (int)seed), "seed_walkers");
-  // initialize_parameters (parameter.f90:21-41): rank 0 draws U(-0.05, 0.05); W.input overrides
-  std::vector<double> u((size_t)in.alphar * (N + 1));
+  // initialize_parameters (parameter.f90:21-41): rank 0 draws U(-0.05, 0.05), complex units first as (re, im)
+  // pairs; W.input overrides
+  std::vector<double> u((size_t)2 * in.alphac * (N + 1) + (size_t)in.alphar * (N + 1));
   lib.ck(rbmpp_rank0_grnd(lib.c, (int)u.size(), u.data()), "rank0_grnd");
-  std::vector<double> br(in.alphar), Wr((size_t)N * in.alphar);
+  std::vector<double> br(in.alphar), Wr((size_t)N * in.alphar), bc((size_t)2 * in.alphac), Wc((size_t)2 * N * in.alphac);
   size_t k = 0;
+  for (int f = 0; f < in.alphac; f++) {
+    bc[2 * f] = 0.1 * (u[k++] - 0.5);
+    bc[2 * f + 1] = 0.1 * (u[k++] - 0.5);
+    if (in.spin_parity == -1) {
+      bc[2 * f] *= 10.0;
+      bc[2 * f + 1] *= 10.0;
+    }
+    for (int iw = 0; iw < N; iw++) {
+      Wc[2 * (iw + (size_t)N * f)] = 0.1 * (u[k++] - 0.5);
+      Wc[2 * (iw + (size_t)N * f) + 1] = 0.1 * (u[k++] - 0.5);
+    }
+  }
   for (int f = 0; f < in.alphar; f++) {
     br[f] = 0.1 * (u[k++] - 0.5);
     if (in.spin_parity == -1) br[f] *= 10.0;
@@ -396,18 +433,23 @@ int main(int argc, char** argv) {
   if (in.have_W) {
     br = in.br;
     Wr = in.Wr;
+    bc = in.bc;
+    Wc = in.Wc;
   }
   // write_initial_parameters (parameter.f90:148-234); rank 4's sub_initial_W.txt is the same content
-  write_W(dir + "/initial_W.txt", N, in.alphar, br, Wr);
-  write_W(dir + "/sub_initial_W.txt", N, in.alphar, br, Wr);
+  write_W(dir + "/initial_W.txt", N, in.alphar, br, Wr, in.alphac, bc, Wc);
+  write_W(dir + "/sub_initial_W.txt", N, in.alphar, br, Wr, in.alphac, bc, Wc);
   write_input_checks(dir, in);
   std::vector<double> sl = in.slater;
-  lib.ck(rbmpp_set_params(lib.c, Wr.data(), br.data(), nullptr, nullptr, sl.data(), 0.0), "set_params");
+  lib.ck(rbmpp_set_params(lib.c, Wr.data(), br.data(), in.alphac ? Wc.data() : nullptr,
+                          in.alphac ? bc.data() : nullptr, sl.data(), 0.0),
+         "set_params");
 
   // optimisation loop, main.f90:300-455
   FILE* fe = std::fopen((dir + "/Energy_vs_Iteration.txt").c_str(), "w");
   if (!fe) die("cannot write Energy_vs_Iteration.txt");
   std::vector<double> br_av(in.alphar, 0.0), Wr_av(Wr.size(), 0.0), sl_av(sl.size(), 0.0);
+  std::vector<double> bc_av(bc.size(), 0.0), Wc_av(Wc.size(), 0.0);
   double shift_av = 0.0;
   int nav_chk = 0;
   for (int it = 1; it <= in.Nstep; it++) {
@@ -427,6 +469,9 @@ int main(int argc, char** argv) {
       nav_chk++;
       shift_av += shift_now;
       lib.ck(rbmpp_get_params(lib.c, Wr.data(), br.data(), sl.data(), nullptr), "get_params");
+      if (in.alphac) lib.ck(rbmpp_get_params_c(lib.c, Wc.data(), bc.data()), "get_params_c");
+      for (size_t q = 0; q < bc.size(); q++) bc_av[q] += bc[q];
+      for (size_t q = 0; q < Wc.size(); q++) Wc_av[q] += Wc[q];
       for (size_t q = 0; q < br.size(); q++) br_av[q] += br[q];
       for (size_t q = 0; q < Wr.size(); q++) Wr_av[q] += Wr[q];
       for (size_t q = 0; q < sl.size(); q++) sl_av[q] += sl[q];
@@ -435,14 +480,19 @@ int main(int argc, char** argv) {
   std::fclose(fe);
   if (in.Nav < 1 || nav_chk != in.Nav) die("Nav_chk /= Nav");
   // averaged parameters (:455-485) and write_optimized_parameters (parameter.f90:238-277)
+  for (double& v : bc_av) v /= (double)in.Nav;
+  for (double& v : Wc_av) v /= (double)in.Nav;
   for (double& v : br_av) v /= (double)in.Nav;
   for (double& v : Wr_av) v /= (double)in.Nav;
   for (double& v : sl_av) v /= (double)in.Nav;
   shift_av /= (double)in.Nav;
-  lib.ck(rbmpp_set_params(lib.c, Wr_av.data(), br_av.data(), nullptr, nullptr, sl_av.data(), shift_av), "set_params");
-  write_W(dir + "/optimized_W.txt", N, in.alphar, br_av, Wr_av);
+  lib.ck(rbmpp_set_params(lib.c, Wr_av.data(), br_av.data(), in.alphac ? Wc_av.data() : nullptr,
+                          in.alphac ? bc_av.data() : nullptr, sl_av.data(), shift_av),
+         "set_params");
+  write_W(dir + "/optimized_W.txt", N, in.alphar, br_av, Wr_av, in.alphac, bc_av, Wc_av);
   write_zqp(dir + "/zqp_orbital_opt.dat", sl_av);
-  write_W(dir + "/sub_optimized_W.txt", N, in.alphar, br_av, Wr_av);  // rank 3's copies (parameter.f90:280-311)
+  // rank 3's copies (parameter.f90:280-311)
+  write_W(dir + "/sub_optimized_W.txt", N, in.alphar, br_av, Wr_av, in.alphac, bc_av, Wc_av);
   write_zqp(dir + "/sub_zqp_orbital_opt.dat", sl_av);
 
   // final energy (:486-575): warm up, then Nav measurements

@@ -253,11 +253,19 @@ def read_zqp(path: str, n_slater: int, rescale: bool = True) -> np.ndarray:
     return out
 
 
-def write_W(path: str, br: np.ndarray, Wr: np.ndarray) -> None:
-    """W.input / initial_W.txt / optimized_W.txt layout (parameter.f90:159-175), real RBM."""
+def write_W(path: str, br: np.ndarray, Wr: np.ndarray, bc=None, Wc=None) -> None:
+    """W.input / initial_W.txt / optimized_W.txt layout (parameter.f90:159-175): the complex units bc, Wc(N, alphac)
+    first (when given), then the real ones."""
     N, alphar = Wr.shape
     with open(path, "w") as f:
         f.write("# index for independent neurons (f), index for interaction (iw), irreducible interaction Wirr(iw,f)\n")
+        if Wc is not None:
+            for fi in range(Wc.shape[1]):
+                f.write(f"# bias{fi + 1:6d}{complex(bc[fi]).real:22.15f}{complex(bc[fi]).imag:22.15f}\n")
+                for iw in range(N):
+                    w = complex(Wc[iw, fi])
+                    f.write(f"{fi + 1:6d}{iw + 1:6d}{w.real:22.15f}{w.imag:22.15f}\n")
+                f.write("\n")
         for fi in range(alphar):
             f.write(f"# bias{fi + 1:6d}{float(br[fi]):22.15f}{0.0:22.15f}\n")
             for iw in range(N):
@@ -265,13 +273,28 @@ def write_W(path: str, br: np.ndarray, Wr: np.ndarray) -> None:
             f.write("\n")
 
 
-def read_W(path: str, N: int, alphar: int) -> tuple[np.ndarray, np.ndarray]:
-    """parameter.f90:42-75 (alphac = 0)."""
+def read_W(path: str, N: int, alphar: int, alphac: int = 0):
+    """parameter.f90:42-75: (br, Wr), or (br, Wr, bc, Wc) when alphac > 0 (the complex units come first)."""
     with open(path) as f:
         lines = f.read().splitlines()
     br = np.zeros(alphar)
     Wr = np.zeros((N, alphar))
+    bc = np.zeros(alphac, np.complex128)
+    Wc = np.zeros((N, alphac), np.complex128)
     pos = 1
+    for fi in range(alphac):
+        t = _tokens(lines[pos])
+        pos += 1
+        if int(t[2]) != fi + 1:
+            raise ValueError("i1/=f (W.input)")
+        bc[fi] = complex(_fortran_float(t[3]), _fortran_float(t[4]))
+        for iw in range(N):
+            t = _tokens(lines[pos])
+            pos += 1
+            if int(t[0]) != fi + 1 or int(t[1]) != iw + 1:
+                raise ValueError("index mismatch (W.input)")
+            Wc[iw, fi] = complex(_fortran_float(t[2]), _fortran_float(t[3]))
+        pos += 1
     for fi in range(alphar):
         t = _tokens(lines[pos])
         pos += 1
@@ -289,7 +312,7 @@ def read_W(path: str, N: int, alphar: int) -> tuple[np.ndarray, np.ndarray]:
             if abs(_fortran_float(t[3])) > 1e-15:
                 raise ValueError("r2 /= 0 (W.input)")
         pos += 1
-    return br, Wr
+    return (br, Wr, bc, Wc) if alphac > 0 else (br, Wr)
 
 
 def spin_projection_weights(spin_parity: int = 1, transverse: bool = False) -> np.ndarray:
@@ -322,6 +345,8 @@ class Problem:
     br: np.ndarray | None = None
     Wr: np.ndarray | None = None
     extra: dict = field(default_factory=dict)
+    bc: np.ndarray | None = None  # complex units (alphac > 0), from W.input
+    Wc: np.ndarray | None = None
 
     @property
     def N(self) -> int:
@@ -329,7 +354,7 @@ class Problem:
 
     @property
     def Nv(self) -> int:
-        return self.inp.alphar * (self.N + 1) + self.n_slater
+        return 2 * self.inp.alphac * (self.N + 1) + self.inp.alphar * (self.N + 1) + self.n_slater
 
 
 def synthetic_problem(L: int, *, translations: bool, alphar: int, orbital: str = "full", nsample: int = 1024,
@@ -360,7 +385,7 @@ def write_problem(dirname: str, p: Problem) -> None:
     write_orbital_idx(os.path.join(dirname, "orbitalidx.def"), p.n_slater, p.orbital_idx)
     write_zqp(os.path.join(dirname, "zqp_orbital_initial.dat"), p.slater)
     if p.Wr is not None:
-        write_W(os.path.join(dirname, "W.input"), p.br, p.Wr)
+        write_W(os.path.join(dirname, "W.input"), p.br, p.Wr, p.bc, p.Wc)
 
 
 def read_problem(dirname: str) -> Problem:
@@ -369,8 +394,11 @@ def read_problem(dirname: str) -> Problem:
     sym = read_sym_info(os.path.join(dirname, "sym_info.txt"), N)
     n_slater, idx = read_orbital_idx(os.path.join(dirname, "orbitalidx.def"), N)
     slater = read_zqp(os.path.join(dirname, "zqp_orbital_initial.dat"), n_slater)
-    br = Wr = None
+    br = Wr = bc = Wc = None
     wpath = os.path.join(dirname, "W.input")
     if os.path.exists(wpath):
-        br, Wr = read_W(wpath, N, inp.alphar)
-    return Problem(inp=inp, sym=sym, n_slater=n_slater, orbital_idx=idx, slater=slater, br=br, Wr=Wr)
+        if inp.alphac > 0:
+            br, Wr, bc, Wc = read_W(wpath, N, inp.alphar, inp.alphac)
+        else:
+            br, Wr = read_W(wpath, N, inp.alphar)
+    return Problem(inp=inp, sym=sym, n_slater=n_slater, orbital_idx=idx, slater=slater, br=br, Wr=Wr, bc=bc, Wc=Wc)

@@ -189,3 +189,46 @@ def test_driver_transverse_matches_oracle(tmp_path):
     for it in range(1, nstep + 1):
         rec = loop.iteration_step()
         assert abs(got[it - 1, 1] - rec["Etot"]) <= 1e-9 * abs(rec["Etot"]), (it, got[it - 1, 1], rec["Etot"])
+
+
+def _complex_units_problem(nw, ns, nstep, seed):
+    p = fm.synthetic_problem(4, translations=False, alphar=1, nsample=nw * ns, seed=seed, Nstep=nstep, Nav=1)
+    p.inp.alphac = 1
+    rng = np.random.default_rng(seed)
+    p.bc = 0.05 * (rng.normal(size=1) + 1j * rng.normal(size=1))
+    p.Wc = 0.05 * (rng.normal(size=(16, 1)) + 1j * rng.normal(size=(16, 1)))
+    return p
+
+
+def test_complex_units_w_input_round_trip(tmp_path):
+    """W.input with complex units (parameter.f90:42-75: a (re, im) block per complex unit before the real ones)."""
+    p = _complex_units_problem(8, 8, 2, 5)
+    fm.write_problem(str(tmp_path), p)
+    q = fm.read_problem(str(tmp_path))
+    assert q.inp.alphac == 1 and np.allclose(q.bc, p.bc, atol=1e-15) and np.allclose(q.Wc, p.Wc, atol=1e-15)
+    assert np.allclose(q.br, p.br, atol=1e-15) and np.allclose(q.Wr, p.Wr, atol=1e-15)
+    out = subprocess.run([_driver(), "--dir", str(tmp_path), "--walkers", "8", "--check-inputs"],
+                         capture_output=True, text=True, timeout=60)
+    assert out.returncode == 0, out.stderr
+
+
+@pytest.mark.gpu
+def test_driver_complex_units_matches_oracle(tmp_path):
+    """alpha_c = 1 through the driver (complex W.input in, complex optimized_W.txt out) against the oracle's loop."""
+    import pyoracle as po
+    nw, ns, nstep, seed = 8, 8, 3, 4545
+    p = _complex_units_problem(nw, ns, nstep, 19)
+    fm.write_problem(str(tmp_path), p)
+    out = subprocess.run([_driver(), "--dir", str(tmp_path), "--walkers", str(nw), "--seed", str(seed)],
+                         capture_output=True, text=True, timeout=600)
+    assert out.returncode == 0, out.stderr + out.stdout
+    got = np.loadtxt(os.path.join(tmp_path, "Energy_vs_Iteration.txt"))
+    q = fm.read_problem(str(tmp_path))
+    o = po.Oracle(q, nranks=nw, nsample_per_rank=ns, nthreads=4)
+    loop = po.VMCLoop(o, q, iseed0=seed)
+    for it in range(1, nstep + 1):
+        rec = loop.iteration_step()
+        assert abs(got[it - 1, 1] - rec["Etot"]) <= 1e-9 * abs(rec["Etot"]), (it, got[it - 1, 1], rec["Etot"])
+    br, Wr, bc, Wc = fm.read_W(os.path.join(tmp_path, "optimized_W.txt"), 16, 1, 1)
+    bco, Wco = o.get_params_c()
+    assert np.allclose(Wc, Wco, rtol=1e-9, atol=1e-13) and np.allclose(bc, bco, rtol=1e-9, atol=1e-13)
