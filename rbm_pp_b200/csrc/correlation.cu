@@ -38,7 +38,10 @@ struct Cor {
   int nqw;
 };
 
-__host__ __device__ __forceinline__ size_t cor_layout(const DevDims& d, int nqw, char* base, WS* w, Cor* e) {
+// Shared-memory layout of one correlation block.  With gbuf the nqw tiles and the pair table psx live in a
+// per-block slice of a global scratch buffer (block sizes whose tiles do not fit one block's shared memory).
+__host__ __device__ __forceinline__ size_t cor_layout(const DevDims& d, int nqw, char* base, WS* w, Cor* e,
+                                                      bool gbuf = false) {
   size_t off = 0;
   auto take = [&](size_t bytes) -> char* {
     char* p = base ? base + off : nullptr;
@@ -70,19 +73,24 @@ __host__ __device__ __forceinline__ size_t cor_layout(const DevDims& d, int nqw,
   t.dsc = (double*)take(32 * 8);
   Cor x;
   x.pfw = (double*)take((size_t)d.n_qp * 8);
-  x.psx = (double*)take((size_t)Np * Np * 8);
+  x.psx = gbuf ? nullptr : (double*)take((size_t)Np * Np * 8);
   x.perm = (int*)take((size_t)kCorWarps * Np * 4);
   x.vp = (double*)take((size_t)kCorWarps * Np * 8);
   x.rb = (double*)take((size_t)kCorWarps * Np * 8);
   x.bsum = (double*)take((size_t)4 * N * 8);
   const size_t tile = (size_t)Np * (Np + 1) * 8;
-  size_t tiles_bytes = (size_t)nqw * tile;
-  const size_t signbuf = (size_t)kCorWarps * N * 4;  // sign_PP scratch reuses the tile area
-  if (tiles_bytes < signbuf) tiles_bytes = signbuf;
-  x.tiles = (double*)take(tiles_bytes);
+  const size_t signbuf = (size_t)kCorWarps * N * 4;
+  if (gbuf) {
+    x.tiles = nullptr;
+    t.wu = (double*)take(signbuf);  // per-warp N-int buffers of cta_sign_pp
+  } else {
+    size_t tiles_bytes = (size_t)nqw * tile;
+    if (tiles_bytes < signbuf) tiles_bytes = signbuf;  // sign_PP scratch reuses the tile area
+    x.tiles = (double*)take(tiles_bytes);
+    t.wu = x.tiles;
+  }
   x.nqw = nqw;
   t.tile = x.tiles;
-  t.wu = x.tiles;
   t.wv = nullptr;
   if (w) *w = t;
   if (e) *e = x;
@@ -90,19 +98,12 @@ __host__ __device__ __forceinline__ size_t cor_layout(const DevDims& d, int nqw,
 }
 
 template <int KPL, int NP>
-__global__ void __launch_bounds__(kCorThreads, 1)
-    correlation_kernel(const __grid_constant__ DevDims d, const __grid_constant__ DevTables t,
-                       const __grid_constant__ DevParams p, const int8_t* xs, int n, double* out_psi,
-                       double* out_hpsi, double* rows, double* sdr, int* out_nap, int* out_status, int nqw) {
-  extern __shared__ __align__(16) char smem[];
-  __shared__ WS s;
-  __shared__ Cor e;
-  if (threadIdx.x == 0) cor_layout(d, nqw, smem, &s, &e);
-  __syncthreads();
+__device__ __forceinline__ void correlation_config(const DevDims& d, const DevTables& t, const DevParams& p,
+                                                   const int8_t* xs, int n, double* out_psi, double* out_hpsi,
+                                                   double* rows, double* sdr, int* out_nap, int* out_status,
+                                                   const WS& s, const Cor& e, int cfgi) {
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
   const int N = d.N, Np = NP > 0 ? NP : d.Np, ld = Np + 1, NB = 4 * N;
-  const int cfgi = blockIdx.x;
-  if (cfgi >= n) return;
 
   for (int i = tid; i < N; i += blockDim.x) s.x[i] = (int)xs[(size_t)cfgi * N + i];
   for (int k = tid; k < Np * Np; k += blockDim.x) e.psx[k] = 0.0;
@@ -368,6 +369,32 @@ __global__ void fill_kernel(double* a, long long n, double v) {
     a[i] = v;
 }
 
+template <int KPL, int NP>
+__global__ void __launch_bounds__(kCorThreads, 1)
+    correlation_kernel(const __grid_constant__ DevDims d, const __grid_constant__ DevTables t,
+                       const __grid_constant__ DevParams p, const int8_t* xs, int n, double* out_psi,
+                       double* out_hpsi, double* rows, double* sdr, int* out_nap, int* out_status, int nqw,
+                       double* gbuf) {
+  extern __shared__ __align__(16) char smem[];
+  __shared__ WS s;
+  __shared__ Cor e;
+  const int Np = NP > 0 ? NP : d.Np, ld = Np + 1;
+  if (threadIdx.x == 0) {
+    cor_layout(d, nqw, smem, &s, &e, gbuf != nullptr);
+    if (gbuf) {
+      e.tiles = gbuf + (size_t)blockIdx.x * ((size_t)nqw * Np * ld + (size_t)Np * Np);
+      e.psx = e.tiles + (size_t)nqw * Np * ld;
+      s.tile = e.tiles;
+    }
+  }
+  __syncthreads();
+  // one sample per block, or (global scratch) the samples blockIdx.x, blockIdx.x + gridDim.x, ...
+  for (int cfgi = blockIdx.x; cfgi < n; cfgi += gridDim.x) {
+    __syncthreads();
+    correlation_config<KPL, NP>(d, t, p, xs, n, out_psi, out_hpsi, rows, sdr, out_nap, out_status, s, e, cfgi);
+  }
+}
+
 int cor_tile_warps(const DevDims& d, int max_smem) {
   for (int q = kCorWarps; q >= 1; q--)
     if ((long long)cor_layout(d, q, nullptr, nullptr, nullptr) <= max_smem) return q;
@@ -377,7 +404,12 @@ int cor_tile_warps(const DevDims& d, int max_smem) {
 }  // namespace
 
 // Projections inverted together per round, 0 when one block's shared memory cannot hold the workspace.
-int rbmpp_correlation_fits(const DevDims& d, int max_smem) { return cor_tile_warps(d, max_smem); }
+// 1 when the correlation kernel can run at this shape (tiles in shared memory, or in global scratch when the
+// rest of its workspace fits), else 0.
+int rbmpp_correlation_fits(const DevDims& d, int max_smem) {
+  if (cor_tile_warps(d, max_smem) >= 1) return 1;
+  return (long long)cor_layout(d, kCorWarps, nullptr, nullptr, nullptr, true) <= max_smem ? 1 : 0;
+}
 
 cudaError_t rbmpp_launch_correlation(const DevDims& d, const DevTables& t, const DevParams& p, const int8_t* xs, int n,
                                      double* out_psi, double* out_hpsi, double* rows, double* sdr, int* out_nap,
@@ -386,19 +418,38 @@ cudaError_t rbmpp_launch_correlation(const DevDims& d, const DevTables& t, const
   int dev = 0, maxsm = 0;
   cudaGetDevice(&dev);
   cudaDeviceGetAttribute(&maxsm, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
-  const int nqw = cor_tile_warps(d, maxsm);
-  if (nqw < 1) return cudaErrorInvalidValue;
-  const size_t smem = cor_layout(d, nqw, nullptr, nullptr, nullptr);
+  int nqw = cor_tile_warps(d, maxsm);
+  size_t smem = 0;
+  double* gbuf = nullptr;
+  int grid = n;
+  if (nqw >= 1) {
+    smem = cor_layout(d, nqw, nullptr, nullptr, nullptr);
+  } else {
+    // tiles and pair table beyond one block's shared memory (N/2 beyond about 100): one block per SM loops over
+    // the samples with a stream-ordered scratch slice of global memory
+    nqw = kCorWarps;
+    smem = cor_layout(d, nqw, nullptr, nullptr, nullptr, true);
+    if ((long long)smem > maxsm) return cudaErrorInvalidValue;
+    int nsm = 0;
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    grid = n < nsm ? n : nsm;
+    const size_t per = (size_t)nqw * d.Np * (d.Np + 1) + (size_t)d.Np * d.Np;
+    cudaError_t e = cudaMallocAsync((void**)&gbuf, (size_t)grid * per * sizeof(double), st);
+    if (e != cudaSuccess) return e;
+  }
   const int kpl = (d.Np + 31) / 32;
+  cudaError_t rc = cudaErrorInvalidValue;
 #define LAUNCH(K, NPC)                                                                                          \
   do {                                                                                                          \
-    cudaError_t e = cudaFuncSetAttribute(correlation_kernel<K, NPC>, cudaFuncAttributeMaxDynamicSharedMemorySize, \
-                                         (int)smem);                                                            \
-    if (e != cudaSuccess) return e;                                                                             \
-    rbmpp_note_launch();                                                                                        \
-    correlation_kernel<K, NPC><<<n, kCorThreads, smem, st>>>(d, t, p, xs, n, out_psi, out_hpsi, rows, sdr,       \
-                                                              out_nap, out_status, nqw);                         \
-    return cudaGetLastError();                                                                                  \
+    rc = cudaFuncSetAttribute(correlation_kernel<K, NPC>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem); \
+    if (rc == cudaSuccess) {                                                                                    \
+      rbmpp_note_launch();                                                                                      \
+      correlation_kernel<K, NPC><<<grid, kCorThreads, smem, st>>>(d, t, p, xs, n, out_psi, out_hpsi, rows, sdr,  \
+                                                                   out_nap, out_status, nqw, gbuf);              \
+      rc = cudaGetLastError();                                                                                  \
+    }                                                                                                           \
+    if (gbuf) cudaFreeAsync(gbuf, st);                                                                          \
+    return rc;                                                                                                  \
   } while (0)
   switch (d.Np) {
     case 8: LAUNCH(1, 8);
@@ -410,8 +461,10 @@ cudaError_t rbmpp_launch_correlation(const DevDims& d, const DevTables& t, const
   if (kpl <= 1) LAUNCH(1, 0);
   if (kpl <= 2) LAUNCH(2, 0);
   if (kpl <= 4) LAUNCH(4, 0);
+  if (kpl <= 8) LAUNCH(8, 0);
 #undef LAUNCH
-  return cudaErrorInvalidValue;
+  if (gbuf) cudaFreeAsync(gbuf, st);
+  return rc;
 }
 
 cudaError_t rbmpp_fill(double* a, long long n, double v, cudaStream_t st) {

@@ -125,3 +125,24 @@ def test_estimator_large_blocks(L):
     _eval_match(o, g, _configs(L * L, 6, seed=L))
     _measure_match(o, g, _configs(L * L, nw * ns, seed=L + 1))
     g.close()
+
+
+@pytest.mark.parametrize("L,nw", [(16, 2), (18, 1)])
+def test_correlation_large_blocks(L, nw):
+    """The correlation measurement where its tiles and the N/2 x N/2 table of exchanged amplitudes no longer fit
+    one block's shared memory (global scratch per block, one block per SM looping over the samples), against the
+    oracle at 1e-10."""
+    ns = 1
+    p, o, g = _pair(L, False, 2, nw, ns, seed=150 + L)
+    x = _configs(L * L, nw * ns, seed=L + 2)
+    o.seed(2025)
+    g.seed(2025)
+    o.set_samples(x)
+    g.set_samples(x)
+    mo = o.measure_correlation()
+    mg = g.measure_correlation()
+    for k in ("Etot", "Etot2", "norm", "wf_av", "wf_sgn"):
+        assert abs(mg[k] - mo[k]) <= RTOL * abs(mo[k]), k
+    assert _rel(mg["chi_sp"], mo["chi_sp"]) < RTOL
+    assert _rel(mg["chi_vbs"], mo["chi_vbs"]) < RTOL
+    g.close()
