@@ -27,8 +27,7 @@ struct Stream {
   double* stage;  // [ST][Np*Np]; also the Gauss-Jordan tile outside passes
   uint64_t* full;
   uint64_t* empty;
-  double* pS;     // [kPairs][Np] row sums Y v of the deferred exchange (each half writes its rows)
-  double* pA;     // [kPairs][Np] column ua of Y
+  double* pAS;    // [kPairs][Np][2] (A_j, S_j) = (Y(j, ua), (Y v)_j) of the deferred exchange (each half its rows)
   double* pscal;  // [kPairs][2 slots][2 halves][4] ratio terms of each half
   int ST;
   uint32_t tile_bytes;
@@ -51,8 +50,7 @@ __host__ __device__ __forceinline__ size_t stream_layout(const DevDims& d, int S
   t.stage = (double*)take(stage_bytes > gj ? stage_bytes : gj, 128);
   t.full = (uint64_t*)take(8 * (size_t)ST, 8);
   t.empty = (uint64_t*)take(8 * (size_t)ST, 8);
-  t.pS = (double*)take((size_t)kPairs * d.Np * 8, 16);
-  t.pA = (double*)take((size_t)kPairs * d.Np * 8, 16);
+  t.pAS = (double*)take((size_t)kPairs * d.Np * 16, 16);
   t.pscal = (double*)take((size_t)kPairs * 16 * 8, 16);
   if (w) w->tile = t.stage;
   if (st) *st = t;
@@ -63,59 +61,53 @@ struct Move {
   int ua, db, s_up, s_dn;  // up electron, down electron (local index), their sites before the move
 };
 
-// Tile math is templated on KPL (columns per lane) and NP: NP > 0 is the block size Np known at compile time
-// (the even-L lattices 4x4 .. 10x10 have Np = 8, 18, 32, 50), so loops unroll fully and tile addresses
-// become immediate offsets; NP = 0 reads Np from the dimensions.
-template <int NP>
-__device__ __forceinline__ int np_of(const DevDims& d) {
-  return NP > 0 ? NP : d.Np;
-}
+// Tile math.  NP is the block size Np, a compile-time constant: the even-L square lattices 4x4 .. 10x10 have
+// Np = 8, 18, 32, 50, the shapes this sampler takes.  Lane l of a consumer warp owns the column pair
+// (2l, 2l+1) of every tile row, so a row is read and written with one 16-byte shared access per lane (rows
+// start on 16-byte boundaries because Np is even).  Lanes with 2l >= NP hold nothing.
+__device__ __forceinline__ double2 ld2(const double* p) { return *reinterpret_cast<const double2*>(p); }
+__device__ __forceinline__ void st2(double* p, double2 v) { *reinterpret_cast<double2*>(p) = v; }
 
-// Lane-held gathers of one exchange for one projection: u = new row ua of X, v = new column db of X,
-// c = their shared corner (the gathers of pfupdate_two.f90:48-52 in block form).
-template <int KPL>
+// Lane-held gathers of one exchange for one projection at the lane's column pair: u = new row ua of X,
+// v = new column db of X, c = their shared corner, which u holds at column db and v at column ua (the
+// gathers of pfupdate_two.f90:48-52 in block form).
 struct UV {
-  double u[KPL], v[KPL], c;
+  double2 u, v;
+  double c;
 };
 
-template <int KPL, int NP>
+template <int NP>
 __device__ __forceinline__ void gather_regs(const DevDims& d, const DevParams& p, int qp, const int* idx,
-                                            const Move& m, UV<KPL>& g) {
-  const int lane = threadIdx.x & 31, Np = np_of<NP>(d), N = d.N;
-  const double* XFq = p.XF + (size_t)qp * N * N;
-  const double* XFTq = p.XFT + (size_t)qp * N * N;
-  g.c = __ldg(XFq + (size_t)m.s_dn * N + m.s_up);
-#pragma unroll
-  for (int q = 0; q < KPL; q++) {
-    const int j = lane + 32 * q;
-    g.u[q] = 0.0;
-    g.v[q] = 0.0;
-    if (j < Np) {
-      g.u[q] = (j == m.db) ? 0.0 : __ldg(XFq + (size_t)m.s_dn * N + idx[Np + j]);
-      g.v[q] = (j == m.ua) ? 0.0 : __ldg(XFTq + (size_t)m.s_up * N + idx[j]);
-    }
+                                            const Move& m, UV& g) {
+  const int k = 2 * (threadIdx.x & 31), N = d.N;
+  const double* xr = p.XF + (size_t)qp * N * N + (size_t)m.s_dn * N;
+  const double* xc = p.XFT + (size_t)qp * N * N + (size_t)m.s_up * N;
+  g.c = __ldg(xr + m.s_up);
+  g.u = make_double2(0.0, 0.0);
+  g.v = make_double2(0.0, 0.0);
+  if (k < NP) {
+    const int2 iu = *reinterpret_cast<const int2*>(idx + NP + k);
+    const int2 iv = *reinterpret_cast<const int2*>(idx + k);
+    g.u.x = (k == m.db) ? g.c : __ldg(xr + iu.x);
+    g.u.y = (k + 1 == m.db) ? g.c : __ldg(xr + iu.y);
+    g.v.x = (k == m.ua) ? g.c : __ldg(xc + iv.x);
+    g.v.y = (k + 1 == m.ua) ? g.c : __ldg(xc + iv.y);
   }
 }
 
-template <int KPL, int NP>
-__device__ __forceinline__ double store_regs(const DevDims& d, const Move& m, const UV<KPL>& g, double* u, double* v) {
-  const int lane = threadIdx.x & 31, Np = np_of<NP>(d);
-#pragma unroll
-  for (int q = 0; q < KPL; q++) {
-    const int j = lane + 32 * q;
-    if (j < Np) {
-      u[j] = (j == m.db) ? g.c : g.u[q];
-      v[j] = (j == m.ua) ? g.c : g.v[q];
-    }
-  }
-  return g.c;
+// u (and v) of the lane's columns into the warp's shared vectors
+template <int NP>
+__device__ __forceinline__ void store_u(const UV& g, double* u) {
+  const int k = 2 * (threadIdx.x & 31);
+  if (k < NP) st2(u + k, g.u);
 }
-
-// Rows [r0, r1) of half h of a pair: the first (Np+1)/2 rows, or the rest.
-__device__ __forceinline__ void half_rows(int Np, int h, int& r0, int& r1) {
-  const int m = (Np + 1) >> 1;
-  r0 = h ? m : 0;
-  r1 = h ? Np : m;
+template <int NP>
+__device__ __forceinline__ void store_uv(const UV& g, double* u, double* v) {
+  const int k = 2 * (threadIdx.x & 31);
+  if (k < NP) {
+    st2(u + k, g.u);
+    st2(v + k, g.v);
+  }
 }
 
 // Barrier of the two warps of pair g (named barrier 1 + g, 64 threads) that also returns, on every thread,
@@ -133,133 +125,118 @@ __device__ __forceinline__ bool pair_sync_or(int g, bool flag) {
   return out != 0;
 }
 
-// acc[q] = sum over rows r0 .. r0+nr-1 of u_j Y[j][k], k = lane + 32 q, as two interleaved FMA chains
-template <int KPL, int NP>
-__device__ __forceinline__ void col_sums_rows(const double* Y, const double* u, int Np, int r0, int nr,
-                                              double (&acc)[KPL]) {
-  const int lane = threadIdx.x & 31;
-  double a1[KPL];
+// (u^T Y)_k at the lane's column pair over the NR rows r0 .. r0+NR-1 (one half of a tile), as two
+// interleaved FMA chains per column (even and odd rows).
+template <int NP, int NR>
+__device__ __forceinline__ double2 col_sums(const double* Y, const double* u, int r0) {
+  const int k = 2 * (threadIdx.x & 31);
+  double2 a = make_double2(0.0, 0.0), b = make_double2(0.0, 0.0);
+  if (k < NP) {
+    const double* y = Y + r0 * NP + k;
+    const double* uu = u + r0;
 #pragma unroll
-  for (int q = 0; q < KPL; q++) acc[q] = a1[q] = 0.0;
-#pragma unroll 4
-  for (int jj = 0; jj + 1 < nr; jj += 2) {
-    const int j = r0 + jj;
-    const double u0 = u[j], u1 = u[j + 1];
-#pragma unroll
-    for (int q = 0; q < KPL; q++) {
-      const int k = lane + 32 * q;
-      if (k < Np) {
-        acc[q] = fma(u0, Y[j * Np + k], acc[q]);
-        a1[q] = fma(u1, Y[(j + 1) * Np + k], a1[q]);
-      }
+    for (int jj = 0; jj + 1 < NR; jj += 2) {
+      const double2 y0 = ld2(y + jj * NP), y1 = ld2(y + (jj + 1) * NP);
+      const double u0 = uu[jj], u1 = uu[jj + 1];
+      a.x = fma(u0, y0.x, a.x);
+      a.y = fma(u0, y0.y, a.y);
+      b.x = fma(u1, y1.x, b.x);
+      b.y = fma(u1, y1.y, b.y);
+    }
+    if (NR & 1) {
+      const double2 y0 = ld2(y + (NR - 1) * NP);
+      const double u0 = uu[NR - 1];
+      a.x = fma(u0, y0.x, a.x);
+      a.y = fma(u0, y0.y, a.y);
     }
   }
-  if (nr & 1) {
-    const int j = r0 + nr - 1;
-#pragma unroll
-    for (int q = 0; q < KPL; q++) {
-      const int k = lane + 32 * q;
-      if (k < Np) acc[q] = fma(u[j], Y[j * Np + k], acc[q]);
-    }
-  }
-#pragma unroll
-  for (int q = 0; q < KPL; q++) acc[q] += a1[q];
+  return make_double2(a.x + b.x, a.y + b.y);
 }
 
-// value of acc at column k0, taken from the lane that owns it (valid on all lanes)
-template <int KPL>
-__device__ __forceinline__ double lane_pick(const double (&acc)[KPL], int k0) {
-  double mine = 0.0;
-#pragma unroll
-  for (int q = 0; q < KPL; q++)
-    if (q == (k0 >> 5)) mine = acc[q];
-  return __shfl_sync(0xffffffffu, mine, k0 & 31);
+// value of a lane-pair vector at column col, taken from the lane that owns it (valid on all lanes)
+__device__ __forceinline__ double pick(double2 a, int col) {
+  return __shfl_sync(0xffffffffu, (col & 1) ? a.y : a.x, col >> 1);
 }
 
-// rows counted by half h; a compile-time constant for even NP
+// (Y v)_j for row j (one row per lane).  The column pairs are visited in the order c ^ sig(j): rows are NP/2
+// 16-byte words apart, so when gcd(NP/2, 8) = G > 1 the rows of a quarter-warp fall G to a bank group, and
+// sig(j) in [0, G) moves those G rows onto distinct groups (G = 1 for NP = 18, 50: sig = 0 at compile time).
 template <int NP>
-__device__ __forceinline__ int half_count(int r0, int r1) {
-  return (NP > 0 && (NP & 1) == 0) ? NP / 2 : r1 - r0;
+__device__ __forceinline__ double row_dot(const double* Y, const double* v, int j) {
+  constexpr int M2 = NP / 2;
+  constexpr int G = (M2 & -M2) < 8 ? (M2 & -M2) : 8;
+  const int sig = (j / (8 / G)) & (G - 1);
+  const double* yr = Y + j * NP;
+  double a0 = 0.0, a1 = 0.0;
+#pragma unroll
+  for (int cc = 0; cc < M2; cc++) {
+    const int c2 = 2 * (cc ^ sig);
+    const double2 y = ld2(yr + c2), w = ld2(v + c2);
+    a0 = fma(y.x, w.x, a0);
+    a1 = fma(y.y, w.y, a1);
+  }
+  return a0 + a1;
 }
 
-// Half h of the deferred rank-2 update of a tile for an accepted exchange (the algebra of
+// Half h (rows h*NP/2 .. ) of the deferred rank-2 update of a tile for an accepted exchange (the algebra of
 // pfupdate_two.f90:113-224 in block form): Y' = Y - A B^T / R1 - s1 t1^T / R2, with A = Y e_ua,
 // B = u^T Y - e_ua^T, s1 = Y v - A (u^T Y v - c)/R1 - e_db, t1 = e_db^T Y - Y(db,ua) B^T / R1, R2 = R / R1.
-// Each half forms its rows' part of u^T Y, Y v and A, the pair exchanges them at one barrier, and each half
-// rewrites its own rows.  bad enters as this warp's failure flag and leaves as the pair's (uniform).
-template <int KPL, int NP>
-__device__ __forceinline__ bool update_half(const DevDims& d, double* Y, const Move& m, double c, const double* u,
-                                            const double* v, int g, int h, double* my_acc, const double* other_acc,
-                                            double* pS, double* pA, bool bad) {
-  const int lane = threadIdx.x & 31, Np = np_of<NP>(d);
-  int r0, r1;
-  half_rows(Np, h, r0, r1);
-  const int nr = half_count<NP>(r0, r1);
-  double accp[KPL], rho[KPL];
+// With S = Y v, bk = B / R1, tk = t1 / R2 and wc = (u^T Y v - c) / R1 this is
+//   Y'_jk = Y_jk - A_j (bk_k - wc tk_k) - S_j tk_k + [j = db] tk_k,
+// one pass over the rows with (A_j, S_j) read as one 16-byte word.  Each half forms its rows' part of u^T Y
+// and its rows' A and S, the pair exchanges them at one barrier, and each half rewrites its own rows.
+// bad enters as this warp's failure flag and leaves as the pair's (uniform).
+template <int NP>
+__device__ __forceinline__ bool update_half(double* Y, const Move& m, double c, const double* u, const double* v,
+                                            int g, int h, double* my_acc, const double* other_acc, double* pAS,
+                                            bool bad) {
+  constexpr int NR = NP / 2;
+  const int lane = threadIdx.x & 31, k = 2 * lane, r0 = h * NR;
+  double2 accp = make_double2(0.0, 0.0), rho = make_double2(0.0, 0.0);
   double ydbua = 0.0;
   if (!bad) {
-    col_sums_rows<KPL, NP>(Y, u, Np, r0, nr, accp);
-    // this half's row sums S = Y v (lane <-> row; each lane starts at its own column so the 64-bit shared
-    // loads of a half-warp fall in distinct banks) and its part of column ua
-    const int j = r0 + lane;
-    if (lane < nr) {
-      double a0 = 0.0, a1 = 0.0;
-      int k = j;
-#pragma unroll 5
-      for (int kk = 0; kk + 1 < Np; kk += 2) {
-        const int k1 = (k + 1 == Np) ? 0 : k + 1;
-        a0 = fma(Y[j * Np + k], v[k], a0);
-        a1 = fma(Y[j * Np + k1], v[k1], a1);
-        k = (k1 + 1 == Np) ? 0 : k1 + 1;
-      }
-      if (Np & 1) a0 = fma(Y[j * Np + k], v[k], a0);
-      pS[j] = a0 + a1;
-      pA[j] = Y[j * Np + m.ua];
+    accp = col_sums<NP, NR>(Y, u, r0);
+    if (lane < NR) {
+      const int j = r0 + lane;
+      st2(pAS + 2 * j, make_double2(Y[j * NP + m.ua], row_dot<NP>(Y, v, j)));
     }
-#pragma unroll
-    for (int q = 0; q < KPL; q++) {
-      const int k = lane + 32 * q;
-      rho[q] = 0.0;
-      if (k < Np) {
-        rho[q] = Y[m.db * Np + k];  // row db, read before either half rewrites it
-        my_acc[k] = accp[q];
-      }
+    if (k < NP) {
+      rho = ld2(Y + m.db * NP + k);  // row db, read before either half rewrites it
+      st2(my_acc + k, accp);
     }
-    ydbua = Y[m.db * Np + m.ua];
+    ydbua = Y[m.db * NP + m.ua];
   }
   if (pair_sync_or(g, bad)) return true;
-  double acc[KPL], wv = 0.0;
-#pragma unroll
-  for (int q = 0; q < KPL; q++) {
-    const int k = lane + 32 * q;
-    acc[q] = 0.0;
-    if (k < Np) {
-      const double o = other_acc[k];
-      acc[q] = h == 0 ? accp[q] + o : o + accp[q];  // both halves form acc_0 + acc_1
-      wv = fma(acc[q], v[k], wv);
-    }
+  double2 acc = make_double2(0.0, 0.0);
+  double wv = 0.0;
+  if (k < NP) {
+    const double2 o = ld2(other_acc + k), vk = ld2(v + k);
+    acc = make_double2(accp.x + o.x, accp.y + o.y);  // both halves form the same sums (addition commutes)
+    wv = fma(acc.y, vk.y, acc.x * vk.x);
   }
-  const double ra = lane_pick<KPL>(acc, m.ua);
+  const double ra = pick(acc, m.ua);
   wv = warp_sum(wv);
-  const double R1 = ra, R = ra * pS[m.db] - ydbua * (wv - c);
+  const double R1 = ra, R = ra * pAS[2 * m.db + 1] - ydbua * (wv - c);
   const double inv_r1 = 1.0 / R1, r1_over_r = R1 / R, wc = (wv - c) * inv_r1;
-  double bk[KPL], tk[KPL];
-#pragma unroll
-  for (int q = 0; q < KPL; q++) {
-    const int k = lane + 32 * q;
-    const double B = acc[q] - (k == m.ua ? 1.0 : 0.0);
-    bk[q] = B * inv_r1;
-    tk[q] = (rho[q] - ydbua * B * inv_r1) * r1_over_r;
-  }
+  const double bx = (acc.x - (k == m.ua ? 1.0 : 0.0)) * inv_r1, by = (acc.y - (k + 1 == m.ua ? 1.0 : 0.0)) * inv_r1;
+  const double tx = (rho.x - ydbua * bx) * r1_over_r, ty = (rho.y - ydbua * by) * r1_over_r;
+  const double cx = bx - wc * tx, cy = by - wc * ty;
+  if (k < NP) {
+    double* y = Y + r0 * NP + k;
+    const double* as = pAS + 2 * r0;
 #pragma unroll 5
-  for (int jj = 0; jj < nr; jj++) {
-    const int j = r0 + jj;
-    const double Aj = pA[j];
-    const double s1 = pS[j] - Aj * wc - (j == m.db ? 1.0 : 0.0);
-#pragma unroll
-    for (int q = 0; q < KPL; q++) {
-      const int k = lane + 32 * q;
-      if (k < Np) Y[j * Np + k] = Y[j * Np + k] - Aj * bk[q] - s1 * tk[q];
+    for (int jj = 0; jj < NR; jj++) {
+      const double2 a = ld2(as + 2 * jj);
+      double2 yv = ld2(y + jj * NP);
+      yv.x = yv.x - a.x * cx - a.y * tx;
+      yv.y = yv.y - a.x * cy - a.y * ty;
+      st2(y + jj * NP, yv);
+    }
+    if (m.db >= r0 && m.db < r0 + NR) {
+      double2 yv = ld2(Y + m.db * NP + k);
+      yv.x += tx;
+      yv.y += ty;
+      st2(Y + m.db * NP + k, yv);
     }
   }
   __syncwarp();
@@ -268,40 +245,30 @@ __device__ __forceinline__ bool update_half(const DevDims& d, double* Y, const M
 
 // Half h's terms of the ratio R = (u^T Y)_ua (Y v)_db - Y(db,ua) (u^T Y v - c): its rows' part of u^T Y v
 // and of (u^T Y)_ua, and, from the half that holds row db, (Y v)_db and Y(db,ua).  v comes from the
-// lane's registers (columns lane + 32 q).  Lane 0 writes them to scal[0..3].
-template <int KPL, int NP>
-__device__ __forceinline__ void ratio_half(const DevDims& d, const double* Y, const Move& m, double c, const double* u,
-                                           const UV<KPL>& g, int h, double* scal) {
-  const int lane = threadIdx.x & 31, Np = np_of<NP>(d);
-  int r0, r1;
-  half_rows(Np, h, r0, r1);
-  double acc[KPL];
-  col_sums_rows<KPL, NP>(Y, u, Np, r0, half_count<NP>(r0, r1), acc);
-  const bool owner = m.db >= r0 && m.db < r1;
-  double wv = 0.0, sb = 0.0;
-#pragma unroll
-  for (int q = 0; q < KPL; q++) {
-    const int k = lane + 32 * q;
-    if (k < Np) {
-      const double vk = (k == m.ua) ? c : g.v[q];
-      wv = fma(acc[q], vk, wv);
-      if (owner) sb = fma(Y[m.db * Np + k], vk, sb);
-    }
-  }
-  const double ra = lane_pick<KPL>(acc, m.ua);
-#pragma unroll
-  for (int o = 16; o > 0; o >>= 1) {
-    wv += __shfl_xor_sync(0xffffffffu, wv, o);
-    sb += __shfl_xor_sync(0xffffffffu, sb, o);
-  }
-  if (lane == 0) {
-    scal[0] = wv;
-    scal[1] = ra;
+// lane's registers.  The two warp sums share one shuffle tree; lanes 0 and 16 write scal[0..3].
+template <int NP>
+__device__ __forceinline__ void ratio_half(const double* Y, const Move& m, const double* u, const UV& g, int h,
+                                           double* scal) {
+  constexpr int NR = NP / 2;
+  const int lane = threadIdx.x & 31, k = 2 * lane, r0 = h * NR;
+  const double2 acc = col_sums<NP, NR>(Y, u, r0);
+  const bool owner = m.db >= r0 && m.db < r0 + NR;
+  double t[2] = {0.0, 0.0};  // u^T Y v, (Y v)_db
+  if (k < NP) {
+    t[0] = fma(acc.y, g.v.y, acc.x * g.v.x);
     if (owner) {
-      scal[2] = sb;
-      scal[3] = Y[m.db * Np + m.ua];
+      const double2 yd = ld2(Y + m.db * NP + k);
+      t[1] = fma(yd.y, g.v.y, yd.x * g.v.x);
     }
   }
+  const double ra = pick(acc, m.ua);
+  const double s = warp_transpose_sum<2>(t, lane);  // lanes 0-15: sum of t[0]; lanes 16-31: sum of t[1]
+  if (lane == 0) {
+    scal[0] = s;
+    scal[1] = ra;
+    if (owner) scal[3] = Y[m.db * NP + m.ua];
+  }
+  if (lane == 16 && owner) scal[2] = s;
 }
 
 struct Pipe {
@@ -410,7 +377,7 @@ __device__ __forceinline__ bool pass_consume(const SCtx& c, const Stream& sm, co
                                              const int* mv, double& pre, double& pim, volatile int* abort_flag) {
   const DevDims& d = c.d;
   const WS& s = c.s;
-  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, Np = d.Np, n = d.n_qp;
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, Np = NP, n = d.n_qp;
   const int cw = warp - 1, g = cw >> 1, h = cw & 1, partner = 1 + 2 * g + (1 - h);
   const size_t NN = (size_t)Np * Np;
   double* u = s.wu + (size_t)warp * Np;
@@ -418,29 +385,29 @@ __device__ __forceinline__ bool pass_consume(const SCtx& c, const Stream& sm, co
   double* V0 = s.wv + (size_t)warp * Np;
   double* my_acc = s.wS + (size_t)warp * Np;
   const double* other_acc = s.wS + (size_t)partner * Np;
-  double* pS = sm.pS + (size_t)g * Np;
-  double* pA = sm.pA + (size_t)g * Np;
+  double* pAS = sm.pAS + (size_t)g * 2 * Np;
   double* pscal = sm.pscal + (size_t)g * 16;
-  UV<KPL> gk, gn;
+  UV gk, gn;
   Move mn{0, 0, 0, 0};
   bool have_move = false, stored = false;
   int slot = 0;
   int t = g;
-  if (pend && t < n) gather_regs<KPL, NP>(d, c.p, t, s.idx, mk, gk);
+  if (pend && t < n) gather_regs<NP>(d, c.p, t, s.idx, mk, gk);
   for (; t < n; t += kPairs) {
     const uint32_t T = pp.T0 + t;
     const int st = (int)(T % sm.ST);
     const int tn = t + kPairs;
     double ck = 0.0;
     if (pend) {
-      ck = store_regs<KPL, NP>(d, mk, gk, U0, V0);
-      if (tn < n) gather_regs<KPL, NP>(d, c.p, tn, s.idx, mk, gk);
+      store_uv<NP>(gk, U0, V0);
+      ck = gk.c;
+      if (tn < n) gather_regs<NP>(d, c.p, tn, s.idx, mk, gk);
     }
     __syncwarp();
     bool bad = (*abort_flag != 0) || !mbar_wait(&sm.full[st], (T / sm.ST) & 1u, wait_polls(c));
     double* Y = sm.stage + (size_t)st * NN;
     if (pend) {
-      if (update_half<KPL, NP>(d, Y, mk, ck, U0, V0, g, h, my_acc, other_acc, pS, pA, bad)) return false;
+      if (update_half<NP>(Y, mk, ck, U0, V0, g, h, my_acc, other_acc, pAS, bad)) return false;
       fence_proxy_async_smem();
     }
     double* sc = pscal + slot * 8 + h * 4;
@@ -462,14 +429,15 @@ __device__ __forceinline__ bool pass_consume(const SCtx& c, const Stream& sm, co
         if (!bad) {
           mn = Move{mv[0], mv[1], mv[2], mv[3]};
           have_move = true;
-          gather_regs<KPL, NP>(d, c.p, t, s.idx, mn, gn);
+          gather_regs<NP>(d, c.p, t, s.idx, mn, gn);
         }
       }
       if (!bad) {
-        cn = store_regs<KPL, NP>(d, mn, gn, u, V0);
+        store_u<NP>(gn, u);
+        cn = gn.c;
         __syncwarp();
-        ratio_half<KPL, NP>(d, Y, mn, cn, u, gn, h, sc);
-        if (tn < n) gather_regs<KPL, NP>(d, c.p, tn, s.idx, mn, gn);
+        ratio_half<NP>(Y, mn, u, gn, h, sc);
+        if (tn < n) gather_regs<NP>(d, c.p, tn, s.idx, mn, gn);
       }
     }
     if (pair_sync_or(g, bad)) return false;
@@ -477,7 +445,7 @@ __device__ __forceinline__ bool pass_consume(const SCtx& c, const Stream& sm, co
       if (prop) {
         const double* s0 = pscal + slot * 8;
         const double* s1 = s0 + 4;
-        const double* so = (mn.db < ((Np + 1) >> 1)) ? s0 : s1;
+        const double* so = (mn.db < NP / 2) ? s0 : s1;
         const double wv = s0[0] + s1[0], ra = s0[1] + s1[1];
         const double R = ra * so[2] - so[3] * (wv - cn);
         const double pfn = R * s.pf[t];
@@ -737,7 +705,7 @@ int rbmpp_stream_stages(const DevDims& d, int max_smem) {
   // pass then belong to the same pair, so a pair never waits on a stage two loads ahead of it, where the
   // mbarrier's phase parity could not tell the two loads apart.  No fallback to fewer stages: the
   // direct sampler takes shapes whose stages do not fit.
-  if (d.Np > 64) return 0;
+  if (d.Np != 8 && d.Np != 18 && d.Np != 32 && d.Np != 50) return 0;  // the compiled block sizes
   const int st = d.n_qp < kPairs ? d.n_qp : kPairs;
   return (long long)stream_layout(d, st, nullptr, nullptr, nullptr) <= max_smem ? st : 0;
 }
@@ -747,7 +715,6 @@ size_t rbmpp_stream_smem(const DevDims& d, int st) { return stream_layout(d, st,
 cudaError_t rbmpp_launch_sampler_stream(const DevDims& d, const DevTables& t, const DevParams& p, const DevWalkers& W,
                                         int first, int st, cudaStream_t stream) {
   size_t smem = rbmpp_stream_smem(d, st);
-  int kpl = (d.Np + 31) / 32;
 #define LAUNCH(K, NPC)                                                                                        \
   do {                                                                                                        \
     cudaError_t e = cudaFuncSetAttribute(sampler_stream_kernel<K, NPC>,                                       \
@@ -763,8 +730,6 @@ cudaError_t rbmpp_launch_sampler_stream(const DevDims& d, const DevTables& t, co
     case 50: LAUNCH(2, 50);
     default: break;
   }
-  if (kpl <= 1) LAUNCH(1, 0);
-  if (kpl <= 2) LAUNCH(2, 0);
 #undef LAUNCH
   return cudaErrorInvalidValue;
 }
