@@ -1,32 +1,38 @@
 // sampler_stream.cu -- Metropolis sampler that streams each walker's projections through shared memory
 // with TMA bulk copies (make_sample.f90:4-240, same RNG order as sampler.cu).
 //
-// One CTA per walker.  Warp 0 is the control warp: its lane 0 draws every random number and issues the
-// bulk loads, and the warp evaluates theta' and the cosh products of the proposal.  Warps 1..14 are seven
-// pairs of consumers.  A tile is one projection's Y = X^{-1} (Np x Np FP64, row major), and each pair
-// works on one tile at a time, each warp of the pair on half of its rows.  Every proposal is one pass over
-// the n_qp tiles through an ST-stage ring:
-//   producer:  cp.async.bulk global->shared (mbarrier complete_tx) into a stage as soon as it is released;
-//   pair:      applies the deferred rank-2 update of the previously accepted exchange (if any) to the tile
-//              in place, evaluates the determinant ratio of the current proposal on it, writes an updated
-//              tile back with cp.async.bulk shared->global, and releases the stage.
+// One CTA per walker.  Warp 0 is the control warp: its lane 0 draws every random number, and the warp
+// evaluates theta', the cosh products and the amplitude weights of the proposal.  Warp 1 is the producer
+// (its lane 0 issues the bulk loads).  Warps 2..15 are seven pairs of consumers.  A tile is one projection's
+// Y = X^{-1} (Np x Np FP64, row major); pair g takes tiles g, g + 7, ..., each warp of the pair half of the
+// rows.  Every proposal is one pass over the n_qp tiles through an ST-stage ring, ST >= 7 where shared
+// memory allows, so that loads are in flight while every pair computes:
+//   producer:  cp.async.bulk global->shared (mbarrier complete_tx) into stage T mod ST as soon as tile
+//              T - ST has released it, after posting the stage's ticket T;
+//   pair:      waits for the ticket and the load, applies the deferred rank-2 update of the previously
+//              accepted exchange (if any) to the tile in place, evaluates the determinant ratio of the
+//              current proposal on it, writes an updated tile back with cp.async.bulk shared->global, and
+//              releases the stage.
 // The halves combine only vectors and scalars (partial column sums, row db, the ratio's terms) through
 // shared memory at two pair barriers per tile.  A proposal costs one read of Y and an accepted move one
 // write: the algorithmic minimum (pfupdate_two.f90 reads InvM once per ratio and rewrites it per accepted
-// move).  The first tiles of a pass are requested before the candidate is drawn, and the pairs apply the
-// deferred update while the control warp draws the candidate.
+// move).  The producer starts a pass at once; the control warp publishes the candidate as soon as it is
+// drawn and computes theta' and the weights while the pairs work, and the amplitude of the proposal is
+// summed after the pass.
 #include "sampler_common.cuh"
 
 namespace {
 
 constexpr int kPairs = 7;
-constexpr int kWarps = 1 + 2 * kPairs;  // warp 0: control (RNG, candidate, theta', producer); 1..14: pairs
+constexpr int kWarps = 2 + 2 * kPairs;  // warp 0: control (RNG, candidate, theta'); 1: producer; 2..15: pairs
+constexpr int kMaxStages = 16;
 #define ST_TIMEOUT 22
 
 struct Stream {
   double* stage;  // [ST][Np*Np]; also the Gauss-Jordan tile outside passes
   uint64_t* full;
   uint64_t* empty;
+  int* ticket;    // [ST] tile index last issued into the stage (the producer posts it before the load)
   double* pAS;    // [kPairs][Np][2] (A_j, S_j) = (Y(j, ua), (Y v)_j) of the deferred exchange (each half its rows)
   double* pscal;  // [kPairs][2 slots][2 halves][4] ratio terms of each half
   int ST;
@@ -50,6 +56,7 @@ __host__ __device__ __forceinline__ size_t stream_layout(const DevDims& d, int S
   t.stage = (double*)take(stage_bytes > gj ? stage_bytes : gj, 128);
   t.full = (uint64_t*)take(8 * (size_t)ST, 8);
   t.empty = (uint64_t*)take(8 * (size_t)ST, 8);
+  t.ticket = (int*)take(4 * (size_t)ST, 4);
   t.pAS = (double*)take((size_t)kPairs * d.Np * 16, 16);
   t.pscal = (double*)take((size_t)kPairs * 16 * 8, 16);
   if (w) w->tile = t.stage;
@@ -272,9 +279,12 @@ __device__ __forceinline__ void ratio_half(const double* Y, const Move& m, const
 }
 
 struct Pipe {
-  uint32_t T0;          // tiles issued before this pass (same value in every thread)
-  int last_issued[16];  // per stage: last tile index loaded (thread 0 only), -1 if none
+  uint32_t T0;                  // tiles issued before this pass (same value in every thread)
+  int last_issued[kMaxStages];  // per stage: last tile index loaded (producer thread only), -1 if none
 };
+
+// Thread of warp 1 that issues the bulk loads; its Pipe::last_issued is the one that counts.
+constexpr int kProducerThread = 32;
 
 // Verification hook: walker 0 never issues load number skip_load (1-based over the launch), so the consumer's
 // bounded wait on it runs out and the CTA takes its timeout path.  The load is not recorded as issued.
@@ -283,51 +293,69 @@ __device__ __forceinline__ bool skipped_load(const SCtx& c, uint32_t T) {
 }
 __device__ __forceinline__ int wait_polls(const SCtx& c) { return c.d.wait_polls > 0 ? c.d.wait_polls : (1 << 22); }
 
-// producer (thread 0): first min(ST, n_qp) loads of a pass.  Every store of the previous pass has
-// completed: the consumer that issued it waited for it before the pass-ending barrier.
-__device__ __forceinline__ void pass_issue_first(const SCtx& c, const Stream& sm, Pipe& pp) {
-  const int n = c.d.n_qp, n0 = n < sm.ST ? n : sm.ST;
-  fence_proxy_async_global();
+// Load of tile t (global index T) into its stage: the ticket first, so that a consumer waiting on the stage
+// knows that the stage's previous load was consumed and the full barrier's next phase is this load's.
+__device__ __forceinline__ void issue_tile(const SCtx& c, const Stream& sm, Pipe& pp, int t, uint32_t T) {
   const size_t NN = (size_t)c.d.Np * c.d.Np;
-  for (int t = 0; t < n0; t++) {
-    uint32_t T = pp.T0 + t;
-    int s = (int)(T % sm.ST);
-    if (skipped_load(c, T)) continue;
-    mbar_arrive_expect_tx(&sm.full[s], sm.tile_bytes);
-    bulk_load(sm.stage + (size_t)s * NN, c.Yw + (size_t)t * NN, sm.tile_bytes, &sm.full[s]);
-    pp.last_issued[s] = (int)T;
-  }
+  const int s = (int)(T % sm.ST);
+  if (skipped_load(c, T)) return;
+  *(volatile int*)&sm.ticket[s] = (int)T;
+  __threadfence_block();
+  mbar_arrive_expect_tx(&sm.full[s], sm.tile_bytes);
+  bulk_load(sm.stage + (size_t)s * NN, c.Yw + (size_t)t * NN, sm.tile_bytes, &sm.full[s]);
+  pp.last_issued[s] = (int)T;
 }
 
-// producer (thread 0): refill each stage as soon as its consumer releases it
+// Producer (one thread): the first min(ST, n_qp) loads of a pass at once (every stage was released in the
+// previous pass and every store of that pass has completed: the consumer that issued it waited for it before
+// the pass-ending barrier), then each further load as soon as the stage's previous tile is released.  The
+// waits on a release give up after wait_polls polls, or when a consumer has aborted the pass.
 __device__ __forceinline__ bool pass_produce(const SCtx& c, const Stream& sm, Pipe& pp, volatile int* abort_flag) {
-  const int n = c.d.n_qp, ST = sm.ST;
-  const size_t NN = (size_t)c.d.Np * c.d.Np;
+  const int n = c.d.n_qp, ST = sm.ST, n0 = n < ST ? n : ST;
+  fence_proxy_async_global();
+  for (int t = 0; t < n0; t++) issue_tile(c, sm, pp, t, pp.T0 + t);
+  const int polls = wait_polls(c);
   for (int t = ST; t < n; t++) {
-    uint32_t T = pp.T0 + t, Tp = T - ST;
-    int s = (int)(T % ST);
-    if (!mbar_wait(&sm.empty[s], (Tp / ST) & 1u, wait_polls(c))) return false;
-    if (*abort_flag) return false;
-    if (skipped_load(c, T)) continue;
-    mbar_arrive_expect_tx(&sm.full[s], sm.tile_bytes);
-    bulk_load(sm.stage + (size_t)s * NN, c.Yw + (size_t)t * NN, sm.tile_bytes, &sm.full[s]);
-    pp.last_issued[s] = (int)T;
+    const uint32_t T = pp.T0 + t, Tp = T - ST;
+    const int s = (int)(T % ST);
+    bool released = false;
+    for (int it = 0; it < polls && !released; it++) {
+      released = mbar_try_wait(&sm.empty[s], (Tp / ST) & 1u);
+      if (!released && *abort_flag) return false;
+    }
+    if (!released || *abort_flag) return false;
+    issue_tile(c, sm, pp, t, T);
   }
   return true;
 }
 
-// Control warp, proposal pass: candidate (thread 0), then theta', sgn', cosh products on the warp,
-// then publish the move to the consumers (who meanwhile apply the deferred update).
+// Consumer side of a stage's ticket: true once the producer has posted tile T on it (bounded; gives up when
+// the pass is aborted).
+__device__ __forceinline__ bool wait_ticket(const Stream& sm, int st, uint32_t T, int polls, volatile int* abort_flag) {
+  for (int it = 0; it < polls; it++) {
+    if (*(volatile int*)&sm.ticket[st] == (int)T) {
+      __threadfence_block();
+      return true;
+    }
+    if (*abort_flag) return false;
+    __nanosleep(32);
+  }
+  return false;
+}
+
+// Control warp, proposal pass: the candidate (thread 0), published to the pairs at once; then, while the
+// pairs work, theta', sgn' and the cosh products on the warp, and the weight psi_wo_pf of every projection
+// into psip (the pass's end multiplies it by the new Pfaffian).  A failed candidate search is published too:
+// the pairs read the status.
 __device__ __forceinline__ void control_propose(const SCtx& c, volatile int* cand_flag, int pass_id, int* mv) {
   const DevDims& d = c.d;
   const WS& s = c.s;
   const int lane = threadIdx.x & 31;
-  if (lane == 0) candidate_search(c);
-  __syncwarp();
-  if (!status(c)) {
-    const int i1 = s.iflag[F_I1], i2 = s.iflag[F_I2];
-    const int i3 = s.cfg[i1], i4 = s.cfg[i2];
-    if (lane == 0) {
+  if (lane == 0) {
+    candidate_search(c);
+    if (!status(c)) {
+      const int i1 = s.iflag[F_I1], i2 = s.iflag[F_I2];
+      const int i3 = s.cfg[i1], i4 = s.cfg[i2];
       if (s.x[i1] == 1) {
         mv[0] = i3;
         mv[1] = i4 - d.Np;
@@ -340,32 +368,37 @@ __device__ __forceinline__ void control_propose(const SCtx& c, volatile int* can
         mv[3] = i1;
       }
     }
-    // update_theta RBM.f90:95-148 and the new signs (make_sample.f90:195-197) on the warp
-    const int A2 = 2 * d.alphar;
-    const double x1 = (double)s.x[i1], x2 = (double)s.x[i2];
-    for (int j = lane; j < d.Mr; j += 32) {
-      int mp = j / A2, rem = j - mp * A2;
-      double sg = rem < d.alphar ? 1.0 : -1.0;
-      int f = rem < d.alphar ? rem : rem - d.alphar;
-      const double* Wf = c.p.Wr + (size_t)f * d.N;
-      int iw1 = c.t.wmap[(size_t)mp * d.N + i1], iw2 = c.t.wmap[(size_t)mp * d.N + i2];
-      double v = s.th[j];
-      v = v - 2.0 * Wf[iw1] * x1 * sg;
-      v = v - 2.0 * Wf[iw2] * x2 * sg;
-      s.thp[j] = v;
-    }
-    const int flipsign = (c.t.subB[i1] ? -1 : 1) * (c.t.subB[i2] ? -1 : 1);
-    for (int mp = lane; mp < d.n_mp; mp += 32) s.sgnp[mp] = -s.sgn[mp] * flipsign;
-    __syncwarp();
-    for (int qp = lane; qp < d.n_qp; qp += 32) {
-      double r = 1.0;
-      for (int f = 0; f < d.alphar; f++) r = r * cosh(s.thp[qp * d.alphar + f]);
-      s.rbm[qp] = r;
-    }
+    __threadfence_block();
+    *cand_flag = pass_id;
   }
   __syncwarp();
-  __threadfence_block();
-  if (lane == 0) *cand_flag = pass_id;
+  if (status(c)) return;
+  const int i1 = s.iflag[F_I1], i2 = s.iflag[F_I2];
+  // update_theta RBM.f90:95-148 and the new signs (make_sample.f90:195-197) on the warp
+  const int A2 = 2 * d.alphar;
+  const double x1 = (double)s.x[i1], x2 = (double)s.x[i2];
+  for (int j = lane; j < d.Mr; j += 32) {
+    int mp = j / A2, rem = j - mp * A2;
+    double sg = rem < d.alphar ? 1.0 : -1.0;
+    int f = rem < d.alphar ? rem : rem - d.alphar;
+    const double* Wf = c.p.Wr + (size_t)f * d.N;
+    int iw1 = c.t.wmap[(size_t)mp * d.N + i1], iw2 = c.t.wmap[(size_t)mp * d.N + i2];
+    double v = s.th[j];
+    v = v - 2.0 * Wf[iw1] * x1 * sg;
+    v = v - 2.0 * Wf[iw2] * x2 * sg;
+    s.thp[j] = v;
+  }
+  const int flipsign = (c.t.subB[i1] ? -1 : 1) * (c.t.subB[i2] ? -1 : 1);
+  for (int mp = lane; mp < d.n_mp; mp += 32) s.sgnp[mp] = -s.sgn[mp] * flipsign;
+  __syncwarp();
+  for (int qp = lane; qp < d.n_qp; qp += 32) {
+    double r = 1.0;
+    for (int f = 0; f < d.alphar; f++) r = r * cosh(s.thp[qp * d.alphar + f]);
+    s.rbm[qp] = r;
+    const cplx cw = psi_wo_pf(d, c.t, r, s.sgnp[qp >> 1], qp);
+    s.psip[2 * qp] = cw.re;
+    s.psip[2 * qp + 1] = cw.im;
+  }
 }
 
 // Pairs: deferred update (pend) and/or proposal ratio (prop) per tile.  Pair g takes tiles g, g + kPairs, ...
@@ -374,11 +407,12 @@ __device__ __forceinline__ void control_propose(const SCtx& c, volatile int* can
 template <int KPL, int NP>
 __device__ __forceinline__ bool pass_consume(const SCtx& c, const Stream& sm, const Pipe& pp, bool pend,
                                              const Move& mk, bool prop, volatile int* cand_flag, int pass_id,
-                                             const int* mv, double& pre, double& pim, volatile int* abort_flag) {
+                                             const int* mv, volatile int* abort_flag) {
   const DevDims& d = c.d;
   const WS& s = c.s;
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, Np = NP, n = d.n_qp;
-  const int cw = warp - 1, g = cw >> 1, h = cw & 1, partner = 1 + 2 * g + (1 - h);
+  const int cw = warp - 2, g = cw >> 1, h = cw & 1, partner = 2 + 2 * g + (1 - h);
+  const int polls = wait_polls(c);
   const size_t NN = (size_t)Np * Np;
   double* u = s.wu + (size_t)warp * Np;
   double* U0 = s.wA + (size_t)warp * Np;
@@ -404,7 +438,8 @@ __device__ __forceinline__ bool pass_consume(const SCtx& c, const Stream& sm, co
       if (tn < n) gather_regs<NP>(d, c.p, tn, s.idx, mk, gk);
     }
     __syncwarp();
-    bool bad = (*abort_flag != 0) || !mbar_wait(&sm.full[st], (T / sm.ST) & 1u, wait_polls(c));
+    bool bad = (*abort_flag != 0) || !wait_ticket(sm, st, T, polls, abort_flag) ||
+               !mbar_wait(&sm.full[st], (T / sm.ST) & 1u, polls);
     double* Y = sm.stage + (size_t)st * NN;
     if (pend) {
       if (update_half<NP>(Y, mk, ck, U0, V0, g, h, my_acc, other_acc, pAS, bad)) return false;
@@ -448,13 +483,7 @@ __device__ __forceinline__ bool pass_consume(const SCtx& c, const Stream& sm, co
         const double* so = (mn.db < NP / 2) ? s0 : s1;
         const double wv = s0[0] + s1[0], ra = s0[1] + s1[1];
         const double R = ra * so[2] - so[3] * (wv - cn);
-        const double pfn = R * s.pf[t];
-        s.pfp[t] = pfn;
-        cplx cw2 = psi_wo_pf(d, c.t, s.rbm[t], s.sgnp[t >> 1], t);
-        s.psip[2 * t] = cw2.re * pfn;
-        s.psip[2 * t + 1] = cw2.im * pfn;
-        pre += cw2.re * pfn;
-        pim += cw2.im * pfn;
+        s.pfp[t] = R * s.pf[t];
       }
       if (pend) {  // write the updated tile back; the stage is released once the copy has read it
         bulk_store(c.Yw + (size_t)t * NN, Y, sm.tile_bytes);
@@ -481,26 +510,40 @@ __device__ __forceinline__ void run_pass(const SCtx& c, const Stream& sm, Pipe& 
                                          bool prop, volatile int* cand_flag, int pass_id, int* mv,
                                          volatile int* abort_flag) {
   const int tid = threadIdx.x, warp = tid >> 5, lane = tid & 31;
-  double pre = 0.0, pim = 0.0;
+  const WS& s = c.s;
   bool ok = true;
   if (warp == 0) {
-    if (lane == 0) pass_issue_first(c, sm, pp);
-    __syncwarp();
     if (prop) control_propose(c, cand_flag, pass_id, mv);
-    if (lane == 0 && !status(c)) ok = pass_produce(c, sm, pp, abort_flag);
+  } else if (warp == 1) {
+    if (lane == 0) ok = pass_produce(c, sm, pp, abort_flag);
   } else {
-    ok = pass_consume<KPL, NP>(c, sm, pp, pend, mk, prop, cand_flag, pass_id, mv, pre, pim, abort_flag);
+    ok = pass_consume<KPL, NP>(c, sm, pp, pend, mk, prop, cand_flag, pass_id, mv, abort_flag);
   }
   if (!ok) {
     *abort_flag = 1;
     if (!status(c)) status(c) = ST_TIMEOUT;
     bulk_wait_all();  // this thread's stores in flight, if any
   }
-  if (lane == 0 && warp > 0) {
-    c.s.red[warp] = pre;
-    c.s.red[32 + warp] = pim;
-  }
   __syncthreads();
+  // psi' = sum over projections of weight x new Pfaffian (sub.f90:47-70), each lane over every 32nd projection
+  if (prop && warp == 0 && !status(c)) {
+    double re = 0.0, im = 0.0;
+    for (int t = lane; t < c.d.n_qp; t += 32) {
+      const double pf = s.pfp[t];
+      const double a = s.psip[2 * t] * pf, b = s.psip[2 * t + 1] * pf;
+      s.psip[2 * t] = a;
+      s.psip[2 * t + 1] = b;
+      re += a;
+      im += b;
+    }
+    re = warp_sum(re);
+    im = warp_sum(im);
+    if (lane == 0) {
+      s.dsc[D_PSIPR] = re;
+      s.dsc[D_PSIPI] = im;
+    }
+  }
+  if (prop) __syncthreads();
   pp.T0 += (uint32_t)c.d.n_qp;
 }
 
@@ -530,6 +573,7 @@ __global__ void __launch_bounds__(kWarps * 32, 1)
     for (int k = 0; k < ST; k++) {
       mbar_init(&sm.full[k], 1);
       mbar_init(&sm.empty[k], 1);
+      sm.ticket[k] = -1;
     }
     fence_mbar_init();
     pend_s[0] = 0;
@@ -548,7 +592,7 @@ __global__ void __launch_bounds__(kWarps * 32, 1)
   const int w = c.w, N = d.N;
   Pipe pp;
   pp.T0 = 0;
-  for (int k = 0; k < 16; k++) pp.last_issued[k] = -1;
+  for (int k = 0; k < kMaxStages; k++) pp.last_issued[k] = -1;
   int pass_id = 0;
 
   for (int k = tid; k < 625; k += blockDim.x) s.mt[k] = W.mt[(size_t)w * 625 + k];
@@ -609,13 +653,7 @@ __global__ void __launch_bounds__(kWarps * 32, 1)
       const int i1 = s.iflag[F_I1], i2 = s.iflag[F_I2];
       const int i3 = s.cfg[i1], i4 = s.cfg[i2];
       if (tid == 0) {
-        double re = 0.0, im = 0.0;
-        for (int k = 1; k < kWarps; k++) {
-          re += s.red[k];
-          im += s.red[32 + k];
-        }
-        s.dsc[D_PSIPR] = re;
-        s.dsc[D_PSIPI] = im;
+        const double re = s.dsc[D_PSIPR], im = s.dsc[D_PSIPI];
         (void)grnd(s.mt);  // sub.f90:72
         double r1 = (hypot(re, im) + d.shift) / (hypot(s.dsc[D_PSI0R], s.dsc[D_PSI0I]) + d.shift);
         const double u = grnd(s.mt);
@@ -677,8 +715,8 @@ __global__ void __launch_bounds__(kWarps * 32, 1)
     run_pass<KPL, NP>(c, sm, pp, true, mk, false, &cand_flag, ++pass_id, mv, &abort_flag);
   }
   // every bulk copy of this CTA has landed before the CTA exits (bounded waits)
-  if (tid == 0)
-    for (int k = 0; k < sm.ST && k < 16; k++)
+  if (tid == kProducerThread)
+    for (int k = 0; k < sm.ST && k < kMaxStages; k++)
       if (pp.last_issued[k] >= 0) (void)mbar_wait(&sm.full[k], ((uint32_t)pp.last_issued[k] / sm.ST) & 1u);
   bulk_wait_all();
   __syncthreads();
@@ -701,13 +739,16 @@ __global__ void __launch_bounds__(kWarps * 32, 1)
 
 // Stage count and shared memory of the streaming sampler; 0 when it does not apply.
 int rbmpp_stream_stages(const DevDims& d, int max_smem) {
-  // One stage per pair (or per projection when there are fewer): the tiles that reuse a stage within a
-  // pass then belong to the same pair, so a pair never waits on a stage two loads ahead of it, where the
-  // mbarrier's phase parity could not tell the two loads apart.  No fallback to fewer stages: the
-  // direct sampler takes shapes whose stages do not fit.
+  // As many stages as fit, up to two per pair (a pair's next tile then loads while it computes the
+  // current one) and no more than there are projections; at least one per pair, else the direct sampler
+  // takes the shape.  The stage tickets keep the mbarrier phases unambiguous for any count.
   if (d.Np != 8 && d.Np != 18 && d.Np != 32 && d.Np != 50) return 0;  // the compiled block sizes
-  const int st = d.n_qp < kPairs ? d.n_qp : kPairs;
-  return (long long)stream_layout(d, st, nullptr, nullptr, nullptr) <= max_smem ? st : 0;
+  int hi = 2 * kPairs < kMaxStages ? 2 * kPairs : kMaxStages;
+  if (d.n_qp < hi) hi = d.n_qp;
+  const int lo = d.n_qp < kPairs ? d.n_qp : kPairs;
+  for (int st = hi; st >= lo; st--)
+    if ((long long)stream_layout(d, st, nullptr, nullptr, nullptr) <= max_smem) return st;
+  return 0;
 }
 
 size_t rbmpp_stream_smem(const DevDims& d, int st) { return stream_layout(d, st, nullptr, nullptr, nullptr); }
