@@ -30,7 +30,7 @@ sys.path.insert(0, ROOT)
 METRIC = "MC samples/s and SR steps/s at 10x10 J2=0.5, chosen vs plain FP64, dE/site"
 # DRAM bytes (read + write) that ncu counted for one sampler_stream_kernel launch of the 1-wave 10x10
 # workload (one walker per SM, one stored sample), divided by that launch's algorithmic bytes
-SAMPLER_TRAFFIC_PER_ALG_BYTE = (2.0798e12 + 0.6537e12) / 3.1765e12
+SAMPLER_TRAFFIC_PER_ALG_BYTE = (2.0793e12 + 0.6517e12) / 3.1765e12
 # wall-clock budget of one bench process: the plain all-FP64 twin trajectory gets as many of the K steps as fit
 PAIR_BUDGET_S = 1450.0
 T_START = time.perf_counter()
