@@ -231,25 +231,13 @@ __device__ __forceinline__ bool update_half(double* Y, const Move& m, double c, 
   if (k < NP) {
     double* y = Y + r0 * NP + k;
     const double* as = pAS + 2 * r0;
-    // rows in batches whose loads all precede their stores (the compiler cannot move a load of pAS past a
-    // store to the tile, so a row-at-a-time loop would wait one shared-memory round trip per row)
-    constexpr int B = 5;
-#pragma unroll
-    for (int j0 = 0; j0 < NR; j0 += B) {
-      double2 a[B], yv[B];
-#pragma unroll
-      for (int b = 0; b < B; b++)
-        if (j0 + b < NR) {
-          a[b] = ld2(as + 2 * (j0 + b));
-          yv[b] = ld2(y + (j0 + b) * NP);
-        }
-#pragma unroll
-      for (int b = 0; b < B; b++)
-        if (j0 + b < NR) {
-          yv[b].x = yv[b].x - a[b].x * cx - a[b].y * tx;
-          yv[b].y = yv[b].y - a[b].x * cy - a[b].y * ty;
-          st2(y + (j0 + b) * NP, yv[b]);
-        }
+#pragma unroll 5
+    for (int jj = 0; jj < NR; jj++) {
+      const double2 a = ld2(as + 2 * jj);
+      double2 yv = ld2(y + jj * NP);
+      yv.x = yv.x - a.x * cx - a.y * tx;
+      yv.y = yv.y - a.x * cy - a.y * ty;
+      st2(y + jj * NP, yv);
     }
     if (m.db >= r0 && m.db < r0 + NR) {
       double2 yv = ld2(Y + m.db * NP + k);
