@@ -1133,18 +1133,8 @@ int rbmpp_sr_step(rbmpp_ctx* c, const rbmpp_sr_in* in, rbmpp_sr_out* out, double
   }
   double sdiag = 0, srb = 0, spp = 0;  // :104-140
   i1 = i2 = 0;
-  int kmaxS = -100, kminS = -100;
-  double Smax = 0.0, Smin = std::exp(50.0);
   for (int k = 0; k < Nv; k++)
-    if (dg[k] > 0.0) {
-      if (dg[k] > Smax) {
-        Smax = dg[k];
-        kmaxS = k + 1;
-      }
-      if (dg[k] < Smin) {
-        Smin = dg[k];
-        kminS = k + 1;
-      }
+    if (dg[k] > 0.0) {  // (the reference's Smax/Smin/kmaxS/kminS only feed its diagnostics output)
       sdiag += dg[k];
       if (k < Nrbm) {
         i1++;
@@ -1154,8 +1144,6 @@ int rbmpp_sr_step(rbmpp_ctx* c, const rbmpp_sr_in* in, rbmpp_sr_out* out, double
         spp += dg[k];
       }
     }
-  (void)kmaxS;
-  (void)kminS;
   sdiag = sdiag / (double)(i1 + i2);
   srb = (Nrbm > 0) ? srb / (double)i1 : 1.0;
   spp = spp / (double)i2;

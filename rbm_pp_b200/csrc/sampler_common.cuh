@@ -46,13 +46,30 @@ __device__ __forceinline__ void warp_scratch_all(const SCtx& c, const int* idx, 
       }
       double* Yq = c.Yw + (size_t)qp * Np * Np;
       if (diff) {  // make_sample.f90:106-113
+        // the stored Y comes from HBM: a batch of RB rows is loaded before any is compared
+        constexpr int RB = 10;
         double mx = 0.0, md = 0.0;
-        for (int a = 0; a < Np; a++)
-          for (int b = lane; b < Np; b += 32) {
-            const double nv = T[a * ld + perm[b]];
-            mx = fmax(mx, fabs(nv));
-            md = fmax(md, fabs(Yq[a * Np + b] - nv));
-          }
+        for (int a0 = 0; a0 < Np; a0 += RB) {
+          double yv[RB][KPL];
+#pragma unroll
+          for (int r = 0; r < RB; r++)
+#pragma unroll
+            for (int q = 0; q < KPL; q++) {
+              const int a = a0 + r, b = lane + 32 * q;
+              yv[r][q] = (a < Np && b < Np) ? Yq[a * Np + b] : 0.0;
+            }
+#pragma unroll
+          for (int r = 0; r < RB; r++)
+#pragma unroll
+            for (int q = 0; q < KPL; q++) {
+              const int a = a0 + r, b = lane + 32 * q;
+              if (a < Np && b < Np) {
+                const double nv = T[a * ld + perm[b]];
+                mx = fmax(mx, fabs(nv));
+                md = fmax(md, fabs(yv[r][q] - nv));
+              }
+            }
+        }
         mx = warp_max(mx);
         md = warp_max(md);
         wratio = fmax(wratio, md / mx);
