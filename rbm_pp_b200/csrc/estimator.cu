@@ -379,42 +379,30 @@ __device__ __forceinline__ void estimator_config(const DevDims& d, const DevTabl
         const cplx cw = psi_wo_pf_s(d, t, s, s.sgn[mp], qp);
         const double cc = pfq * d.sp_cc[sp] * cw.re, ss = pfq * d.sp_ss[sp] * cw.re;
         const int npr = Np * Np;
-        if (d.orb_injective) {
-          // every (up, down) pair of one projection has its own two targets, so a thread may load the
-          // targets of SB pairs before it stores any of them
-          constexpr int SB = 8;
-          for (int pr0 = tid; pr0 < npr; pr0 += SB * kEstThreads) {
-            double y[SB], v1[SB], v2[SB];
-            int a1[SB], a2[SB];
+        // Each thread loads the values and targets of SB pairs before it adds any, and adds with fire-and-forget
+        // reductions in L2 (the thread never waits for the old value).  With an injective orbital map every
+        // (up, down) pair of one projection has its own two targets, and projections follow one another
+        // (barrier below), so every target receives its terms in projection order: the sums are
+        // deterministic.  A non-injective map can hit a target twice within one projection.
+        constexpr int SB = 8;
+        for (int pr0 = tid; pr0 < npr; pr0 += SB * kEstThreads) {
+          double y[SB];
+          int a1[SB], a2[SB];
 #pragma unroll
-            for (int u = 0; u < SB; u++) {
-              const int pr = pr0 + u * kEstThreads, prc = pr < npr ? pr : npr - 1;
-              const int j = prc / Np, i = prc - j * Np;  // j: down electron, i: up electron
-              y[u] = Tw[j * ld + srcw[i]];               // Y(j, i) = (M^-1)(Np+j, i)
-              const int tu = wm[s.idx[i]], td = wm[s.idx[Np + j]];
-              a1[u] = off_pp + t.orb[(size_t)tu * N + td];
-              a2[u] = off_pp + t.orb[(size_t)td * N + tu];
-            }
-#pragma unroll
-            for (int u = 0; u < SB; u++) {
-              v1[u] = cc != 0.0 ? Orow[a1[u]] : 0.0;
-              v2[u] = ss != 0.0 ? Orow[a2[u]] : 0.0;
-            }
-#pragma unroll
-            for (int u = 0; u < SB; u++)
-              if (pr0 + u * kEstThreads < npr) {
-                if (cc != 0.0) Orow[a1[u]] = v1[u] + y[u] * cc;
-                if (ss != 0.0) Orow[a2[u]] = v2[u] + y[u] * ss;
-              }
-          }
-        } else {
-          for (int pr = tid; pr < npr; pr += blockDim.x) {
-            const int j = pr / Np, i = pr - j * Np;
-            const double y = Tw[j * ld + srcw[i]];
+          for (int u = 0; u < SB; u++) {
+            const int pr = pr0 + u * kEstThreads, prc = pr < npr ? pr : npr - 1;
+            const int j = prc / Np, i = prc - j * Np;  // j: down electron, i: up electron
+            y[u] = Tw[j * ld + srcw[i]];               // Y(j, i) = (M^-1)(Np+j, i)
             const int tu = wm[s.idx[i]], td = wm[s.idx[Np + j]];
-            if (cc != 0.0) atomicAdd(Orow + off_pp + t.orb[(size_t)tu * N + td], y * cc);
-            if (ss != 0.0) atomicAdd(Orow + off_pp + t.orb[(size_t)td * N + tu], y * ss);
+            a1[u] = off_pp + t.orb[(size_t)tu * N + td];
+            a2[u] = off_pp + t.orb[(size_t)td * N + tu];
           }
+#pragma unroll
+          for (int u = 0; u < SB; u++)
+            if (pr0 + u * kEstThreads < npr) {
+              if (cc != 0.0) atomicAdd(Orow + a1[u], y[u] * cc);
+              if (ss != 0.0) atomicAdd(Orow + a2[u], y[u] * ss);
+            }
         }
         __syncthreads();
       }
